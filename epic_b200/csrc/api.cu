@@ -1,0 +1,494 @@
+// C ABI of the B200 EPIC step (include/epic_gpu.h): context lifecycle,
+// host <-> device parcel/field exchange and the step driver
+// (epic3d.f90:135-153, ls_rk.f90:88-217).
+#include "ctx.hpp"
+
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+
+using namespace epic;
+
+struct epic_ctx {
+    Ctx c;
+};
+
+namespace epic {
+
+void* Ctx::get_scratch(size_t bytes) {
+    if (bytes > scratch_bytes) {
+        if (scratch) CK(cudaFreeAsync(scratch, stream));
+        size_t nb = std::max(bytes, scratch_bytes + scratch_bytes / 2);
+        CK(cudaMallocAsync(&scratch, nb, stream));
+        scratch_bytes = nb;
+    }
+    return scratch;
+}
+
+void* Ctx::get_scratch2(size_t bytes) {
+    if (bytes > scratch2_bytes) {
+        if (scratch2) CK(cudaFreeAsync(scratch2, stream));
+        size_t nb = std::max(bytes, scratch2_bytes + scratch2_bytes / 2);
+        CK(cudaMallocAsync(&scratch2, nb, stream));
+        scratch2_bytes = nb;
+    }
+    return scratch2;
+}
+
+// Reads the device error word once and turns it into the reference's abort
+// messages (mpi_exit_on_error call sites).
+void check_device_error(Ctx& c) {
+    unsigned e = 0;
+    CK(cudaMemcpyAsync(&e, &c.dsc->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (!e) return;
+    CK(cudaMemsetAsync(&c.dsc->err, 0, sizeof(unsigned), c.stream));
+    if (e & ERRB_B33) throw CudaError(EPIC_ERR_NUMERICAL, "in parcel_ellipsoid::get_B33: Division by small number!");
+    if (e & ERRB_NO_NEIGHBOUR) throw CudaError(EPIC_ERR_NUMERICAL, "Merge error: no near enough neighbour found.");
+    if (e & ERRB_TREE) throw CudaError(EPIC_ERR_NUMERICAL, "in parcel_nearest::resolve_tree: First stage error");
+    if (e & ERRB_CELL) throw CudaError(EPIC_ERR_NUMERICAL, "in nearest_parcel_to_local_cell_index: Parcel not in local domain.");
+    if (e & ERRB_DT) throw CudaError(EPIC_ERR_NUMERICAL, "Time step <= 0!");
+    if (e & ERRB_ZRANGE) throw CudaError(EPIC_ERR_NUMERICAL, "interpolation point outside the vertical halo");
+    if (e & (1u << 30)) throw CudaError(EPIC_ERR_PARCEL_COUNT, "par2grid: Wrong total number of parcels!");
+    throw CudaError(EPIC_ERR_NUMERICAL, "device error word " + std::to_string(e));
+}
+
+}  // namespace epic
+
+// ---------------------------------------------------------------------------
+// layout conversion kernels: Fortran (ncomp, n) <-> structure of arrays
+__global__ void k_deinterleave(const double* src, int ncomp, long long n, PView pv, int a0) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * ncomp;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long p = i / ncomp;
+        int k = (int)(i - p * ncomp);
+        pv.at(a0 + k, p) = src[i];
+    }
+}
+__global__ void k_interleave(double* dst, int ncomp, long long n, PView pv, int a0) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * ncomp;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long p = i / ncomp;
+        int k = (int)(i - p * ncomp);
+        dst[i] = pv.at(a0 + k, p);
+    }
+}
+__global__ void k_int_to_double(const int* a, double* b, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
+static int cgrid(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 16)); }
+
+static void upload_attr(Ctx& c, const double* h, int ncomp, int a0) {
+    long long n = c.n;
+    if (n == 0) return;
+    double* tmp = reinterpret_cast<double*>(c.get_scratch2(sizeof(double) * ncomp * n));
+    CK(cudaMemcpyAsync(tmp, h, sizeof(double) * ncomp * n, cudaMemcpyHostToDevice, c.stream));
+    k_deinterleave<<<cgrid(n * ncomp), 256, 0, c.stream>>>(tmp, ncomp, n, c.pv, a0);
+    CKL();
+}
+
+static void download_attr(Ctx& c, double* h, int ncomp, int a0) {
+    long long n = c.n;
+    if (n == 0 || !h) return;
+    double* tmp = reinterpret_cast<double*>(c.get_scratch2(sizeof(double) * ncomp * n));
+    k_interleave<<<cgrid(n * ncomp), 256, 0, c.stream>>>(tmp, ncomp, n, c.pv, a0);
+    CKL();
+    CK(cudaMemcpyAsync(h, tmp, sizeof(double) * ncomp * n, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+}
+
+// parameters.f90:93-165, physics.f90:170-185
+static void setup_params(Ctx& c) {
+    const epic_cfg& g = c.cfg;
+    Params& P = c.P;
+    std::memset(&P, 0, sizeof(P));
+    P.nx = g.nx; P.ny = g.ny; P.nz = g.nz;
+    P.nzh = g.nz + 3;
+    P.fsz = (long long)g.nx * g.ny * P.nzh;
+    int nn[3] = {g.nx, g.ny, g.nz};
+    for (int k = 0; k < 3; ++k) {
+        P.lower[k] = g.lower[k];
+        P.extent[k] = g.extent[k];
+        P.upper[k] = P.lower[k] + P.extent[k];
+        P.extenti[k] = 1.0 / P.extent[k];
+        P.dx[k] = P.extent[k] / (double)nn[k];
+        P.dxi[k] = 1.0 / P.dx[k];
+        P.center[k] = 0.5 * (P.lower[k] + P.upper[k]);
+        P.hli[k] = 1.0 / (P.extent[k] / 2.0);
+    }
+    P.halo_lower[0] = P.lower[0] - P.dx[0];
+    P.halo_lower[1] = P.lower[1] - P.dx[1];
+    P.vcell = P.dx[0] * P.dx[1] * P.dx[2];
+    P.vcelli = 1.0 / P.vcell;
+    P.vdomaini = 1.0 / (P.extent[0] * P.extent[1] * P.extent[2]);
+    P.vmin = P.vcell / g.min_vratio;
+    double amax = std::pow(0.75 * (1.0 / M_PI), 1.0 / 3.0) * std::min(P.dx[0], std::min(P.dx[1], P.dx[2]));
+    P.amax2 = amax * amax;
+    P.lambda_max = g.lambda_max;
+    P.glat = g.gravity * g.L_v / (g.c_p * g.theta_0);
+    P.lambda_c = 1.0 / g.height_c;
+    P.q_0 = g.q_0;
+    if (g.l_planetary_vorticity) {
+        double lat = g.lat_degrees * (M_PI / 180.0);
+        P.f_cor[1] = 2.0 * g.ang_vel * std::cos(lat);
+        P.f_cor[2] = 2.0 * g.ang_vel * std::sin(lat);
+    }
+    P.zeta_zero[0] = g.bndry_zeta_zero[0] != 0;
+    P.zeta_zero[1] = g.bndry_zeta_zero[1] != 0;
+    P.dzi = P.dxi[2];
+    P.hdzi = 0.5 * P.dxi[2];
+    P.ap = P.dxi[2] * P.dxi[2];
+    // ls_rk.f90:32-54
+    if (g.rk_order == 4) {
+        const double ca[5] = {-567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                              -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0, 0.0};
+        const double cb[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                              1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                              2277821191437.0 / 14882151754819.0};
+        std::memcpy(c.ca, ca, sizeof(ca));
+        std::memcpy(c.cb, cb, sizeof(cb));
+        c.n_stages = 5;
+    } else if (g.rk_order == 3) {
+        const double ca[3] = {-5.0 / 9.0, -153.0 / 128.0, 0.0};
+        const double cb[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+        std::memcpy(c.ca, ca, sizeof(ca));
+        std::memcpy(c.cb, cb, sizeof(cb));
+        c.n_stages = 3;
+    } else {
+        throw CudaError(EPIC_ERR_CONFIG, "Only third and fourth order RK supported.");
+    }
+}
+
+static void free_ctx(Ctx& c) {
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    spectral_free(c);
+    void* ptrs[] = {c.pv.base, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.dvor_bar};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c.scratch) cudaFree(c.scratch);
+    if (c.scratch2) cudaFree(c.scratch2);
+    if (c.hsc) cudaFreeHost(c.hsc);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    c.stream = nullptr;
+}
+
+#define API_BEGIN                                   \
+    if (!ctx) return EPIC_ERR_ARG;                  \
+    try {
+#define API_END                                     \
+    } catch (const CudaError& e) {                  \
+        ctx->c.err = e.what();                      \
+        return e.code;                              \
+    } catch (const std::exception& e) {             \
+        ctx->c.err = e.what();                      \
+        return EPIC_ERR_STATE;                      \
+    }                                               \
+    return EPIC_OK;
+
+#define NEED_PARCELS                                                           \
+    if (!ctx->c.has_parcels) throw CudaError(EPIC_ERR_STATE, "no parcels set (call epic_gpu_set_parcels first)");
+
+extern "C" {
+
+int epic_gpu_default_config(epic_cfg* g) {
+    if (!g) return EPIC_ERR_ARG;
+    std::memset(g, 0, sizeof(*g));
+    g->size_factor = 1.0; g->grow_factor = 1.2; g->shrink_factor = 0.8; g->n_per_cell = 8;
+    g->lambda_max = 4.0; g->min_vratio = 20.0; g->correction_iters = 2; g->gradient_pref = 1.8;
+    g->max_compression = 0.5; g->t_initial = 0.0; g->t_limit = 0.0; g->alpha = 0.2;
+    g->precise_stop = 0; g->use_fixed_dt = 0; g->fixed_dt = 1.0; g->rk_order = 4;
+    g->gravity = 9.80616; g->L_v = (double)2.501e6f; g->c_p = 1005.7; g->theta_0 = 288.15;
+    g->q_0 = 0.015; g->height_c = 1000.0; g->ang_vel = 0.000072921; g->lat_degrees = 45.0;
+    g->l_planetary_vorticity = 0;
+    g->capacity = 0; g->precision = EPIC_PRECISION_FP64; g->keep_order = 1;
+    return EPIC_OK;
+}
+
+int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
+    if (!cfg || !out) return EPIC_ERR_ARG;
+    if (cfg->nx < 4 || cfg->ny < 4 || cfg->nz < 2 || cfg->nx % 2 || cfg->ny % 2) return EPIC_ERR_CONFIG;
+    if (cfg->extent[0] <= 0 || cfg->extent[1] <= 0 || cfg->extent[2] <= 0) return EPIC_ERR_CONFIG;
+    if (cfg->precision != EPIC_PRECISION_FP64) return EPIC_ERR_CONFIG;
+    auto* ctx = new epic_ctx();
+    Ctx& c = ctx->c;
+    c.cfg = *cfg;
+    try {
+        setup_params(c);
+        int dev_count = 0;
+        CK(cudaGetDeviceCount(&dev_count));
+        CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        const Params& P = c.P;
+        c.cap = cfg->capacity > 0 ? cfg->capacity
+                                  : (long long)(2.0 * (double)P.nx * P.ny * P.nz * std::max(1, cfg->n_per_cell)) + 1024;
+        c.pv.cap = c.cap;
+        CK(cudaMalloc(&c.pv.base, sizeof(double) * (size_t)N_ATTR * c.cap));
+        CK(cudaMemsetAsync(c.pv.base, 0, sizeof(double) * (size_t)N_ATTR * c.cap, c.stream));
+        CK(cudaMalloc(&c.fields, sizeof(double) * (size_t)N_FIELDS * P.fsz));
+        CK(cudaMemsetAsync(c.fields, 0, sizeof(double) * (size_t)N_FIELDS * P.fsz, c.stream));
+        CK(cudaMalloc(&c.nparg, sizeof(int) * P.fsz));
+        CK(cudaMalloc(&c.nsparg, sizeof(int) * P.fsz));
+        CK(cudaMemsetAsync(c.nparg, 0, sizeof(int) * P.fsz, c.stream));
+        CK(cudaMemsetAsync(c.nsparg, 0, sizeof(int) * P.fsz, c.stream));
+        c.n_work = N_WORK;
+        CK(cudaMalloc(&c.work, sizeof(double) * (size_t)N_WORK * P.fsz));
+        CK(cudaMemsetAsync(c.work, 0, sizeof(double) * (size_t)N_WORK * P.fsz, c.stream));
+        CK(cudaMalloc(&c.dsc, sizeof(StepScalars)));
+        CK(cudaMemsetAsync(c.dsc, 0, sizeof(StepScalars), c.stream));
+        CK(cudaMallocHost(&c.hsc, sizeof(StepScalars)));
+        CK(cudaMalloc(&c.partials, sizeof(double) * 148 * 8 * 64));
+        CK(cudaMalloc(&c.dvor_bar, sizeof(double) * 8));
+        CK(cudaMemsetAsync(c.dvor_bar, 0, sizeof(double) * 8, c.stream));
+        spectral_init(c);
+        CK(cudaStreamSynchronize(c.stream));
+    } catch (const CudaError& e) {
+        int code = e.code;
+        free_ctx(c);
+        delete ctx;
+        return code;
+    }
+    *out = ctx;
+    return EPIC_OK;
+}
+
+void epic_gpu_destroy(epic_ctx* ctx) {
+    if (!ctx) return;
+    free_ctx(ctx->c);
+    delete ctx;
+}
+
+const char* epic_gpu_last_error(const epic_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
+
+int epic_gpu_sync(epic_ctx* ctx) {
+    API_BEGIN
+    CK(cudaStreamSynchronize(ctx->c.stream));
+    check_device_error(ctx->c);
+    API_END
+}
+
+int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const double* vor, const double* B,
+                         const double* vol, const double* buoy, const double* hum) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (n < 0 || !pos || !vor || !B || !vol || !buoy) throw CudaError(EPIC_ERR_ARG, "set_parcels: bad arguments");
+    if (n > c.cap) throw CudaError(EPIC_ERR_CAPACITY, "set_parcels: more parcels than the device capacity");
+    c.n = n;
+    CK(cudaMemsetAsync(c.pv.base, 0, sizeof(double) * (size_t)N_ATTR * c.cap, c.stream));
+    upload_attr(c, pos, 3, A_X);
+    upload_attr(c, vor, 3, A_VX);
+    upload_attr(c, B, 5, A_B11);
+    upload_attr(c, vol, 1, A_VOL);
+    upload_attr(c, buoy, 1, A_BUOY);
+    if (hum) upload_attr(c, hum, 1, A_HUM);
+    c.has_parcels = true;
+    CK(cudaStreamSynchronize(c.stream));
+    API_END
+}
+
+int epic_gpu_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, double* vor, double* B,
+                         double* vol, double* buoy, double* hum) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!n) throw CudaError(EPIC_ERR_ARG, "get_parcels: null count");
+    *n = c.n;
+    if (cap < c.n) throw CudaError(EPIC_ERR_ARG, "get_parcels: capacity too small");
+    download_attr(c, pos, 3, A_X);
+    download_attr(c, vor, 3, A_VX);
+    download_attr(c, B, 5, A_B11);
+    download_attr(c, vol, 1, A_VOL);
+    download_attr(c, buoy, 1, A_BUOY);
+    download_attr(c, hum, 1, A_HUM);
+    API_END
+}
+
+int epic_gpu_num_parcels(epic_ctx* ctx, int64_t* n) {
+    API_BEGIN
+    if (!n) throw CudaError(EPIC_ERR_ARG, "null");
+    *n = ctx->c.n;
+    API_END
+}
+
+int epic_gpu_get_parcel_rk(epic_ctx* ctx, int64_t cap, int64_t* n, double* dpos, double* dvor, double* strain,
+                           double* dB) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!n) throw CudaError(EPIC_ERR_ARG, "null");
+    *n = c.n;
+    if (cap < c.n) throw CudaError(EPIC_ERR_ARG, "get_parcel_rk: capacity too small");
+    download_attr(c, dpos, 3, A_DX);
+    download_attr(c, dvor, 3, A_DVX);
+    download_attr(c, strain, 8, A_S0);
+    download_attr(c, dB, 5, A_DB0);
+    API_END
+}
+
+int epic_gpu_set_parcel_rk(epic_ctx* ctx, int64_t n, const double* dpos, const double* dvor, const double* dB) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (n != c.n) throw CudaError(EPIC_ERR_ARG, "set_parcel_rk: count mismatch");
+    if (dpos) upload_attr(c, dpos, 3, A_DX);
+    if (dvor) upload_attr(c, dvor, 3, A_DVX);
+    if (dB) upload_attr(c, dB, 5, A_DB0);
+    CK(cudaStreamSynchronize(c.stream));
+    API_END
+}
+
+int epic_gpu_get_field(epic_ctx* ctx, int id, double* out) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!out || id < 0 || id >= EPIC_FIELD_COUNT) throw CudaError(EPIC_ERR_ARG, "get_field: bad field id");
+    if (id == EPIC_FIELD_NPARG || id == EPIC_FIELD_NSPARG) {
+        double* tmp = reinterpret_cast<double*>(c.get_scratch2(sizeof(double) * c.P.fsz));
+        k_int_to_double<<<cgrid(c.P.fsz), 256, 0, c.stream>>>(id == EPIC_FIELD_NPARG ? c.nparg : c.nsparg, tmp, c.P.fsz);
+        CKL();
+        CK(cudaMemcpyAsync(out, tmp, sizeof(double) * c.P.fsz, cudaMemcpyDeviceToHost, c.stream));
+    } else {
+        CK(cudaMemcpyAsync(out, c.field(id), sizeof(double) * c.P.fsz, cudaMemcpyDeviceToHost, c.stream));
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    API_END
+}
+
+int epic_gpu_set_field(epic_ctx* ctx, int id, const double* in) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!in || id < 0 || id >= EPIC_FIELD_NPARG) throw CudaError(EPIC_ERR_ARG, "set_field: bad field id");
+    CK(cudaMemcpyAsync(c.field(id), in, sizeof(double) * c.P.fsz, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    API_END
+}
+
+int epic_gpu_init_correction(epic_ctx* ctx) {
+    API_BEGIN NEED_PARCELS init_correction(ctx->c); check_device_error(ctx->c); API_END
+}
+int epic_gpu_apply_vortcor(epic_ctx* ctx) {
+    API_BEGIN NEED_PARCELS apply_vortcor(ctx->c); check_device_error(ctx->c); API_END
+}
+int epic_gpu_par2grid(epic_ctx* ctx, int reuse) {
+    API_BEGIN NEED_PARCELS par2grid(ctx->c, reuse != 0, true); check_device_error(ctx->c); API_END
+}
+int epic_gpu_vor2vel(epic_ctx* ctx) { API_BEGIN vor2vel(ctx->c); check_device_error(ctx->c); API_END }
+int epic_gpu_vorticity_tendency(epic_ctx* ctx) {
+    API_BEGIN vorticity_tendency(ctx->c); check_device_error(ctx->c); API_END
+}
+int epic_gpu_time_step(epic_ctx* ctx, double t, double* dt) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!dt) throw CudaError(EPIC_ERR_ARG, "null dt");
+    CK(cudaMemcpyAsync(&c.dsc->t, &t, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    time_step_reduce(c);
+    CK(cudaMemcpyAsync(dt, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    check_device_error(c);
+    API_END
+}
+int epic_gpu_grid2par(epic_ctx* ctx, int add) {
+    API_BEGIN NEED_PARCELS grid2par(ctx->c, add != 0); check_device_error(ctx->c); API_END
+}
+
+static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
+    // ls_rk_step (ls_rk.f90:88-136)
+    double tt = t;
+    CK(cudaMemcpyAsync(&c.dsc->t, &tt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    par2grid(c, t > c.cfg.t_initial, true);
+    vor2vel(c);
+    vorticity_tendency(c);
+    time_step_reduce(c);
+    if (fstats) field_diagnostics(c, fstats);
+    g2p_rk_stage(c, 1, pstats != nullptr);
+    if (pstats) finish_parcel_diag(c, pstats);
+    for (int s = 2; s <= c.n_stages; ++s) {
+        par2grid(c, false, true);
+        vor2vel(c);
+        vorticity_tendency(c);
+        g2p_rk_stage(c, s, false);
+    }
+    double dt = 0.0;
+    CK(cudaMemcpyAsync(&dt, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    check_device_error(c);
+    t = t + dt;
+    return dt;
+}
+
+int epic_gpu_rk_step(epic_ctx* ctx, double* t, double* dt) {
+    API_BEGIN
+    NEED_PARCELS
+    if (!t) throw CudaError(EPIC_ERR_ARG, "null t");
+    double d = rk_step(ctx->c, *t, nullptr, nullptr);
+    if (dt) *dt = d;
+    API_END
+}
+
+int epic_gpu_merge(epic_ctx* ctx, int64_t* n_merge) {
+    API_BEGIN
+    NEED_PARCELS
+    long long m = parcel_merge(ctx->c);
+    check_device_error(ctx->c);
+    if (n_merge) *n_merge = m;
+    API_END
+}
+
+int epic_gpu_get_merge_pairs(epic_ctx* ctx, int64_t cap, int64_t* n, int32_t* isma, int32_t* iclo) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!n) throw CudaError(EPIC_ERR_ARG, "null");
+    *n = (int64_t)c.last_isma.size();
+    if (cap < *n) throw CudaError(EPIC_ERR_ARG, "get_merge_pairs: capacity too small");
+    for (size_t m = 0; m < c.last_isma.size(); ++m) {
+        if (isma) isma[m] = c.last_isma[m] + 1;
+        if (iclo) iclo[m] = c.last_iclo[m] + 1;
+    }
+    API_END
+}
+
+int epic_gpu_split(epic_ctx* ctx, int64_t* n_split) {
+    API_BEGIN
+    NEED_PARCELS
+    long long s = parcel_split(ctx->c);
+    check_device_error(ctx->c);
+    if (n_split) *n_split = s;
+    API_END
+}
+
+int epic_gpu_apply_laplace(epic_ctx* ctx, int reuse) {
+    API_BEGIN NEED_PARCELS apply_laplace(ctx->c, reuse != 0); check_device_error(ctx->c); API_END
+}
+int epic_gpu_apply_gradient(epic_ctx* ctx, int reuse) {
+    API_BEGIN NEED_PARCELS apply_gradient(ctx->c, reuse != 0); check_device_error(ctx->c); API_END
+}
+int epic_gpu_vol2grid(epic_ctx* ctx, int reuse) {
+    API_BEGIN NEED_PARCELS vol2grid(ctx->c, reuse != 0); check_device_error(ctx->c); API_END
+}
+int epic_gpu_parcel_diagnostics(epic_ctx* ctx, double* st) {
+    API_BEGIN NEED_PARCELS parcel_diagnostics(ctx->c, st); check_device_error(ctx->c); API_END
+}
+int epic_gpu_field_diagnostics(epic_ctx* ctx, double* st) {
+    API_BEGIN field_diagnostics(ctx->c, st); check_device_error(ctx->c); API_END
+}
+
+int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info) {
+    API_BEGIN
+    NEED_PARCELS
+    Ctx& c = ctx->c;
+    if (!t) throw CudaError(EPIC_ERR_ARG, "null t");
+    epic_step_info tmp;
+    if (!info) info = &tmp;
+    std::memset(info, 0, sizeof(*info));
+    long long s0 = c.n_parcel_splits, m0 = c.n_parcel_merges;
+    apply_vortcor(c);
+    info->dt = rk_step(c, *t, info->parcel_stats, info->field_stats);
+    parcel_merge(c);
+    parcel_split(c);
+    for (int it = 1; it <= c.cfg.correction_iters; ++it) {
+        apply_laplace(c, it > 1);
+        apply_gradient(c, true);
+    }
+    check_device_error(c);
+    info->t = *t;
+    info->n_parcels = c.n;
+    info->n_splits = c.n_parcel_splits - s0;
+    info->n_merges = c.n_parcel_merges - m0;
+    API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+// Host-side context of one simulation: device state, tables and launchers.
+#pragma once
+#include "../../include/epic_gpu.h"
+#include "common.cuh"
+
+#include <string>
+#include <vector>
+#include <stdexcept>
+
+namespace epic {
+
+struct CudaError : std::runtime_error {
+    int code;
+    CudaError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            throw ::epic::CudaError(EPIC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+#define CKL() CK(cudaGetLastError())
+
+// Mixed-radix plan for the shared-memory Stockham FFT.
+struct FFTPlan {
+    int n = 0;
+    int nfac = 0;
+    int fac[16] = {0};
+    double2* tw = nullptr;   // device: exp(-2 pi i m / n), m = 0 .. n-1
+};
+
+// Spectral tables (inversion_utils.f90:23-48, sta3dfft.f90:17-22).
+struct Tables {
+    // per (kx, ky): k2l2i, hrkx factor for diffx, hrky factor for diffy
+    double* k2l2i = nullptr;       // nx*ny, index kx*ny + ky
+    double* fdx = nullptr;         // nx: si * hrkx(dkx) (0 at kx = 0 and Nyquist)
+    double* fdy = nullptr;         // ny
+    // per column (kx, ky) x z: layout like spectral fields (fidx)
+    double* filt = nullptr, *green = nullptr, *phim = nullptr, *phip = nullptr;
+    double* thetam = nullptr, *thetap = nullptr, *dthetam = nullptr, *dthetap = nullptr;
+    double* etdv = nullptr, *htdv = nullptr;
+    double* rkz = nullptr, *rkzi = nullptr, *gamtop = nullptr, *gambot = nullptr;  // nz+1
+    // z-transform matrices, (nz+1) x (nz+1) row-major: DST-I (rows/cols 1..nz-1), DCT-I
+    double* mdst = nullptr, *mdct = nullptr;
+};
+
+// Device scalars of one step (kept on the device between kernels).
+struct StepScalars {
+    double dt;
+    double t;
+    unsigned long long gmax_bits;   // max |eigenvalue| of the strain (as ordered bits)
+    unsigned long long bmax_bits;   // max |grad b|^2
+    unsigned err;
+    int n_iter_flag;
+    long long n;                    // parcel count
+    long long count;                // scratch counter
+    double vsum, vor[3];            // vorticity correction sums
+};
+
+struct Ctx {
+    epic_cfg cfg;
+    Params P;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int n_stages = 5;
+    double ca[5], cb[5];
+    // parcels
+    long long cap = 0;
+    long long n = 0;
+    PView pv{nullptr, 0};
+    // fields: velog 3, vortg 3, vtend 3, velgradg 8, tbuoyg, dbuoyg, humg, volg = 21
+    double* fields = nullptr;
+    int* nparg = nullptr, *nsparg = nullptr;
+    // spectral work arrays (each fsz doubles)
+    int n_work = 0;
+    double* work = nullptr;
+    FFTPlan px, py;
+    Tables T;
+    StepScalars* dsc = nullptr;     // device
+    StepScalars* hsc = nullptr;     // pinned host mirror
+    double vor_bar[3] = {0, 0, 0};
+    double* dvor_bar = nullptr;
+    // reduction partials
+    double* partials = nullptr;
+    int n_partials = 0;
+    // merge / split scratch
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    void* scratch2 = nullptr;
+    size_t scratch2_bytes = 0;
+    std::vector<int> last_isma, last_iclo;
+    long long n_parcel_splits = 0, n_parcel_merges = 0, n_big_close = 0;
+    bool has_parcels = false;
+
+    double* field(int id) const { return fields + (long long)id * P.fsz; }
+    double* velog(int c) const { return field(EPIC_FIELD_VELOG_X + c); }
+    double* vortg(int c) const { return field(EPIC_FIELD_VORTG_X + c); }
+    double* vtend(int c) const { return field(EPIC_FIELD_VTEND_X + c); }
+    double* velgrad(int c) const { return field(EPIC_FIELD_VELGRAD_0 + c); }
+    double* tbuoyg() const { return field(EPIC_FIELD_TBUOYG); }
+    double* dbuoyg() const { return field(EPIC_FIELD_DBUOYG); }
+    double* humg() const { return field(EPIC_FIELD_HUMG); }
+    double* volg() const { return field(EPIC_FIELD_VOLG); }
+    double* w(int k) const { return work + (long long)k * P.fsz; }
+    void* get_scratch(size_t bytes);
+    void* get_scratch2(size_t bytes);
+};
+
+constexpr int N_FIELDS = 21;
+constexpr int N_WORK = 14;
+
+// spectral.cu
+void spectral_init(Ctx& c);
+void spectral_free(Ctx& c);
+void fft_xy(Ctx& c, const double* const* in, double* const* out, int nf, bool forward);
+void vor2vel(Ctx& c);
+void vorticity_tendency(Ctx& c);
+void diverge_laplace(Ctx& c, double* phi, double* grad[3]);
+void time_step_reduce(Ctx& c);
+void make_phi(Ctx& c, double* phi);
+
+// parcels.cu
+void par2grid(Ctx& c, bool reuse, bool store_vectors);
+void vol2grid(Ctx& c, bool reuse);
+void grid2par(Ctx& c, bool add);
+void g2p_rk_stage(Ctx& c, int stage, bool with_diag);
+void rk_substep1_dBdt(Ctx& c);
+void apply_vortcor(Ctx& c);
+void init_correction(Ctx& c);
+void apply_laplace(Ctx& c, bool reuse);
+void apply_gradient(Ctx& c, bool reuse);
+void parcel_diagnostics(Ctx& c, double* out);
+void field_diagnostics(Ctx& c, double* out);
+long long parcel_split(Ctx& c);
+void periodic_all(Ctx& c);
+void reflective_all(Ctx& c);
+void finish_parcel_diag(Ctx& c, double* out);
+
+// merge.cu
+long long parcel_merge(Ctx& c);
+
+// api.cu
+void check_device_error(Ctx& c);
+void sync_scalars(Ctx& c);
+
+}  // namespace epic

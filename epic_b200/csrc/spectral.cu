@@ -1,0 +1,1160 @@
+// Spectral part of the step on the device: batched shared-memory FFTs along x
+// and y in the reference's Hermitian storage, vertical sine/cosine transforms,
+// and the vorticity inversion (vor2vel), vorticity tendency, divergent-flow
+// solve (diverge + lapinv1) and the time-step reduction.
+//
+// Reference semantics:
+//   fftxyp2s / fftxys2p  sta3dfft.f90:134-257, forfft / revfft stafft.f90:196-403
+//   dst / dct            stafft.f90:410-550
+//   diffx / diffy        sta3dfft.f90:301-374 (+ reverse_x/y, mpi_reverse.f90:332-398)
+//   vor2vel, vel2vgrad   inversion.f90:25-317
+//   vorticity_tendency   inversion.f90:321-404
+//   diverge, lapinv1     inversion.f90:410-455, inversion_utils.f90:567-589
+//   get_time_step        rk_utils.f90:70-183
+#include "ctx.hpp"
+#include "eigen.cuh"
+
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#include <cstring>
+#include <initializer_list>
+#include <utility>
+
+namespace epic {
+
+// ---------------------------------------------------------------------------
+// Batched real FFT of lines along x or y, one tile of T lines per CTA.
+// Two real lines are packed into one complex line (z = a + i b), transformed
+// with a mixed-radix Stockham FFT in shared memory, and separated with the
+// conjugate-symmetry identities.  Output uses the stafft Hermitian layout:
+//   out[k] = Re X_k / sqrt(n) (k <= n/2),  out[n-k] = Im X_k / sqrt(n).
+constexpr int MAXF = 12;
+
+struct FFTBatch {
+    const double* in[MAXF];
+    double* out[MAXF];
+    long long es;          // element stride along the transformed axis
+    long long row_stride;  // stride between rows of lines
+    int nl;                // lines per row (nz + 1, contiguous)
+    int T;                 // lines per tile (even)
+    int n;
+    int nfac;
+    int fac[16];
+    const double2* tw;
+    double scale;
+};
+
+EPIC_DEV double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+EPIC_DEV double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+EPIC_DEV double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+// Stockham autosort passes on L complex lines of length n held in a / b.
+// Returns the buffer holding the result.
+EPIC_DEV double2* stockham(double2* a, double2* b, int L, int n, int nfac, const int* fac,
+                           const double2* tw) {
+    int Ns = 1;
+    for (int s = 0; s < nfac; ++s) {
+        int p = fac[s];
+        int m = n / p;
+        int tstep = n / (Ns * p);
+        for (int idx = threadIdx.x; idx < L * m; idx += blockDim.x) {
+            int l2 = idx / m, j = idx - l2 * m;
+            int k = j % Ns;
+            const double2* src = a + (long long)l2 * n;
+            double2* dst = b + (long long)l2 * n;
+            double2 v[5];
+            for (int r = 0; r < p; ++r) v[r] = src[j + r * m];
+            for (int r = 1; r < p; ++r) v[r] = cmul(v[r], tw[(k * r * tstep) % n]);
+            double2 o[5];
+            if (p == 2) {
+                o[0] = cadd(v[0], v[1]);
+                o[1] = csub(v[0], v[1]);
+            } else if (p == 4) {
+                double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+                double2 t2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+                double2 t3 = make_double2(d.y, -d.x);   // -i * d
+                o[0] = cadd(t0, t2);
+                o[2] = csub(t0, t2);
+                o[1] = cadd(t1, t3);
+                o[3] = csub(t1, t3);
+            } else {
+                int step = n / p;
+                for (int q = 0; q < p; ++q) {
+                    double2 acc = v[0];
+                    for (int r = 1; r < p; ++r) acc = cadd(acc, cmul(v[r], tw[((q * r) % p) * step]));
+                    o[q] = acc;
+                }
+            }
+            int base = (j / Ns) * Ns * p + k;
+            for (int r = 0; r < p; ++r) dst[base + r * Ns] = o[r];
+        }
+        __syncthreads();
+        double2* t = a; a = b; b = t;
+        Ns *= p;
+    }
+    return a;
+}
+
+template <bool FWD>
+__global__ void __launch_bounds__(256) k_fft_lines(FFTBatch B) {
+    extern __shared__ double smem[];
+    const int n = B.n, T = B.T, L = T / 2;
+    double* sx = smem;
+    double2* cz = reinterpret_cast<double2*>(sx + (long long)T * n);
+    double2* cw = cz + (long long)L * n;
+    double2* stw = cw + (long long)L * n;
+    const double* in = B.in[blockIdx.z];
+    double* out = B.out[blockIdx.z];
+    const int l0 = blockIdx.x * T;
+    const long long rowbase = (long long)blockIdx.y * B.row_stride + 1;
+
+    for (int i = threadIdx.x; i < n; i += blockDim.x) stw[i] = B.tw[i];
+    for (int idx = threadIdx.x; idx < T * n; idx += blockDim.x) {
+        int l = idx % T, e = idx / T;
+        int line = l0 + l;
+        sx[e * T + l] = (line < B.nl) ? in[rowbase + line + (long long)e * B.es] : 0.0;
+    }
+    __syncthreads();
+    const int h = n / 2;
+    if (FWD) {
+        for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+            int l2 = idx / n, e = idx - l2 * n;
+            cz[idx] = make_double2(sx[e * T + 2 * l2], sx[e * T + 2 * l2 + 1]);
+        }
+    } else {
+        // Hermitian lines a, b -> conj(Xa + i Xb)
+        for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+            int l2 = idx / n, k = idx - l2 * n;
+            int la = 2 * l2, lb = la + 1;
+            double ra, ia, rb, ib;
+            if (k == 0 || k == h) {
+                ra = sx[k * T + la]; ia = 0.0;
+                rb = sx[k * T + lb]; ib = 0.0;
+            } else if (k < h) {
+                ra = sx[k * T + la]; ia = sx[(n - k) * T + la];
+                rb = sx[k * T + lb]; ib = sx[(n - k) * T + lb];
+            } else {
+                ra = sx[(n - k) * T + la]; ia = -sx[k * T + la];
+                rb = sx[(n - k) * T + lb]; ib = -sx[k * T + lb];
+            }
+            cz[idx] = make_double2(ra - ib, -(ia + rb));
+        }
+    }
+    __syncthreads();
+    double2* res = stockham(cz, cw, L, n, B.nfac, B.fac, stw);
+    if (FWD) {
+        for (int idx = threadIdx.x; idx < L * (h + 1); idx += blockDim.x) {
+            int l2 = idx / (h + 1), k = idx - l2 * (h + 1);
+            double2 zk = res[(long long)l2 * n + k];
+            double2 zn = res[(long long)l2 * n + ((n - k) % n)];
+            int la = 2 * l2, lb = la + 1;
+            sx[k * T + la] = 0.5 * (zk.x + zn.x);
+            sx[k * T + lb] = 0.5 * (zk.y + zn.y);
+            if (k > 0 && k < h) {
+                sx[(n - k) * T + la] = 0.5 * (zk.y - zn.y);
+                sx[(n - k) * T + lb] = 0.5 * (zn.x - zk.x);
+            }
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < L * n; idx += blockDim.x) {
+            int l2 = idx / n, e = idx - l2 * n;
+            double2 z = res[idx];
+            sx[e * T + 2 * l2] = z.x;
+            sx[e * T + 2 * l2 + 1] = -z.y;
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < T * n; idx += blockDim.x) {
+        int l = idx % T, e = idx / T;
+        int line = l0 + l;
+        if (line < B.nl) out[rowbase + line + (long long)e * B.es] = sx[e * T + l] * B.scale;
+    }
+}
+
+static void make_plan(FFTPlan& p, int n, cudaStream_t st) {
+    p.n = n;
+    p.nfac = 0;
+    int rem = n;
+    for (int f : {4, 2, 3, 5})
+        while (rem % f == 0) { p.fac[p.nfac++] = f; rem /= f; }
+    if (rem != 1 || n % 2 != 0)
+        throw CudaError(EPIC_ERR_CONFIG, "horizontal grid sizes must be even and factor into 2, 3, 5");
+    std::vector<double2> tw(n);
+    for (int m = 0; m < n; ++m) {
+        double a = -2.0 * M_PI * (double)m / (double)n;
+        tw[m] = make_double2(std::cos(a), std::sin(a));
+    }
+    CK(cudaMalloc(&p.tw, sizeof(double2) * n));
+    CK(cudaMemcpyAsync(p.tw, tw.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, st));
+}
+
+static int tile_lines(int n) {
+    int T = 4096 / n;
+    T = std::max(2, std::min(32, T));
+    return T & ~1;
+}
+
+static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* const* in,
+                         double* const* out, int nf, bool forward) {
+    const Params& P = c.P;
+    FFTBatch B;
+    for (int f = 0; f < nf; ++f) { B.in[f] = in[f]; B.out[f] = out[f]; }
+    B.n = pl.n;
+    B.nfac = pl.nfac;
+    for (int k = 0; k < 16; ++k) B.fac[k] = pl.fac[k];
+    B.tw = pl.tw;
+    B.nl = P.nz + 1;
+    B.T = tile_lines(pl.n);
+    B.scale = 1.0 / std::sqrt((double)pl.n);
+    int nrows;
+    if (axis == 0) { B.es = (long long)P.ny * P.nzh; B.row_stride = P.nzh; nrows = P.ny; }
+    else { B.es = P.nzh; B.row_stride = (long long)P.ny * P.nzh; nrows = P.nx; }
+    size_t sm = sizeof(double) * (size_t)B.T * B.n + 2 * sizeof(double2) * (size_t)(B.T / 2) * B.n +
+                sizeof(double2) * B.n;
+    dim3 grid((B.nl + B.T - 1) / B.T, nrows, nf);
+    if (forward) {
+        CK(cudaFuncSetAttribute(k_fft_lines<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fft_lines<true><<<grid, 256, sm, c.stream>>>(B);
+    } else {
+        CK(cudaFuncSetAttribute(k_fft_lines<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fft_lines<false><<<grid, 256, sm, c.stream>>>(B);
+    }
+    CKL();
+}
+
+// fftxyp2s: y then x (forward); fftxys2p: x then y (reverse).  Only rows
+// z = 0 .. nz are read and written.
+void fft_xy(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
+    for (int f0 = 0; f0 < nf; f0 += MAXF) {
+        int k = std::min(MAXF, nf - f0);
+        if (forward) {
+            run_fft_axis(c, c.py, 1, in + f0, out + f0, k, true);
+            run_fft_axis(c, c.px, 0, out + f0, out + f0, k, true);
+        } else {
+            run_fft_axis(c, c.px, 0, in + f0, out + f0, k, false);
+            run_fft_axis(c, c.py, 1, out + f0, out + f0, k, false);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Vertical (column) kernels.  A CTA holds 32 columns (kx, ky) of nz+1 values
+// in shared memory as x[j * 33 + col]; matrix-vector products with the DST-I /
+// DCT-I matrices read each matrix entry once per warp (broadcast) and keep
+// all 32 lanes busy on different columns.
+constexpr int CT = 32;
+constexpr int CP = 33;
+
+struct ColArgs {
+    const double* tab[8];
+    const double* in[4];
+    double* out[4];
+    const double* mdst;
+    const double* mdct;
+    int ncol;      // nx * ny
+    int nz;
+    int nzh;
+    double dzi, hdzi;
+};
+
+EPIC_DEV void col_load(const double* f, double* xs, int c0, const ColArgs& A) {
+    int nzp = A.nz + 1;
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx / nzp, j = idx - col * nzp;
+        int c = c0 + col;
+        xs[j * CP + col] = (c < A.ncol) ? f[(long long)c * A.nzh + 1 + j] : 0.0;
+    }
+}
+EPIC_DEV void col_store(double* f, const double* xs, int c0, const ColArgs& A) {
+    int nzp = A.nz + 1;
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx / nzp, j = idx - col * nzp;
+        int c = c0 + col;
+        if (c < A.ncol) f[(long long)c * A.nzh + 1 + j] = xs[j * CP + col];
+    }
+}
+// table value for (column c, z = j)
+EPIC_DEV double tabv(const double* t, int c, int j, const ColArgs& A) {
+    return t[(long long)c * A.nzh + 1 + j];
+}
+// ys[k] = sum_{j=lo..hi} M[k][j] xs[j] for k = lo..hi (M row-major (nz+1)^2)
+EPIC_DEV void col_matvec(const double* M, int lo, int hi, const double* xs, double* ys, int nz) {
+    int col = threadIdx.x & 31;
+    int grp = threadIdx.x >> 5;
+    int ngrp = blockDim.x >> 5;
+    for (int k = lo + grp; k <= hi; k += ngrp) {
+        const double* row = M + (long long)k * (nz + 1);
+        double s = 0.0;
+        for (int j = lo; j <= hi; ++j) s = fma(row[j], xs[j * CP + col], s);
+        ys[k * CP + col] = s;
+    }
+}
+
+// field_decompose_semi_spectral (inversion_utils.f90:370-401), optionally
+// followed by the Hou-Li filter and/or preceded by central_diffz_semi_spectral
+// (inversion_utils.f90:460-480).  mode bit 1: filter, bit 2: central diff.
+__global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
+    extern __shared__ double sm[];
+    int nzp = A.nz + 1, nz = A.nz;
+    double* xs = sm;
+    double* ys = sm + nzp * CP;
+    int c0 = blockIdx.x * CT;
+    const double* phim = A.tab[0];
+    const double* phip = A.tab[1];
+    const double* filt = A.tab[2];
+    col_load(A.in[blockIdx.y], xs, c0, A);
+    __syncthreads();
+    if (mode & 2) {
+        for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+            int col = idx % CT, j = idx / CT;
+            double v;
+            if (j == 0) v = A.dzi * (xs[1 * CP + col] - xs[col]);
+            else if (j == nz) v = A.dzi * (xs[nz * CP + col] - xs[(nz - 1) * CP + col]);
+            else v = (xs[(j + 1) * CP + col] - xs[(j - 1) * CP + col]) * A.hdzi;
+            ys[j * CP + col] = v;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) xs[idx % CT + (idx / CT) * CP] = ys[idx % CT + (idx / CT) * CP];
+        __syncthreads();
+    }
+    // subtract harmonic part
+    for (int idx = threadIdx.x; idx < CT * (nz - 1); idx += blockDim.x) {
+        int col = idx % CT, j = 1 + idx / CT;
+        int c = min(c0 + col, A.ncol - 1);
+        xs[j * CP + col] = xs[j * CP + col] - (xs[col] * tabv(phim, c, j, A) + xs[nz * CP + col] * tabv(phip, c, j, A));
+    }
+    __syncthreads();
+    col_matvec(A.mdst, 1, nz - 1, xs, ys, nz);
+    for (int col = threadIdx.x; col < CT; col += blockDim.x) {
+        ys[col] = xs[col];
+        ys[nz * CP + col] = xs[nz * CP + col];
+    }
+    __syncthreads();
+    if (mode & 1) {
+        for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+            int col = idx % CT, j = idx / CT;
+            int c = min(c0 + col, A.ncol - 1);
+            ys[j * CP + col] = tabv(filt, c, j, A) * ys[j * CP + col];
+        }
+        __syncthreads();
+    }
+    col_store(A.out[blockIdx.y], ys, c0, A);
+}
+
+// field_combine_semi_spectral (inversion_utils.f90:421-456)
+__global__ void __launch_bounds__(256) k_col_combine(ColArgs A) {
+    extern __shared__ double sm[];
+    int nzp = A.nz + 1, nz = A.nz;
+    double* xs = sm;
+    double* ys = sm + nzp * CP;
+    int c0 = blockIdx.x * CT;
+    const double* phim = A.tab[0];
+    const double* phip = A.tab[1];
+    col_load(A.in[blockIdx.y], xs, c0, A);
+    __syncthreads();
+    col_matvec(A.mdst, 1, nz - 1, xs, ys, nz);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx % CT, j = idx / CT;
+        int c = min(c0 + col, A.ncol - 1);
+        double v;
+        if (j == 0) v = xs[col];
+        else if (j == nz) v = xs[nz * CP + col];
+        else v = ys[j * CP + col] + xs[col] * tabv(phim, c, j, A) + xs[nz * CP + col] * tabv(phip, c, j, A);
+        xs[j * CP + col] = v;
+    }
+    __syncthreads();
+    col_store(A.out[blockIdx.y], xs, c0, A);
+}
+
+// Vertical-velocity solve of vor2vel (inversion.f90:97-150): in[0] = D
+// (source) -> out[0] = w (semi-spectral), out[1] = dw/dz part es.
+__global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
+    extern __shared__ double sm[];
+    int nzp = A.nz + 1, nz = A.nz;
+    double* ds = sm;
+    double* as = sm + nzp * CP;
+    double* bs = sm + 2 * nzp * CP;
+    double* es = sm + 3 * nzp * CP;
+    int c0 = blockIdx.x * CT;
+    const double* thetam = A.tab[0];
+    const double* thetap = A.tab[1];
+    const double* dthetam = A.tab[2];
+    const double* dthetap = A.tab[3];
+    const double* green = A.tab[4];
+    const double* rkz = A.tab[5];
+    col_load(A.in[0], ds, c0, A);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx % CT, j = idx / CT;
+        int c = min(c0 + col, A.ncol - 1);
+        double d0 = ds[col], dn = ds[nz * CP + col];
+        if (j >= 1 && j <= nz - 1) bs[j * CP + col] = d0 * tabv(thetam, c, j, A) + dn * tabv(thetap, c, j, A);
+        es[j * CP + col] = d0 * tabv(dthetam, c, j, A) + dn * tabv(dthetap, c, j, A);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx % CT, j = idx / CT;
+        int c = min(c0 + col, A.ncol - 1);
+        if (j >= 1 && j <= nz - 1) {
+            double g = tabv(green, c, j, A) * ds[j * CP + col];
+            ds[j * CP + col] = g;
+            as[j * CP + col] = rkz[j] * g;
+        } else {
+            as[j * CP + col] = 0.0;
+        }
+    }
+    __syncthreads();
+    // dct(as) -> into bs? keep bs; use es-add directly: es += DCT(as)
+    {
+        int col = threadIdx.x & 31, grp = threadIdx.x >> 5, ngrp = blockDim.x >> 5;
+        for (int k = grp; k <= nz; k += ngrp) {
+            const double* row = A.mdct + (long long)k * nzp;
+            double s = 0.0;
+            for (int j = 0; j <= nz; ++j) s = fma(row[j], as[j * CP + col], s);
+            es[k * CP + col] = es[k * CP + col] + s;
+        }
+        __syncthreads();
+        // dst(ds(1:nz-1)) into as rows 1..nz-1
+        for (int k = 1 + grp; k <= nz - 1; k += ngrp) {
+            const double* row = A.mdst + (long long)k * nzp;
+            double s = 0.0;
+            for (int j = 1; j <= nz - 1; ++j) s = fma(row[j], ds[j * CP + col], s);
+            as[k * CP + col] = s;
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx % CT, j = idx / CT;
+        ds[j * CP + col] = (j >= 1 && j <= nz - 1) ? as[j * CP + col] + bs[j * CP + col] : 0.0;
+    }
+    __syncthreads();
+    col_store(A.out[0], ds, c0, A);
+    col_store(A.out[1], es, c0, A);
+}
+
+// ---------------------------------------------------------------------------
+// Pointwise spectral kernels.  Element (kx, ky, iz), iz = 0 .. nz.
+struct SpecArgs {
+    const double* in[6];
+    double* out[6];
+    const double* k2l2i;
+    const double* fdx;
+    const double* fdy;
+    const double* zbuf;    // (0,0)-column replacement values (2 x (nz+1))
+    int nx, ny, nz, nzh;
+    long long nel;         // nx * ny * (nz + 1)
+};
+
+struct SpecIdx {
+    long long a;     // address of (kx, ky, iz)
+    long long ax;    // address of (nx-kx, ky, iz)
+    long long ay;    // address of (kx, ny-ky, iz)
+    int kx, ky, iz;
+};
+
+EPIC_DEV SpecIdx spec_idx(const SpecArgs& S, long long i) {
+    SpecIdx r;
+    int nzp = S.nz + 1;
+    long long c = i / nzp;
+    r.iz = (int)(i - c * nzp);
+    r.kx = (int)(c / S.ny);
+    r.ky = (int)(c - (long long)r.kx * S.ny);
+    int px = r.kx == 0 ? 0 : S.nx - r.kx;
+    int py = r.ky == 0 ? 0 : S.ny - r.ky;
+    r.a = ((long long)r.kx * S.ny + r.ky) * S.nzh + 1 + r.iz;
+    r.ax = ((long long)px * S.ny + r.ky) * S.nzh + 1 + r.iz;
+    r.ay = ((long long)r.kx * S.ny + py) * S.nzh + 1 + r.iz;
+    return r;
+}
+
+#define SPEC_LOOP(S) for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (S).nel; \
+                          i += (long long)gridDim.x * blockDim.x)
+
+// out0 = Dx(in0) - Dy(in1)  (used for D = B_x - A_y and for the w source
+// Dy(A) - Dx(B) with swapped signs via `sign`)
+__global__ void k_spec_dxdy(SpecArgs S, double sx, double sy) {
+    SPEC_LOOP(S) {
+        SpecIdx q = spec_idx(S, i);
+        S.out[0][q.a] = sx * S.fdx[q.kx] * S.in[0][q.ax] + sy * S.fdy[q.ky] * S.in[1][q.ay];
+    }
+}
+
+// svor_x = k2l2i (Dx(es) + Dy(ds)); svor_y = k2l2i (Dy(es) - Dx(ds));
+// (0,0) column unchanged (inversion.f90:76-87).  in0 = es, in1 = ds.
+__global__ void k_spec_project(SpecArgs S) {
+    SPEC_LOOP(S) {
+        SpecIdx q = spec_idx(S, i);
+        if (q.kx == 0 && q.ky == 0) continue;
+        double k2 = S.k2l2i[(long long)q.kx * S.ny + q.ky];
+        double ex = S.fdx[q.kx] * S.in[0][q.ax], ey = S.fdy[q.ky] * S.in[0][q.ay];
+        double dx = S.fdx[q.kx] * S.in[1][q.ax], dy = S.fdy[q.ky] * S.in[1][q.ay];
+        S.out[0][q.a] = k2 * (ex + dy);
+        S.out[1][q.a] = k2 * (ey - dx);
+    }
+}
+
+// u = k2l2i (Dx(es) + Dy(cs)), v = k2l2i (Dy(es) - Dx(cs)); (0,0) = ubar, vbar
+// (inversion.f90:180-226).  in0 = es, in1 = cs.
+__global__ void k_spec_uv(SpecArgs S) {
+    SPEC_LOOP(S) {
+        SpecIdx q = spec_idx(S, i);
+        if (q.kx == 0 && q.ky == 0) {
+            S.out[0][q.a] = S.zbuf[q.iz];
+            S.out[1][q.a] = S.zbuf[S.nz + 1 + q.iz];
+            continue;
+        }
+        double k2 = S.k2l2i[(long long)q.kx * S.ny + q.ky];
+        double ex = S.fdx[q.kx] * S.in[0][q.ax], ey = S.fdy[q.ky] * S.in[0][q.ay];
+        double cx = S.fdx[q.kx] * S.in[1][q.ax], cy = S.fdy[q.ky] * S.in[1][q.ay];
+        S.out[0][q.a] = k2 * (ex + cy);
+        S.out[1][q.a] = k2 * (ey - cx);
+    }
+}
+
+// velocity gradients (inversion.f90:259-290): in = u, v, w ->
+// out = du/dx, du/dy, dw/dx, dv/dy, dw/dy
+__global__ void k_spec_grad(SpecArgs S) {
+    SPEC_LOOP(S) {
+        SpecIdx q = spec_idx(S, i);
+        double fx = S.fdx[q.kx], fy = S.fdy[q.ky];
+        S.out[0][q.a] = fx * S.in[0][q.ax];
+        S.out[1][q.a] = fy * S.in[0][q.ay];
+        S.out[2][q.a] = fx * S.in[2][q.ax];
+        S.out[3][q.a] = fy * S.in[1][q.ay];
+        S.out[4][q.a] = fy * S.in[2][q.ay];
+    }
+}
+
+// vorticity tendency: out_c = Dx(Fx_c) + Dy(Fy_c), in = Fx0, Fy0, Fx1, Fy1, Fx2, Fy2
+__global__ void k_spec_divxy(SpecArgs S) {
+    SPEC_LOOP(S) {
+        SpecIdx q = spec_idx(S, i);
+        double fx = S.fdx[q.kx], fy = S.fdy[q.ky];
+        for (int c = 0; c < 3; ++c)
+            S.out[c][q.a] = fx * S.in[2 * c][q.ax] + fy * S.in[2 * c + 1][q.ay];
+    }
+}
+
+// diverge (inversion.f90:431-451): us = Dx(ds), vs = Dy(ds),
+// ws = central_diffz_semi_spectral(ds) with ws(0) = ws(nz) = 0.
+__global__ void k_spec_lapgrad(SpecArgs S, double hdzi) {
+    SPEC_LOOP(S) {
+        SpecIdx q = spec_idx(S, i);
+        const double* d = S.in[0];
+        S.out[0][q.a] = S.fdx[q.kx] * d[q.ax];
+        S.out[1][q.a] = S.fdy[q.ky] * d[q.ay];
+        S.out[2][q.a] = (q.iz == 0 || q.iz == S.nz) ? 0.0 : (d[q.a + 1] - d[q.a - 1]) * hdzi;
+    }
+}
+
+// Mean flow (inversion.f90:158-176), one CTA: zbuf = (ubar, vbar).
+__global__ void k_mean_flow(const double* svx, const double* svy, const double* rkzi, const double* gamtop,
+                            const double* gambot, const double* mdct, double* zbuf, int nz) {
+    extern __shared__ double sm[];
+    double* u = sm;
+    double* v = sm + nz + 1;
+    for (int iz = threadIdx.x; iz <= nz; iz += blockDim.x) {
+        bool in = iz >= 1 && iz <= nz - 1;
+        u[iz] = in ? -rkzi[iz] * svy[1 + iz] : 0.0;
+        v[iz] = in ? rkzi[iz] * svx[1 + iz] : 0.0;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k <= nz; k += blockDim.x) {
+        const double* row = mdct + (long long)k * (nz + 1);
+        double su = 0.0, sv = 0.0;
+        for (int j = 0; j <= nz; ++j) { su = fma(row[j], u[j], su); sv = fma(row[j], v[j], sv); }
+        zbuf[k] = su + svy[1 + nz] * gamtop[k] - svy[1] * gambot[k];
+        zbuf[nz + 1 + k] = sv - svx[1 + nz] * gamtop[k] + svx[1] * gambot[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Physical-space helpers.  Element (ix, iy, iz) with iz = -1 .. nz+1.
+struct PhysArgs {
+    const double* in[8];
+    double* out[8];
+    int mode[8];
+    int nf;
+    int nx, ny, nz, nzh;
+    long long ncol;
+};
+
+// z halo rows: mode 0 = linear extrapolation, 1 = anti-symmetry
+__global__ void k_halo(PhysArgs A) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= A.ncol * A.nf) return;
+    int f = (int)(t / A.ncol);
+    long long c = t - (long long)f * A.ncol;
+    double* p = A.out[f] + c * A.nzh + 1;
+    int nz = A.nz;
+    if (A.mode[f] == 0) {
+        p[-1] = 2.0 * p[0] - p[1];
+        p[nz + 1] = 2.0 * p[nz] - p[nz - 1];
+    } else {
+        p[-1] = -p[1];
+        p[nz + 1] = -p[nz - 1];
+    }
+}
+
+struct Ptr8 {
+    const double* p[8];
+};
+struct MPtr8 {
+    double* p[8];
+};
+
+// vel2vgrad tail (inversion.f90:308-312) over all rows incl. the halo rows.
+__global__ void k_velgrad_fill(MPtr8 vg, Ptr8 vort, long long fsz) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < fsz;
+         i += (long long)gridDim.x * blockDim.x) {
+        vg.p[I_DUDZ][i] = vg.p[I_DWDX][i] + vort.p[1][i];
+        vg.p[I_DVDX][i] = vg.p[I_DUDY][i] + vort.p[2][i];
+        vg.p[I_DVDZ][i] = vg.p[I_DWDY][i] - vort.p[0][i];
+    }
+}
+
+struct FluxArgs {
+    const double* vort[3];
+    const double* vel[3];
+    const double* b;
+    double* f[6];
+    double fc[3];
+    int nx, ny, nz, nzh;
+    long long nel;   // nx * ny * (nz+1)
+};
+
+// Flux products of vorticity_tendency (inversion.f90:327-348), rows 0..nz.
+__global__ void k_flux(FluxArgs A) {
+    int nzp = A.nz + 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.nel;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long c = i / nzp;
+        long long a = c * A.nzh + 1 + (i - c * nzp);
+        double wx = A.vort[0][a] + A.fc[0], wy = A.vort[1][a] + A.fc[1];
+        double b = A.b[a];
+        double u = A.vel[0][a], v = A.vel[1][a], w = A.vel[2][a];
+        A.f[0][a] = wx * u;
+        A.f[1][a] = wy * u + b;
+        A.f[2][a] = wx * v - b;
+        A.f[3][a] = wy * v;
+        A.f[4][a] = wx * w;
+        A.f[5][a] = wy * w;
+    }
+}
+
+// vtend_c(0:nz) = divxy_c + central_diffz((zeta + f_z) u_c), with the zeta
+// boundary zeroing (inversion.f90:374-384, inversion_utils.f90:485-510).
+__global__ void k_vtend_rows(FluxArgs A, Ptr8 divxy, MPtr8 vt, double dzi, double hdzi, int z0, int z1) {
+    int nzp = A.nz + 1, nz = A.nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.nel;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long c = i / nzp;
+        int iz = (int)(i - c * nzp);
+        long long a = c * A.nzh + 1 + iz;
+        const double* wz = A.vort[2];
+        double fz = A.fc[2];
+        for (int k = 0; k < 3; ++k) {
+            const double* u = A.vel[k];
+            double dz;
+            if (iz == 0) dz = dzi * ((wz[a + 1] + fz) * u[a + 1] - (wz[a] + fz) * u[a]);
+            else if (iz == nz) dz = dzi * ((wz[a] + fz) * u[a] - (wz[a - 1] + fz) * u[a - 1]);
+            else dz = ((wz[a + 1] + fz) * u[a + 1] - (wz[a - 1] + fz) * u[a - 1]) * hdzi;
+            double v = divxy.p[k][a] + dz;
+            if (k == 2 && ((iz == 0 && z0) || (iz == nz && z1))) v = 0.0;
+            vt.p[k][a] = v;
+        }
+    }
+}
+
+// lapinv1 (inversion_utils.f90:567-589), one thread per column; the (0,0)
+// column is zero (inversion.f90:423-426 and inversion_utils.f90:584-587).
+__global__ void k_lapinv(double* fs, const double* etdv, const double* htdv, double ap, int ncol, int nz, int nzh) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncol) return;
+    double* f = fs + (long long)c * nzh + 1;
+    const double* e = etdv + (long long)c * nzh + 1;
+    const double* h = htdv + (long long)c * nzh + 1;
+    if (c == 0) {
+        for (int iz = 0; iz <= nz; ++iz) f[iz] = 0.0;
+        return;
+    }
+    double prev = f[0] * h[0];
+    f[0] = prev;
+    for (int iz = 1; iz <= nz - 1; ++iz) {
+        prev = (f[iz] - ap * prev) * h[iz];
+        f[iz] = prev;
+    }
+    f[nz] = (f[nz] - 2.0 * ap * prev) * h[nz];
+    for (int iz = nz - 1; iz >= 0; --iz) f[iz] = e[iz] * f[iz + 1] + f[iz];
+}
+
+// phi = volg * vcelli - 1 (parcel_correction.f90:158)
+__global__ void k_phi(const double* volg, double* phi, double vcelli, long long fsz) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < fsz;
+         i += (long long)gridDim.x * blockDim.x)
+        phi[i] = volg[i] * vcelli - 1.0;
+}
+
+// ---------------------------------------------------------------------------
+// get_time_step reductions (rk_utils.f90:96-143)
+__global__ void k_timestep_reduce(Params P, Ptr8 vg, const double* b, StepScalars* sc) {
+    double gmax = 0.0, dbmax = 0.0;
+    long long nel = (long long)P.nx * P.ny * (P.nz + 1);
+    int nzp = P.nz + 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nel;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long c = i / nzp;
+        int iz = (int)(i - c * nzp);
+        int ix = (int)(c / P.ny), iy = (int)(c - (long long)ix * P.ny);
+        long long a = c * P.nzh + 1 + iz;
+        double v[8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) v[l] = vg.p[l][a];
+        double S[9];
+        S[0] = v[I_DUDX];
+        S[3] = 0.5 * (v[I_DUDY] + v[I_DVDX]);
+        S[6] = 0.5 * (v[I_DUDZ] + v[I_DWDX]);
+        S[1] = S[3];
+        S[4] = v[I_DVDY];
+        S[7] = 0.5 * (v[I_DVDZ] + v[I_DWDY]);
+        S[2] = S[6];
+        S[5] = S[7];
+        S[8] = -(v[I_DUDX] + v[I_DVDY]);
+        double D[3];
+        sz_eigenvalues<FastOps>(S, D);
+        gmax = fmax(gmax, fmax(fabs(D[0]), fmax(fabs(D[1]), fabs(D[2]))));
+        int ixp = ix + 1 == P.nx ? 0 : ix + 1, ixm = ix == 0 ? P.nx - 1 : ix - 1;
+        int iyp = iy + 1 == P.ny ? 0 : iy + 1, iym = iy == 0 ? P.ny - 1 : iy - 1;
+        double gx = 0.5 * P.dxi[0] * (b[fidx(P, iz, iy, ixp)] - b[fidx(P, iz, iy, ixm)]);
+        double db2 = gx * gx;
+        double gy = 0.5 * P.dxi[1] * (b[fidx(P, iz, iyp, ix)] - b[fidx(P, iz, iym, ix)]);
+        db2 = db2 + gy * gy;
+        double gz = 0.5 * P.dxi[2] * (b[a + 1] - b[a - 1]);
+        dbmax = fmax(dbmax, db2 + gz * gz);
+    }
+    __shared__ double s1[32], s2[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        gmax = fmax(gmax, __shfl_xor_sync(0xffffffff, gmax, o));
+        dbmax = fmax(dbmax, __shfl_xor_sync(0xffffffff, dbmax, o));
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { s1[w] = gmax; s2[w] = dbmax; }
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        gmax = l < nw ? s1[l] : 0.0;
+        dbmax = l < nw ? s2[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            gmax = fmax(gmax, __shfl_xor_sync(0xffffffff, gmax, o));
+            dbmax = fmax(dbmax, __shfl_xor_sync(0xffffffff, dbmax, o));
+        }
+        if (l == 0) {
+            atomic_max_nonneg(&sc->gmax_bits, gmax);
+            atomic_max_nonneg(&sc->bmax_bits, dbmax);
+        }
+    }
+}
+
+// dt = min(alpha / gmax, alpha / bmax) with the reference's guards
+// (rk_utils.f90:96-99, 133-182); t is read from the device scalars.
+__global__ void k_timestep_final(StepScalars* sc, double alpha, int fixed, double fixed_dt, int precise,
+                                 double t_limit) {
+    const double eps = 2.220446049250313e-16;
+    double gmax = fmax(eps, __longlong_as_double((long long)sc->gmax_bits));
+    double bmax = sqrt(sqrt(__longlong_as_double((long long)sc->bmax_bits)));
+    bmax = fmax(eps, bmax);
+    double dt = fixed ? fixed_dt : fmin(alpha / gmax, alpha / bmax);
+    if (precise && (sc->t + dt > t_limit)) dt = t_limit - sc->t;
+    if (!(dt > 0.0)) sc->err |= ERRB_DT;
+    sc->dt = dt;
+}
+
+// ---------------------------------------------------------------------------
+// Host orchestration
+
+static int nblocks(long long n, int bs = 256) {
+    long long b = (n + bs - 1) / bs;
+    return (int)std::min<long long>(b, 148LL * 64);
+}
+
+static ColArgs col_args(Ctx& c) {
+    ColArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.mdst = c.T.mdst;
+    A.mdct = c.T.mdct;
+    A.ncol = c.P.nx * c.P.ny;
+    A.nz = c.P.nz;
+    A.nzh = c.P.nzh;
+    A.dzi = c.P.dzi;
+    A.hdzi = c.P.hdzi;
+    return A;
+}
+
+static SpecArgs spec_args(Ctx& c) {
+    SpecArgs S;
+    std::memset(&S, 0, sizeof(S));
+    S.k2l2i = c.T.k2l2i;
+    S.fdx = c.T.fdx;
+    S.fdy = c.T.fdy;
+    S.nx = c.P.nx; S.ny = c.P.ny; S.nz = c.P.nz; S.nzh = c.P.nzh;
+    S.nel = (long long)c.P.nx * c.P.ny * (c.P.nz + 1);
+    return S;
+}
+
+static void halo(Ctx& c, std::initializer_list<std::pair<double*, int>> list) {
+    PhysArgs A;
+    std::memset(&A, 0, sizeof(A));
+    int f = 0;
+    for (auto& e : list) { A.out[f] = e.first; A.mode[f] = e.second; ++f; }
+    A.nf = f;
+    A.nx = c.P.nx; A.ny = c.P.ny; A.nz = c.P.nz; A.nzh = c.P.nzh;
+    A.ncol = (long long)c.P.nx * c.P.ny;
+    long long tot = A.ncol * f;
+    k_halo<<<(int)((tot + 255) / 256), 256, 0, c.stream>>>(A);
+    CKL();
+}
+
+static size_t col_smem(const Ctx& c, int arrays) { return sizeof(double) * (size_t)arrays * (c.P.nz + 1) * CP; }
+
+static void col_decompose(Ctx& c, const double* const* in, double* const* out, int nf, int mode) {
+    ColArgs A = col_args(c);
+    A.tab[0] = c.T.phim; A.tab[1] = c.T.phip; A.tab[2] = c.T.filt;
+    for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
+    size_t sm = col_smem(c, 2);
+    CK(cudaFuncSetAttribute(k_col_decompose, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_col_decompose<<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A, mode);
+    CKL();
+}
+
+static void col_combine(Ctx& c, const double* const* in, double* const* out, int nf) {
+    ColArgs A = col_args(c);
+    A.tab[0] = c.T.phim; A.tab[1] = c.T.phip;
+    for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
+    size_t sm = col_smem(c, 2);
+    CK(cudaFuncSetAttribute(k_col_combine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_col_combine<<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A);
+    CKL();
+}
+
+void vor2vel(Ctx& c) {
+    const Params& P = c.P;
+    SpecArgs S = spec_args(c);
+    int sb = nblocks(S.nel);
+    double* sv[3] = {c.w(0), c.w(1), c.w(2)};
+    double *ds = c.w(3), *es = c.w(4), *cs = c.w(5);
+    // decompose and filter (inversion.f90:36-40)
+    {
+        const double* in[3] = {c.vortg(0), c.vortg(1), c.vortg(2)};
+        fft_xy(c, in, sv, 3, true);
+        col_decompose(c, sv, sv, 3, 1);
+    }
+    // solenoidal projection (inversion.f90:43-87)
+    S.in[0] = sv[1]; S.in[1] = sv[0]; S.out[0] = ds;
+    k_spec_dxdy<<<sb, 256, 0, c.stream>>>(S, 1.0, -1.0);
+    CKL();
+    {
+        const double* in[1] = {sv[2]};
+        double* out[1] = {cs};
+        col_combine(c, in, out, 1);
+        const double* in2[1] = {cs};
+        double* out2[1] = {es};
+        col_decompose(c, in2, out2, 1, 2);
+    }
+    S.in[0] = es; S.in[1] = ds; S.out[0] = sv[0]; S.out[1] = sv[1];
+    k_spec_project<<<sb, 256, 0, c.stream>>>(S);
+    CKL();
+    // vorticity in physical space (inversion.f90:91-93); halo rows keep the
+    // par2grid extrapolation, as in the reference
+    {
+        double* tmp[3] = {c.w(10), c.w(11), c.w(12)};
+        col_combine(c, sv, tmp, 3);
+        double* outv[3] = {c.vortg(0), c.vortg(1), c.vortg(2)};
+        fft_xy(c, tmp, outv, 3, false);
+    }
+    // vertical velocity (inversion.f90:97-150)
+    S.in[0] = sv[1]; S.in[1] = sv[0]; S.out[0] = ds;
+    k_spec_dxdy<<<sb, 256, 0, c.stream>>>(S, -1.0, 1.0);
+    CKL();
+    {
+        ColArgs A = col_args(c);
+        A.tab[0] = c.T.thetam; A.tab[1] = c.T.thetap; A.tab[2] = c.T.dthetam; A.tab[3] = c.T.dthetap;
+        A.tab[4] = c.T.green; A.tab[5] = c.T.rkz;
+        A.in[0] = ds;
+        A.out[0] = c.w(9);
+        A.out[1] = es;
+        size_t sm = col_smem(c, 4);
+        CK(cudaFuncSetAttribute(k_col_wsolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_col_wsolve<<<(A.ncol + CT - 1) / CT, 256, sm, c.stream>>>(A);
+        CKL();
+        const double* in[1] = {sv[2]};
+        double* out[1] = {cs};
+        col_combine(c, in, out, 1);
+    }
+    // mean flow (inversion.f90:158-176)
+    double* zbuf = c.w(13);   // first 2 (nz+1) entries used as scratch
+    k_mean_flow<<<1, 256, 2 * sizeof(double) * (P.nz + 1), c.stream>>>(
+        sv[0], sv[1], c.T.rkzi, c.T.gamtop, c.T.gambot, c.T.mdct, zbuf, P.nz);
+    CKL();
+    // u, v (inversion.f90:180-226)
+    S.in[0] = es; S.in[1] = cs; S.out[0] = c.w(7); S.out[1] = c.w(8); S.zbuf = zbuf;
+    k_spec_uv<<<sb, 256, 0, c.stream>>>(S);
+    CKL();
+    // velocity gradients (inversion.f90:259-300)
+    S.in[0] = c.w(7); S.in[1] = c.w(8); S.in[2] = c.w(9);
+    S.out[0] = c.w(10); S.out[1] = c.w(11); S.out[2] = c.w(12); S.out[3] = c.w(3); S.out[4] = c.w(6);
+    k_spec_grad<<<sb, 256, 0, c.stream>>>(S);
+    CKL();
+    {
+        const double* in[8] = {c.w(7), c.w(8), c.w(9), c.w(10), c.w(11), c.w(12), c.w(3), c.w(6)};
+        double* out[8] = {c.velog(0), c.velog(1), c.velog(2), c.velgrad(I_DUDX), c.velgrad(I_DUDY),
+                          c.velgrad(I_DWDX), c.velgrad(I_DVDY), c.velgrad(I_DWDY)};
+        fft_xy(c, in, out, 8, false);
+    }
+    halo(c, {{c.velgrad(I_DUDX), 0}, {c.velgrad(I_DUDY), 0}, {c.velgrad(I_DWDX), 1},
+             {c.velgrad(I_DVDY), 0}, {c.velgrad(I_DWDY), 1},
+             {c.velog(0), 0}, {c.velog(1), 0}, {c.velog(2), 1}});
+    MPtr8 vg;
+    Ptr8 vo;
+    for (int k = 0; k < 8; ++k) vg.p[k] = c.velgrad(k);
+    for (int k = 0; k < 3; ++k) vo.p[k] = c.vortg(k);
+    k_velgrad_fill<<<nblocks(P.fsz), 256, 0, c.stream>>>(vg, vo, P.fsz);
+    CKL();
+}
+
+void vorticity_tendency(Ctx& c) {
+    const Params& P = c.P;
+    FluxArgs F;
+    std::memset(&F, 0, sizeof(F));
+    for (int k = 0; k < 3; ++k) { F.vort[k] = c.vortg(k); F.vel[k] = c.velog(k); F.fc[k] = P.f_cor[k]; }
+    F.b = c.tbuoyg();
+    for (int k = 0; k < 6; ++k) F.f[k] = c.w(k);
+    F.nx = P.nx; F.ny = P.ny; F.nz = P.nz; F.nzh = P.nzh;
+    F.nel = (long long)P.nx * P.ny * (P.nz + 1);
+    int nb = nblocks(F.nel);
+    k_flux<<<nb, 256, 0, c.stream>>>(F);
+    CKL();
+    double* fl[6] = {c.w(0), c.w(1), c.w(2), c.w(3), c.w(4), c.w(5)};
+    fft_xy(c, fl, fl, 6, true);
+    SpecArgs S = spec_args(c);
+    for (int k = 0; k < 6; ++k) S.in[k] = c.w(k);
+    S.out[0] = c.w(6); S.out[1] = c.w(7); S.out[2] = c.w(8);
+    k_spec_divxy<<<nblocks(S.nel), 256, 0, c.stream>>>(S);
+    CKL();
+    double* dv[3] = {c.w(6), c.w(7), c.w(8)};
+    fft_xy(c, dv, dv, 3, false);
+    Ptr8 d;
+    MPtr8 vt;
+    for (int k = 0; k < 3; ++k) { d.p[k] = c.w(6 + k); vt.p[k] = c.vtend(k); }
+    k_vtend_rows<<<nb, 256, 0, c.stream>>>(F, d, vt, P.dzi, P.hdzi, P.zeta_zero[0], P.zeta_zero[1]);
+    CKL();
+    halo(c, {{c.vtend(0), 0}, {c.vtend(1), 0}, {c.vtend(2), 0}});
+}
+
+// phi -> grad = gradient of the solution of Lap(psi) = phi (diverge,
+// inversion.f90:410-455), grad halo rows extrapolated (parcel_correction.f90:163-165)
+void diverge_laplace(Ctx& c, double* phi, double* grad[3]) {
+    const Params& P = c.P;
+    double* ds = c.w(0);
+    const double* in[1] = {phi};
+    double* out[1] = {ds};
+    fft_xy(c, in, out, 1, true);
+    int ncol = P.nx * P.ny;
+    k_lapinv<<<(ncol + 127) / 128, 128, 0, c.stream>>>(ds, c.T.etdv, c.T.htdv, P.ap, ncol, P.nz, P.nzh);
+    CKL();
+    SpecArgs S = spec_args(c);
+    S.in[0] = ds;
+    S.out[0] = c.w(1); S.out[1] = c.w(2); S.out[2] = c.w(3);
+    k_spec_lapgrad<<<nblocks(S.nel), 256, 0, c.stream>>>(S, P.hdzi);
+    CKL();
+    const double* gi[3] = {c.w(1), c.w(2), c.w(3)};
+    fft_xy(c, gi, grad, 3, false);
+    halo(c, {{grad[0], 0}, {grad[1], 0}, {grad[2], 0}});
+}
+
+void make_phi(Ctx& c, double* phi) {
+    k_phi<<<nblocks(c.P.fsz), 256, 0, c.stream>>>(c.volg(), phi, c.P.vcelli, c.P.fsz);
+    CKL();
+}
+
+void time_step_reduce(Ctx& c) {
+    CK(cudaMemsetAsync(&c.dsc->gmax_bits, 0, 2 * sizeof(unsigned long long), c.stream));
+    Ptr8 vg;
+    for (int k = 0; k < 8; ++k) vg.p[k] = c.velgrad(k);
+    long long nel = (long long)c.P.nx * c.P.ny * (c.P.nz + 1);
+    k_timestep_reduce<<<nblocks(nel), 256, 0, c.stream>>>(c.P, vg, c.tbuoyg(), c.dsc);
+    CKL();
+    const epic_cfg& g = c.cfg;
+    k_timestep_final<<<1, 1, 0, c.stream>>>(c.dsc, g.alpha, g.use_fixed_dt, g.fixed_dt, g.precise_stop, g.t_limit);
+    CKL();
+}
+
+// ---------------------------------------------------------------------------
+// Tables (sta3dfft.f90:52-109, inversion_utils.f90:79-351), computed on the
+// host in FP64 and uploaded once.
+static double ipow(double x, int n) {
+    double r = 1.0, b = x;
+    while (n > 0) {
+        if (n & 1) r *= b;
+        b *= b;
+        n >>= 1;
+    }
+    return r;
+}
+
+void spectral_init(Ctx& c) {
+    const Params& P = c.P;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    cudaStream_t st = c.stream;
+    make_plan(c.px, nx, st);
+    make_plan(c.py, ny, st);
+    const double pi = M_PI;
+    // wavenumbers (sta2dfft.f90:63-67, sta3dfft.f90:88-104, deriv1d.f90:12-33)
+    std::vector<double> hrkx(nx + 1), hrky(ny + 1), rkx(nx, 0.0), rky(ny, 0.0), rkz(nz + 1, 0.0), rkzi(nz + 1, 0.0);
+    for (int k = 1; k <= nx; ++k) hrkx[k] = (pi / P.extent[0]) * (double)k;
+    for (int k = 1; k <= ny; ++k) hrky[k] = (pi / P.extent[1]) * (double)k;
+    int nwx = nx / 2, nwy = ny / 2;
+    for (int k = 1; k <= nwx - 1; ++k) rkx[k] = rkx[nx - k] = hrkx[2 * k];
+    rkx[nwx] = hrkx[nx];
+    for (int k = 1; k <= nwy - 1; ++k) rky[k] = rky[ny - k] = hrky[2 * k];
+    rky[nwy] = hrky[ny];
+    for (int i = 1; i <= nz; ++i) rkz[i] = (pi / P.extent[2]) * (double)i;
+    for (int i = 1; i <= nz - 1; ++i) rkzi[i] = 1.0 / rkz[i];
+    // derivative factors (sta3dfft.f90:318-335)
+    std::vector<double> fdx(nx, 0.0), fdy(ny, 0.0);
+    for (int kx = 1; kx < nx; ++kx) {
+        int dk = std::min(2 * kx, 2 * (nx - kx));
+        fdx[kx] = (kx >= nwx + 1 ? 1.0 : -1.0) * hrkx[dk];
+    }
+    fdx[nwx] = 0.0;
+    for (int ky = 1; ky < ny; ++ky) {
+        int dk = std::min(2 * ky, 2 * (ny - ky));
+        fdy[ky] = (ky >= nwy + 1 ? 1.0 : -1.0) * hrky[dk];
+    }
+    fdy[nwy] = 0.0;
+    // k2l2, k2l2i (inversion_utils.f90:115-127)
+    std::vector<double> k2l2((size_t)nx * ny), k2l2i((size_t)nx * ny);
+    for (int kx = 0; kx < nx; ++kx)
+        for (int ky = 0; ky < ny; ++ky) k2l2[(size_t)kx * ny + ky] = rkx[kx] * rkx[kx] + rky[ky] * rky[ky];
+    k2l2[0] = 1.0;
+    for (size_t h = 0; h < k2l2.size(); ++h) k2l2i[h] = 1.0 / k2l2[h];
+    k2l2[0] = 0.0;
+    k2l2i[0] = 0.0;
+    // filter (inversion_utils.f90:129-150)
+    double kxmaxi = 1.0 / *std::max_element(rkx.begin(), rkx.end());
+    double kymaxi = 1.0 / *std::max_element(rky.begin(), rky.end());
+    double kzmaxi = 1.0 / *std::max_element(rkz.begin(), rkz.end());
+    std::vector<double> skx(nx), sky(ny), skz(nz + 1);
+    for (int k = 0; k < nx; ++k) skx[k] = -36.0 * ipow(kxmaxi * rkx[k], 36);
+    for (int k = 0; k < ny; ++k) sky[k] = -36.0 * ipow(kymaxi * rky[k], 36);
+    for (int k = 0; k <= nz; ++k) skz[k] = -36.0 * ipow(kzmaxi * rkz[k], 36);
+
+    const size_t fsz = (size_t)P.fsz;
+    std::vector<double> filt(fsz, 0.0), green(fsz, 0.0), phim(fsz, 0.0), phip(fsz, 0.0), thm(fsz, 0.0),
+        thp(fsz, 0.0), dthm(fsz, 0.0), dthp(fsz, 0.0), etdv(fsz, 0.0), htdv(fsz, 0.0);
+    auto S = [&](int iz, int ky, int kx) { return ((size_t)kx * ny + ky) * P.nzh + 1 + iz; };
+    std::vector<double> zm(nz + 1), zp(nz + 1);
+    for (int iz = 0; iz <= nz; ++iz) {
+        double z = P.lower[2] + P.dx[2] * (double)iz;
+        zm[iz] = P.upper[2] - z;
+        zp[iz] = z - P.lower[2];
+    }
+    const double dzisq = P.dxi[2] * P.dxi[2];
+    for (int kx = 0; kx < nx; ++kx)
+        for (int ky = 0; ky < ny; ++ky) {
+            size_t h = (size_t)kx * ny + ky;
+            double f0 = std::exp(skx[kx] + sky[ky]);
+            filt[S(0, ky, kx)] = f0;
+            filt[S(nz, ky, kx)] = f0;
+            for (int kz = 1; kz <= nz - 1; ++kz) filt[S(kz, ky, kx)] = f0 * std::exp(skz[kz]);
+            for (int kz = 1; kz <= nz; ++kz) green[S(kz, ky, kx)] = -1.0 / (k2l2[h] + rkz[kz] * rkz[kz]);
+            green[S(0, ky, kx)] = -k2l2i[h];
+            if (kx == 0 && ky == 0) {
+                for (int iz = 0; iz <= nz; ++iz) {
+                    filt[S(iz, 0, 0)] = 1.0;
+                    phim[S(iz, 0, 0)] = zm[iz] / P.extent[2];
+                    phip[S(iz, 0, 0)] = zp[iz] / P.extent[2];
+                }
+            } else {
+                // set_hyperbolic_functions (inversion_utils.f90:257-351)
+                double kl = std::sqrt(k2l2[h]);
+                double fac = kl * P.extent[2];
+                double ef = std::exp(-fac);
+                double div = 1.0 / (1.0 - ef * ef);
+                double k2ifac = 0.5 * k2l2i[h];
+                for (int iz = 0; iz <= nz; ++iz) {
+                    double Lm = kl * zm[iz], Lp = kl * zp[iz];
+                    double ep = std::exp(-Lp), em = std::exp(-Lm);
+                    size_t s = S(iz, ky, kx);
+                    double pm = div * (ep - ef * em), pp = div * (em - ef * ep);
+                    double dpm = -kl * div * (ep + ef * em), dpp = kl * div * (em + ef * ep);
+                    phim[s] = pm;
+                    phip[s] = pp;
+                    double Q = div * (1.0 + ef * ef), R = div * 2.0 * ef;
+                    thm[s] = k2ifac * (R * Lm * pp - Q * Lp * pm);
+                    thp[s] = k2ifac * (R * Lp * pm - Q * Lm * pp);
+                    dthm[s] = -k2ifac * ((Q * Lp - 1.0) * dpm - R * Lm * dpp);
+                    dthp[s] = -k2ifac * ((Q * Lm - 1.0) * dpp - R * Lp * dpm);
+                }
+            }
+            // tridiagonal coefficients (inversion_utils.f90:230-250)
+            double a0 = -2.0 * dzisq - k2l2[h];
+            double ap = dzisq;
+            htdv[S(0, ky, kx)] = 1.0 / a0;
+            etdv[S(0, ky, kx)] = -2.0 * ap * htdv[S(0, ky, kx)];
+            for (int iz = 1; iz <= nz - 1; ++iz) {
+                htdv[S(iz, ky, kx)] = 1.0 / (a0 + ap * etdv[S(iz - 1, ky, kx)]);
+                etdv[S(iz, ky, kx)] = -ap * htdv[S(iz, ky, kx)];
+            }
+            if (kx == 0 && ky == 0) etdv[S(nz - 1, 0, 0)] = 0.0;
+            htdv[S(nz, ky, kx)] = 1.0 / (a0 + 2.0 * ap * etdv[S(nz - 1, ky, kx)]);
+            if (kx == 0 && ky == 0)
+                for (int iz = 0; iz <= nz; ++iz) { htdv[S(iz, 0, 0)] = 0.0; etdv[S(iz, 0, 0)] = 0.0; }
+        }
+    std::vector<double> gamtop(nz + 1), gambot(nz + 1);
+    for (int iz = 0; iz <= nz; ++iz) {
+        double p00 = zp[iz] / P.extent[2];
+        gamtop[iz] = 0.5 * P.extent[2] * (p00 * p00 - 1.0 / 3.0);
+    }
+    for (int iz = 0; iz <= nz; ++iz) gambot[iz] = gamtop[nz - iz];
+    // z-transform matrices: DST-I and DCT-I with factor sqrt(2/nz)
+    std::vector<double> mdst((size_t)(nz + 1) * (nz + 1), 0.0), mdct((size_t)(nz + 1) * (nz + 1), 0.0);
+    double sn = std::sqrt(2.0 / (double)nz);
+    for (int k = 0; k <= nz; ++k)
+        for (int j = 0; j <= nz; ++j) {
+            long m = ((long)j * k) % (2 * nz);
+            double ang = pi * (double)m / (double)nz;
+            if (k >= 1 && k <= nz - 1 && j >= 1 && j <= nz - 1) mdst[(size_t)k * (nz + 1) + j] = sn * std::sin(ang);
+            double w = (j == 0 || j == nz) ? 0.5 : 1.0;
+            mdct[(size_t)k * (nz + 1) + j] = sn * w * std::cos(ang);
+        }
+    auto up = [&](double** dst, const std::vector<double>& v) {
+        CK(cudaMalloc(dst, sizeof(double) * v.size()));
+        CK(cudaMemcpyAsync(*dst, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, st));
+    };
+    up(&c.T.k2l2i, k2l2i); up(&c.T.fdx, fdx); up(&c.T.fdy, fdy);
+    up(&c.T.filt, filt); up(&c.T.green, green); up(&c.T.phim, phim); up(&c.T.phip, phip);
+    up(&c.T.thetam, thm); up(&c.T.thetap, thp); up(&c.T.dthetam, dthm); up(&c.T.dthetap, dthp);
+    up(&c.T.etdv, etdv); up(&c.T.htdv, htdv);
+    up(&c.T.rkz, rkz); up(&c.T.rkzi, rkzi); up(&c.T.gamtop, gamtop); up(&c.T.gambot, gambot);
+    up(&c.T.mdst, mdst); up(&c.T.mdct, mdct);
+    CK(cudaStreamSynchronize(st));
+}
+
+void spectral_free(Ctx& c) {
+    double** all[] = {&c.T.k2l2i, &c.T.fdx, &c.T.fdy, &c.T.filt, &c.T.green, &c.T.phim, &c.T.phip,
+                      &c.T.thetam, &c.T.thetap, &c.T.dthetam, &c.T.dthetap, &c.T.etdv, &c.T.htdv,
+                      &c.T.rkz, &c.T.rkzi, &c.T.gamtop, &c.T.gambot, &c.T.mdst, &c.T.mdct};
+    for (auto p : all) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (c.px.tw) cudaFree(c.px.tw);
+    if (c.py.tw) cudaFree(c.py.tw);
+    c.px.tw = c.py.tw = nullptr;
+}
+
+}  // namespace epic

@@ -1,0 +1,187 @@
+/*
+ * epic_gpu.h -- C ABI of the B200-native EPIC 3-D parcel step.
+ *
+ * The reference has no plugin API: the 3-D step is a set of Fortran module
+ * procedures acting on module-global state (parcels, fields, inversion
+ * tables, options).  Each entry point below replaces one of those calls; the
+ * cited file:line is the reference procedure whose semantics it reproduces
+ * (paths relative to the EPIC source tree, version 0.14.3).
+ *
+ * Conventions
+ *   - All arithmetic of the plain form is IEEE FP64.
+ *   - Parcel arrays use the reference's Fortran layout: an attribute with
+ *     c components is a column-major (c, n) array, i.e. the c components of
+ *     parcel 0 come first (parcel_container.f90:29-56).  Parcel indices in
+ *     the merge/split reports are 1-based like the reference's.
+ *   - Gridded fields are exchanged as (nz+3) x ny x nx arrays, z fastest,
+ *     z = -1 .. nz+1 (the reference's vertical halo), y = 0 .. ny-1,
+ *     x = 0 .. nx-1 (periodic; the reference's x/y halo columns are
+ *     periodic copies of these, field_mpi.f90:765-1018).
+ *   - Every function returns EPIC_OK (0) or one of the EPIC_ERR_* codes and
+ *     leaves a message for epic_gpu_last_error().  The reference aborts via
+ *     mpi_exit_on_error (mpi_utils.f90:15-31) in the same situations.
+ *   - A context is not thread-safe; it owns one CUDA stream and all device
+ *     memory of one simulation.  Host arrays are never retained.
+ */
+#ifndef EPIC_GPU_H
+#define EPIC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EPIC_OK               0
+#define EPIC_ERR_CONFIG       1  /* invalid configuration (options.f90, parameters.f90:93-165) */
+#define EPIC_ERR_CAPACITY     2  /* parcel container full (parcel_split.f90:93-98 would resize) */
+#define EPIC_ERR_NUMERICAL    3  /* B33 division by small number, dt <= 0, no near neighbour */
+#define EPIC_ERR_CUDA         4  /* CUDA runtime error */
+#define EPIC_ERR_TIMEOUT      5  /* a bounded device wait gave up */
+#define EPIC_ERR_ARG          6  /* bad argument (null pointer, size) */
+#define EPIC_ERR_STATE        7  /* call out of order (e.g. step before set_parcels) */
+#define EPIC_ERR_PARCEL_COUNT 8  /* par2grid parcel count check (parcel_interpl.f90:248-250) */
+
+/* Field identifiers for epic_gpu_get_field / epic_gpu_set_field
+ * (fields.f90:21-51). */
+enum epic_field_id {
+    EPIC_FIELD_VELOG_X = 0, EPIC_FIELD_VELOG_Y = 1, EPIC_FIELD_VELOG_Z = 2,
+    EPIC_FIELD_VORTG_X = 3, EPIC_FIELD_VORTG_Y = 4, EPIC_FIELD_VORTG_Z = 5,
+    EPIC_FIELD_VTEND_X = 6, EPIC_FIELD_VTEND_Y = 7, EPIC_FIELD_VTEND_Z = 8,
+    /* velocity gradient tensor: du/dx du/dy du/dz dv/dx dv/dy dv/dz dw/dx dw/dy */
+    EPIC_FIELD_VELGRAD_0 = 9,  /* .. 16 */
+    EPIC_FIELD_TBUOYG = 17, EPIC_FIELD_DBUOYG = 18, EPIC_FIELD_HUMG = 19,
+    EPIC_FIELD_VOLG = 20,
+    EPIC_FIELD_NPARG = 21, EPIC_FIELD_NSPARG = 22,   /* returned as doubles */
+    EPIC_FIELD_COUNT = 23
+};
+
+/* Precision forms. */
+#define EPIC_PRECISION_FP64  0   /* plain: every quantity FP64 */
+#define EPIC_PRECISION_MIXED 1   /* FP32 attributes/interpolation/FFTs, FP64 positions,
+                                    volume, RK position update, B33 and tridiagonal */
+
+/* Run configuration: the reference's &EPIC and &PHYSICS namelists plus the
+ * domain read from its field file (options.f90:35-122, physics.f90:47-89,
+ * parameters.f90:93-165).  Fill with epic_gpu_default_config first. */
+typedef struct epic_cfg {
+    int32_t nx, ny, nz;             /* grid cells                               */
+    double  lower[3];               /* domain origin                            */
+    double  extent[3];              /* domain size                              */
+    /* parcel options (options.f90:83-97) */
+    double  size_factor;            /* 1.0                                      */
+    double  grow_factor;            /* 1.2                                      */
+    double  shrink_factor;          /* 0.8                                      */
+    int32_t n_per_cell;             /* 8                                        */
+    double  lambda_max;             /* 4.0                                      */
+    double  min_vratio;             /* 20.0                                     */
+    int32_t correction_iters;       /* 2                                        */
+    double  gradient_pref;          /* 1.8                                      */
+    double  max_compression;        /* 0.5                                      */
+    /* time options (options.f90:101-110) */
+    double  t_initial;              /* 0                                        */
+    double  t_limit;                /* 0                                        */
+    double  alpha;                  /* 0.2                                      */
+    int32_t precise_stop;           /* 0                                        */
+    int32_t use_fixed_dt;           /* 0                                        */
+    double  fixed_dt;               /* 1.0                                      */
+    int32_t rk_order;               /* 4 (5-stage) or 3                         */
+    /* physics (physics.f90:47-89) */
+    double  gravity, L_v, c_p, theta_0, q_0, height_c, ang_vel, lat_degrees;
+    int32_t l_planetary_vorticity;  /* 0                                        */
+    /* boundary (options.f90:35-50, parameters.f90:168-217) */
+    int32_t bndry_zeta_zero[2];     /* l_bndry_zeta_zero(lower, upper)          */
+    /* device capacity in parcels (0 = derive like max_num_parcels,
+       parameters.f90:152-163) */
+    int64_t capacity;
+    int32_t precision;              /* EPIC_PRECISION_*                         */
+    int32_t keep_order;             /* 1: keep the reference's parcel order     */
+} epic_cfg;
+
+/* Per-step report (epic3d.f90:135-153 plus the statistics the reference
+ * computes every step, parcel_diagnostics.f90:26-44,
+ * field_diagnostics.f90:21-32). */
+typedef struct epic_step_info {
+    double  t;                      /* time after the step                      */
+    double  dt;                     /* time step used                           */
+    int64_t n_parcels;              /* parcels after the step                   */
+    int64_t n_splits;               /* parcels added by parcel_split            */
+    int64_t n_merges;               /* small parcels merged by parcel_merge     */
+    double  parcel_stats[18];       /* IDX_APE .. IDX_MAX_BUOY, 0-based         */
+    double  field_stats[11];        /* IDX_RMS_V .. IDX_MIN_BUOY, 0-based       */
+} epic_step_info;
+
+typedef struct epic_ctx epic_ctx;
+
+/* Defaults of options.f90 / physics.f90 for an nx*ny*nz grid. */
+int epic_gpu_default_config(epic_cfg* cfg);
+
+/* Allocate the device state for one simulation (replaces field_alloc,
+ * parcels%allocate, init_inversion: fields.f90:59-101,
+ * parcel_ellipsoid.f90:86-133, inversion_utils.f90:79-253). */
+int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out);
+void epic_gpu_destroy(epic_ctx* ctx);
+const char* epic_gpu_last_error(const epic_ctx* ctx);
+int epic_gpu_sync(epic_ctx* ctx);
+
+/* Copy parcels in/out (Fortran container layout, parcel_container.f90:18-106).
+ * pos, vor: (3,n); B: (5,n) = B11,B12,B13,B22,B23; vol, buoy, hum: (n). */
+int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const double* vor,
+                         const double* B, const double* vol, const double* buoy,
+                         const double* hum);
+int epic_gpu_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, double* vor,
+                         double* B, double* vol, double* buoy, double* hum);
+int epic_gpu_num_parcels(epic_ctx* ctx, int64_t* n);
+/* LS-RK accumulators (delta_pos(3,n), delta_vor(3,n), strain(8,n), delta_b(5,n)). */
+int epic_gpu_get_parcel_rk(epic_ctx* ctx, int64_t cap, int64_t* n, double* delta_pos,
+                           double* delta_vor, double* strain, double* delta_b);
+int epic_gpu_set_parcel_rk(epic_ctx* ctx, int64_t n, const double* delta_pos,
+                           const double* delta_vor, const double* delta_b);
+
+/* Gridded fields in the layout described above. */
+int epic_gpu_get_field(epic_ctx* ctx, int field_id, double* out);
+int epic_gpu_set_field(epic_ctx* ctx, int field_id, const double* in);
+
+/* init_parcel_correction (parcel_correction.f90:42-83): vor_bar = sum(v w)/sum(v). */
+int epic_gpu_init_correction(epic_ctx* ctx);
+/* apply_vortcor (parcel_correction.f90:89-138). */
+int epic_gpu_apply_vortcor(epic_ctx* ctx);
+/* par2grid (parcel_interpl.f90:146-323); reuse = l_reuse. */
+int epic_gpu_par2grid(epic_ctx* ctx, int reuse);
+/* vor2vel + vel2vgrad (inversion.f90:25-317). */
+int epic_gpu_vor2vel(epic_ctx* ctx);
+/* vorticity_tendency (inversion.f90:321-404). */
+int epic_gpu_vorticity_tendency(epic_ctx* ctx);
+/* get_time_step (rk_utils.f90:70-183). */
+int epic_gpu_time_step(epic_ctx* ctx, double t, double* dt);
+/* grid2par (parcel_interpl.f90:405-470); add = present(add) .and. add. */
+int epic_gpu_grid2par(epic_ctx* ctx, int add);
+/* ls_rk_step (ls_rk.f90:88-136): advances t by dt. */
+int epic_gpu_rk_step(epic_ctx* ctx, double* t, double* dt);
+/* parcel_merge (parcel_merge.f90:47-108) incl. find_nearest/resolve_tree
+ * (parcel_nearest.f90:375-1377) with single-rank semantics; n_merge out. */
+int epic_gpu_merge(epic_ctx* ctx, int64_t* n_merge);
+/* The merge pairs of the last epic_gpu_merge (isma, iclo; 1-based, m order). */
+int epic_gpu_get_merge_pairs(epic_ctx* ctx, int64_t cap, int64_t* n, int32_t* isma,
+                             int32_t* iclo);
+/* parcel_split (parcel_split.f90:37-198); n_split out. */
+int epic_gpu_split(epic_ctx* ctx, int64_t* n_split);
+/* apply_laplace / apply_gradient (parcel_correction.f90:142-259). */
+int epic_gpu_apply_laplace(epic_ctx* ctx, int reuse);
+int epic_gpu_apply_gradient(epic_ctx* ctx, int reuse);
+/* vol2grid (parcel_interpl.f90:92-135). */
+int epic_gpu_vol2grid(epic_ctx* ctx, int reuse);
+/* calculate_parcel_diagnostics / calculate_field_diagnostics
+ * (parcel_diagnostics.f90:51-159, field_diagnostics.f90:40-154). */
+int epic_gpu_parcel_diagnostics(epic_ctx* ctx, double stats[18]);
+int epic_gpu_field_diagnostics(epic_ctx* ctx, double stats[11]);
+/* One iteration of the run loop (epic3d.f90:135-153): apply_vortcor,
+ * ls_rk_step, parcel_merge, parcel_split, correction_iters x
+ * (apply_laplace, apply_gradient). */
+int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EPIC_GPU_H */

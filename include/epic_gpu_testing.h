@@ -1,0 +1,32 @@
+/*
+ * epic_gpu_testing.h -- known-answer hooks of the B200 EPIC library.
+ *
+ * Not part of the reference's interface; they let tests run single device
+ * routines on given inputs.
+ */
+#ifndef EPIC_GPU_TESTING_H
+#define EPIC_GPU_TESTING_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Scherzinger eigen decomposition (scherzinger.f90:31-147) of n symmetric
+ * matrices given as rows (A11, A12, A13, A22, A23, A33).  D: (n, 3)
+ * descending; V: (n, 9), eigenvector j in V[9i + 3j .. 9i + 3j + 2].
+ * exact != 0 selects the non-contracted arithmetic used for decisions. */
+int epic_gpu_test_eigen(int64_t n, const double* A6, double* D, double* V, int exact, int values_only);
+
+struct epic_ctx;
+/* diverge (inversion.f90:410-455) of a given field phi ((nz+3) x ny x nx,
+ * z fastest) on the context's grid; grad receives 3 fields of that shape
+ * with the halo rows extrapolated like apply_laplace. */
+int epic_gpu_test_diverge(struct epic_ctx* ctx, const double* phi, double* grad);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
