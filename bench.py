@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Throughput of the EPIC 3-D parcel step on B200s (parcel-steps/s).
+
+One step = one iteration of the reference run loop (epic3d.f90:135-153):
+vorticity correction, 5-stage low-storage RK4 (par2grid, vor2vel,
+vorticity tendency, grid2par per stage), merge, split and two correction
+passes.  parcel-steps = sum over timed steps of the parcels at step start.
+
+Default workload: the rising thermal, 128^3 grid, 8 parcels per cell
+(16,777,216 parcels), plain FP64.  With N GPUs (torchrun) every rank runs
+an independent replica of the workload (replicas only: a single EPIC run
+has no data-parallel shard without halos), and the reported value is the
+whole-job parcel-steps/s over the max-over-ranks device time.
+
+--impl reference times the CPU restatement of the reference step
+(oracle/, OpenMP build, all host threads) on the same workload; the
+reference Fortran cannot be built on this image (no Fortran compiler, MPI
+or NetCDF).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "parcel-steps/s at 1 B200 (FP64 plain vs mixed vs served), p50/p99 at fixed error"
+UNIT = "parcel-steps/s"
+
+
+def peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (nvidia-smi sampling)
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int) -> float:
+    """Minimal compulsory DRAM bytes of one launch (FP64 plain)."""
+    gh = nx * ny * (nz + 3)
+    if kernel == "p2g":
+        # read x3 w3 B5 V b q per parcel; write 7 scattered fields + 2 int counts
+        return 14 * 8.0 * n + 7 * 8.0 * gh + 2 * 4.0 * gh
+    if kernel == "g2p":
+        # read x3 w3 B5 V + dx3 dw3 dB5; write x3 w3 B5 + dx3 dw3 dB5; read 14 fields
+        return (23 + 22) * 8.0 * n + 14 * 8.0 * gh
+    if kernel == "fft":
+        # one pass over a (nz+1) x ny x nx field: read + write
+        return 2 * 8.0 * nx * ny * (nz + 1)
+    raise KeyError(kernel)
+
+
+def run_ours(args):
+    import torch
+    import epic_b200
+    from epic_b200 import initial, abi
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    setup = initial.config(args.workload)
+    lib = epic_b200.load()
+    ctx = epic_b200.make_context(setup, lib)
+    import ctypes as C
+    sp = C.c_void_p()
+    lib.lib.epic_gpu_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.lib.epic_gpu_get_stream(ctx.h, C.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value, device=dev)
+    lib.lib.epic_gpu_profile_kernel.argtypes = [C.c_void_p, C.c_char_p]
+    lib.lib.epic_gpu_kernel_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    lib.lib.epic_gpu_launch_count.argtypes = [C.POINTER(C.c_int64)]
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    t = 0.0
+    for _ in range(args.warmup):
+        t, _info = ctx.step(t)
+    # ---- device-resident timed region
+    lib.lib.epic_gpu_profile_kernel(ctx.h, args.roofline_kernel.encode())
+    clocks = ClockSampler(dev if world == 1 else local)
+    barrier()
+    torch.cuda.synchronize()
+    ctx.sync()
+    clocks.start()
+    l0 = C.c_int64()
+    lib.lib.epic_gpu_launch_count(C.byref(l0))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    psteps = 0
+    nmin = nmax = ctx.num_parcels()
+    infos = []
+    for _ in range(args.steps):
+        n_start = ctx.num_parcels()
+        psteps += n_start
+        t, info = ctx.step(t)
+        infos.append(info)
+        nmin = min(nmin, info.n_parcels)
+        nmax = max(nmax, info.n_parcels)
+    e1.record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    l1 = C.c_int64()
+    lib.lib.epic_gpu_launch_count(C.byref(l1))
+    kms = C.c_double()
+    kl = C.c_int64()
+    lib.lib.epic_gpu_kernel_time(ctx.h, C.byref(kms), C.byref(kl))
+    lib.lib.epic_gpu_profile_kernel(ctx.h, b"")
+
+    # max over ranks, sum of work
+    tt = torch.tensor([ms, float(psteps)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        mx = tt.clone(); dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = tt.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, ps_total = float(mx[0]), float(sm[1])
+    else:
+        ms_max, ps_total = ms, float(psteps)
+    value = ps_total / (ms_max * 1e-3)
+
+    # roofline of the dominant kernel
+    peak, peak_kind = peaks()
+    avg_n = psteps / args.steps
+    kavg_ms = kms.value / max(kl.value, 1)
+    alg = algorithmic_bytes(args.roofline_kernel, int(avg_n), setup.nx, setup.ny, setup.nz)
+    achieved = alg / (kavg_ms * 1e-3) / 1e9 if kl.value else None
+    roofline = {"bound": "hbm", "kernel": args.roofline_kernel, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": (achieved / peak if achieved else None), "traffic": None,
+                "peak_source": peak_kind, "avg_launch_ms": kavg_ms, "launches": kl.value,
+                "share_of_step_time": kms.value / ms if ms else None,
+                "algorithmic_bytes_per_launch": alg}
+    if args.traffic is not None:
+        roofline["traffic"] = args.traffic
+
+    # ---- end-to-end through the C ABI with host buffers (drop-in serial step:
+    # the host container owns the parcels; every step copies them in, steps,
+    # and copies them back, like a caller keeping the reference's container)
+    e2e = None
+    if not args.no_e2e:
+        cap = int(ctx.num_parcels() * 1.5) + 1024
+        host = {k: torch.empty((cap, c), dtype=torch.float64, pin_memory=True).numpy()
+                for k, c in (("pos", 3), ("vor", 3), ("B", 5), ("vol", 1), ("buoy", 1), ("hum", 1))}
+        n_now = ctx.num_parcels()
+        st = ctx.get_parcels()
+        for k in host:
+            host[k][:n_now] = st[k].reshape(n_now, -1)
+        P = C.POINTER(C.c_double)
+        fn_set = lib.fn["set_parcels"]
+        fn_get = lib.fn["get_parcels"]
+        barrier()
+        torch.cuda.synchronize()
+        h2d = d2h = 0
+        eps = 0
+        w0 = time.perf_counter()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.e2e_steps):
+            rc = fn_set(ctx.h, C.c_int64(n_now), *(host[k].ctypes.data_as(P) for k in ("pos", "vor", "B", "vol", "buoy", "hum")))
+            assert rc == 0, ctx.lib.fn["last_error"](ctx.h)
+            h2d += n_now * 14 * 8
+            eps += n_now
+            t, info = ctx.step(t)
+            nn = C.c_int64()
+            rc = fn_get(ctx.h, C.c_int64(cap), C.byref(nn), *(host[k].ctypes.data_as(P) for k in ("pos", "vor", "B", "vol", "buoy", "hum")))
+            assert rc == 0
+            n_now = nn.value
+            d2h += n_now * 14 * 8
+        f1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        ems = f0.elapsed_time(f1)
+        te = torch.tensor([ems, float(eps)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            import torch.distributed as dist
+            mx = te.clone(); dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            sm = te.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+            ems_max, eps_total = float(mx[0]), float(sm[1])
+        else:
+            ems_max, eps_total = ems, float(eps)
+        e2e = {"value": eps_total / (ems_max * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
+               "steps": args.e2e_steps, "wall_s": wall,
+               "mode": "host-owned parcel container: set_parcels (pinned H2D) + step + get_parcels (D2H) every step"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: rising thermal, 128^3 grid, domain 6.28^3, 8 parcels/cell "
+                               "(16,777,216 parcels at t=0), seeded noise, plain FP64, merge/split/corrections on"
+                   if args.workload == "thermal-128" else args.workload,
+                   "grid": [setup.nx, setup.ny, setup.nz], "parcels_at_start": int(setup.n),
+                   "parcels_range_timed": [int(nmin), int(nmax)], "precision": "fp64-plain",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (parcel store 5.2 GB, fields 0.5 GB)"},
+        "roofline": roofline,
+        "clocks": clk,
+        "e2e": e2e,
+        "gpu_launches": int(l1.value - l0.value),
+        "dt_last": infos[-1].dt if infos else None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+def oracle_sample_workload():
+    """The bounded CPU sample: the same rising thermal on a 64^3 grid
+    (2,097,152 parcels, same parcel density and physics), one step."""
+    from epic_b200 import initial
+    return initial.thermal(64, name="thermal-64")
+
+
+def cpu_baseline(args):
+    import oracle
+    lib = oracle.load(threads=True)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    from epic_b200 import make_context
+    s = oracle_sample_workload()
+    ctx = make_context(s, lib)
+    t = 0.0
+    t0 = time.perf_counter()
+    n0 = ctx.num_parcels()
+    t, info = ctx.step(t)
+    el = time.perf_counter() - t0
+    return {"value": n0 / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"1 step of the rising thermal on a 64^3 grid ({n0} parcels, same density and physics), "
+                      f"{el:.1f} s wall, oracle OpenMP build",
+            "seconds": el}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    import oracle
+    lib = oracle.load(threads=True)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    from epic_b200 import make_context
+    s = oracle_sample_workload()
+    ctx = make_context(s, lib)
+    t = 0.0
+    for _ in range(args.warmup):
+        t, _ = ctx.step(t)
+    ps = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ps += ctx.num_parcels()
+        t, _ = ctx.step(t)
+    el = time.perf_counter() - t0
+    v = ps / el
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "sample": "each step is one step of the rising thermal on a "
+                       "64^3 grid (2,097,152 parcels, 8/cell, same physics) as a bounded sample of the workload"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "64^3 rising thermal, one step per timed step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference Fortran not buildable here (no Fortran compiler, MPI or NetCDF); "
+                    "timed the CPU restatement of its step (oracle/, OpenMP)"}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="thermal-128")
+    ap.add_argument("--roofline-kernel", default="p2g", choices=["p2g", "g2p", "fft"])
+    ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of that kernel")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

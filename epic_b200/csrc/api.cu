@@ -15,6 +15,36 @@ struct epic_ctx {
 
 namespace epic {
 
+std::atomic<long long> g_launches{0};
+
+void prof_begin(Ctx& c, const char* name) {
+    if (c.prof.target.empty() || c.prof.target != name) return;
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, c.stream));
+    c.prof.ev.push_back(e);
+}
+
+void prof_end(Ctx& c, const char* name) {
+    if (c.prof.target.empty() || c.prof.target != name) return;
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, c.stream));
+    c.prof.ev.push_back(e);
+    c.prof.launches += 1;
+}
+
+static void prof_resolve(Ctx& c) {
+    CK(cudaStreamSynchronize(c.stream));
+    for (size_t k = 0; k + 1 < c.prof.ev.size(); k += 2) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, c.prof.ev[k], c.prof.ev[k + 1]));
+        c.prof.ms += ms;
+    }
+    for (auto e : c.prof.ev) cudaEventDestroy(e);
+    c.prof.ev.clear();
+}
+
 void* Ctx::get_scratch(size_t bytes) {
     if (bytes > scratch_bytes) {
         if (scratch) CK(cudaFreeAsync(scratch, stream));
@@ -163,6 +193,8 @@ static void setup_params(Ctx& c) {
 
 static void free_ctx(Ctx& c) {
     if (c.stream) cudaStreamSynchronize(c.stream);
+    for (auto e : c.prof.ev) cudaEventDestroy(e);
+    c.prof.ev.clear();
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.dvor_bar};
     for (void* p : ptrs)
@@ -489,6 +521,42 @@ int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info) {
     info->n_splits = c.n_parcel_splits - s0;
     info->n_merges = c.n_parcel_merges - m0;
     API_END
+}
+
+// ---------------------------------------------------------------------------
+// Instrumentation (no counterpart in the reference)
+
+int epic_gpu_get_stream(epic_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return EPIC_ERR_ARG;
+    *stream = (void*)ctx->c.stream;
+    return EPIC_OK;
+}
+
+int epic_gpu_profile_kernel(epic_ctx* ctx, const char* name) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    prof_resolve(c);
+    c.prof.target = name ? name : "";
+    c.prof.ms = 0.0;
+    c.prof.launches = 0;
+    API_END
+}
+
+int epic_gpu_kernel_time(epic_ctx* ctx, double* total_ms, int64_t* launches) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    prof_resolve(c);
+    if (total_ms) *total_ms = c.prof.ms;
+    if (launches) *launches = c.prof.launches;
+    c.prof.ms = 0.0;
+    c.prof.launches = 0;
+    API_END
+}
+
+int epic_gpu_launch_count(int64_t* n) {
+    if (!n) return EPIC_ERR_ARG;
+    *n = g_launches.load();
+    return EPIC_OK;
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 #include "../../include/epic_gpu.h"
 #include "common.cuh"
 
+#include <atomic>
 #include <string>
 #include <vector>
 #include <stdexcept>
@@ -20,7 +21,13 @@ struct CudaError : std::runtime_error {
         if (e_ != cudaSuccess)                                                              \
             throw ::epic::CudaError(EPIC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
-#define CKL() CK(cudaGetLastError())
+// Every kernel launch of the library is followed by CKL(), which also counts it.
+extern std::atomic<long long> g_launches;
+#define CKL()                                                        \
+    do {                                                             \
+        ::epic::g_launches.fetch_add(1, std::memory_order_relaxed);  \
+        CK(cudaGetLastError());                                      \
+    } while (0)
 
 // Mixed-radix plan for the shared-memory Stockham FFT.
 struct FFTPlan {
@@ -58,7 +65,16 @@ struct StepScalars {
     double vsum, vor[3];            // vorticity correction sums
 };
 
+// CUDA-event timing of every launch of one named kernel on the context stream.
+struct KernelTimer {
+    std::string target;
+    std::vector<cudaEvent_t> ev;   // begin/end pairs
+    double ms = 0.0;
+    long long launches = 0;
+};
+
 struct Ctx {
+    KernelTimer prof;
     epic_cfg cfg;
     Params P;
     std::string err;
@@ -141,6 +157,8 @@ void finish_parcel_diag(Ctx& c, double* out);
 long long parcel_merge(Ctx& c);
 
 // api.cu
+void prof_begin(Ctx& c, const char* name);
+void prof_end(Ctx& c, const char* name);
 void check_device_error(Ctx& c);
 void sync_scalars(Ctx& c);
 

@@ -509,6 +509,7 @@ long long parcel_merge(Ctx& c) {
     int* dcount = a1.take<int>(8);
     void* tmp1 = a1.take<char>(cub1);
     k_bin_locals<<<mgrid(N), MB, 0, st>>>(P, B, c.pv, N, cell0, small, bits, err);
+    CKL();
     k_iota<<<mgrid(N), MB, 0, st>>>(idx, N);
     CKL();
     CK(cub::DeviceSelect::Flagged(tmp1, cub1, idx, small, Ls, dcount, N, st));
@@ -564,6 +565,7 @@ long long parcel_merge(Ctx& c) {
     const long long NT = (long long)N + ncp;
     CK(cudaMemsetAsync(copyidx, 0xff, sizeof(int) * 8 * (size_t)nls, st));
     k_make_copies<<<mgrid(8LL * nls), MB, 0, st>>>(P, B, c.pv, Ls, nls, F, off, C, cell + N, copyidx, err);
+    CKL();
     k_iota<<<mgrid(NT), MB, 0, st>>>(vals, NT);
     CKL();
     int endbit = 1;
@@ -597,8 +599,11 @@ long long parcel_merge(Ctx& c) {
     for (int it = 0;; ++it) {
         CK(cudaMemsetAsync(dcount, 0, sizeof(int), st));
         k_tree_a<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail);
+        CKL();
         k_tree_b<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf);
+        CKL();
         k_tree_c<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail);
+        CKL();
         k_tree_d<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail, dcount);
         CKL();
         if (!read_int(c, dcount)) break;
@@ -609,7 +614,9 @@ long long parcel_merge(Ctx& c) {
     int* minv = ar.take<int>(N);
     CK(cudaMemsetAsync(minv, 0xff, sizeof(int) * (size_t)N, st));
     k_set_minv<<<g, MB, 0, st>>>(Ls, nls, minv);
+    CKL();
     k_tree_e<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail);
+    CKL();
     k_tree_f_init<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail, dom, status, err);
     CKL();
     for (int it = 0;; ++it) {
@@ -620,6 +627,7 @@ long long parcel_merge(Ctx& c) {
         if (it > 1000000) throw CudaError(EPIC_ERR_TIMEOUT, "resolve_tree: stage 2 did not terminate");
     }
     k_tree_f_apply<<<g, MB, 0, st>>>(Ls, nls, status, avail, dom);
+    CKL();
     k_tree_g<<<g, MB, 0, st>>>(iclo, nls, status, avail, dom);
     CKL();
     check_device_error(c);
@@ -628,6 +636,7 @@ long long parcel_merge(Ctx& c) {
     int* domi = ar.take<int>((size_t)nls + 1);
     int* dpos = ar.take<int>((size_t)nls + 1);
     k_char_to_int<<<g, MB, 0, st>>>(dom, domi, nls);
+    CKL();
     CK(cudaMemsetAsync(domi + nls, 0, sizeof(int), st));
     {
         size_t b = cubb;
@@ -662,6 +671,7 @@ long long parcel_merge(Ctx& c) {
     int* gidx = ar.take<int>(nm);
     int* gstart = ar.take<int>(nm);
     k_iota<<<mgrid(nm), MB, 0, st>>>(mvals, nm);
+    CKL();
     int nbits = 1;
     while ((1LL << nbits) <= N) ++nbits;
     {
@@ -669,6 +679,7 @@ long long parcel_merge(Ctx& c) {
         CK(cub::DeviceRadixSort::SortPairs(ctmp, b, icl, gk, mvals, gv, nm, 0, nbits, st));
     }
     k_group_heads<<<mgrid(nm), MB, 0, st>>>(gk, nm, head);
+    CKL();
     k_iota<<<mgrid(nm), MB, 0, st>>>(gidx, nm);
     CKL();
     {
@@ -684,6 +695,7 @@ long long parcel_merge(Ctx& c) {
     char* del = merged;
     CK(cudaMemsetAsync(del, 0, N, st));
     k_mark_deleted<<<mgrid(nm), MB, 0, st>>>(ism, nm, del);
+    CKL();
     int* hf = head;      // reuse nm-sized arrays
     int* holes = gidx;
     k_hole_flags<<<mgrid(nm), MB, 0, st>>>(ism, nm, newN, hf);
@@ -698,6 +710,7 @@ long long parcel_merge(Ctx& c) {
         int* sidx = gk;
         int* srcs = gv;
         k_src_flags<<<mgrid(nm), MB, 0, st>>>(del, newN, N, sf);
+        CKL();
         k_iota<<<mgrid(nm), MB, 0, st>>>(sidx, nm);
         CKL();
         size_t b = cubb;

@@ -225,9 +225,11 @@ void par2grid(Ctx& c, bool reuse, bool store_vectors) {
     CK(cudaMemsetAsync(c.nparg, 0, sizeof(int) * P.fsz, c.stream));
     CK(cudaMemsetAsync(c.nsparg, 0, sizeof(int) * P.fsz, c.stream));
     CK(cudaMemsetAsync(&c.dsc->count, 0, sizeof(long long), c.stream));
+    prof_begin(c, "p2g");
     k_p2g<<<pgrid(c.n), PB, 0, c.stream>>>(P, c.pv, c.n, F, c.nparg, c.nsparg, reuse, store_vectors,
                                             &c.dsc->err);
     CKL();
+    prof_end(c, "p2g");
     long long ncol = (long long)P.nx * P.ny;
     k_p2g_fold<<<(int)((ncol + 255) / 256), 256, 0, c.stream>>>(P, F, 7, c.nparg, c.nsparg, &c.dsc->count);
     CKL();
@@ -478,8 +480,10 @@ void g2p_rk_stage(Ctx& c, int stage, bool with_diag) {
     S.cb = c.cb[stage - 1];
     int g = pgrid(c.n);
     c.n_partials = g;
+    prof_begin(c, "g2p");
     k_g2p<<<g, PB, 0, c.stream>>>(c.P, c.pv, c.n, gather_fields(c), S, c.dsc, c.partials, &c.dsc->err);
     CKL();
+    prof_end(c, "g2p");
 }
 
 // Parcel statistics from the block partials (parcel_diagnostics.f90:126-157).

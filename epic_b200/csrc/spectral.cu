@@ -215,14 +215,17 @@ static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* cons
     size_t sm = sizeof(double) * (size_t)B.T * B.n + 2 * sizeof(double2) * (size_t)(B.T / 2) * B.n +
                 sizeof(double2) * B.n;
     dim3 grid((B.nl + B.T - 1) / B.T, nrows, nf);
+    prof_begin(c, "fft");
     if (forward) {
         CK(cudaFuncSetAttribute(k_fft_lines<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_fft_lines<true><<<grid, 256, sm, c.stream>>>(B);
+        CKL();
     } else {
         CK(cudaFuncSetAttribute(k_fft_lines<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_fft_lines<false><<<grid, 256, sm, c.stream>>>(B);
+        CKL();
     }
-    CKL();
+    prof_end(c, "fft");
 }
 
 // fftxyp2s: y then x (forward); fftxys2p: x then y (reverse).  Only rows

@@ -180,6 +180,15 @@ int epic_gpu_field_diagnostics(epic_ctx* ctx, double stats[11]);
  * (apply_laplace, apply_gradient). */
 int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info);
 
+/* ------------------------------------------------------------------------
+ * Instrumentation.  These have no counterpart in the reference; they expose
+ * the context's CUDA stream and CUDA-event timings of one named kernel
+ * ("p2g", "g2p", "fft", "merge", ...) for measurement. */
+int epic_gpu_get_stream(epic_ctx* ctx, void** stream);
+int epic_gpu_profile_kernel(epic_ctx* ctx, const char* name);
+int epic_gpu_kernel_time(epic_ctx* ctx, double* total_ms, int64_t* launches);
+int epic_gpu_launch_count(int64_t* n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,9 @@
 
 #include <memory>
 #include <numeric>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 using namespace oracle;
 
@@ -260,8 +263,9 @@ typedef std::vector<double> Arr;
 void fftxyp2s(Ctx& c, const Arr& fp, Arr& fs) {
     int nx = c.nx, ny = c.ny, nz = c.nz;
     fs.assign((size_t)nx * ny * (nz + 1), 0.0);
-    std::vector<double> line(std::max(nx, ny));
+#pragma omp parallel for schedule(static)
     for (int iz = 0; iz <= nz; ++iz) {
+        std::vector<double> line(std::max(nx, ny));
         for (int ix = 0; ix < nx; ++ix) {
             for (int iy = 0; iy < ny; ++iy) line[iy] = fp[c.fi(iz, iy, ix)];
             c.fy.forfft(line.data());
@@ -278,9 +282,10 @@ void fftxyp2s(Ctx& c, const Arr& fp, Arr& fs) {
 // fftxys2p (sta3dfft.f90:196-257): writes fp(0:nz) only.
 void fftxys2p(Ctx& c, const Arr& fs, Arr& fp) {
     int nx = c.nx, ny = c.ny, nz = c.nz;
-    std::vector<double> line(std::max(nx, ny));
     Arr tmp((size_t)nx * ny * (nz + 1));
+#pragma omp parallel for schedule(static)
     for (int iz = 0; iz <= nz; ++iz) {
+        std::vector<double> line(std::max(nx, ny));
         for (int ky = 0; ky < ny; ++ky) {
             for (int kx = 0; kx < nx; ++kx) line[kx] = fs[c.si(iz, ky, kx)];
             c.fx.revfft(line.data());
@@ -330,7 +335,7 @@ void diffy(Ctx& c, const Arr& fs, Arr& ds) {
 // field_decompose_semi_spectral (inversion_utils.f90:370-401)
 void field_decompose_semi_spectral(Ctx& c, Arr& s) {
     int nx = c.nx, ny = c.ny, nz = c.nz;
-    std::vector<double> col(nz + 1);
+#pragma omp parallel for schedule(static)
     for (int kx = 0; kx < nx; ++kx)
         for (int ky = 0; ky < ny; ++ky) {
             double* p = &s[c.si(0, ky, kx)];
@@ -346,6 +351,7 @@ void field_decompose_semi_spectral(Ctx& c, Arr& s) {
 // field_combine_semi_spectral (inversion_utils.f90:421-456)
 void field_combine_semi_spectral(Ctx& c, Arr& s) {
     int nx = c.nx, ny = c.ny, nz = c.nz;
+#pragma omp parallel for schedule(static)
     for (int kx = 0; kx < nx; ++kx)
         for (int ky = 0; ky < ny; ++ky) {
             double* p = &s[c.si(0, ky, kx)];
@@ -403,6 +409,7 @@ void central_diffz(Ctx& c, const Arr& f, Arr& df) {
 // lapinv1 (inversion_utils.f90:567-589)
 void lapinv1(Ctx& c, Arr& fs) {
     int nx = c.nx, ny = c.ny, nz = c.nz;
+#pragma omp parallel for schedule(static)
     for (int kx = 0; kx < nx; ++kx)
         for (int ky = 0; ky < ny; ++ky) {
             long t = c.si(0, ky, kx);
@@ -496,6 +503,7 @@ void vor2vel(Ctx& c) {
     diffy(c, svor[0], ds);
     diffx(c, svor[1], es);
     for (long i = 0; i < ss; ++i) ds[i] = ds[i] - es[i];
+#pragma omp parallel for schedule(static)
     for (long h = 0; h < (long)nx * ny; ++h) {
         long t = h * (nz + 1);
         for (int iz = 1; iz <= nz - 1; ++iz)
@@ -737,39 +745,75 @@ void free_slip_fold(Ctx& c, Arr& f) {
 }
 
 // vol2grid (parcel_interpl.f90:92-135)
-void vol2grid(Ctx& c, bool reuse) {
-    std::fill(c.volg.begin(), c.volg.end(), 0.0);
+static void v2g_parcel(Ctx& c, long n, bool reuse, double* vg) {
     double pts[4][3], ww[2][2][2];
     int is, js, ks;
-    for (long n = 0; n < c.n; ++n) {
-        double pvol = c.vol[n];
-        get_points(c, n, reuse, pts);
-        for (int p = 0; p < 4; ++p) {
-            trilinear(c, pts[p], is, js, ks, ww);
-            check_k(c, ks);
-            for (int i = 0; i < 2; ++i)
-                for (int j = 0; j < 2; ++j)
-                    for (int k = 0; k < 2; ++k)
-                        c.volg[c.fi(ks + k, c.wrapy(js + j), c.wrapx(is + i))] += f14 * ww[k][j][i] * pvol;
-        }
+    double pvol = c.vol[n];
+    get_points(c, n, reuse, pts);
+    for (int p = 0; p < 4; ++p) {
+        trilinear(c, pts[p], is, js, ks, ww);
+        check_k(c, ks);
+        for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j)
+                for (int k = 0; k < 2; ++k)
+                    vg[c.fi(ks + k, c.wrapy(js + j), c.wrapx(is + i))] += f14 * ww[k][j][i] * pvol;
     }
+}
+
+void vol2grid(Ctx& c, bool reuse) {
+    std::fill(c.volg.begin(), c.volg.end(), 0.0);
+#ifdef _OPENMP
+    int nt = std::min(omp_get_max_threads(), 32);
+    std::vector<std::vector<double>> priv(nt, std::vector<double>(c.fsz, 0.0));
+#pragma omp parallel num_threads(nt)
+    {
+        double* vg = priv[omp_get_thread_num()].data();
+#pragma omp for schedule(static)
+        for (long n = 0; n < c.n; ++n) v2g_parcel(c, n, reuse, vg);
+    }
+#pragma omp parallel for schedule(static)
+    for (long g = 0; g < c.fsz; ++g)
+        for (int t = 0; t < nt; ++t) c.volg[g] += priv[t][g];
+#else
+    for (long n = 0; n < c.n; ++n) v2g_parcel(c, n, reuse, c.volg.data());
+#endif
     free_slip_fold(c, c.volg);
 }
 
 // par2grid (parcel_interpl.f90:146-323)
+// Scatter of parcel n into the 7 accumulation fields f[0..6] (vortg x,y,z,
+// dbuoyg, humg, tbuoyg, volg).
+static void p2g_parcel(Ctx& c, long n, bool reuse, double* const* f) {
+    double pts[4][3], ww[2][2][2];
+    int is, js, ks;
+    double pvol = c.vol[n];
+    double q_c = c.hum[n] - c.q_0 * std::exp(c.lambda_c * (c.lower[2] - c.pos[3 * n + 2]));
+    q_c = std::max(zero, q_c);
+    double btot = c.buoy[n] + c.glat * q_c;
+    get_points(c, n, reuse, pts);
+    double vals[6] = {c.vor[3 * n], c.vor[3 * n + 1], c.vor[3 * n + 2], c.buoy[n], c.hum[n], btot};
+    for (int p = 0; p < 4; ++p) {
+        trilinear(c, pts[p], is, js, ks, ww);
+        check_k(c, ks);
+        for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j)
+                for (int k = 0; k < 2; ++k) {
+                    long g = c.fi(ks + k, c.wrapy(js + j), c.wrapx(is + i));
+                    double w = f14 * pvol * ww[k][j][i];
+                    for (int l = 0; l < 6; ++l) f[l][g] += w * vals[l];
+                    f[6][g] += w;
+                }
+    }
+}
+
 void par2grid(Ctx& c, bool reuse) {
     for (auto* f : {&c.vortg[0], &c.vortg[1], &c.vortg[2], &c.volg, &c.dbuoyg, &c.humg, &c.tbuoyg})
         std::fill(f->begin(), f->end(), 0.0);
     std::fill(c.nparg.begin(), c.nparg.end(), 0);
     std::fill(c.nsparg.begin(), c.nsparg.end(), 0);
-    double pts[4][3], ww[2][2][2];
-    int is, js, ks;
+    double* tgt[7] = {c.vortg[0].data(), c.vortg[1].data(), c.vortg[2].data(), c.dbuoyg.data(), c.humg.data(),
+                      c.tbuoyg.data(), c.volg.data()};
     for (long n = 0; n < c.n; ++n) {
-        double pvol = c.vol[n];
-        double q_c = c.hum[n] - c.q_0 * std::exp(c.lambda_c * (c.lower[2] - c.pos[3 * n + 2]));
-        q_c = std::max(zero, q_c);
-        double btot = c.buoy[n] + c.glat * q_c;
-        get_points(c, n, reuse, pts);
         int i0 = ffloor((c.pos[3 * n] - c.lower[0]) * c.dxi[0]);
         int j0 = ffloor((c.pos[3 * n + 1] - c.lower[1]) * c.dxi[1]);
         int k0 = ffloor((c.pos[3 * n + 2] - c.lower[2]) * c.dxi[2]);
@@ -777,22 +821,27 @@ void par2grid(Ctx& c, bool reuse) {
         long cidx = c.fi(k0, c.wrapy(j0), c.wrapx(i0));
         c.nparg[cidx] += 1;
         if (c.vol[n] <= c.vmin) c.nsparg[cidx] += 1;
-        for (int p = 0; p < 4; ++p) {
-            trilinear(c, pts[p], is, js, ks, ww);
-            check_k(c, ks);
-            for (int i = 0; i < 2; ++i)
-                for (int j = 0; j < 2; ++j)
-                    for (int k = 0; k < 2; ++k) {
-                        long g = c.fi(ks + k, c.wrapy(js + j), c.wrapx(is + i));
-                        double w = f14 * pvol * ww[k][j][i];
-                        for (int l = 0; l < 3; ++l) c.vortg[l][g] += w * c.vor[3 * n + l];
-                        c.dbuoyg[g] += w * c.buoy[n];
-                        c.humg[g] += w * c.hum[n];
-                        c.tbuoyg[g] += w * btot;
-                        c.volg[g] += w;
-                    }
-        }
     }
+#ifdef _OPENMP
+    // per-thread accumulation then a fixed-order sum (the reference uses an
+    // OpenMP array reduction, parcel_interpl.f90:172-176)
+    int nt = std::min(omp_get_max_threads(), 32);
+    std::vector<std::vector<double>> priv(nt, std::vector<double>(7 * c.fsz, 0.0));
+#pragma omp parallel num_threads(nt)
+    {
+        int tid = omp_get_thread_num();
+        double* f[7];
+        for (int l = 0; l < 7; ++l) f[l] = priv[tid].data() + (size_t)l * c.fsz;
+#pragma omp for schedule(static)
+        for (long n = 0; n < c.n; ++n) p2g_parcel(c, n, reuse, f);
+    }
+#pragma omp parallel for schedule(static)
+    for (long g = 0; g < c.fsz; ++g)
+        for (int t = 0; t < nt; ++t)
+            for (int l = 0; l < 7; ++l) tgt[l][g] += priv[t][(size_t)l * c.fsz + g];
+#else
+    for (long n = 0; n < c.n; ++n) p2g_parcel(c, n, reuse, tgt);
+#endif
     // parcel counts: fold z halo (:237-243) and check (:245-250)
     long total = 0;
     for (int ix = 0; ix < c.nx; ++ix)
@@ -838,9 +887,10 @@ void grid2par(Ctx& c, bool add) {
         std::fill(c.dpos.begin(), c.dpos.begin() + 3 * c.n, 0.0);
         std::fill(c.dvor.begin(), c.dvor.begin() + 3 * c.n, 0.0);
     }
-    double pts[4][3], ww[2][2][2];
-    int is, js, ks;
+#pragma omp parallel for schedule(static)
     for (long n = 0; n < c.n; ++n) {
+        double pts[4][3], ww[2][2][2];
+        int is, js, ks;
         for (int l = 0; l < 8; ++l) c.strain[8 * n + l] = zero;
         get_points(c, n, false, pts);
         for (int p = 0; p < 4; ++p) {
@@ -857,6 +907,7 @@ void grid2par(Ctx& c, bool add) {
 double get_time_step(Ctx& c, double t) {
     const epic_cfg& g = c.cfg;
     double gmax = 2.220446049250313e-16;
+#pragma omp parallel for schedule(static) reduction(max : gmax)
     for (int ix = 0; ix < c.nx; ++ix)
         for (int iy = 0; iy < c.ny; ++iy)
             for (int iz = 0; iz <= c.nz; ++iz) {
@@ -881,6 +932,7 @@ double get_time_step(Ctx& c, double t) {
             }
     double dbmax = -1.0;
     const Arr& b = c.tbuoyg;
+#pragma omp parallel for schedule(static) reduction(max : dbmax)
     for (int ix = 0; ix < c.nx; ++ix)
         for (int iy = 0; iy < c.ny; ++iy)
             for (int iz = 0; iz <= c.nz; ++iz) {
@@ -1012,9 +1064,10 @@ void apply_laplace(Ctx& c, bool reuse) {                                 // :142
     for (long i = 0; i < c.fsz; ++i) phi[i] = c.volg[i] * c.vcelli - one;
     diverge(c, phi, grad);
     for (int k = 0; k < 3; ++k) extrap_halo(c, grad[k]);
-    double ww[2][2][2];
-    int is, js, ks;
+#pragma omp parallel for schedule(static)
     for (long n = 0; n < c.n; ++n) {
+        double ww[2][2][2];
+        int is, js, ks;
         trilinear(c, &c.pos[3 * n], is, js, ks, ww);
         check_k(c, ks);
         double d[3];
@@ -1028,9 +1081,10 @@ void apply_gradient(Ctx& c, double prefactor, double max_compression, bool reuse
     vol2grid(c, reuse);
     Arr phi(c.fsz);
     for (long i = 0; i < c.fsz; ++i) phi[i] = c.volg[i] * c.vcelli - one;
-    double w[2][2][2];
-    int is, js, ks;
+#pragma omp parallel for schedule(static)
     for (long n = 0; n < c.n; ++n) {
+        double w[2][2][2];
+        int is, js, ks;
         trilinear(c, &c.pos[3 * n], is, js, ks, w);
         check_k(c, ks);
         int i0 = c.wrapx(is), i1 = c.wrapx(is + 1), j0 = c.wrapy(js), j1 = c.wrapy(js + 1);
@@ -1076,6 +1130,7 @@ void rk_substep(Ctx& c, double dt, int step) {
     double ca = c.ca[step - 1], cb = c.cb[step - 1];
     double Bout[5];
     if (step == 1) {
+#pragma omp parallel for schedule(static) private(Bout)
         for (long n = 0; n < c.n; ++n) {
             get_dBdt(c, n, Bout);
             for (int k = 0; k < 5; ++k) c.dB[5 * n + k] = Bout[k];
@@ -1084,11 +1139,13 @@ void rk_substep(Ctx& c, double dt, int step) {
         vor2vel(c);
         vorticity_tendency(c);
         grid2par(c, true);
+#pragma omp parallel for schedule(static) private(Bout)
         for (long n = 0; n < c.n; ++n) {
             get_dBdt(c, n, Bout);
             for (int k = 0; k < 5; ++k) c.dB[5 * n + k] = c.dB[5 * n + k] + Bout[k];
         }
     }
+#pragma omp parallel for schedule(static)
     for (long n = 0; n < c.n; ++n) {
         for (int k = 0; k < 3; ++k) c.pos[3 * n + k] = c.pos[3 * n + k] + cb * dt * c.dpos[3 * n + k];
         for (int k = 0; k < 3; ++k) c.vor[3 * n + k] = c.vor[3 * n + k] + cb * dt * c.dvor[3 * n + k];

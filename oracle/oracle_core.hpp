@@ -263,7 +263,8 @@ struct CFFT {
         for (int kk = 0; kk < len; ++kk) out[kk] = scratch[kk];
     }
     void forward(const std::complex<double>* in, std::complex<double>* out) const {
-        std::vector<std::complex<double>> scratch(n);
+        thread_local std::vector<std::complex<double>> scratch;
+        if ((int)scratch.size() < n) scratch.resize(n);
         rec(in, out, n, 1, 0, 1, scratch.data());
     }
 };
@@ -275,7 +276,8 @@ struct RealFFT {
     void init(int n_) { n = n_; c.init(n_); }
     // forfft (stafft.f90:196-287)
     void forfft(double* x) const {
-        std::vector<std::complex<double>> a(n), b(n);
+        thread_local std::vector<std::complex<double>> a, b;
+        if ((int)a.size() < n) { a.resize(n); b.resize(n); }
         for (int j = 0; j < n; ++j) a[j] = x[j];
         c.forward(a.data(), b.data());
         double s = one / std::sqrt((double)n);
@@ -288,7 +290,8 @@ struct RealFFT {
     }
     // revfft (stafft.f90:296-403)
     void revfft(double* x) const {
-        std::vector<std::complex<double>> a(n), b(n);
+        thread_local std::vector<std::complex<double>> a, b;
+        if ((int)a.size() < n) { a.resize(n); b.resize(n); }
         double rn = std::sqrt((double)n);
         a[0] = x[0] * rn;
         for (int k = 1; 2 * k < n; ++k) {
@@ -312,7 +315,9 @@ struct TrigTransform {
     // dst(1, n, x(1:n)): x[0..n-1] holds x(1..n); x(n) is ignored on input and
     // zero on output.
     void dst(double* x) const {
-        std::vector<std::complex<double>> a(2 * n), b(2 * n);
+        thread_local std::vector<std::complex<double>> a, b;
+        if ((int)a.size() < 2 * n) { a.resize(2 * n); b.resize(2 * n); }
+        std::fill(a.begin(), a.begin() + 2 * n, std::complex<double>(0.0));
         for (int j = 1; j < n; ++j) { a[j] = x[j - 1]; a[2 * n - j] = -x[j - 1]; }
         c2.forward(a.data(), b.data());
         double s = std::sqrt(two / (double)n);
@@ -321,7 +326,8 @@ struct TrigTransform {
     }
     // dct(1, n, x(0:n))
     void dct(double* x) const {
-        std::vector<std::complex<double>> a(2 * n), b(2 * n);
+        thread_local std::vector<std::complex<double>> a, b;
+        if ((int)a.size() < 2 * n) { a.resize(2 * n); b.resize(2 * n); }
         for (int j = 0; j <= n; ++j) a[j] = x[j];
         for (int j = 1; j < n; ++j) a[2 * n - j] = x[j];
         c2.forward(a.data(), b.data());
