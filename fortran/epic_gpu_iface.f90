@@ -1,0 +1,98 @@
+! =============================================================================
+! ISO_C_BINDING interfaces of the B200 EPIC step (include/epic_gpu.h).
+! Replaces, under ENABLE_B200, the calls of the run loop at
+! src/3d/epic3d.f90:137-151 (see INTEGRATION.md for the call sequence).
+! =============================================================================
+module epic_gpu_iface
+    use iso_c_binding
+    implicit none
+
+    integer(c_int), parameter :: EPIC_OK = 0
+
+    type, bind(C) :: epic_cfg
+        integer(c_int32_t) :: nx, ny, nz
+        real(c_double)     :: lower(3), extent(3)
+        real(c_double)     :: size_factor, grow_factor, shrink_factor
+        integer(c_int32_t) :: n_per_cell
+        real(c_double)     :: lambda_max, min_vratio
+        integer(c_int32_t) :: correction_iters
+        real(c_double)     :: gradient_pref, max_compression
+        real(c_double)     :: t_initial, t_limit, alpha
+        integer(c_int32_t) :: precise_stop, use_fixed_dt
+        real(c_double)     :: fixed_dt
+        integer(c_int32_t) :: rk_order
+        real(c_double)     :: gravity, L_v, c_p, theta_0, q_0, height_c, ang_vel, lat_degrees
+        integer(c_int32_t) :: l_planetary_vorticity
+        integer(c_int32_t) :: bndry_zeta_zero(2)
+        integer(c_int64_t) :: capacity
+        integer(c_int32_t) :: precision
+        integer(c_int32_t) :: keep_order
+    end type epic_cfg
+
+    type, bind(C) :: epic_step_info
+        real(c_double)     :: t, dt
+        integer(c_int64_t) :: n_parcels, n_splits, n_merges
+        real(c_double)     :: parcel_stats(18)
+        real(c_double)     :: field_stats(11)
+    end type epic_step_info
+
+    interface
+        integer(c_int) function epic_gpu_default_config(cfg) bind(C, name="epic_gpu_default_config")
+            import :: c_int, epic_cfg
+            type(epic_cfg), intent(inout) :: cfg
+        end function
+
+        integer(c_int) function epic_gpu_create(cfg, ctx) bind(C, name="epic_gpu_create")
+            import :: c_int, c_ptr, epic_cfg
+            type(epic_cfg), intent(in) :: cfg
+            type(c_ptr), intent(out)   :: ctx
+        end function
+
+        subroutine epic_gpu_destroy(ctx) bind(C, name="epic_gpu_destroy")
+            import :: c_ptr
+            type(c_ptr), value :: ctx
+        end subroutine
+
+        type(c_ptr) function epic_gpu_last_error(ctx) bind(C, name="epic_gpu_last_error")
+            import :: c_ptr
+            type(c_ptr), value :: ctx
+        end function
+
+        integer(c_int) function epic_gpu_set_parcels(ctx, n, pos, vor, B, vol, buoy, hum) &
+                bind(C, name="epic_gpu_set_parcels")
+            import :: c_int, c_int64_t, c_ptr, c_double
+            type(c_ptr), value         :: ctx
+            integer(c_int64_t), value  :: n
+            real(c_double), intent(in) :: pos(3, *), vor(3, *), B(5, *), vol(*), buoy(*), hum(*)
+        end function
+
+        integer(c_int) function epic_gpu_get_parcels(ctx, cap, n, pos, vor, B, vol, buoy, hum) &
+                bind(C, name="epic_gpu_get_parcels")
+            import :: c_int, c_int64_t, c_ptr, c_double
+            type(c_ptr), value          :: ctx
+            integer(c_int64_t), value   :: cap
+            integer(c_int64_t)          :: n
+            real(c_double), intent(out) :: pos(3, *), vor(3, *), B(5, *), vol(*), buoy(*), hum(*)
+        end function
+
+        integer(c_int) function epic_gpu_init_correction(ctx) bind(C, name="epic_gpu_init_correction")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+        end function
+
+        integer(c_int) function epic_gpu_step(ctx, t, info) bind(C, name="epic_gpu_step")
+            import :: c_int, c_ptr, c_double, epic_step_info
+            type(c_ptr), value   :: ctx
+            real(c_double)       :: t
+            type(epic_step_info) :: info
+        end function
+
+        integer(c_int) function epic_gpu_get_field(ctx, field_id, out) bind(C, name="epic_gpu_get_field")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value     :: ctx
+            integer(c_int), value  :: field_id
+            real(c_double)         :: out(*)
+        end function
+    end interface
+
+end module epic_gpu_iface
