@@ -106,6 +106,20 @@ def dist_setup():
     return world, rank, local
 
 
+def reduce_timing(ms: float, work: float, device: str = "cuda"):
+    """Max of the device times and sum of the work over ranks (replicas)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms, work], dtype=torch.float64, device=device)
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(t[0]), float(t[1])
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(sm[1])
+
+
 def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int) -> float:
     """Minimal compulsory DRAM bytes of one launch (FP64 plain)."""
     gh = nx * ny * (nz + 3)
@@ -191,14 +205,7 @@ def run_ours(args):
     lib.lib.epic_gpu_profile_kernel(ctx.h, b"")
 
     # max over ranks, sum of work
-    tt = torch.tensor([ms, float(psteps)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-        mx = tt.clone(); dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = tt.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, ps_total = float(mx[0]), float(sm[1])
-    else:
-        ms_max, ps_total = ms, float(psteps)
+    ms_max, ps_total = reduce_timing(ms, float(psteps))
     value = ps_total / (ms_max * 1e-3)
 
     # roofline of the dominant kernel
@@ -253,14 +260,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
         ems = f0.elapsed_time(f1)
-        te = torch.tensor([ems, float(eps)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            import torch.distributed as dist
-            mx = te.clone(); dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-            sm = te.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-            ems_max, eps_total = float(mx[0]), float(sm[1])
-        else:
-            ems_max, eps_total = ems, float(eps)
+        ems_max, eps_total = reduce_timing(ems, float(eps))
         e2e = {"value": eps_total / (ems_max * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
                "steps": args.e2e_steps, "wall_s": wall,

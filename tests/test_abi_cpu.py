@@ -1,0 +1,55 @@
+"""The C ABI library loads and exports every symbol its headers declare
+(no device calls: runs without a GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(epic_gpu_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.mark.parametrize("header", ["epic_gpu.h", "epic_gpu_testing.h"])
+def test_library_exports_declared_symbols(header):
+    import epic_b200
+    lib = ctypes.CDLL(epic_b200.LIB_PATH)
+    names = _declared(header)
+    assert len(names) >= (30 if header == "epic_gpu.h" else 2)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_abi():
+    import epic_b200
+    lib = epic_b200.load()      # binds every signature of epic_b200/abi.py
+    assert lib.prefix == "epic_gpu_"
+
+
+def test_oracle_exports_same_abi(olib):
+    names = [n.replace("epic_gpu_", "epic_oracle_") for n in _declared("epic_gpu.h")
+             if not n.startswith(("epic_gpu_get_stream", "epic_gpu_profile", "epic_gpu_kernel_time",
+                                  "epic_gpu_launch_count", "epic_gpu_apply_vortcor_noalloc"))]
+    missing = [n for n in names if not hasattr(olib.lib, n)]
+    assert not missing, missing
+
+
+def test_config_struct_matches_header():
+    """sizeof(epic_cfg) / sizeof(epic_step_info) of the ctypes mirror match C."""
+    import subprocess, tempfile
+    from epic_b200.abi import EpicCfg, EpicStepInfo
+    src = ('#include "epic_gpu.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+           'int main(){printf("%zu %zu %zu\\n", sizeof(epic_cfg), sizeof(epic_step_info), offsetof(epic_cfg, capacity));}')
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "t")
+        subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe])
+        a, b, off = map(int, subprocess.check_output([exe]).split())
+    assert a == ctypes.sizeof(EpicCfg) and b == ctypes.sizeof(EpicStepInfo)
+    assert off == EpicCfg.capacity.offset

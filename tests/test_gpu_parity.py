@@ -257,3 +257,15 @@ def test_vol2grid(olib, glib, stretch):
     oc, gc = pair(s, olib, glib)
     oc.vol2grid(False); gc.vol2grid(False)
     _cmp_fields(oc, gc, [abi.VOLG])
+
+
+@pytest.mark.parametrize("case", ["p1", "p2", "p3", "p4"])
+def test_nearest_constellations_gpu(olib, glib, case):
+    """test_mpi_nearest_1..4 on the device: counts and pairs equal the oracle's."""
+    from tests import test_oracle_cpu as T
+    placement, expected = {"p1": (T._p1, 200), "p2": (T._p2, 200), "p3": (T._p3, 100), "p4": (T._p4, 100)}[case]
+    oc, _ = T._nearest_case(olib, placement)
+    gc, _ = T._nearest_case(glib, placement)
+    assert gc.merge() == expected == oc.merge()
+    assert all(np.array_equal(a, b) for a, b in zip(gc.merge_pairs(), oc.merge_pairs()))
+    _cmp_parcels(oc, gc)

@@ -1,0 +1,186 @@
+"""The oracle against the reference's own known answers (CPU only).
+
+Golden vectors: unit-tests/3d/{B,D,V}.asc (tests/golden/scherzinger_BDV.npz).
+Analytic KATs restated from unit-tests/3d: test_scherzinger_2, test_mpi_vor2vel,
+test_mpi_trilinear, test_mpi_grid2par, test_mpi_nearest_1..4,
+test_mpi_laplace_correction_3d; the transforms against numpy."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from epic_b200 import abi, initial, make_context
+
+F32 = lambda x: float(np.float32(x))  # noqa: E731  Fortran single-precision literal
+
+
+def test_scherzinger_golden(olib):
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "scherzinger_BDV.npz"))
+    D, V = oracle.eigen(olib, g["B"])
+    err = 0.0
+    for n in range(len(D)):
+        e = np.abs(g["D"][n] - D[n]).sum()
+        Q = g["V"][n].reshape(3, 3)
+        for k in range(3):
+            q = Q[k].copy()
+            if q[0] / V[n][0, k] < 0:
+                q = -q
+            e = max(e, np.abs(q - V[n][:, k]).sum())
+        err = max(err, e)
+    assert err < 1e-12          # test_scherzinger_2.f90:47
+    Dv, _ = oracle.eigen(olib, g["B"], values_only=True)
+    assert np.abs(Dv - g["D"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("n", [8, 16, 48, 64, 96, 128])
+def test_transforms(olib, n):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((3, n))
+    y = oracle.transform(olib, "forfft", x)
+    X = np.fft.fft(x, axis=1) / np.sqrt(n)
+    ref = np.zeros_like(x)
+    for k in range(0, n // 2 + 1):
+        ref[:, k] = X[:, k].real
+    for k in range(1, (n + 1) // 2):
+        ref[:, n - k] = X[:, k].imag
+    assert np.abs(y - ref).max() < 1e-13
+    assert np.abs(oracle.transform(olib, "revfft", y) - x).max() < 1e-13
+    xs = rng.standard_normal((2, n)); xs[:, -1] = 0
+    j = np.arange(1, n)
+    S = np.sqrt(2 / n) * np.sin(np.pi * np.outer(j, j) / n)
+    assert np.abs(oracle.transform(olib, "dst", xs)[:, :n - 1] - xs[:, :n - 1] @ S.T).max() < 1e-12
+    xc = rng.standard_normal((2, n + 1))
+    jj = np.arange(n + 1); w = np.ones(n + 1); w[0] = w[-1] = 0.5
+    Cm = np.sqrt(2 / n) * np.cos(np.pi * np.outer(jj, jj) / n) * w[None, :]
+    yc = oracle.transform(olib, "dct", xc)
+    assert np.abs(yc - xc @ Cm.T).max() < 1e-12
+    assert np.abs(oracle.transform(olib, "dct", yc) - xc).max() < 1e-12   # self-inverse
+
+
+def test_vor2vel_taylor_green(olib):
+    """test_mpi_vor2vel.f90: 64^3, max err < 1e-14."""
+    nx = ny = nz = 64
+    lower = (-math.pi, -math.pi, -0.5 * math.pi)
+    extent = (2 * math.pi,) * 3
+    ctx = abi.EpicContext(olib, olib.default_config(nx, ny, nz, lower, extent))
+    dx = np.array(extent) / 64
+    X, Y, Z = np.meshgrid(lower[0] + np.arange(nx) * dx[0], lower[1] + np.arange(ny) * dx[1],
+                          lower[2] + np.arange(-1, nz + 2) * dx[2], indexing="ij")
+    ctx.set_field(abi.VORTG[0], -3.0 * np.sin(X) * np.cos(Y) * np.cos(Z))
+    ctx.set_field(abi.VORTG[1], 3.0 * np.cos(X) * np.sin(Y) * np.cos(Z))
+    ctx.set_field(abi.VORTG[2], 0.0 * X)
+    ctx.vor2vel()
+    ref = [np.cos(X) * np.sin(Y) * np.sin(Z), np.sin(X) * np.cos(Y) * np.sin(Z), -2 * np.sin(X) * np.sin(Y) * np.cos(Z)]
+    err = max(np.abs(ctx.get_field(abi.VELOG[i])[:, :, 1:-1] - ref[i][:, :, 1:-1]).max() for i in range(3))
+    assert err < 1e-14
+
+
+def test_trilinear_conservation(olib):
+    """test_mpi_trilinear.f90: 32^3, 27 parcels per cell, constant vorticity."""
+    n = 32
+    lower = (-1.5, -1.5, -1.5)
+    extent = (0.4, 0.4, 0.4)
+    pos, vol, B = initial.regular_parcels(n, n, n, lower, extent, 27)
+    cfg = olib.default_config(n, n, n, lower, extent, min_vratio=27.0, n_per_cell=27)
+    ctx = abi.EpicContext(olib, cfg)
+    vor = np.zeros((len(vol), 3)); vor[:, 0] = 1.5
+    ctx.set_parcels(pos, vor, B, vol, np.zeros(len(vol)))
+    ctx.par2grid(False)
+    ngrid = n * n * (n + 1)
+    vcell = np.prod(np.array(extent) / n)
+    sx = ctx.get_field(abi.VORTG[0])[:, :, 1:-1].sum()
+    sv = ctx.get_field(abi.VOLG)[:, :, 1:-1].sum()
+    assert abs(sx - 1.5 * ngrid) < 1e-10          # reference bound 1e-15 with its order
+    assert abs(sv - ngrid * vcell) < 3e-14
+
+
+def test_grid2par_constant_fields(olib):
+    """test_mpi_grid2par.f90: constant fields interpolate to the constant."""
+    s = initial.thermal(16, seed=1)
+    ctx = make_context(s, olib)
+    vals = {}
+    for k, fid in enumerate(list(abi.VELOG) + list(abi.VELGRADG) + list(abi.VTEND)):
+        vals[fid] = 0.5 + k
+        ctx.set_field(fid, np.full(ctx.field_shape, vals[fid]))
+    ctx.grid2par(False)
+    rk = ctx.get_parcel_rk()
+    for c in range(3):
+        assert np.abs(rk["delta_pos"][:, c] - vals[abi.VELOG[c]]).max() < 1e-14
+        assert np.abs(rk["delta_vor"][:, c] - vals[abi.VTEND[c]]).max() < 1e-14
+    for c in range(8):
+        assert np.abs(rk["strain"][:, c] - vals[abi.VELGRADG[c]]).max() < 1e-13
+
+
+def _nearest_case(olib, placement):
+    """A 10^3 unit box with one z layer of cells (test_mpi_nearest_*); works
+    with any library binding (oracle or CUDA)."""
+    nx = 10
+    dx = 0.1
+    vcell = dx ** 3
+    vmin = vcell / 8.0
+    pos, vol = [], []
+    for j in range(nx):
+        for i in range(nx):
+            for (px, py, v) in placement(i, j, dx):
+                pos.append((px, py, 1.5 * dx)); vol.append(v * vmin)
+    pos = np.array(pos); vol = np.array(vol)
+    r2 = (0.75 * vol / math.pi) ** (2.0 / 3.0)
+    B = np.zeros((len(vol), 5)); B[:, 0] = r2; B[:, 3] = r2
+    cfg = olib.default_config(nx, nx, nx, (0, 0, 0), (1, 1, 1), lambda_max=5.0, min_vratio=8.0)
+    ctx = abi.EpicContext(olib, cfg)
+    ctx.set_parcels(pos, np.zeros((len(vol), 3)), B, vol, np.arange(len(vol), dtype=float))
+    return ctx, len(vol)
+
+
+def _p1(i, j, dx):   # test_mpi_nearest_1.f90:113-153 (a = b)
+    x, y = (0.5 + i) * dx, (0.5 + j) * dx
+    out = [(x, y, 1.1)]
+    out += [(x + m * dx * F32(0.45), y, 0.9) for m in (-1, 1)]
+    out += [(x, y + m * dx * F32(0.45), 0.9) for m in (-1, 1)]
+    return out
+
+
+def _p2(i, j, dx):   # test_mpi_nearest_2.f90:112-153 ((2) a = b)
+    x, y = (0.5 + i) * dx, (0.5 + j) * dx
+    out = [(x, y, 1.1)]
+    out += [(x + m * dx * F32(0.44), y + dx * F32(0.44), 0.9) for m in (-1, 1)]
+    out += [(x + m * dx * F32(0.44), y - dx * F32(0.44), 0.9) for m in (-1, 1)]
+    return out
+
+
+def _p3(i, j, dx):   # test_mpi_nearest_3.f90:95-135 (a - B)
+    x, y = (0.5 + i) * dx, (0.500001 + j) * dx
+    return [(x + 0.1 * dx, y, 1.1), (x + dx * 0.35, y, 0.9), (x - 0.42 * dx, y, 1.1)]
+
+
+def _p4(i, j, dx):   # test_mpi_nearest_4.f90:95-135 ((2) a - B)
+    x, y = (0.500001 + i) * dx, (0.5 + j) * dx
+    return [(x, y + 0.1 * dx, 1.1), (x, y + dx * 0.35, 0.9), (x, y - 0.42 * dx, 1.1)]
+
+
+@pytest.mark.parametrize("placement,expected", [(_p1, 200), (_p2, 200), (_p3, 100), (_p4, 100)])
+def test_nearest_constellations(olib, placement, expected):
+    ctx, n0 = _nearest_case(olib, placement)
+    nm = ctx.merge()
+    assert nm == expected
+    assert ctx.num_parcels() == n0 - nm
+
+
+def test_laplace_correction_reduces_volume_error(olib):
+    """test_mpi_laplace_correction_3d.f90: the volume error decreases."""
+    s = initial.thermal(16, seed=9)
+    rng = np.random.default_rng(9)
+    s.pos = s.pos + rng.uniform(-0.25, 0.25, s.pos.shape) * s.dx[None, :]
+    s.pos[:, 2] = np.clip(s.pos[:, 2], 1e-6, s.extent[2] - 1e-6)
+    ctx = make_context(s, olib)
+    errs = []
+    for it in range(6):
+        ctx.vol2grid(False)
+        v = ctx.get_field(abi.VOLG)[:, :, 1:-1]
+        errs.append(np.abs(v / np.prod(s.dx) - 1).max())
+        ctx.apply_laplace(False)
+        ctx.apply_gradient(True)
+    assert errs[-1] < errs[0]
+    assert all(b <= a * 1.05 for a, b in zip(errs, errs[1:]))
