@@ -129,6 +129,11 @@ def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int) -> float:
     if kernel == "g2p":
         # read x3 w3 B5 V + dx3 dw3 dB5; write x3 w3 B5 + dx3 dw3 dB5; read 14 fields
         return (23 + 22) * 8.0 * n + 14 * 8.0 * gh
+    if kernel == "stage":
+        # fused grid2par + RK update + next par2grid: read state (14) and
+        # accumulators (11), write state (11) and accumulators (11) per parcel;
+        # read 14 gathered fields, write 7 scattered fields + 2 int counts
+        return 47 * 8.0 * n + 14 * 8.0 * gh + 7 * 8.0 * gh + 2 * 4.0 * gh
     if kernel == "fft":
         # one pass over a (nz+1) x ny x nx field: read + write
         return 2 * 8.0 * nx * ny * (nz + 1)
@@ -151,7 +156,9 @@ def run_ours(args):
 
     setup = initial.config(args.workload)
     lib = epic_b200.load()
-    ctx = epic_b200.make_context(setup, lib)
+    # the device keeps parcels ordered by 8^3-cell tiles (keep_order=0); the
+    # parcel set is the reference's, its storage order is not
+    ctx = epic_b200.make_context(setup, lib, keep_order=0)
     import ctypes as C
     sp = C.c_void_p()
     lib.lib.epic_gpu_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
@@ -202,6 +209,16 @@ def run_ours(args):
     kms = C.c_double()
     kl = C.c_int64()
     lib.lib.epic_gpu_kernel_time(ctx.h, C.byref(kms), C.byref(kl))
+    lib.lib.epic_gpu_profile_kernel(ctx.h, b"")
+
+    # per-kernel CUDA-event times over one extra (untimed) step each
+    kernel_times = {}
+    for kname in [k for k in args.profile_kernels.split(",") if k]:
+        lib.lib.epic_gpu_profile_kernel(ctx.h, kname.encode())
+        t, _ = ctx.step(t)
+        km, kn = C.c_double(), C.c_int64()
+        lib.lib.epic_gpu_kernel_time(ctx.h, C.byref(km), C.byref(kn))
+        kernel_times[kname] = {"ms_per_step": km.value, "launches_per_step": kn.value}
     lib.lib.epic_gpu_profile_kernel(ctx.h, b"")
 
     # max over ranks, sum of work
@@ -281,6 +298,7 @@ def run_ours(args):
         "clocks": clk,
         "e2e": e2e,
         "gpu_launches": int(l1.value - l0.value),
+        "kernel_times": kernel_times,
         "dt_last": infos[-1].dt if infos else None,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -360,8 +378,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="thermal-128")
-    ap.add_argument("--roofline-kernel", default="p2g", choices=["p2g", "g2p", "fft"])
+    ap.add_argument("--roofline-kernel", default="stage", choices=["stage", "p2g", "g2p", "fft"])
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of that kernel")
+    ap.add_argument("--profile-kernels", default="", help="comma list of kernels to time over one extra step each")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -196,7 +196,8 @@ static void free_ctx(Ctx& c) {
     for (auto e : c.prof.ev) cudaEventDestroy(e);
     c.prof.ev.clear();
     spectral_free(c);
-    void* ptrs[] = {c.pv.base, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.dvor_bar};
+    void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
+                    c.dvor_bar};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.scratch) cudaFree(c.scratch);
@@ -270,6 +271,8 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         CK(cudaMemsetAsync(c.dsc, 0, sizeof(StepScalars), c.stream));
         CK(cudaMallocHost(&c.hsc, sizeof(StepScalars)));
         CK(cudaMalloc(&c.partials, sizeof(double) * 148 * 8 * 64));
+        CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)(c.cap / 2048 + 2)));
+        if (!cfg->keep_order) CK(cudaMalloc(&c.pv_alt, sizeof(double) * (size_t)N_ATTR * c.cap));
         CK(cudaMalloc(&c.dvor_bar, sizeof(double) * 8));
         CK(cudaMemsetAsync(c.dvor_bar, 0, sizeof(double) * 8, c.stream));
         spectral_init(c);
@@ -419,22 +422,38 @@ int epic_gpu_grid2par(epic_ctx* ctx, int add) {
 }
 
 static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
-    // ls_rk_step (ls_rk.f90:88-136)
+    // ls_rk_step (ls_rk.f90:88-136); each stage's grid2par + update is fused
+    // with the following par2grid (stage.cu)
     double tt = t;
     CK(cudaMemcpyAsync(&c.dsc->t, &tt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
     par2grid(c, t > c.cfg.t_initial, true);
+    prof_begin(c, "vor2vel");
     vor2vel(c);
+    prof_end(c, "vor2vel");
+    prof_begin(c, "vtend");
     vorticity_tendency(c);
+    prof_end(c, "vtend");
+    prof_begin(c, "timestep");
     time_step_reduce(c);
+    prof_end(c, "timestep");
     if (fstats) field_diagnostics(c, fstats);
-    g2p_rk_stage(c, 1, pstats != nullptr);
-    if (pstats) finish_parcel_diag(c, pstats);
-    for (int s = 2; s <= c.n_stages; ++s) {
-        par2grid(c, false, true);
-        vor2vel(c);
-        vorticity_tendency(c);
-        g2p_rk_stage(c, s, false);
+    for (int s = 1; s <= c.n_stages; ++s) {
+        if (s > 1) {
+            prof_begin(c, "vor2vel");
+            vor2vel(c);
+            prof_end(c, "vor2vel");
+            prof_begin(c, "vtend");
+            vorticity_tendency(c);
+            prof_end(c, "vtend");
+        }
+        fused_stage(c, s, s == 1 && pstats != nullptr);
+        if (s < c.n_stages) {
+            prof_begin(c, "p2g_tail");
+            p2g_tail(c);
+            prof_end(c, "p2g_tail");
+        }
     }
+    if (pstats) finish_parcel_diag(c, pstats);
     double dt = 0.0;
     CK(cudaMemcpyAsync(&dt, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     check_device_error(c);
@@ -507,13 +526,24 @@ int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info) {
     if (!info) info = &tmp;
     std::memset(info, 0, sizeof(*info));
     long long s0 = c.n_parcel_splits, m0 = c.n_parcel_merges;
+    prof_begin(c, "sort");
+    if (!c.cfg.keep_order) sort_parcels(c);
+    prof_end(c, "sort");
     apply_vortcor(c);
     info->dt = rk_step(c, *t, info->parcel_stats, info->field_stats);
+    prof_begin(c, "merge");
     parcel_merge(c);
+    prof_end(c, "merge");
+    prof_begin(c, "split");
     parcel_split(c);
+    prof_end(c, "split");
     for (int it = 1; it <= c.cfg.correction_iters; ++it) {
+        prof_begin(c, "laplace");
         apply_laplace(c, it > 1);
+        prof_end(c, "laplace");
+        prof_begin(c, "gradient");
         apply_gradient(c, true);
+        prof_end(c, "gradient");
     }
     check_device_error(c);
     info->t = *t;

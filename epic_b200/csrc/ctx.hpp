@@ -99,7 +99,11 @@ struct Ctx {
     double* dvor_bar = nullptr;
     // reduction partials
     double* partials = nullptr;
+    double* stage_partials = nullptr;   // per-CTA diagnostics of the fused stage kernel
+    const double* diag_buf = nullptr;   // partials read by finish_parcel_diag
     int n_partials = 0;
+    // second parcel store for the cell-tile reordering (keep_order == 0)
+    double* pv_alt = nullptr;
     // merge / split scratch
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -152,6 +156,13 @@ long long parcel_split(Ctx& c);
 void periodic_all(Ctx& c);
 void reflective_all(Ctx& c);
 void finish_parcel_diag(Ctx& c, double* out);
+
+// stage.cu
+void scatter_p2g(Ctx& c, bool reuse, bool store);
+void scatter_v2g(Ctx& c, bool reuse);
+void fused_stage(Ctx& c, int stage, bool with_diag);
+void sort_parcels(Ctx& c);
+void p2g_tail(Ctx& c);
 
 // merge.cu
 long long parcel_merge(Ctx& c);

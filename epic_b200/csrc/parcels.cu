@@ -9,8 +9,7 @@
 //   apply_*                         parcel_correction.f90:42-259, parcel_bc.f90:17-57
 //   parcel_split                    parcel_split.f90:37-198
 //   diagnostics                     parcel_diagnostics.f90:51-159, field_diagnostics.f90:40-154
-#include "ctx.hpp"
-#include "eigen.cuh"
+#include "parcel_ops.cuh"
 
 #include <cub/cub.cuh>
 #include <cstring>
@@ -19,139 +18,8 @@
 
 namespace epic {
 
-constexpr int PB = 256;          // threads per block for parcel kernels
-constexpr int PGRID = 148 * 8;   // fixed grid for deterministic reductions
-
-static int pgrid(long long n) {
-    long long b = (n + PB - 1) / PB;
-    return (int)std::max<long long>(1, std::min<long long>(b, PGRID));
-}
-
-#define PLOOP(n) for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); \
-                      i += (long long)gridDim.x * blockDim.x)
-
-struct Tri {
-    int is, js, ks;
-    double w[2][2][2];   // w[k][j][i]
-};
-
-// trilinear (interpl.f90:17-56)
-EPIC_DEV Tri trilinear(const Params& P, const double* p) {
-    Tri t;
-    double x = (p[0] - P.lower[0]) * P.dxi[0];
-    double y = (p[1] - P.lower[1]) * P.dxi[1];
-    double z = (p[2] - P.lower[2]) * P.dxi[2];
-    t.is = (int)floor(x); t.js = (int)floor(y); t.ks = (int)floor(z);
-    double px = x - (double)t.is, pxc = 1.0 - px;
-    double py = y - (double)t.js, pyc = 1.0 - py;
-    double pz = z - (double)t.ks, pzc = 1.0 - pz;
-    double w00 = pyc * pxc, w10 = pyc * px, w01 = py * pxc, w11 = py * px;
-    t.w[0][0][0] = pzc * w00; t.w[0][0][1] = pzc * w10; t.w[0][1][0] = pzc * w01; t.w[0][1][1] = pzc * w11;
-    t.w[1][0][0] = pz * w00;  t.w[1][0][1] = pz * w10;  t.w[1][1][0] = pz * w01;  t.w[1][1][1] = pz * w11;
-    return t;
-}
-
-// Addresses of the 8 corners (periodic in x, y).  Returns false if the
-// vertical index leaves the halo (the reference would index out of bounds).
-EPIC_DEV bool corners(const Params& P, const Tri& t, long long a[2][2]) {
-    if (t.ks < -1 || t.ks > P.nz) return false;
-    int i0 = wrapi(t.is, P.nx), i1 = wrapi(t.is + 1, P.nx);
-    int j0 = wrapi(t.js, P.ny), j1 = wrapi(t.js + 1, P.ny);
-    a[0][0] = fidx(P, t.ks, j0, i0);
-    a[0][1] = fidx(P, t.ks, j0, i1);
-    a[1][0] = fidx(P, t.ks, j1, i0);
-    a[1][1] = fidx(P, t.ks, j1, i1);
-    return true;
-}
-
-// sum(weights * f(ks:ks+1, js:js+1, is:is+1)) in column-major order
-EPIC_DEV double csum(const double* f, const Tri& t, const long long a[2][2]) {
-    double s = 0.0;
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            long long b = a[j][i];
-            s = fma(t.w[0][j][i], f[b], s);
-            s = fma(t.w[1][j][i], f[b + 1], s);
-        }
-    return s;
-}
-
-EPIC_DEV void load_B(const PView& pv, long long i, double* b) {
-#pragma unroll
-    for (int k = 0; k < 5; ++k) b[k] = pv.at(A_B11 + k, i);
-}
-
-// Support vectors: recomputed, or reused from the parcel store (l_reuse).
-EPIC_DEV void get_vectors(const PView& pv, long long i, bool reuse, bool store, double* eta, double* tau,
-                          double* D, unsigned* err) {
-    if (reuse) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { eta[k] = pv.at(A_ETA0 + k, i); tau[k] = pv.at(A_TAU0 + k, i); }
-        return;
-    }
-    double b[5];
-    load_B(pv, i, b);
-    support_vectors<FastOps>(b, pv.at(A_VOL, i), eta, tau, D, err);
-    if (store) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { pv.at(A_ETA0 + k, i) = eta[k]; pv.at(A_TAU0 + k, i) = tau[k]; }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // par2grid scatter (parcel_interpl.f90:160-233)
-struct ScatterFields {
-    double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg
-};
-
-__global__ void __launch_bounds__(PB) k_p2g(Params P, PView pv, long long n, ScatterFields F, int* nparg,
-                                           int* nsparg, int reuse, int store, unsigned* err) {
-    PLOOP(n) {
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
-        double vol = pv.at(A_VOL, i), buoy = pv.at(A_BUOY, i), hum = pv.at(A_HUM, i);
-        double q_c = hum - P.q_0 * exp(P.lambda_c * (P.lower[2] - pos[2]));
-        q_c = fmax(0.0, q_c);
-        double btot = buoy + P.glat * q_c;
-        double vals[6] = {pv.at(A_VX, i), pv.at(A_VY, i), pv.at(A_VZ, i), buoy, hum, btot};
-        double eta[3], tau[3];
-        get_vectors(pv, i, reuse != 0, store != 0, eta, tau, nullptr, err);
-        // parcel counts (get_index, fields.f90:165-172)
-        int ci = (int)floor((pos[0] - P.lower[0]) * P.dxi[0]);
-        int cj = (int)floor((pos[1] - P.lower[1]) * P.dxi[1]);
-        int ck = (int)floor((pos[2] - P.lower[2]) * P.dxi[2]);
-        if (ck < -1 || ck > P.nz) {
-            set_err(err, ERRB_ZRANGE);
-        } else {
-            long long g = fidx(P, ck, wrapi(cj, P.ny), wrapi(ci, P.nx));
-            atomicAdd(&nparg[g], 1);
-            if (vol <= P.vmin) atomicAdd(&nsparg[g], 1);
-        }
-        for (int p = 0; p < 4; ++p) {
-            double cp = support_cos(p), sp = support_sin(p);
-            double pt[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-            Tri t = trilinear(P, pt);
-            long long a[2][2];
-            if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
-            double pw = 0.25 * vol;
-#pragma unroll
-            for (int ii = 0; ii < 2; ++ii)
-#pragma unroll
-                for (int jj = 0; jj < 2; ++jj)
-#pragma unroll
-                    for (int kk = 0; kk < 2; ++kk) {
-                        long long g = a[jj][ii] + kk;
-                        double w = pw * t.w[kk][jj][ii];
-#pragma unroll
-                        for (int l = 0; l < 6; ++l) atomicAdd(&F.f[l][g], w * vals[l]);
-                        atomicAdd(&F.f[6][g], w);
-                    }
-        }
-    }
-}
 
 // z folds (parcel_interpl.f90:237-243, 256-275), per (x, y) column
 __global__ void k_p2g_fold(Params P, ScatterFields F, int nf, int* nparg, int* nsparg, long long* count) {
@@ -216,20 +84,14 @@ __global__ void k_count_check(StepScalars* sc, long long n) {
     if (sc->count != n) sc->err |= (1u << 30);
 }
 
-void par2grid(Ctx& c, bool reuse, bool store_vectors) {
+// z folds, parcel-count check, division by the gridded volume, zeta
+// zeroing and halo extrapolation after a par2grid scatter
+// (parcel_interpl.f90:235-319).
+void p2g_tail(Ctx& c) {
     const Params& P = c.P;
     ScatterFields F;
     F.f[0] = c.vortg(0); F.f[1] = c.vortg(1); F.f[2] = c.vortg(2);
     F.f[3] = c.dbuoyg(); F.f[4] = c.humg(); F.f[5] = c.tbuoyg(); F.f[6] = c.volg();
-    for (int l = 0; l < 7; ++l) CK(cudaMemsetAsync(F.f[l], 0, sizeof(double) * P.fsz, c.stream));
-    CK(cudaMemsetAsync(c.nparg, 0, sizeof(int) * P.fsz, c.stream));
-    CK(cudaMemsetAsync(c.nsparg, 0, sizeof(int) * P.fsz, c.stream));
-    CK(cudaMemsetAsync(&c.dsc->count, 0, sizeof(long long), c.stream));
-    prof_begin(c, "p2g");
-    k_p2g<<<pgrid(c.n), PB, 0, c.stream>>>(P, c.pv, c.n, F, c.nparg, c.nsparg, reuse, store_vectors,
-                                            &c.dsc->err);
-    CKL();
-    prof_end(c, "p2g");
     long long ncol = (long long)P.nx * P.ny;
     k_p2g_fold<<<(int)((ncol + 255) / 256), 256, 0, c.stream>>>(P, F, 7, c.nparg, c.nsparg, &c.dsc->count);
     CKL();
@@ -241,37 +103,16 @@ void par2grid(Ctx& c, bool reuse, bool store_vectors) {
     CKL();
 }
 
-// vol2grid (parcel_interpl.f90:92-135)
-__global__ void __launch_bounds__(PB) k_v2g(Params P, PView pv, long long n, double* volg, int reuse, unsigned* err) {
-    PLOOP(n) {
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
-        double vol = pv.at(A_VOL, i);
-        double eta[3], tau[3];
-        get_vectors(pv, i, reuse != 0, true, eta, tau, nullptr, err);
-        for (int p = 0; p < 4; ++p) {
-            double cp = support_cos(p), sp = support_sin(p);
-            double pt[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-            Tri t = trilinear(P, pt);
-            long long a[2][2];
-            if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
-#pragma unroll
-            for (int ii = 0; ii < 2; ++ii)
-#pragma unroll
-                for (int jj = 0; jj < 2; ++jj)
-#pragma unroll
-                    for (int kk = 0; kk < 2; ++kk)
-                        atomicAdd(&volg[a[jj][ii] + kk], 0.25 * t.w[kk][jj][ii] * vol);
-        }
-    }
+void par2grid(Ctx& c, bool reuse, bool store_vectors) {
+    scatter_p2g(c, reuse, store_vectors);
+    p2g_tail(c);
 }
+
+// vol2grid (parcel_interpl.f90:92-135)
 
 void vol2grid(Ctx& c, bool reuse) {
     const Params& P = c.P;
-    CK(cudaMemsetAsync(c.volg(), 0, sizeof(double) * P.fsz, c.stream));
-    k_v2g<<<pgrid(c.n), PB, 0, c.stream>>>(P, c.pv, c.n, c.volg(), reuse, &c.dsc->err);
-    CKL();
+    scatter_v2g(c, reuse);
     ScatterFields F;
     F.f[0] = c.volg();
     long long ncol = (long long)P.nx * P.ny;
@@ -282,47 +123,6 @@ void vol2grid(Ctx& c, bool reuse) {
 // ---------------------------------------------------------------------------
 // grid2par (+ LS-RK stage).  Gathers the 14 interpolated quantities at the 4
 // support points, then (stage mode) computes dB/dt and advances the parcel.
-struct GatherFields {
-    const double* f[14];   // velog 3, velgradg 8, vtend 3
-};
-
-struct StageArgs {
-    int mode;          // 0: grid2par only, 1: RK stage
-    int add;           // grid2par(add)
-    int stage;         // 1-based
-    int last;
-    int store_strain;
-    int diag;          // accumulate parcel diagnostics (stage 1)
-    double ca, cb;
-};
-
-// get_dBdt (parcel_ellipsoid.f90:466-507)
-EPIC_DEV void dBdt(const double* s, const double* b, double B33, double* o) {
-    double dwdz = -(s[I_DUDX] + s[I_DVDY]);
-    o[0] = 2.0 * (s[I_DUDX] * b[0] + s[I_DUDY] * b[1] + s[I_DUDZ] * b[2]);
-    o[1] = s[I_DVDX] * b[0] - dwdz * b[1] + s[I_DVDZ] * b[2] + s[I_DUDY] * b[3] + s[I_DUDZ] * b[4];
-    o[2] = s[I_DWDX] * b[0] + s[I_DWDY] * b[1] - s[I_DVDY] * b[2] + s[I_DUDY] * b[4] + s[I_DUDZ] * B33;
-    o[3] = 2.0 * (s[I_DVDX] * b[1] + s[I_DVDY] * b[3] + s[I_DVDZ] * b[4]);
-    o[4] = s[I_DWDX] * b[1] + s[I_DVDX] * b[2] + s[I_DWDY] * b[3] - s[I_DUDX] * b[4] + s[I_DVDZ] * B33;
-}
-
-// apply_periodic_bc / apply_reflective_bc (parcel_bc.f90:17-42)
-EPIC_DEV void periodic_bc(const Params& P, double* p) {
-    p[0] = p[0] - P.extent[0] * (double)(int)((p[0] - P.center[0]) * P.hli[0]);
-    p[1] = p[1] - P.extent[1] * (double)(int)((p[1] - P.center[1]) * P.hli[1]);
-}
-EPIC_DEV void reflective_bc(const Params& P, double* p, double* b) {
-    if (p[2] > P.upper[2]) {
-        p[2] = 2.0 * P.upper[2] - p[2];
-        b[2] = -b[2]; b[4] = -b[4];
-    } else if (p[2] < P.lower[2]) {
-        p[2] = 2.0 * P.lower[2] - p[2];
-        b[2] = -b[2]; b[4] = -b[4];
-    }
-}
-
-constexpr int NDIAG = 12;   // KE ENS LAM LAM2 VOL VOL2 NSMALL XI2 ETA2 ZETA2 BMIN BMAX
-
 __global__ void __launch_bounds__(PB) k_g2p(Params P, PView pv, long long n, GatherFields G, StageArgs S,
                                            const StepScalars* sc, double* partials, unsigned* err) {
     double acc[NDIAG];
@@ -489,7 +289,9 @@ void g2p_rk_stage(Ctx& c, int stage, bool with_diag) {
 // Parcel statistics from the block partials (parcel_diagnostics.f90:126-157).
 void finish_parcel_diag(Ctx& c, double* st) {
     std::vector<double> h((size_t)c.n_partials * NDIAG);
-    CK(cudaMemcpyAsync(h.data(), c.partials, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream));
+    const double* src = c.diag_buf ? c.diag_buf : c.partials;
+    CK(cudaMemcpyAsync(h.data(), src, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream));
+    c.diag_buf = nullptr;
     CK(cudaStreamSynchronize(c.stream));
     double acc[NDIAG] = {0};
     for (int b = 0; b < c.n_partials; ++b)

@@ -269,3 +269,26 @@ def test_nearest_constellations_gpu(olib, glib, case):
     assert gc.merge() == expected == oc.merge()
     assert all(np.array_equal(a, b) for a, b in zip(gc.merge_pairs(), oc.merge_pairs()))
     _cmp_parcels(oc, gc)
+
+
+def test_full_steps_reordered_store(olib, glib):
+    """keep_order=0: the device reorders parcels by cell tiles each step; the
+    parcel set must still equal the oracle's (matched by position)."""
+    from scipy.spatial import cKDTree
+    s = small_state("thermal", small_frac=0.02, seed=4)
+    from epic_b200 import make_context
+    oc = make_context(s, olib)
+    gc = make_context(s, glib, keep_order=0)
+    to = tg = 0.0
+    for k in range(2):
+        to, io = oc.step(to)
+        tg, ig = gc.step(tg)
+        assert io.n_parcels == ig.n_parcels
+        assert io.n_merges == ig.n_merges and io.n_splits == ig.n_splits
+        assert rel_err(tg, to) < TOL
+        assert rel_err(np.array(ig.parcel_stats), np.array(io.parcel_stats)) < 1e-9
+    a, b = gc.get_parcels(), oc.get_parcels()
+    d, j = cKDTree(a["pos"]).query(b["pos"])
+    assert d.max() < 1e-9 and len(set(j.tolist())) == len(j)
+    for k in ("vor", "B", "vol", "buoy"):
+        assert rel_err(a[k][j], b[k]) < 1e-9, k
