@@ -197,7 +197,7 @@ static void free_ctx(Ctx& c) {
     c.prof.ev.clear();
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
-                    c.dvor_bar};
+                    c.dvor_bar, c.box_start};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.scratch) cudaFree(c.scratch);
@@ -271,8 +271,12 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         CK(cudaMemsetAsync(c.dsc, 0, sizeof(StepScalars), c.stream));
         CK(cudaMallocHost(&c.hsc, sizeof(StepScalars)));
         CK(cudaMalloc(&c.partials, sizeof(double) * 148 * 8 * 64));
-        CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)(c.cap / 2048 + 2)));
-        if (!cfg->keep_order) CK(cudaMalloc(&c.pv_alt, sizeof(double) * (size_t)N_ATTR * c.cap));
+        CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)stage_grid_max(P, c.cap)));
+        if (!cfg->keep_order) {
+            CK(cudaMalloc(&c.pv_alt, sizeof(double) * (size_t)N_ATTR * c.cap));
+            c.nbox = box_count(P);
+            CK(cudaMalloc(&c.box_start, sizeof(int) * ((size_t)c.nbox + 1)));
+        }
         CK(cudaMalloc(&c.dvor_bar, sizeof(double) * 8));
         CK(cudaMemsetAsync(c.dvor_bar, 0, sizeof(double) * 8, c.stream));
         spectral_init(c);
@@ -309,6 +313,7 @@ int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const doub
     if (n < 0 || !pos || !vor || !B || !vol || !buoy) throw CudaError(EPIC_ERR_ARG, "set_parcels: bad arguments");
     if (n > c.cap) throw CudaError(EPIC_ERR_CAPACITY, "set_parcels: more parcels than the device capacity");
     c.n = n;
+    c.n_box = 0;
     CK(cudaMemsetAsync(c.pv.base, 0, sizeof(double) * (size_t)N_ATTR * c.cap, c.stream));
     upload_attr(c, pos, 3, A_X);
     upload_attr(c, vor, 3, A_VX);

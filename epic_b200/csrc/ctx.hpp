@@ -102,8 +102,13 @@ struct Ctx {
     double* stage_partials = nullptr;   // per-CTA diagnostics of the fused stage kernel
     const double* diag_buf = nullptr;   // partials read by finish_parcel_diag
     int n_partials = 0;
-    // second parcel store for the cell-tile reordering (keep_order == 0)
+    // second parcel store for the box reordering (keep_order == 0)
     double* pv_alt = nullptr;
+    // box ranges of the sorted store: parcels [box_start[b], box_start[b + 1])
+    // of [0, n_box) lie in box b at the last sort
+    int* box_start = nullptr;
+    int nbox = 0;
+    long long n_box = 0;
     // merge / split scratch
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -162,6 +167,8 @@ void scatter_p2g(Ctx& c, bool reuse, bool store);
 void scatter_v2g(Ctx& c, bool reuse);
 void fused_stage(Ctx& c, int stage, bool with_diag);
 void sort_parcels(Ctx& c);
+int box_count(const Params& P);
+long long stage_grid_max(const Params& P, long long cap);
 void p2g_tail(Ctx& c);
 
 // merge.cu

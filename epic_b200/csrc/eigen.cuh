@@ -58,7 +58,10 @@ EPIC_DEV void sz_evaluate(double* A, double* r, double* eta, double* D) {
     double rm = rl0;
     if (rl1 > rm) { i = 1; rm = rl1; }
     if (rl2 > rm) { i = 2; rm = rl2; }
-    double s1[3] = {r[3 * i] / rm, r[3 * i + 1] / rm, r[3 * i + 2] / rm};
+    // column i of r, selected without a run-time array index (keeps r in registers)
+    double s1[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) / rm;
     if (i == 1) { r[3] = r[0]; r[4] = r[1]; r[5] = r[2]; }
     else if (i == 2) { r[6] = r[0]; r[7] = r[1]; r[8] = r[2]; }
     r[0] = s1[0]; r[1] = s1[1]; r[2] = s1[2];
@@ -73,7 +76,9 @@ EPIC_DEV void sz_evaluate(double* A, double* r, double* eta, double* D) {
     rl2 = nrm3<O>(&r[6]);
     int j = (rl2 > rl1) ? 2 : 1;
     double rj = (j == 2) ? rl2 : rl1;
-    double s2[3] = {r[3 * j] / rj, r[3 * j + 1] / rj, r[3 * j + 2] / rj};
+    double s2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) / rj;
     r[3] = s2[0]; r[4] = s2[1]; r[5] = s2[2];
     double Ar[6];
 #pragma unroll
@@ -142,7 +147,7 @@ EPIC_DEV void sz_diagonalise(double* A, double* D, double* V) {
         int i = (l1 > l0) ? 1 : 0;
         double li = i ? l1 : l0;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) V[6 + k] = Ar[3 * i + k] / li;
+        for (int k = 0; k < 3; ++k) V[6 + k] = (i ? Ar[3 + k] : Ar[k]) / li;
         cross3<O>(&V[6], &V[0], &V[3]);
         cross3<O>(&V[0], &V[3], &V[6]);
         double n0 = nrm3<O>(&V[0]), n1 = nrm3<O>(&V[3]), n2 = nrm3<O>(&V[6]);

@@ -723,6 +723,7 @@ long long parcel_merge(Ctx& c) {
     CK(cudaStreamSynchronize(st));
     c.n_big_close += (long long)hb;
     c.n = newN;
+    c.n_box = std::min<long long>(c.n_box, newN);   // holes below newN now hold parcels from the end
     c.n_parcel_merges += nm;
     k_periodic_m<<<mgrid(newN), MB, 0, st>>>(P, c.pv, newN);
     CKL();

@@ -1,48 +1,70 @@
-// Windowed shared-memory scatter (par2grid, vol2grid), the fused LS-RK
-// stage kernel, and the cell-tile ordering of the parcel store.
+// Box-decomposed scatter (par2grid, vol2grid), the fused LS-RK stage kernel,
+// and the box ordering of the parcel store.
 //
-// Scatter: a CTA takes a contiguous chunk of SCHUNK parcels, finds the
-// bounding box of their cells, and accumulates the 4 support points x 8
-// corners of every parcel into a shared-memory window of the grid covering
-// that box plus the support-point reach (parcel_interpl.f90:160-233).  The
-// window is added to the global fields once per CTA; points outside the
-// window (strays, or a chunk too spread out for the window) go straight to
-// global memory.  When the parcel store is ordered by cell tiles a chunk
-// spans ~8x8x4 cells, so the global updates drop from 224 per parcel to
-// about 7 per grid point of a window.
+// Ordering: at the start of a step the parcel store is sorted by box of
+// BOXX x BOXY x BOXZ cells (cells z fastest inside a box), and the first
+// parcel of every box is recorded.  One CTA takes one box; parcels appended
+// later (split children) are handled in tail chunks of SCHUNK parcels, and
+// parcels moved into merge holes as strays.
+//
+// Scatter (parcel_interpl.f90:160-233): a CTA first finds the bounding box of
+// the cells of its parcels (ignoring parcels more than STRAY cells outside
+// its box) and the largest contribution of each field, then accumulates the
+// 4 support points x 8 corners of every parcel into a shared-memory window
+// covering that box plus the support-point reach, and adds the window to the
+// global fields once.  Window sums are fixed point: each contribution is
+// scaled by a power of two so that its magnitude is at most 2^b (b <= 50),
+// rounded to an integer, and added as three 32-bit limbs (two unsigned
+// 18-bit limbs and a signed top limb) with integer shared-memory atomics,
+// which run at several times the rate of FP64 shared atomics, do not
+// serialise on equal addresses, and make the window sums independent of the
+// order of the adds.  A round holds at most ROUND parcels (at most 4 ROUND
+// contributions per grid point), which keeps every limb sum inside 32 bits
+// and the total inside 62.  Points outside the window go straight to the
+// global fields (FP64 atomics).
 //
 // Fused stage (ls_rk.f90:142-217 + parcel_interpl.f90:405-470 + the next
 // stage's par2grid): pass A gathers the 14 interpolated quantities at the
-// support points (using the support vectors stored by the preceding scatter,
-// computed from the same B, parcel_ellipsoid.f90:216-247), computes dB/dt,
-// advances x, w, B and scales the accumulators; pass B (same chunk, data hot
-// in L2) computes the support vectors of the advanced shape, stores them,
-// and scatters into the next stage's fields.  One parcel pass and one
-// eigen-decomposition per parcel per stage instead of two of each.
+// support points (support vectors stored by the preceding scatter, computed
+// from the same B, parcel_ellipsoid.f90:216-247), computes dB/dt, advances
+// x, w, B and scales the accumulators; pass B (same parcels, hot in L1/L2)
+// computes the support vectors of the advanced shape, stores them, and
+// scatters into the next stage's fields.
 #include "parcel_ops.cuh"
 
 #include <cub/cub.cuh>
+#include <climits>
 #include <cstring>
 
 namespace epic {
 
-constexpr int SCHUNK = 2048;     // parcels per CTA
-constexpr int WMAX = 1536;       // grid points per shared-memory window
+constexpr int BOXX = 8, BOXY = 4, BOXZ = 4;   // cells per box
+constexpr int BOXC = BOXX * BOXY * BOXZ;
+constexpr int SCHUNK = 2048;    // parcels per tail chunk
+constexpr int ROUND = 4096;     // parcels per fixed-point round
+constexpr int WCAP = 1024;      // grid points per shared-memory window
+constexpr int STRAY = 2;        // cells outside its box a parcel may be and still shape the window
+constexpr int NLIMB = 3;
+constexpr int SB = 2;           // CTAs per SM the scatter kernels are sized for
 
-// Parcel slot of iteration k of this thread in a scatter pass: the 32 lanes
-// of a warp take parcels 64 apart in the (cell-ordered) chunk, i.e. about 8
-// cells apart, so one warp-wide shared-memory atomic rarely has two lanes on
-// the same grid point (same-address FP64 atomics serialise); a thread's
-// consecutive iterations take consecutive parcels.
-EPIC_DEV int scatter_slot(int k) {
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    return lane * (SCHUNK / 32) + warp * (SCHUNK / PB) + k;
-}
+// Box ranges of the sorted parcel store.
+struct Boxes {
+    const int* start;   // nbox + 1 first-parcel offsets
+    int nbox;           // 0 when the store is not box ordered
+    int nby, nbz;       // boxes along y and z
+    long long n_box;    // parcels [0, n_box) belong to the box ranges
+};
 
 struct Window {
-    int gx0, gy0, gz0;           // window origin (grid point, unwrapped)
-    int WX, WY, WZ;              // extents
+    int gx0, gy0, gz0;   // window origin (grid point; x, y unwrapped)
+    int WX, WY, WZ;      // extents
     int ok;
+};
+
+// Parcel range and reference cell of this CTA.
+struct Range {
+    long long r0, r1;
+    int ref[3], ext[3], margin;
 };
 
 // Cell of a position (get_index, fields.f90:165-172).
@@ -52,50 +74,175 @@ EPIC_DEV void cell_of(const Params& P, const double* p, int& ci, int& cj, int& c
     ck = (int)floor((p[2] - P.lower[2]) * P.dxi[2]);
 }
 
-struct WinBuild {
+EPIC_DEV Range cta_range(const Params& P, const PView& pv, const Boxes& B, long long n) {
+    Range R;
+    int b = blockIdx.x;
+    if (b < B.nbox) {
+        R.r0 = min((long long)B.start[b], B.n_box);
+        R.r1 = min((long long)B.start[b + 1], B.n_box);
+        int bz = b % B.nbz, r = b / B.nbz;
+        int by = r % B.nby, bx = r / B.nby;
+        R.ref[0] = bx * BOXX; R.ref[1] = by * BOXY; R.ref[2] = bz * BOXZ;
+        R.ext[0] = BOXX; R.ext[1] = BOXY; R.ext[2] = BOXZ;
+        R.margin = STRAY;
+    } else {
+        long long t = b - B.nbox;
+        R.r0 = B.n_box + t * SCHUNK;
+        R.r1 = min(R.r0 + SCHUNK, n);
+        R.ref[0] = R.ref[1] = R.ref[2] = 0;
+        if (R.r0 < R.r1) {
+            double p[3] = {pv.at(A_X, R.r0), pv.at(A_Y, R.r0), pv.at(A_Z, R.r0)};
+            cell_of(P, p, R.ref[0], R.ref[1], R.ref[2]);
+            R.ref[0] = wrapi(R.ref[0], P.nx);
+            R.ref[1] = wrapi(R.ref[1], P.ny);
+        }
+        R.ext[0] = R.ext[1] = R.ext[2] = 1;
+        R.margin = 1 << 20;
+    }
+    return R;
+}
+
+// Offset of cell c from the reference cell r, periodic, in [-n/2, n - n/2).
+EPIC_DEV int rel_periodic(int c, int r, int n) {
+    int d = wrapi(c - r, n);
+    return d >= n - n / 2 ? d - n : d;
+}
+
+// Per-thread partial of the window pass.
+template <int NF>
+struct WinPart {
     int mn[3], mx[3];
+    double vmax[NF];
+    EPIC_DEV void init() {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { mn[k] = INT_MAX; mx[k] = INT_MIN; }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) vmax[f] = 0.0;
+    }
+    // a parcel at position p with contributions vp[f]
+    EPIC_DEV void add(const Params& P, const Range& R, const double* p, const double* vp) {
+        int c[3];
+        cell_of(P, p, c[0], c[1], c[2]);
+        int d[3] = {rel_periodic(c[0], R.ref[0], P.nx), rel_periodic(c[1], R.ref[1], P.ny), c[2] - R.ref[2]};
+        bool in = true;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) in = in && d[k] >= -R.margin && d[k] < R.ext[k] + R.margin;
+        if (in) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { mn[k] = min(mn[k], d[k]); mx[k] = max(mx[k], d[k]); }
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            double a = fabs(vp[f]);
+            vmax[f] = (a > vmax[f] || a != a) ? a : vmax[f];   // keeps a NaN once seen
+        }
+    }
 };
 
-EPIC_DEV void win_init(WinBuild* wb) {
+template <int NF>
+struct WinShared {
+    int mn[3], mx[3];
+    unsigned long long vbits[NF];
+    Window W;
+    double scale[NF], inv[NF];
+};
+
+template <int NF>
+EPIC_DEV void win_begin(WinShared<NF>* ws) {
     if (threadIdx.x == 0) {
-        for (int k = 0; k < 3; ++k) { wb->mn[k] = 2147483647; wb->mx[k] = -2147483647; }
+        for (int k = 0; k < 3; ++k) { ws->mn[k] = INT_MAX; ws->mx[k] = INT_MIN; }
+        for (int f = 0; f < NF; ++f) ws->vbits[f] = 0ull;
     }
 }
 
-EPIC_DEV void win_add(WinBuild* wb, int lmn[3], int lmx[3]) {
+// Block reduction of the partials (after win_begin and a barrier).
+template <int NF>
+EPIC_DEV void win_reduce(WinShared<NF>* ws, WinPart<NF>& wp) {
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
-        int a = lmn[k], b = lmx[k];
+        int a = wp.mn[k], b = wp.mx[k];
         for (int o = 16; o > 0; o >>= 1) {
             a = min(a, __shfl_xor_sync(0xffffffff, a, o));
             b = max(b, __shfl_xor_sync(0xffffffff, b, o));
         }
-        if ((threadIdx.x & 31) == 0) { atomicMin(&wb->mn[k], a); atomicMax(&wb->mx[k], b); }
+        wp.mn[k] = a; wp.mx[k] = b;
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        // fmax drops NaN: carry it as +inf so that the round falls back to FP64
+        double v = isnan(wp.vmax[f]) ? INFINITY : wp.vmax[f];
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffff, v, o));
+        wp.vmax[f] = v;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; ++k) { atomicMin(&ws->mn[k], wp.mn[k]); atomicMax(&ws->mx[k], wp.mx[k]); }
+        // non-negative doubles order like their bit patterns
+        for (int f = 0; f < NF; ++f) atomicMax(&ws->vbits[f], (unsigned long long)__double_as_longlong(wp.vmax[f]));
     }
 }
 
-EPIC_DEV Window win_make(const Params& P, const WinBuild* wb) {
-    Window W;
-    W.gx0 = wb->mn[0] - 1;
-    W.gy0 = wb->mn[1] - 1;
-    W.gz0 = max(wb->mn[2] - 1, -1);
-    W.WX = wb->mx[0] - wb->mn[0] + 4;
-    W.WY = wb->mx[1] - wb->mn[1] + 4;
-    int gz1 = min(wb->mx[2] + 2, P.nz + 1);
+// Window and fixed-point scales of a round of `count` parcels (one thread).
+template <int NF>
+EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long long count) {
+    Window& W = ws->W;
+    W.gx0 = R.ref[0] + ws->mn[0] - 1;
+    W.gy0 = R.ref[1] + ws->mn[1] - 1;
+    W.gz0 = max(R.ref[2] + ws->mn[2] - 1, -1);
+    W.WX = ws->mx[0] - ws->mn[0] + 4;
+    W.WY = ws->mx[1] - ws->mn[1] + 4;
+    int gz1 = min(R.ref[2] + ws->mx[2] + 2, P.nz + 1);
     W.WZ = gz1 - W.gz0 + 1;
-    W.ok = (wb->mn[0] <= wb->mx[0]) && W.WX > 0 && W.WY > 0 && W.WZ > 0 &&
-           W.WX <= P.nx && W.WY <= P.ny && (long long)W.WX * W.WY * W.WZ <= WMAX;
-    return W;
+    bool ok = ws->mn[0] <= ws->mx[0] && W.WX <= P.nx && W.WY <= P.ny && W.WZ > 0 &&
+              (long long)W.WX * W.WY * W.WZ <= WCAP;
+    // contributions per grid point <= 4 count <= 2^lg; |window sum| <= 2^(bits + lg) <= 2^62
+    int lg = 32 - __clz((unsigned)(4 * count - 1));
+    int bits = min(50, 62 - lg);
+    for (int f = 0; f < NF; ++f) {
+        double m = __longlong_as_double((long long)ws->vbits[f]);
+        if (!(m <= 1.0e300)) ok = false;
+        int e = 0;
+        if (m > 0.0) frexp(m, &e);          // m < 2^e
+        ws->scale[f] = ldexp(1.0, bits - e);
+        ws->inv[f] = ldexp(1.0, e - bits);
+    }
+    W.ok = ok;
 }
 
-// Scatter NF values (val[f] * weight) of one support point.  Window layout
-// z fastest: w = ((x - gx0) * WY + (y - gy0)) * WZ + (z - gz0).
+struct Fields7 {
+    double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg
+};
+
+// Fixed-point accumulation.  r = wt * vs + 1.5 * 2^52 rounds wt * vs
+// (|wt * vs| <= 2^50) to the integer q once; the low 52 bits of r hold
+// m = 2^51 + q, split as q = ((m >> 36) - 2^15) * 2^36
+// + ((m >> 18) & 0x3ffff) * 2^18 + (m & 0x3ffff).
+constexpr double FX_MAGIC = 6755399441055744.0;   // 1.5 * 2^52
+
+EPIC_DEV void fx_add(unsigned* acc, int w, double wt, double vs) {
+    double r = fma(wt, vs, FX_MAGIC);
+    unsigned lo = (unsigned)__double2loint(r), hi = (unsigned)__double2hiint(r);
+    atomicAdd(&acc[w], lo & 0x3ffffu);
+    atomicAdd(&acc[WCAP + w], (lo >> 18) | ((hi & 0xfu) << 14));
+    atomicAdd(&acc[2 * WCAP + w], ((hi & 0xfffffu) >> 4) - 32768u);
+}
+
+EPIC_DEV double fx_value(const unsigned* acc, int w, double inv) {
+    long long q = (long long)(int)acc[2 * WCAP + w] * (1ll << 36) + (long long)acc[WCAP + w] * (1ll << 18) +
+                  (long long)acc[w];
+    return (double)q * inv;
+}
+
+EPIC_DEV int wrap_to(int l, int n) { return ((unsigned)l < (unsigned)n) ? l : wrapi(l, n); }
+
+// Scatter one support point: vp[f] = value * point weight * volume, vs[f] =
+// vp[f] in fixed-point units.
 template <int NF>
-EPIC_DEV void scatter_point(const Params& P, const Window& W, double* acc, double* const* F, const double* pt,
-                            const double* val, double pw, unsigned* err) {
+EPIC_DEV void scatter_point(const Params& P, const Window& W, unsigned* acc, const Fields7& F, const double* pt,
+                            const double* vp, const double* vs, unsigned* err) {
     Tri t = trilinear(P, pt);
     if (t.ks < -1 || t.ks > P.nz) { set_err(err, ERRB_ZRANGE); return; }
-    int lx = t.is - W.gx0, ly = t.js - W.gy0, lz = t.ks - W.gz0;
-    if (W.ok && lx >= 0 && lx + 1 < W.WX && ly >= 0 && ly + 1 < W.WY && lz >= 0 && lz + 1 < W.WZ) {
+    int lx = wrap_to(t.is - W.gx0, P.nx), ly = wrap_to(t.js - W.gy0, P.ny), lz = t.ks - W.gz0;
+    if (W.ok && lx + 1 < W.WX && ly + 1 < W.WY && lz >= 0 && lz + 1 < W.WZ) {
         int base = (lx * W.WY + ly) * W.WZ + lz;
 #pragma unroll
         for (int ii = 0; ii < 2; ++ii)
@@ -104,9 +251,9 @@ EPIC_DEV void scatter_point(const Params& P, const Window& W, double* acc, doubl
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     int w = base + (ii * W.WY + jj) * W.WZ + kk;
-                    double wt = pw * t.w[kk][jj][ii];
+                    double wt = t.w[kk][jj][ii];
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) atomicAdd(&acc[f * WMAX + w], wt * val[f]);
+                    for (int f = 0; f < NF; ++f) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
                 }
     } else {
         long long a[2][2];
@@ -118,23 +265,24 @@ EPIC_DEV void scatter_point(const Params& P, const Window& W, double* acc, doubl
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     long long g = a[jj][ii] + kk;
-                    double wt = pw * t.w[kk][jj][ii];
+                    double wt = t.w[kk][jj][ii];
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) atomicAdd(&F[f][g], wt * val[f]);
+                    for (int f = 0; f < NF; ++f) atomicAdd(&F.f[f][g], wt * vp[f]);
                 }
     }
 }
 
 template <int NF>
-EPIC_DEV void win_zero(double* acc, const Window& W) {
+EPIC_DEV void win_zero(unsigned* acc, const Window& W) {
     if (!W.ok) return;
     int n = W.WX * W.WY * W.WZ;
-    for (int f = 0; f < NF; ++f)
-        for (int w = threadIdx.x; w < n; w += blockDim.x) acc[f * WMAX + w] = 0.0;
+    for (int f = 0; f < NF * NLIMB; ++f)
+        for (int w = threadIdx.x; w < n; w += blockDim.x) acc[f * WCAP + w] = 0u;
 }
 
 template <int NF>
-EPIC_DEV void win_flush(const Params& P, const double* acc, const Window& W, double* const* F) {
+EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF>* ws, const Fields7& F) {
+    const Window W = ws->W;
     if (!W.ok) return;
     int n = W.WX * W.WY * W.WZ;
     for (int w = threadIdx.x; w < n; w += blockDim.x) {
@@ -145,30 +293,36 @@ EPIC_DEV void win_flush(const Params& P, const double* acc, const Window& W, dou
         long long g = fidx(P, W.gz0 + z, wrapi(W.gy0 + y, P.ny), wrapi(W.gx0 + x, P.nx));
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            double v = acc[f * WMAX + w];
-            if (v != 0.0) atomicAdd(&F[f][g], v);
+            double v = fx_value(acc + f * NLIMB * WCAP, w, ws->inv[f]);
+            if (v != 0.0) atomicAdd(&F.f[f][g], v);
         }
     }
 }
 
-struct Fields7 {
-    double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg
-};
-
-// Values scattered by par2grid for one parcel (parcel_interpl.f90:177-230).
-EPIC_DEV void p2g_values(const Params& P, const PView& pv, long long i, double* val, double& pw) {
-    double z = pv.at(A_Z, i);
-    double vol = pv.at(A_VOL, i), buoy = pv.at(A_BUOY, i), hum = pv.at(A_HUM, i);
+// Contributions of one parcel to the par2grid fields (parcel_interpl.f90:177-230):
+// value * point weight (1/4) * volume.
+EPIC_DEV void p2g_values(const Params& P, const double* vor, double z, double vol, double buoy, double hum,
+                         double* vp) {
     double q_c = hum - P.q_0 * exp(P.lambda_c * (P.lower[2] - z));
     q_c = fmax(0.0, q_c);
-    val[0] = pv.at(A_VX, i);
-    val[1] = pv.at(A_VY, i);
-    val[2] = pv.at(A_VZ, i);
-    val[3] = buoy;
-    val[4] = hum;
-    val[5] = buoy + P.glat * q_c;
-    val[6] = 1.0;
-    pw = 0.25 * vol;
+    double pw = 0.25 * vol;
+    vp[0] = pw * vor[0];
+    vp[1] = pw * vor[1];
+    vp[2] = pw * vor[2];
+    vp[3] = pw * buoy;
+    vp[4] = pw * hum;
+    vp[5] = pw * (buoy + P.glat * q_c);
+    vp[6] = pw;
+}
+
+template <int NF>
+EPIC_DEV void load_values(const Params& P, const PView& pv, long long i, double z, double* vp) {
+    if (NF == 7) {
+        double vor[3] = {pv.at(A_VX, i), pv.at(A_VY, i), pv.at(A_VZ, i)};
+        p2g_values(P, vor, z, pv.at(A_VOL, i), pv.at(A_BUOY, i), pv.at(A_HUM, i), vp);
+    } else {
+        vp[0] = 0.25 * pv.at(A_VOL, i);
+    }
 }
 
 EPIC_DEV void count_parcel(const Params& P, const double* pos, double vol, int* nparg, int* nsparg, unsigned* err) {
@@ -180,174 +334,215 @@ EPIC_DEV void count_parcel(const Params& P, const double* pos, double vol, int* 
     if (vol <= P.vmin) atomicAdd(&nsparg[g], 1);
 }
 
-// par2grid scatter (mode 0) and vol2grid (mode 1).
+// Pass B of a scatter round: support points of parcels [q0, q1) into the
+// window (or the global fields).
 template <int NF>
-__global__ void __launch_bounds__(PB) k_scatter(Params P, PView pv, long long n, Fields7 F, int* nparg, int* nsparg,
-                                               int reuse, int store, unsigned* err) {
-    extern __shared__ double acc[];
-    __shared__ WinBuild wb;
-    __shared__ Window Ws;
-    long long b0 = (long long)blockIdx.x * SCHUNK;
-    long long b1 = min(b0 + (long long)SCHUNK, n);
-    win_init(&wb);
-    __syncthreads();
-    int lmn[3] = {2147483647, 2147483647, 2147483647}, lmx[3] = {-2147483647, -2147483647, -2147483647};
-    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-        double p[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
-        int c[3];
-        cell_of(P, p, c[0], c[1], c[2]);
-        for (int k = 0; k < 3; ++k) { lmn[k] = min(lmn[k], c[k]); lmx[k] = max(lmx[k], c[k]); }
-    }
-    win_add(&wb, lmn, lmx);
-    __syncthreads();
-    if (threadIdx.x == 0) Ws = win_make(P, &wb);
-    __syncthreads();
-    const Window W = Ws;
-    win_zero<NF>(acc, W);
-    __syncthreads();
-    for (int k = 0; k < SCHUNK / PB; ++k) {
-        long long i = b0 + scatter_slot(k);
-        if (i >= b1) continue;
+EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long long q1, const WinShared<NF>* ws,
+                            unsigned* acc, const Fields7& F, int* nparg, int* nsparg, bool reuse, bool store,
+                            unsigned* err) {
+    const Window W = ws->W;
+    double scale[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) scale[f] = ws->scale[f];
+    // The 32 lanes of a warp take parcels about cnt/32 apart (different cells
+    // of the box), so that the addresses of one shared-memory atomic spread
+    // over the banks; consecutive parcels of one cell would pile onto few.
+    const int cnt = (int)(q1 - q0), S = (cnt + 31) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int r = threadIdx.x >> 5; r < S; r += PB / 32) {
+        int slot = lane * S + r;
+        if (slot >= cnt) continue;
+        long long i = q0 + slot;
         double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
         double eta[3], tau[3];
-        get_vectors(pv, i, reuse != 0, store != 0, eta, tau, nullptr, err);
-        double val[7], pw;
-        if (NF == 7) {
-            p2g_values(P, pv, i, val, pw);
-            count_parcel(P, pos, pv.at(A_VOL, i), nparg, nsparg, err);
-        } else {
-            val[0] = 1.0;
-            pw = 0.25 * pv.at(A_VOL, i);
-        }
+        get_vectors(pv, i, reuse, store, eta, tau, nullptr, err);
+        double vp[NF], vs[NF];
+        load_values<NF>(P, pv, i, pos[2], vp);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) vs[f] = vp[f] * scale[f];
+        if (NF == 7) count_parcel(P, pos, pv.at(A_VOL, i), nparg, nsparg, err);
         for (int p = 0; p < 4; ++p) {
             double cp = support_cos(p), sp = support_sin(p);
             double pt[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-            scatter_point<NF>(P, W, acc, F.f, pt, val, pw, err);
+            scatter_point<NF>(P, W, acc, F, pt, vp, vs, err);
         }
     }
-    __syncthreads();
-    win_flush<NF>(P, acc, W, F.f);
+}
+
+// par2grid scatter (NF = 7) and vol2grid (NF = 1).
+template <int NF>
+__global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long long n, Boxes B, Fields7 F,
+                                                    int* nparg, int* nsparg, int reuse, int store, unsigned* err) {
+    extern __shared__ unsigned acc[];
+    __shared__ WinShared<NF> ws;
+    const Range R = cta_range(P, pv, B, n);
+    for (long long q0 = R.r0; q0 < R.r1; q0 += ROUND) {
+        long long q1 = min(q0 + ROUND, R.r1);
+        win_begin(&ws);
+        __syncthreads();
+        WinPart<NF> wp;
+        wp.init();
+        for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+            double p[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+            double vp[NF];
+            load_values<NF>(P, pv, i, p[2], vp);
+            wp.add(P, R, p, vp);
+        }
+        win_reduce(&ws, wp);
+        __syncthreads();
+        if (threadIdx.x == 0) win_make(P, R, &ws, q1 - q0);
+        __syncthreads();
+        win_zero<NF>(acc, ws.W);
+        __syncthreads();
+        scatter_round<NF>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, err);
+        __syncthreads();
+        win_flush<NF>(P, acc, &ws, F);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
 // Fused stage kernel.
 struct FusedArgs {
-    int stage, last, diag, scatter;
+    int stage, last;
     double ca, cb;
 };
 
-__global__ void __launch_bounds__(PB) k_stage(Params P, PView pv, long long n, GatherFields G, Fields7 F, int* nparg,
-                                             int* nsparg, FusedArgs S, const StepScalars* sc, double* partials,
-                                             unsigned* err) {
-    extern __shared__ double acc[];
-    __shared__ WinBuild wb;
-    __shared__ Window Ws;
+template <bool DIAG, bool SCATTER>
+__global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long n, Boxes B, GatherFields G,
+                                                  Fields7 F, int* nparg, int* nsparg, FusedArgs S,
+                                                  const StepScalars* sc, double* partials, unsigned* err) {
+    extern __shared__ unsigned acc[];
+    __shared__ WinShared<7> ws;
     __shared__ double red[PB / 32][NDIAG];
-    double dacc[NDIAG];
+    constexpr int ND = DIAG ? NDIAG : 1;
+    double dacc[ND];
 #pragma unroll
-    for (int k = 0; k < NDIAG; ++k) dacc[k] = 0.0;
+    for (int k = 0; k < ND; ++k) dacc[k] = 0.0;
     const double dt = sc->dt;
-    long long b0 = (long long)blockIdx.x * SCHUNK;
-    long long b1 = min(b0 + (long long)SCHUNK, n);
-    win_init(&wb);
-    __syncthreads();
-    int lmn[3] = {2147483647, 2147483647, 2147483647}, lmx[3] = {-2147483647, -2147483647, -2147483647};
-    // pass A: grid2par + dB/dt + LS-RK update
-    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
-        double b[5];
-        load_B(pv, i, b);
-        double vol = pv.at(A_VOL, i);
-        double eta[3], tau[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { eta[k] = pv.at(A_ETA0 + k, i); tau[k] = pv.at(A_TAU0 + k, i); }
-        double g[14];
-#pragma unroll
-        for (int l = 0; l < 14; ++l) g[l] = 0.0;
-        for (int p = 0; p < 4; ++p) {
-            double cp = support_cos(p), sp = support_sin(p);
-            double pt[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-            Tri t = trilinear(P, pt);
-            long long a[2][2];
-            if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
-#pragma unroll
-            for (int l = 0; l < 14; ++l) g[l] += 0.25 * csum(G.f[l], t, a);
+    const Range R = cta_range(P, pv, B, n);
+    for (long long q0 = R.r0; q0 < R.r1; q0 += ROUND) {
+        long long q1 = min(q0 + ROUND, R.r1);
+        if (SCATTER) {
+            win_begin(&ws);
+            __syncthreads();
         }
-        double dp[3], dv[3], vor[3] = {pv.at(A_VX, i), pv.at(A_VY, i), pv.at(A_VZ, i)};
+        WinPart<7> wp;
+        wp.init();
+        // pass A: grid2par + dB/dt + LS-RK update
+        for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+            double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+            double g[14];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            dp[k] = S.stage > 1 ? pv.at(A_DX + k, i) + g[k] : g[k];
-            dv[k] = S.stage > 1 ? pv.at(A_DVX + k, i) + g[11 + k] : g[11 + k];
+            for (int l = 0; l < 14; ++l) g[l] = 0.0;
+            {
+                double eta[3], tau[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { eta[k] = pv.at(A_ETA0 + k, i); tau[k] = pv.at(A_TAU0 + k, i); }
+                for (int p = 0; p < 4; ++p) {
+                    double cp = support_cos(p), sp = support_sin(p);
+                    double pt[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
+                    Tri t = trilinear(P, pt);
+                    long long a[2][2];
+                    if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
+#pragma unroll
+                    for (int l = 0; l < 14; ++l) g[l] += 0.25 * csum(G.f[l], t, a);
+                }
+            }
+            double b[5];
+            load_B(pv, i, b);
+            double vol = pv.at(A_VOL, i);
+            double dp[3], dv[3], vor[3] = {pv.at(A_VX, i), pv.at(A_VY, i), pv.at(A_VZ, i)};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                dp[k] = S.stage > 1 ? pv.at(A_DX + k, i) + g[k] : g[k];
+                dv[k] = S.stage > 1 ? pv.at(A_DVX + k, i) + g[11 + k] : g[11 + k];
+            }
+            const double* strain = &g[3];
+            if (DIAG) {
+                // parcel diagnostics before the update (ls_rk.f90:116, parcel_diagnostics.f90:66-120)
+                double U[9], D[3];
+                full_matrix<FastOps>(b, get_B33<FastOps>(b, vol, err), U);
+                sz_eigenvalues<FastOps>(U, D);
+                double bu = pv.at(A_BUOY, i);
+                dacc[0] += (dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]) * vol;
+                dacc[1] += (vor[0] * vor[0] + vor[1] * vor[1] + vor[2] * vor[2]) * vol;
+                double lam = sqrt(D[0] / D[2]);
+                dacc[2] += lam;
+                dacc[3] += lam * lam;
+                dacc[4] += vol;
+                dacc[5] += vol * vol;
+                if (vol <= P.vmin) dacc[6] += 1.0;
+                dacc[7] += vol * (vor[0] * vor[0]);
+                dacc[8] += vol * (vor[1] * vor[1]);
+                dacc[9] += vol * (vor[2] * vor[2]);
+                dacc[10] = fmin(dacc[10], bu);
+                dacc[11] = fmax(dacc[11], bu);
+            }
+            double B33 = get_B33<FastOps>(b, vol, err);
+            double db[5];
+            dBdt(strain, b, B33, db);
+            if (S.stage > 1) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) db[k] = pv.at(A_DB0 + k, i) + db[k];
+            }
+            double cdt = S.cb * dt;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                pos[k] = pos[k] + cdt * dp[k];
+                vor[k] = vor[k] + cdt * dv[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 5; ++k) b[k] = b[k] + cdt * db[k];
+            periodic_bc(P, pos);
+            if (S.last) {
+                reflective_bc(P, pos, b);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { dp[k] = S.ca * dp[k]; dv[k] = S.ca * dv[k]; }
+#pragma unroll
+                for (int k = 0; k < 5; ++k) db[k] = S.ca * db[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                pv.at(A_X + k, i) = pos[k];
+                pv.at(A_VX + k, i) = vor[k];
+                pv.at(A_DX + k, i) = dp[k];
+                pv.at(A_DVX + k, i) = dv[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                pv.at(A_B11 + k, i) = b[k];
+                pv.at(A_DB0 + k, i) = db[k];
+            }
+            if (SCATTER) {
+                double vp[7];
+                p2g_values(P, vor, pos[2], vol, pv.at(A_BUOY, i), pv.at(A_HUM, i), vp);
+                wp.add(P, R, pos, vp);
+            }
         }
-        const double* strain = &g[3];
-        if (S.diag) {
-            // parcel diagnostics before the update (ls_rk.f90:116, parcel_diagnostics.f90:66-120)
-            double U[9], D[3];
-            full_matrix<FastOps>(b, get_B33<FastOps>(b, vol, err), U);
-            sz_eigenvalues<FastOps>(U, D);
-            double bu = pv.at(A_BUOY, i);
-            dacc[0] += (dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]) * vol;
-            dacc[1] += (vor[0] * vor[0] + vor[1] * vor[1] + vor[2] * vor[2]) * vol;
-            double lam = sqrt(D[0] / D[2]);
-            dacc[2] += lam;
-            dacc[3] += lam * lam;
-            dacc[4] += vol;
-            dacc[5] += vol * vol;
-            if (vol <= P.vmin) dacc[6] += 1.0;
-            dacc[7] += vol * (vor[0] * vor[0]);
-            dacc[8] += vol * (vor[1] * vor[1]);
-            dacc[9] += vol * (vor[2] * vor[2]);
-            dacc[10] = fmin(dacc[10], bu);
-            dacc[11] = fmax(dacc[11], bu);
+        if (SCATTER) {
+            win_reduce(&ws, wp);
+            __syncthreads();
+            if (threadIdx.x == 0) win_make(P, R, &ws, q1 - q0);
+            __syncthreads();
+            win_zero<7>(acc, ws.W);
+            __syncthreads();
+            // pass B: support vectors of the advanced shape + next par2grid
+            scatter_round<7>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, false, true, err);
+            __syncthreads();
+            win_flush<7>(P, acc, &ws, F);
+            __syncthreads();
         }
-        double B33 = get_B33<FastOps>(b, vol, err);
-        double db[5];
-        dBdt(strain, b, B33, db);
-        if (S.stage > 1) {
-#pragma unroll
-            for (int k = 0; k < 5; ++k) db[k] = pv.at(A_DB0 + k, i) + db[k];
-        }
-        double cdt = S.cb * dt;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            pos[k] = pos[k] + cdt * dp[k];
-            vor[k] = vor[k] + cdt * dv[k];
-        }
-#pragma unroll
-        for (int k = 0; k < 5; ++k) b[k] = b[k] + cdt * db[k];
-        periodic_bc(P, pos);
-        if (S.last) {
-            reflective_bc(P, pos, b);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) { dp[k] = S.ca * dp[k]; dv[k] = S.ca * dv[k]; }
-#pragma unroll
-            for (int k = 0; k < 5; ++k) db[k] = S.ca * db[k];
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            pv.at(A_X + k, i) = pos[k];
-            pv.at(A_VX + k, i) = vor[k];
-            pv.at(A_DX + k, i) = dp[k];
-            pv.at(A_DVX + k, i) = dv[k];
-        }
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            pv.at(A_B11 + k, i) = b[k];
-            pv.at(A_DB0 + k, i) = db[k];
-        }
-        int c[3];
-        cell_of(P, pos, c[0], c[1], c[2]);
-        for (int k = 0; k < 3; ++k) { lmn[k] = min(lmn[k], c[k]); lmx[k] = max(lmx[k], c[k]); }
     }
-    if (S.diag) {
+    if (DIAG) {
         int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
-        for (int k = 0; k < NDIAG; ++k) {
+        for (int k = 0; k < ND; ++k) {
             double v = dacc[k];
             for (int o = 16; o > 0; o >>= 1) {
                 double u = __shfl_xor_sync(0xffffffff, v, o);
@@ -355,54 +550,15 @@ __global__ void __launch_bounds__(PB) k_stage(Params P, PView pv, long long n, G
             }
             if (l == 0) red[w][k] = v;
         }
-    }
-    if (!S.scatter) {
-        if (S.diag) {
-            __syncthreads();
-            if (threadIdx.x < NDIAG) {
-                int k = threadIdx.x;
-                double v = red[0][k];
-                for (int q = 1; q < PB / 32; ++q)
-                    v = (k == 10) ? fmin(v, red[q][k]) : (k == 11) ? fmax(v, red[q][k]) : v + red[q][k];
-                partials[blockIdx.x * NDIAG + k] = v;
-            }
-        }
-        return;
-    }
-    win_add(&wb, lmn, lmx);
-    __syncthreads();
-    if (S.diag && threadIdx.x < NDIAG) {
-        int k = threadIdx.x;
-        double v = red[0][k];
-        for (int q = 1; q < PB / 32; ++q)
-            v = (k == 10) ? fmin(v, red[q][k]) : (k == 11) ? fmax(v, red[q][k]) : v + red[q][k];
-        partials[blockIdx.x * NDIAG + k] = v;
-    }
-    if (threadIdx.x == 0) Ws = win_make(P, &wb);
-    __syncthreads();
-    const Window W = Ws;
-    win_zero<7>(acc, W);
-    __syncthreads();
-    // pass B: support vectors of the advanced shape + next par2grid
-    for (int k = 0; k < SCHUNK / PB; ++k) {
-        long long i = b0 + scatter_slot(k);
-        if (i >= b1) continue;
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
-        double eta[3], tau[3];
-        get_vectors(pv, i, false, true, eta, tau, nullptr, err);
-        double val[7], pw;
-        p2g_values(P, pv, i, val, pw);
-        count_parcel(P, pos, pv.at(A_VOL, i), nparg, nsparg, err);
-        for (int p = 0; p < 4; ++p) {
-            double cp = support_cos(p), sp = support_sin(p);
-            double pt[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-            scatter_point<7>(P, W, acc, F.f, pt, val, pw, err);
+        __syncthreads();
+        if (threadIdx.x < NDIAG) {
+            int k = threadIdx.x;
+            double v = red[0][k];
+            for (int q = 1; q < PB / 32; ++q)
+                v = (k == 10) ? fmin(v, red[q][k]) : (k == 11) ? fmax(v, red[q][k]) : v + red[q][k];
+            partials[blockIdx.x * NDIAG + k] = v;
         }
     }
-    __syncthreads();
-    win_flush<7>(P, acc, W, F.f);
 }
 
 // ---------------------------------------------------------------------------
@@ -413,7 +569,29 @@ static Fields7 fields7(Ctx& c) {
     return F;
 }
 
-static int sgrid(long long n) { return (int)std::max<long long>(1, (n + SCHUNK - 1) / SCHUNK); }
+static Boxes boxes(const Ctx& c) {
+    Boxes B;
+    bool valid = c.box_start != nullptr && c.n_box > 0;
+    B.start = c.box_start;
+    B.nbox = valid ? c.nbox : 0;
+    B.nby = (c.P.ny + BOXY - 1) / BOXY;
+    B.nbz = (c.P.nz + BOXZ - 1) / BOXZ;
+    B.n_box = valid ? std::min(c.n_box, c.n) : 0;
+    return B;
+}
+
+static int sgrid(const Ctx& c, const Boxes& B) {
+    long long tail = c.n - B.n_box;
+    return (int)std::max<long long>(1, B.nbox + (tail + SCHUNK - 1) / SCHUNK);
+}
+
+int box_count(const Params& P) {
+    return ((P.nx + BOXX - 1) / BOXX) * ((P.ny + BOXY - 1) / BOXY) * ((P.nz + BOXZ - 1) / BOXZ);
+}
+
+long long stage_grid_max(const Params& P, long long cap) {
+    return (long long)box_count(P) + (cap + SCHUNK - 1) / SCHUNK + 1;
+}
 
 static void zero_p2g_fields(Ctx& c) {
     const Params& P = c.P;
@@ -425,13 +603,19 @@ static void zero_p2g_fields(Ctx& c) {
     CK(cudaMemsetAsync(&c.dsc->count, 0, sizeof(long long), c.stream));
 }
 
+template <typename K>
+static void set_smem(K kernel, size_t bytes) {
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
 void scatter_p2g(Ctx& c, bool reuse, bool store) {
     zero_p2g_fields(c);
     if (c.n == 0) return;
-    size_t sm = sizeof(double) * 7 * WMAX;
-    CK(cudaFuncSetAttribute(k_scatter<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    size_t sm = sizeof(unsigned) * 7 * NLIMB * WCAP;
+    set_smem(k_scatter<7>, sm);
+    Boxes B = boxes(c);
     prof_begin(c, "p2g");
-    k_scatter<7><<<sgrid(c.n), PB, sm, c.stream>>>(c.P, c.pv, c.n, fields7(c), c.nparg, c.nsparg, reuse, store,
+    k_scatter<7><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, fields7(c), c.nparg, c.nsparg, reuse, store,
                                                      &c.dsc->err);
     CKL();
     prof_end(c, "p2g");
@@ -442,9 +626,10 @@ void scatter_v2g(Ctx& c, bool reuse) {
     if (c.n == 0) return;
     Fields7 F;
     F.f[0] = c.volg();
-    size_t sm = sizeof(double) * 1 * WMAX;
+    size_t sm = sizeof(unsigned) * 1 * NLIMB * WCAP;
+    Boxes B = boxes(c);
     prof_begin(c, "v2g");
-    k_scatter<1><<<sgrid(c.n), PB, sm, c.stream>>>(c.P, c.pv, c.n, F, nullptr, nullptr, reuse, 1, &c.dsc->err);
+    k_scatter<1><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, nullptr, nullptr, reuse, 1, &c.dsc->err);
     CKL();
     prof_end(c, "v2g");
 }
@@ -455,35 +640,41 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     FusedArgs S;
     S.stage = stage;
     S.last = stage == c.n_stages;
-    S.diag = with_diag;
-    S.scatter = !S.last;
     S.ca = c.ca[stage - 1];
     S.cb = c.cb[stage - 1];
+    bool scatter = !S.last;
     GatherFields G;
     for (int k = 0; k < 3; ++k) G.f[k] = c.velog(k);
     for (int k = 0; k < 8; ++k) G.f[3 + k] = c.velgrad(k);
     for (int k = 0; k < 3; ++k) G.f[11 + k] = c.vtend(k);
-    if (S.scatter) zero_p2g_fields(c);
-    int g = sgrid(c.n);
+    if (scatter) zero_p2g_fields(c);
+    Boxes B = boxes(c);
+    int g = sgrid(c, B);
     if (with_diag) {
         c.n_partials = g;
         c.diag_buf = c.stage_partials;
     }
-    size_t sm = S.scatter ? sizeof(double) * 7 * WMAX : 0;
-    CK(cudaFuncSetAttribute(k_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(double) * 7 * WMAX)));
-    prof_begin(c, "stage");
-    k_stage<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, G, fields7(c), c.nparg, c.nsparg, S, c.dsc, c.stage_partials,
-                                      &c.dsc->err);
-    CKL();
-    prof_end(c, "stage");
+    size_t sm = scatter ? sizeof(unsigned) * 7 * NLIMB * WCAP : 0;
+    auto launch = [&](auto kernel) {
+        if (sm) set_smem(kernel, sm);
+        prof_begin(c, "stage");
+        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, G, fields7(c), c.nparg, c.nsparg, S, c.dsc,
+                                        c.stage_partials, &c.dsc->err);
+        CKL();
+        prof_end(c, "stage");
+    };
+    if (with_diag && scatter) launch(k_stage<true, true>);
+    else if (with_diag) launch(k_stage<true, false>);
+    else if (scatter) launch(k_stage<false, true>);
+    else launch(k_stage<false, false>);
 }
 
 // ---------------------------------------------------------------------------
-// Cell-tile ordering of the parcel store: key = 8^3-cell tile (x fastest),
-// then the cell inside the tile (x fastest).  Only the attributes live at the
-// start of a step are moved (state and support vectors).
+// Box ordering of the parcel store: key = box (z fastest), then the cell
+// inside the box (z fastest).  Only the attributes live at the start of a
+// step are moved (state and support vectors).
 __global__ void k_sort_keys(Params P, PView pv, long long n, unsigned* key, int* idx) {
-    int ntx = (P.nx + 7) >> 3, nty = (P.ny + 7) >> 3;
+    int nby = (P.ny + BOXY - 1) / BOXY, nbz = (P.nz + BOXZ - 1) / BOXZ;
     PLOOP(n) {
         double p[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
         int ci, cj, ck;
@@ -491,10 +682,21 @@ __global__ void k_sort_keys(Params P, PView pv, long long n, unsigned* key, int*
         ci = min(max(ci, 0), P.nx - 1);
         cj = min(max(cj, 0), P.ny - 1);
         ck = min(max(ck, 0), P.nz - 1);
-        unsigned tile = (unsigned)(((ck >> 3) * nty + (cj >> 3)) * ntx + (ci >> 3));
-        unsigned local = (unsigned)(((ck & 7) * 8 + (cj & 7)) * 8 + (ci & 7));
-        key[i] = tile * 512u + local;
+        unsigned box = (unsigned)(((ci / BOXX) * nby + cj / BOXY) * nbz + ck / BOXZ);
+        unsigned local = (unsigned)(((ci % BOXX) * BOXY + cj % BOXY) * BOXZ + ck % BOXZ);
+        key[i] = box * (unsigned)BOXC + local;
         idx[i] = (int)i;
+    }
+}
+
+// First parcel of every box, from the sorted keys.
+__global__ void k_box_start(const unsigned* key, long long n, int nbox, int* start) {
+    PLOOP(n) {
+        int b = (int)(key[i] / BOXC);
+        int prev = i > 0 ? (int)(key[i - 1] / BOXC) : -1;
+        for (int v = prev + 1; v <= b; ++v) start[v] = (int)i;
+        if (i == n - 1)
+            for (int v = b + 1; v <= nbox; ++v) start[v] = (int)n;
     }
 }
 
@@ -512,7 +714,8 @@ __global__ void k_permute(PView src, PView dst, long long n, const int* perm) {
 
 void sort_parcels(Ctx& c) {
     long long n = c.n;
-    if (n < 2 || c.pv_alt == nullptr) return;
+    c.n_box = 0;
+    if (n < 2 || c.pv_alt == nullptr || c.box_start == nullptr) return;
     size_t cubb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cubb, (unsigned*)0, (unsigned*)0, (int*)0, (int*)0, (int)n, 0, 32,
                                     c.stream);
@@ -526,15 +729,17 @@ void sort_parcels(Ctx& c) {
     void* tmp = take(cubb);
     k_sort_keys<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, k0, i0);
     CKL();
-    int ntx = (c.P.nx + 7) >> 3, nty = (c.P.ny + 7) >> 3, ntz = (c.P.nz + 7) >> 3;
-    unsigned long long maxkey = (unsigned long long)ntx * nty * ntz * 512ull;
+    unsigned long long maxkey = (unsigned long long)c.nbox * BOXC;
     int endbit = 1;
     while ((1ull << endbit) < maxkey) ++endbit;
     CK(cub::DeviceRadixSort::SortPairs(tmp, cubb, k0, k1, i0, i1, (int)n, 0, endbit, c.stream));
+    k_box_start<<<pgrid(n), PB, 0, c.stream>>>(k1, n, c.nbox, c.box_start);
+    CKL();
     PView dst{c.pv_alt, c.cap};
     k_permute<<<pgrid(n * 20), PB, 0, c.stream>>>(c.pv, dst, n, i1);
     CKL();
     std::swap(c.pv.base, c.pv_alt);
+    c.n_box = n;
 }
 
 }  // namespace epic
