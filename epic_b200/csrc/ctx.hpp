@@ -92,6 +92,7 @@ struct Ctx {
     int n_work = 0;
     double* work = nullptr;
     FFTPlan px, py;
+    bool use_plane_fft = true;   // 2-D plane kernel where the grid allows it
     Tables T;
     StepScalars* dsc = nullptr;     // device
     StepScalars* hsc = nullptr;     // pinned host mirror

@@ -174,6 +174,246 @@ __global__ void __launch_bounds__(256) k_fft_lines(FFTBatch B) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// 2-D plane FFT: one CTA transforms one (field, z) plane of an n x n grid
+// (n = 16 .. 128) held in shared memory as P[ix * S + iy], S = n + 2.  The y
+// pass transforms the line pairs (rows 2p, 2p+1) and the x pass the column
+// pairs (2q, 2q+1), two real lines packed as one complex line, with the same
+// Hermitian storage and 1/sqrt(n) scaling as k_fft_lines.  A complex line of
+// length N = N1 * N2 is done by N2 threads of one warp: a radix-N1 DFT in
+// registers over n1 (stride N2), the twiddles W_N^(t k1), an exchange through
+// the line's own storage, and a radix-N2 DFT in registers; only warp-level
+// synchronisation inside a pass.
+struct C2 {
+    double x, y;
+};
+EPIC_DEV C2 c2(double a, double b) { C2 r; r.x = a; r.y = b; return r; }
+EPIC_DEV C2 operator+(C2 a, C2 b) { return c2(a.x + b.x, a.y + b.y); }
+EPIC_DEV C2 operator-(C2 a, C2 b) { return c2(a.x - b.x, a.y - b.y); }
+EPIC_DEV C2 cmulw(C2 a, C2 w) { return c2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); }
+
+// exp(-2 pi i j / 16): cos(pi/8), sin(pi/8) and sqrt(1/2) rounded to double
+constexpr double FC1 = 0.92387953251128674, FS1 = 0.38268343236508978, FR2 = 0.70710678118654757;
+EPIC_DEV double w16c(int j) {
+    const double c[16] = {1.0, FC1, FR2, FS1, 0.0, -FS1, -FR2, -FC1, -1.0, -FC1, -FR2, -FS1, 0.0, FS1, FR2, FC1};
+    return c[j & 15];
+}
+// a * exp(-2 pi i j / 16) with the quarter turns done exactly
+EPIC_DEV C2 rot16(C2 a, int j) {
+    j &= 15;
+    if (j == 0) return a;
+    if (j == 4) return c2(a.y, -a.x);
+    if (j == 8) return c2(-a.x, -a.y);
+    if (j == 12) return c2(-a.y, a.x);
+    return cmulw(a, c2(w16c(j), -w16c((j + 12) & 15)));
+}
+
+constexpr int bitrev_c(int i, int n) {
+    int r = 0;
+    for (int b = 1; b < n; b <<= 1) { r = (r << 1) | (i & 1); i >>= 1; }
+    return r;
+}
+
+// Forward DFT of N <= 16 values in registers (natural order in and out).
+template <int N>
+EPIC_DEV void fft_reg(C2 (&v)[N]) {
+#pragma unroll
+    for (int half = N / 2; half >= 1; half >>= 1) {
+#pragma unroll
+        for (int blk = 0; blk < N; blk += 2 * half) {
+#pragma unroll
+            for (int j = 0; j < half; ++j) {
+                C2 a = v[blk + j], b = v[blk + j + half];
+                v[blk + j] = a + b;
+                v[blk + j + half] = rot16(a - b, j * (16 / (2 * half)));
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const int r = bitrev_c(i, N);
+        if (r > i) { C2 t = v[i]; v[i] = v[r]; v[r] = t; }
+    }
+}
+
+template <int N> struct Radix;
+template <> struct Radix<16> { static constexpr int N1 = 4, N2 = 4; };
+template <> struct Radix<32> { static constexpr int N1 = 8, N2 = 4; };
+template <> struct Radix<64> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct Radix<128> { static constexpr int N1 = 16, N2 = 8; };
+
+// Line geometry inside the plane: real element c of line a at P[a0 + c*es],
+// of line b at P[a0 + c*es + bo]; complex scratch element c at P[s0 + c*cs].
+struct LineGeo {
+    int a0, es, bo, s0, cs;
+};
+
+template <int N, bool FWD>
+EPIC_DEV void line_fft(double* P, const LineGeo g, int t, const C2* tw, double scale) {
+    constexpr int N1 = Radix<N>::N1, N2 = Radix<N>::N2, KPT = N1 / N2, H = N / 2;
+    C2 v[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) {
+        const int c = t + N2 * m;
+        if (FWD) {
+            v[m] = c2(P[g.a0 + c * g.es], P[g.a0 + c * g.es + g.bo]);
+        } else {
+            // conj(A + i B) from the Hermitian lines a, b
+            double ra, ia, rb, ib;
+            if (c == 0 || c == H) {
+                ra = P[g.a0 + c * g.es]; ia = 0.0;
+                rb = P[g.a0 + c * g.es + g.bo]; ib = 0.0;
+            } else if (c < H) {
+                ra = P[g.a0 + c * g.es]; ia = P[g.a0 + (N - c) * g.es];
+                rb = P[g.a0 + c * g.es + g.bo]; ib = P[g.a0 + (N - c) * g.es + g.bo];
+            } else {
+                ra = P[g.a0 + (N - c) * g.es]; ia = -P[g.a0 + c * g.es];
+                rb = P[g.a0 + (N - c) * g.es + g.bo]; ib = -P[g.a0 + c * g.es + g.bo];
+            }
+            v[m] = c2(ra - ib, -(ia + rb));
+        }
+    }
+    fft_reg<N1>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulw(v[k1], tw[t * k1]);
+    __syncwarp();
+    C2* sc = reinterpret_cast<C2*>(P + g.s0);
+    const int cs2 = g.cs / 2;   // scratch stride in complex elements
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) sc[(k1 * N2 + t) * cs2] = v[k1];
+    __syncwarp();
+    C2 y[KPT][N2];
+#pragma unroll
+    for (int e = 0; e < KPT; ++e)
+#pragma unroll
+        for (int t2 = 0; t2 < N2; ++t2) y[e][t2] = sc[((t * KPT + e) * N2 + t2) * cs2];
+#pragma unroll
+    for (int e = 0; e < KPT; ++e) fft_reg<N2>(y[e]);
+    __syncwarp();
+    if (FWD) {
+        // natural order into the scratch, then split into the two real lines
+#pragma unroll
+        for (int e = 0; e < KPT; ++e)
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) sc[(t * KPT + e + N1 * k2) * cs2] = y[e][k2];
+        __syncwarp();
+        constexpr int KU = H / N2 + 1;
+        C2 zk[KU], zn[KU];
+#pragma unroll
+        for (int j = 0; j < KU; ++j) {
+            const int k = t + N2 * j;
+            if (k <= H) {
+                zk[j] = sc[k * cs2];
+                zn[j] = sc[((N - k) & (N - 1)) * cs2];
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < KU; ++j) {
+            const int k = t + N2 * j;
+            if (k <= H) {
+                P[g.a0 + k * g.es] = 0.5 * (zk[j].x + zn[j].x) * scale;
+                P[g.a0 + k * g.es + g.bo] = 0.5 * (zk[j].y + zn[j].y) * scale;
+                if (k > 0 && k < H) {
+                    P[g.a0 + (N - k) * g.es] = 0.5 * (zk[j].y - zn[j].y) * scale;
+                    P[g.a0 + (N - k) * g.es + g.bo] = 0.5 * (zn[j].x - zk[j].x) * scale;
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < KPT; ++e)
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) {
+                const int k = t * KPT + e + N1 * k2;
+                P[g.a0 + k * g.es] = y[e][k2].x * scale;
+                P[g.a0 + k * g.es + g.bo] = -y[e][k2].y * scale;
+            }
+    }
+    __syncwarp();
+}
+
+struct PlaneBatch {
+    const double* in[MAXF];
+    double* out[MAXF];
+    const double2* tw;   // exp(-2 pi i m / n)
+    int ny, nzh;
+    double scale;        // 1 / sqrt(n), applied per pass
+};
+
+// fftxyp2s (FWD: y then x) / fftxys2p (x then y) of plane z = blockIdx.x of
+// field blockIdx.y, rows z = 0 .. nz.
+template <int N, bool FWD>
+__global__ void __launch_bounds__((N / 2) * Radix<N>::N2) k_fft_plane(PlaneBatch B) {
+    constexpr int S = N + 2, N2 = Radix<N>::N2;
+    extern __shared__ double P[];
+    __shared__ C2 tw[N];
+    const int z = blockIdx.x;
+    const double* in = B.in[blockIdx.y];
+    double* out = B.out[blockIdx.y];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = c2(B.tw[i].x, B.tw[i].y);
+    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+        const int ix = idx / N, iy = idx - ix * N;
+        P[ix * S + iy] = in[((long long)ix * B.ny + iy) * B.nzh + 1 + z];
+    }
+    __syncthreads();
+    const int line = threadIdx.x / N2, t = threadIdx.x - line * N2;
+    // y lines: rows 2p, 2p+1; x lines: columns 2q, 2q+1 (complex pairs)
+    const LineGeo gy = {2 * line * S, 1, S, 2 * line * S, 2};
+    const LineGeo gx = {2 * line, S, 1, 2 * line, S};
+    if (FWD) {
+        line_fft<N, true>(P, gy, t, tw, B.scale);
+        __syncthreads();
+        line_fft<N, true>(P, gx, t, tw, B.scale);
+    } else {
+        line_fft<N, false>(P, gx, t, tw, B.scale);
+        __syncthreads();
+        line_fft<N, false>(P, gy, t, tw, B.scale);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+        const int ix = idx / N, iy = idx - ix * N;
+        out[((long long)ix * B.ny + iy) * B.nzh + 1 + z] = P[ix * S + iy];
+    }
+}
+
+template <int N>
+static void launch_plane(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
+    constexpr int S = N + 2;
+    PlaneBatch B;
+    for (int f = 0; f < nf; ++f) { B.in[f] = in[f]; B.out[f] = out[f]; }
+    B.tw = c.px.tw;
+    B.ny = c.P.ny;
+    B.nzh = c.P.nzh;
+    B.scale = 1.0 / std::sqrt((double)N);
+    size_t sm = sizeof(double) * (size_t)N * S;
+    dim3 grid(c.P.nz + 1, nf);
+    int threads = (N / 2) * Radix<N>::N2;
+    prof_begin(c, "fft");
+    if (forward) {
+        CK(cudaFuncSetAttribute(k_fft_plane<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fft_plane<N, true><<<grid, threads, sm, c.stream>>>(B);
+    } else {
+        CK(cudaFuncSetAttribute(k_fft_plane<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fft_plane<N, false><<<grid, threads, sm, c.stream>>>(B);
+    }
+    CKL();
+    prof_end(c, "fft");
+}
+
+// Plane kernel sizes: square n x n grids with n = 16, 32, 64, 128.
+static bool plane_fft(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
+    const Params& P = c.P;
+    if (P.nx != P.ny) return false;
+    switch (P.nx) {
+        case 16: launch_plane<16>(c, in, out, nf, forward); return true;
+        case 32: launch_plane<32>(c, in, out, nf, forward); return true;
+        case 64: launch_plane<64>(c, in, out, nf, forward); return true;
+        case 128: launch_plane<128>(c, in, out, nf, forward); return true;
+        default: return false;
+    }
+}
+
 static void make_plan(FFTPlan& p, int n, cudaStream_t st) {
     p.n = n;
     p.nfac = 0;
@@ -233,6 +473,7 @@ static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* cons
 void fft_xy(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
     for (int f0 = 0; f0 < nf; f0 += MAXF) {
         int k = std::min(MAXF, nf - f0);
+        if (c.use_plane_fft && plane_fft(c, in + f0, out + f0, k, forward)) continue;
         if (forward) {
             run_fft_axis(c, c.py, 1, in + f0, out + f0, k, true);
             run_fft_axis(c, c.px, 0, out + f0, out + f0, k, true);

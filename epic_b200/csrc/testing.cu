@@ -62,3 +62,9 @@ extern "C" int epic_gpu_test_diverge(epic_ctx* ctx, const double* phi, double* g
     }
     return EPIC_OK;
 }
+
+extern "C" int epic_gpu_test_set_fft_path(epic_ctx* ctx, int plane) {
+    if (!ctx) return EPIC_ERR_ARG;
+    ctx->c.use_plane_fft = plane != 0;
+    return EPIC_OK;
+}

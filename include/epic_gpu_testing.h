@@ -25,6 +25,12 @@ struct epic_ctx;
  * with the halo rows extrapolated like apply_laplace. */
 int epic_gpu_test_diverge(struct epic_ctx* ctx, const double* phi, double* grad);
 
+/* Selects the horizontal FFT implementation of the context: plane != 0 the
+ * 2-D plane kernel (square grids of 16, 32, 64 or 128 points), 0 the batched
+ * line kernels (any even size with factors 2, 3, 5).  Both compute
+ * fftxyp2s / fftxys2p (sta3dfft.f90:134-257). */
+int epic_gpu_test_set_fft_path(struct epic_ctx* ctx, int plane);
+
 #ifdef __cplusplus
 }
 #endif
