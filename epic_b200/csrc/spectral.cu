@@ -20,6 +20,7 @@
 #include <cstring>
 #include <initializer_list>
 #include <utility>
+#include <type_traits>
 
 namespace epic {
 
@@ -524,22 +525,51 @@ EPIC_DEV void col_store(double* f, const double* xs, int c0, const ColArgs& A) {
 EPIC_DEV double tabv(const double* t, int c, int j, const ColArgs& A) {
     return t[(long long)c * A.nzh + 1 + j];
 }
-// ys[k] = sum_{j=lo..hi} M[k][j] xs[j] for k = lo..hi (M row-major (nz+1)^2)
-EPIC_DEV void col_matvec(const double* M, int lo, int hi, const double* xs, double* ys, int nz) {
-    int col = threadIdx.x & 31;
-    int grp = threadIdx.x >> 5;
-    int ngrp = blockDim.x >> 5;
-    for (int k = lo + grp; k <= hi; k += ngrp) {
-        const double* row = M + (long long)k * (nz + 1);
-        double s = 0.0;
-        for (int j = lo; j <= hi; ++j) s = fma(row[j], xs[j * CP + col], s);
-        ys[k * CP + col] = s;
+// ys[k] = sum_{j=lo..hi} M[k][j] xs[j] for k = lo..hi (M row-major (nz+1)^2),
+// all 32 columns of a CTA (256 threads), register tiled: thread (rg, cg)
+// computes rows lo + rg + 32 r (r < R) of columns 4 cg .. 4 cg + 3, 20 FMAs
+// per 9 loads.  ADD accumulates into ys instead of overwriting.
+template <int R, bool ADD>
+EPIC_DEV void col_matvec_t(const double* __restrict__ M, int lo, int hi, const double* xs, double* ys, int nz) {
+    const int nzp = nz + 1;
+    const int cg = threadIdx.x & 7, rg = threadIdx.x >> 3;
+    double acc[R][4];
+    int krow[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        krow[r] = min(lo + rg + 32 * r, hi) * nzp;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
+    }
+    for (int j = lo; j <= hi; ++j) {
+        const double* xr = xs + j * CP + 4 * cg;
+        double x0 = xr[0], x1 = xr[1], x2 = xr[2], x3 = xr[3];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double m = __ldg(M + krow[r] + j);
+            acc[r][0] = fma(m, x0, acc[r][0]);
+            acc[r][1] = fma(m, x1, acc[r][1]);
+            acc[r][2] = fma(m, x2, acc[r][2]);
+            acc[r][3] = fma(m, x3, acc[r][3]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lo + rg + 32 * r;
+        if (k <= hi) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                double* o = ys + k * CP + 4 * cg + q;
+                *o = ADD ? *o + acc[r][q] : acc[r][q];
+            }
+        }
     }
 }
 
 // field_decompose_semi_spectral (inversion_utils.f90:370-401), optionally
 // followed by the Hou-Li filter and/or preceded by central_diffz_semi_spectral
 // (inversion_utils.f90:460-480).  mode bit 1: filter, bit 2: central diff.
+template <int R>
 __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
     extern __shared__ double sm[];
     int nzp = A.nz + 1, nz = A.nz;
@@ -571,7 +601,7 @@ __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
         xs[j * CP + col] = xs[j * CP + col] - (xs[col] * tabv(phim, c, j, A) + xs[nz * CP + col] * tabv(phip, c, j, A));
     }
     __syncthreads();
-    col_matvec(A.mdst, 1, nz - 1, xs, ys, nz);
+    col_matvec_t<R, false>(A.mdst, 1, nz - 1, xs, ys, nz);
     for (int col = threadIdx.x; col < CT; col += blockDim.x) {
         ys[col] = xs[col];
         ys[nz * CP + col] = xs[nz * CP + col];
@@ -589,6 +619,7 @@ __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
 }
 
 // field_combine_semi_spectral (inversion_utils.f90:421-456)
+template <int R>
 __global__ void __launch_bounds__(256) k_col_combine(ColArgs A) {
     extern __shared__ double sm[];
     int nzp = A.nz + 1, nz = A.nz;
@@ -599,7 +630,7 @@ __global__ void __launch_bounds__(256) k_col_combine(ColArgs A) {
     const double* phip = A.tab[1];
     col_load(A.in[blockIdx.y], xs, c0, A);
     __syncthreads();
-    col_matvec(A.mdst, 1, nz - 1, xs, ys, nz);
+    col_matvec_t<R, false>(A.mdst, 1, nz - 1, xs, ys, nz);
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx % CT, j = idx / CT;
@@ -616,6 +647,7 @@ __global__ void __launch_bounds__(256) k_col_combine(ColArgs A) {
 
 // Vertical-velocity solve of vor2vel (inversion.f90:97-150): in[0] = D
 // (source) -> out[0] = w (semi-spectral), out[1] = dw/dz part es.
+template <int R>
 __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
     extern __shared__ double sm[];
     int nzp = A.nz + 1, nz = A.nz;
@@ -652,25 +684,11 @@ __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
         }
     }
     __syncthreads();
-    // dct(as) -> into bs? keep bs; use es-add directly: es += DCT(as)
-    {
-        int col = threadIdx.x & 31, grp = threadIdx.x >> 5, ngrp = blockDim.x >> 5;
-        for (int k = grp; k <= nz; k += ngrp) {
-            const double* row = A.mdct + (long long)k * nzp;
-            double s = 0.0;
-            for (int j = 0; j <= nz; ++j) s = fma(row[j], as[j * CP + col], s);
-            es[k * CP + col] = es[k * CP + col] + s;
-        }
-        __syncthreads();
-        // dst(ds(1:nz-1)) into as rows 1..nz-1
-        for (int k = 1 + grp; k <= nz - 1; k += ngrp) {
-            const double* row = A.mdst + (long long)k * nzp;
-            double s = 0.0;
-            for (int j = 1; j <= nz - 1; ++j) s = fma(row[j], ds[j * CP + col], s);
-            as[k * CP + col] = s;
-        }
-        __syncthreads();
-    }
+    // es += DCT(as); then as(1:nz-1) = DST(ds(1:nz-1))
+    col_matvec_t<R, true>(A.mdct, 0, nz, as, es, nz);
+    __syncthreads();
+    col_matvec_t<R, false>(A.mdst, 1, nz - 1, ds, as, nz);
+    __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx % CT, j = idx / CT;
         ds[j * CP + col] = (j >= 1 && j <= nz - 1) ? as[j * CP + col] + bs[j * CP + col] : 0.0;
@@ -1064,14 +1082,39 @@ static void halo(Ctx& c, std::initializer_list<std::pair<double*, int>> list) {
 
 static size_t col_smem(const Ctx& c, int arrays) { return sizeof(double) * (size_t)arrays * (c.P.nz + 1) * CP; }
 
+// Rows per thread of the tiled column matvec: ceil((nz + 1) / 32), nz <= 511.
+static int col_rows(const Params& P) {
+    int R = (P.nz + 1 + 31) / 32;
+    if (R > 16) throw CudaError(EPIC_ERR_CONFIG, "nz larger than 511 is not supported");
+    return R;
+}
+
+// Calls f(std::integral_constant<int, R'>{}) with R' >= R.
+template <typename F>
+static void with_rows(int R, F&& f) {
+    switch (R) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 3: f(std::integral_constant<int, 3>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        case 5: f(std::integral_constant<int, 5>{}); break;
+        case 6: f(std::integral_constant<int, 6>{}); break;
+        case 7: f(std::integral_constant<int, 7>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        default: f(std::integral_constant<int, 16>{}); break;
+    }
+}
+
 static void col_decompose(Ctx& c, const double* const* in, double* const* out, int nf, int mode) {
     ColArgs A = col_args(c);
     A.tab[0] = c.T.phim; A.tab[1] = c.T.phip; A.tab[2] = c.T.filt;
     for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
     size_t sm = col_smem(c, 2);
-    CK(cudaFuncSetAttribute(k_col_decompose, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_col_decompose<<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A, mode);
-    CKL();
+    with_rows(col_rows(c.P), [&](auto R) {
+        CK(cudaFuncSetAttribute(k_col_decompose<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_col_decompose<R><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A, mode);
+        CKL();
+    });
 }
 
 static void col_combine(Ctx& c, const double* const* in, double* const* out, int nf) {
@@ -1079,9 +1122,11 @@ static void col_combine(Ctx& c, const double* const* in, double* const* out, int
     A.tab[0] = c.T.phim; A.tab[1] = c.T.phip;
     for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
     size_t sm = col_smem(c, 2);
-    CK(cudaFuncSetAttribute(k_col_combine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_col_combine<<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A);
-    CKL();
+    with_rows(col_rows(c.P), [&](auto R) {
+        CK(cudaFuncSetAttribute(k_col_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_col_combine<R><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A);
+        CKL();
+    });
 }
 
 void vor2vel(Ctx& c) {
@@ -1113,11 +1158,13 @@ void vor2vel(Ctx& c) {
     CKL();
     // vorticity in physical space (inversion.f90:91-93); halo rows keep the
     // par2grid extrapolation, as in the reference
+    // (combine(svor_z) is cs from above: svor_z is unchanged since)
     {
-        double* tmp[3] = {c.w(10), c.w(11), c.w(12)};
-        col_combine(c, sv, tmp, 3);
+        double* tmp[2] = {c.w(10), c.w(11)};
+        col_combine(c, sv, tmp, 2);
+        const double* inv[3] = {tmp[0], tmp[1], cs};
         double* outv[3] = {c.vortg(0), c.vortg(1), c.vortg(2)};
-        fft_xy(c, tmp, outv, 3, false);
+        fft_xy(c, inv, outv, 3, false);
     }
     // vertical velocity (inversion.f90:97-150)
     S.in[0] = sv[1]; S.in[1] = sv[0]; S.out[0] = ds;
@@ -1131,12 +1178,12 @@ void vor2vel(Ctx& c) {
         A.out[0] = c.w(9);
         A.out[1] = es;
         size_t sm = col_smem(c, 4);
-        CK(cudaFuncSetAttribute(k_col_wsolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_col_wsolve<<<(A.ncol + CT - 1) / CT, 256, sm, c.stream>>>(A);
-        CKL();
-        const double* in[1] = {sv[2]};
-        double* out[1] = {cs};
-        col_combine(c, in, out, 1);
+        with_rows(col_rows(c.P), [&](auto R) {
+            CK(cudaFuncSetAttribute(k_col_wsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_col_wsolve<R><<<(A.ncol + CT - 1) / CT, 256, sm, c.stream>>>(A);
+            CKL();
+        });
+        // cs = combine(svor_z) still holds (inversion.f90:150)
     }
     // mean flow (inversion.f90:158-176)
     double* zbuf = c.w(13);   // first 2 (nz+1) entries used as scratch
