@@ -197,7 +197,7 @@ static void free_ctx(Ctx& c) {
     c.prof.ev.clear();
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
-                    c.dvor_bar, c.box_start};
+                    c.dvor_bar, c.box_start, c.gpack};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.scratch) cudaFree(c.scratch);
@@ -272,6 +272,7 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         CK(cudaMallocHost(&c.hsc, sizeof(StepScalars)));
         CK(cudaMalloc(&c.partials, sizeof(double) * 148 * 8 * 64));
         CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)stage_grid_max(P, c.cap)));
+        CK(cudaMalloc(&c.gpack, sizeof(double) * 16 * (size_t)P.fsz));
         if (!cfg->keep_order) {
             CK(cudaMalloc(&c.pv_alt, sizeof(double) * (size_t)N_ATTR * c.cap));
             c.nbox = box_count(P);

@@ -93,6 +93,7 @@ struct Ctx {
     double* work = nullptr;
     FFTPlan px, py;
     bool use_plane_fft = true;   // 2-D plane kernel where the grid allows it
+    double* gpack = nullptr;     // gathered fields, 16 doubles per grid point
     Tables T;
     StepScalars* dsc = nullptr;     // device
     StepScalars* hsc = nullptr;     // pinned host mirror

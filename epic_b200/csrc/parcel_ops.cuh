@@ -94,6 +94,7 @@ struct ScatterFields {
 
 struct GatherFields {
     const double* f[14];   // velog 3, velgradg 8, vtend 3
+    const double* pack;    // the same, 16 doubles per grid point (fused stage)
 };
 
 struct StageArgs {

@@ -254,6 +254,7 @@ static GatherFields gather_fields(Ctx& c) {
     for (int k = 0; k < 3; ++k) G.f[k] = c.velog(k);
     for (int k = 0; k < 8; ++k) G.f[3 + k] = c.velgrad(k);
     for (int k = 0; k < 3; ++k) G.f[11 + k] = c.vtend(k);
+    G.pack = nullptr;
     return G;
 }
 

@@ -410,6 +410,58 @@ struct FusedArgs {
     double ca, cb;
 };
 
+// The 14 gathered fields (velog 3, velgradg 8, vtend 3) of a grid point as
+// one 128-byte record: a trilinear corner is one cache line, read with 7
+// 16-byte loads at constant offsets.
+constexpr int GREC = 16;
+
+__global__ void k_pack_gather(GatherFields G, double* pack, long long fsz) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < fsz * (GREC / 2);
+         e += (long long)gridDim.x * blockDim.x) {
+        long long g = e >> 3;
+        int l2 = (int)(e & 7);
+        double2 v = make_double2(0.0, 0.0);
+        if (l2 < 7) v = make_double2(G.f[2 * l2][g], G.f[2 * l2 + 1][g]);
+        reinterpret_cast<double2*>(pack)[e] = v;
+    }
+}
+
+// Corner x/y indices wrapped into the grid; support points lie within a
+// cell or two of the domain, so the modulo is rarely needed.
+EPIC_DEV int wrap_near(int i, int n) {
+    if (i < 0) i += n;
+    else if (i >= n) i -= n;
+    return ((unsigned)i < (unsigned)n) ? i : wrapi(i, n);
+}
+
+// g[l] += sum over the 8 corners of (w / 4) f_l (interpl.f90:17-56, the
+// point weight 1/4 of parcel_interpl.f90:433).  Returns false when the
+// point leaves the vertical halo.
+EPIC_DEV bool gather_point(const Params& P, const double* __restrict__ pack, const double* pt, double* g) {
+    Tri t = trilinear(P, pt);
+    if (t.ks < -1 || t.ks > P.nz) return false;
+    const int i0 = wrap_near(t.is, P.nx), i1 = wrap_near(t.is + 1, P.nx);
+    const int j0 = wrap_near(t.js, P.ny), j1 = wrap_near(t.js + 1, P.ny);
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+            const long long a = fidx(P, t.ks, jj ? j1 : j0, ii ? i1 : i0);
+            const double2* q = reinterpret_cast<const double2*>(pack + a * GREC);
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {
+                const double w = 0.25 * t.w[kk][jj][ii];
+#pragma unroll
+                for (int l2 = 0; l2 < 7; ++l2) {
+                    const double2 v = __ldg(q + kk * (GREC / 2) + l2);
+                    g[2 * l2] = fma(w, v.x, g[2 * l2]);
+                    g[2 * l2 + 1] = fma(w, v.y, g[2 * l2 + 1]);
+                }
+            }
+        }
+    return true;
+}
+
 template <bool DIAG, bool SCATTER>
 __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long n, Boxes B, GatherFields G,
                                                   Fields7 F, int* nparg, int* nsparg, FusedArgs S,
@@ -446,11 +498,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                     double pt[3];
 #pragma unroll
                     for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-                    Tri t = trilinear(P, pt);
-                    long long a[2][2];
-                    if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
-#pragma unroll
-                    for (int l = 0; l < 14; ++l) g[l] += 0.25 * csum(G.f[l], t, a);
+                    if (!gather_point(P, G.pack, pt, g)) set_err(err, ERRB_ZRANGE);
                 }
             }
             double b[5];
@@ -647,6 +695,9 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     for (int k = 0; k < 3; ++k) G.f[k] = c.velog(k);
     for (int k = 0; k < 8; ++k) G.f[3 + k] = c.velgrad(k);
     for (int k = 0; k < 3; ++k) G.f[11 + k] = c.vtend(k);
+    G.pack = c.gpack;
+    k_pack_gather<<<pgrid(c.P.fsz * (GREC / 2)), PB, 0, c.stream>>>(G, c.gpack, c.P.fsz);
+    CKL();
     if (scatter) zero_p2g_fields(c);
     Boxes B = boxes(c);
     int g = sgrid(c, B);
