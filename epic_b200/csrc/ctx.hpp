@@ -94,6 +94,9 @@ struct Ctx {
     FFTPlan px, py;
     bool use_plane_fft = true;   // 2-D plane kernel where the grid allows it
     double* gpack = nullptr;     // gathered fields, 16 doubles per grid point
+    // log2 of the consecutive parcels a lane group scatters (vol2grid,
+    // par2grid, fused stage)
+    int scatter_lg[3] = {1, 1, 0};
     Tables T;
     StepScalars* dsc = nullptr;     // device
     StepScalars* hsc = nullptr;     // pinned host mirror

@@ -932,26 +932,51 @@ __global__ void k_vtend_rows(FluxArgs A, Ptr8 divxy, MPtr8 vt, double dzi, doubl
     }
 }
 
-// lapinv1 (inversion_utils.f90:567-589), one thread per column; the (0,0)
-// column is zero (inversion.f90:423-426 and inversion_utils.f90:584-587).
-__global__ void k_lapinv(double* fs, const double* etdv, const double* htdv, double ap, int ncol, int nz, int nzh) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncol) return;
-    double* f = fs + (long long)c * nzh + 1;
-    const double* e = etdv + (long long)c * nzh + 1;
-    const double* h = htdv + (long long)c * nzh + 1;
-    if (c == 0) {
-        for (int iz = 0; iz <= nz; ++iz) f[iz] = 0.0;
-        return;
+// lapinv1 (inversion_utils.f90:567-589): Thomas solve per (kx, ky) column;
+// the (0,0) column is zero (inversion.f90:423-426, inversion_utils.f90:584-587).
+// A CTA stages 32 columns of f and of the two tables in shared memory with
+// coalesced loads; one warp then solves its 32 columns, one lane each.
+EPIC_DEV void cols_load(const double* f, double* xs, int c0, int ncol, int nzp, int nzh) {
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx / nzp, j = idx - col * nzp;
+        int c = c0 + col;
+        xs[j * CP + col] = (c < ncol) ? f[(long long)c * nzh + 1 + j] : 0.0;
     }
-    double prev = f[0] * h[0];
-    f[0] = prev;
-    for (int iz = 1; iz <= nz - 1; ++iz) {
-        prev = (f[iz] - ap * prev) * h[iz];
-        f[iz] = prev;
+}
+
+__global__ void __launch_bounds__(256) k_lapinv(double* fs, const double* etdv, const double* htdv, double ap,
+                                               int ncol, int nz, int nzh) {
+    extern __shared__ double sm[];
+    const int nzp = nz + 1;
+    double* f = sm;
+    double* e = sm + nzp * CP;
+    double* h = sm + 2 * nzp * CP;
+    const int c0 = blockIdx.x * CT;
+    cols_load(fs, f, c0, ncol, nzp, nzh);
+    cols_load(etdv, e, c0, ncol, nzp, nzh);
+    cols_load(htdv, h, c0, ncol, nzp, nzh);
+    __syncthreads();
+    if (threadIdx.x < CT) {
+        const int col = threadIdx.x, c = c0 + col;
+        if (c == 0) {
+            for (int iz = 0; iz <= nz; ++iz) f[iz * CP + col] = 0.0;
+        } else if (c < ncol) {
+            double prev = f[col] * h[col];
+            f[col] = prev;
+            for (int iz = 1; iz <= nz - 1; ++iz) {
+                prev = (f[iz * CP + col] - ap * prev) * h[iz * CP + col];
+                f[iz * CP + col] = prev;
+            }
+            f[nz * CP + col] = (f[nz * CP + col] - 2.0 * ap * prev) * h[nz * CP + col];
+            for (int iz = nz - 1; iz >= 0; --iz) f[iz * CP + col] = e[iz * CP + col] * f[(iz + 1) * CP + col] + f[iz * CP + col];
+        }
     }
-    f[nz] = (f[nz] - 2.0 * ap * prev) * h[nz];
-    for (int iz = nz - 1; iz >= 0; --iz) f[iz] = e[iz] * f[iz + 1] + f[iz];
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
+        int col = idx / nzp, j = idx - col * nzp;
+        int c = c0 + col;
+        if (c < ncol) fs[(long long)c * nzh + 1 + j] = f[j * CP + col];
+    }
 }
 
 // phi = volg * vcelli - 1 (parcel_correction.f90:158)
@@ -1254,7 +1279,9 @@ void diverge_laplace(Ctx& c, double* phi, double* grad[3]) {
     double* out[1] = {ds};
     fft_xy(c, in, out, 1, true);
     int ncol = P.nx * P.ny;
-    k_lapinv<<<(ncol + 127) / 128, 128, 0, c.stream>>>(ds, c.T.etdv, c.T.htdv, P.ap, ncol, P.nz, P.nzh);
+    size_t lsm = col_smem(c, 3);
+    CK(cudaFuncSetAttribute(k_lapinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    k_lapinv<<<(ncol + CT - 1) / CT, 256, lsm, c.stream>>>(ds, c.T.etdv, c.T.htdv, P.ap, ncol, P.nz, P.nzh);
     CKL();
     SpecArgs S = spec_args(c);
     S.in[0] = ds;

@@ -339,19 +339,25 @@ EPIC_DEV void count_parcel(const Params& P, const double* pos, double vol, int* 
 template <int NF>
 EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long long q1, const WinShared<NF>* ws,
                             unsigned* acc, const Fields7& F, int* nparg, int* nsparg, bool reuse, bool store,
-                            unsigned* err) {
+                            int lg, unsigned* err) {
     const Window W = ws->W;
     double scale[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) scale[f] = ws->scale[f];
-    // The 32 lanes of a warp take parcels about cnt/32 apart (different cells
-    // of the box), so that the addresses of one shared-memory atomic spread
-    // over the banks; consecutive parcels of one cell would pile onto few.
-    const int cnt = (int)(q1 - q0), S = (cnt + 31) >> 5;
-    const int lane = threadIdx.x & 31;
+    // The lanes of a warp take groups of 2^lg consecutive parcels spaced about
+    // cnt/32 * 2^lg apart (different cells of the box), so that the addresses
+    // of one shared-memory atomic spread over the banks (consecutive parcels
+    // of one cell would pile onto few), while a group still shares sectors
+    // of the parcel loads.
+    const int cnt = (int)(q1 - q0);
+    const int U = (cnt + (1 << lg) - 1) >> lg;          // groups
+    const int cols = 32 >> lg;                          // groups side by side in a warp
+    const int S = (U + cols - 1) / cols;                // groups per column
+    const int lane = threadIdx.x & 31, gi = lane >> lg, m = lane & ((1 << lg) - 1);
     for (int r = threadIdx.x >> 5; r < S; r += PB / 32) {
-        int slot = lane * S + r;
-        if (slot >= cnt) continue;
+        const int u = gi * S + r;
+        const int slot = (u << lg) + m;
+        if (u >= U || slot >= cnt) continue;
         long long i = q0 + slot;
         double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
         double eta[3], tau[3];
@@ -374,7 +380,8 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
 // par2grid scatter (NF = 7) and vol2grid (NF = 1).
 template <int NF>
 __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long long n, Boxes B, Fields7 F,
-                                                    int* nparg, int* nsparg, int reuse, int store, unsigned* err) {
+                                                    int* nparg, int* nsparg, int reuse, int store, int lg,
+                                                    unsigned* err) {
     extern __shared__ unsigned acc[];
     __shared__ WinShared<NF> ws;
     const Range R = cta_range(P, pv, B, n);
@@ -396,7 +403,7 @@ __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long lon
         __syncthreads();
         win_zero<NF>(acc, ws.W);
         __syncthreads();
-        scatter_round<NF>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, err);
+        scatter_round<NF>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, lg, err);
         __syncthreads();
         win_flush<NF>(P, acc, &ws, F);
         __syncthreads();
@@ -406,7 +413,7 @@ __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long lon
 // ---------------------------------------------------------------------------
 // Fused stage kernel.
 struct FusedArgs {
-    int stage, last;
+    int stage, last, lg;
     double ca, cb;
 };
 
@@ -581,7 +588,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
             win_zero<7>(acc, ws.W);
             __syncthreads();
             // pass B: support vectors of the advanced shape + next par2grid
-            scatter_round<7>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, false, true, err);
+            scatter_round<7>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, false, true, S.lg, err);
             __syncthreads();
             win_flush<7>(P, acc, &ws, F);
             __syncthreads();
@@ -664,7 +671,7 @@ void scatter_p2g(Ctx& c, bool reuse, bool store) {
     Boxes B = boxes(c);
     prof_begin(c, "p2g");
     k_scatter<7><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, fields7(c), c.nparg, c.nsparg, reuse, store,
-                                                     &c.dsc->err);
+                                                     c.scatter_lg[1], &c.dsc->err);
     CKL();
     prof_end(c, "p2g");
 }
@@ -677,7 +684,8 @@ void scatter_v2g(Ctx& c, bool reuse) {
     size_t sm = sizeof(unsigned) * 1 * NLIMB * WCAP;
     Boxes B = boxes(c);
     prof_begin(c, "v2g");
-    k_scatter<1><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, nullptr, nullptr, reuse, 1, &c.dsc->err);
+    k_scatter<1><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, nullptr, nullptr, reuse, 1,
+                                                     c.scatter_lg[0], &c.dsc->err);
     CKL();
     prof_end(c, "v2g");
 }
@@ -690,6 +698,7 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     S.last = stage == c.n_stages;
     S.ca = c.ca[stage - 1];
     S.cb = c.cb[stage - 1];
+    S.lg = c.scatter_lg[2];
     bool scatter = !S.last;
     GatherFields G;
     for (int k = 0; k < 3; ++k) G.f[k] = c.velog(k);

@@ -68,3 +68,12 @@ extern "C" int epic_gpu_test_set_fft_path(epic_ctx* ctx, int plane) {
     ctx->c.use_plane_fft = plane != 0;
     return EPIC_OK;
 }
+
+extern "C" int epic_gpu_test_set_scatter_groups(epic_ctx* ctx, int lg_vol2grid, int lg_par2grid, int lg_stage) {
+    if (!ctx) return EPIC_ERR_ARG;
+    int v[3] = {lg_vol2grid, lg_par2grid, lg_stage};
+    for (int k = 0; k < 3; ++k)
+        if (v[k] < 0 || v[k] > 5) return EPIC_ERR_ARG;
+    for (int k = 0; k < 3; ++k) ctx->c.scatter_lg[k] = v[k];
+    return EPIC_OK;
+}

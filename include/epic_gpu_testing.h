@@ -31,6 +31,11 @@ int epic_gpu_test_diverge(struct epic_ctx* ctx, const double* phi, double* grad)
  * fftxyp2s / fftxys2p (sta3dfft.f90:134-257). */
 int epic_gpu_test_set_fft_path(struct epic_ctx* ctx, int plane);
 
+/* Lane mapping of the scatter kernels: lanes take groups of 2^lg consecutive
+ * parcels (lg in 0..5) for vol2grid, par2grid and the fused stage.  Any
+ * setting computes the same sums; it only changes the memory access order. */
+int epic_gpu_test_set_scatter_groups(struct epic_ctx* ctx, int lg_vol2grid, int lg_par2grid, int lg_stage);
+
 #ifdef __cplusplus
 }
 #endif
