@@ -120,9 +120,14 @@ def reduce_timing(ms: float, work: float, device: str = "cuda"):
     return float(mx[0]), float(sm[1])
 
 
-def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int) -> float:
-    """Minimal compulsory DRAM bytes of one launch (FP64 plain)."""
+def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int, form: str = "plain") -> float:
+    """Minimal compulsory DRAM bytes of one launch."""
     gh = nx * ny * (nz + 3)
+    if kernel == "stage" and form == "mixed":
+        # state read: x3 V (FP64) + w3 B5 b q (FP32) = 72 B; accumulators
+        # dx3 (FP64) + dw3 dB5 (FP32) = 56 B read and written; state written:
+        # x3 (FP64) + w3 B5 (FP32) = 56 B.  Fields as in the plain form.
+        return (72 + 56 + 56 + 56) * n + 14 * 8.0 * gh + 7 * 8.0 * gh + 2 * 4.0 * gh
     if kernel == "p2g":
         # read x3 w3 B5 V b q per parcel; write 7 scattered fields + 2 int counts
         return 14 * 8.0 * n + 7 * 8.0 * gh + 2 * 4.0 * gh
@@ -156,9 +161,10 @@ def run_ours(args):
 
     setup = initial.config(args.workload)
     lib = epic_b200.load()
-    # the device keeps parcels ordered by 8^3-cell tiles (keep_order=0); the
+    # the device keeps parcels ordered by boxes of cells (keep_order=0); the
     # parcel set is the reference's, its storage order is not
-    ctx = epic_b200.make_context(setup, lib, keep_order=0)
+    mixed = args.form == "mixed"
+    ctx = epic_b200.make_context(setup, lib, keep_order=0, precision=1 if mixed else 0)
     import ctypes as C
     sp = C.c_void_p()
     lib.lib.epic_gpu_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
@@ -229,7 +235,7 @@ def run_ours(args):
     peak, peak_kind = peaks()
     avg_n = psteps / args.steps
     kavg_ms = kms.value / max(kl.value, 1)
-    alg = algorithmic_bytes(args.roofline_kernel, int(avg_n), setup.nx, setup.ny, setup.nz)
+    alg = algorithmic_bytes(args.roofline_kernel, int(avg_n), setup.nx, setup.ny, setup.nz, args.form)
     achieved = alg / (kavg_ms * 1e-3) / 1e9 if kl.value else None
     roofline = {"bound": "hbm", "kernel": args.roofline_kernel, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": (achieved / peak if achieved else None), "traffic": None,
@@ -283,17 +289,24 @@ def run_ours(args):
                "steps": args.e2e_steps, "wall_s": wall,
                "mode": "host-owned parcel container: set_parcels (pinned H2D) + step + get_parcels (D2H) every step"}
 
+    store_gb = int(setup.n) * (184 if mixed else 312) / 1e9
+    field_gb = 21 * 8 * setup.nx * setup.ny * (setup.nz + 3) / 1e9
+    precision = ("mixed: FP32 vorticity, B, buoyancy, humidity, delta_vor, delta_b, support vectors, "
+                 "par2grid sums and grid2par interpolation; FP64 positions, volume, delta_pos, B33 and fields"
+                 if mixed else "fp64-plain")
+    kind = "rising thermal" if args.workload.startswith("thermal") else "Beltrami flow"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: rising thermal, 128^3 grid, domain 6.28^3, 8 parcels/cell "
-                               "(16,777,216 parcels at t=0), seeded noise, plain FP64, merge/split/corrections on"
-                   if args.workload == "thermal-128" else args.workload,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64" if mixed else "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {kind}, {setup.nx}x{setup.ny}x{setup.nz} grid, "
+                               f"{int(setup.n):,} parcels at t=0, seeded, {args.form} form, "
+                               "merge/split/corrections on",
+                   "form": args.form,
                    "grid": [setup.nx, setup.ny, setup.nz], "parcels_at_start": int(setup.n),
-                   "parcels_range_timed": [int(nmin), int(nmax)], "precision": "fp64-plain",
+                   "parcels_range_timed": [int(nmin), int(nmax)], "precision": precision,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (parcel store 5.2 GB, fields 0.5 GB)"},
+                   "l2": f"inputs larger than L2 (parcel state {store_gb:.2f} GB, fields {field_gb:.2f} GB)"},
         "roofline": roofline,
         "clocks": clk,
         "e2e": e2e,
@@ -378,6 +391,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="thermal-128")
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
+                    help="plain FP64, or the mixed-precision form (FP32 attributes and interpolation)")
     ap.add_argument("--roofline-kernel", default="stage", choices=["stage", "p2g", "g2p", "fft"])
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of that kernel")
     ap.add_argument("--profile-kernels", default="", help="comma list of kernels to time over one extra step each")

@@ -92,7 +92,7 @@ __global__ void k_deinterleave(const double* src, int ncomp, long long n, PView 
          i += (long long)gridDim.x * blockDim.x) {
         long long p = i / ncomp;
         int k = (int)(i - p * ncomp);
-        pv.at(a0 + k, p) = src[i];
+        pv.set(a0 + k, p, src[i]);
     }
 }
 __global__ void k_interleave(double* dst, int ncomp, long long n, PView pv, int a0) {
@@ -100,7 +100,7 @@ __global__ void k_interleave(double* dst, int ncomp, long long n, PView pv, int 
          i += (long long)gridDim.x * blockDim.x) {
         long long p = i / ncomp;
         int k = (int)(i - p * ncomp);
-        dst[i] = pv.at(a0 + k, p);
+        dst[i] = pv.get(a0 + k, p);
     }
 }
 __global__ void k_int_to_double(const int* a, double* b, long long n) {
@@ -243,7 +243,7 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
     if (!cfg || !out) return EPIC_ERR_ARG;
     if (cfg->nx < 4 || cfg->ny < 4 || cfg->nz < 2 || cfg->nx % 2 || cfg->ny % 2) return EPIC_ERR_CONFIG;
     if (cfg->extent[0] <= 0 || cfg->extent[1] <= 0 || cfg->extent[2] <= 0) return EPIC_ERR_CONFIG;
-    if (cfg->precision != EPIC_PRECISION_FP64) return EPIC_ERR_CONFIG;
+    if (cfg->precision != EPIC_PRECISION_FP64 && cfg->precision != EPIC_PRECISION_MIXED) return EPIC_ERR_CONFIG;
     auto* ctx = new epic_ctx();
     Ctx& c = ctx->c;
     c.cfg = *cfg;
@@ -255,9 +255,11 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         const Params& P = c.P;
         c.cap = cfg->capacity > 0 ? cfg->capacity
                                   : (long long)(2.0 * (double)P.nx * P.ny * P.nz * std::max(1, cfg->n_per_cell)) + 1024;
+        c.cap = (c.cap + 63) & ~63LL;   // every slot starts on a 256-byte boundary
         c.pv.cap = c.cap;
-        CK(cudaMalloc(&c.pv.base, sizeof(double) * (size_t)N_ATTR * c.cap));
-        CK(cudaMemsetAsync(c.pv.base, 0, sizeof(double) * (size_t)N_ATTR * c.cap, c.stream));
+        c.pv.mixed = cfg->precision == EPIC_PRECISION_MIXED;
+        CK(cudaMalloc(&c.pv.base, c.store_bytes()));
+        CK(cudaMemsetAsync(c.pv.base, 0, c.store_bytes(), c.stream));
         CK(cudaMalloc(&c.fields, sizeof(double) * (size_t)N_FIELDS * P.fsz));
         CK(cudaMemsetAsync(c.fields, 0, sizeof(double) * (size_t)N_FIELDS * P.fsz, c.stream));
         CK(cudaMalloc(&c.nparg, sizeof(int) * P.fsz));
@@ -274,7 +276,7 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)stage_grid_max(P, c.cap)));
         CK(cudaMalloc(&c.gpack, sizeof(double) * 16 * (size_t)P.fsz));
         if (!cfg->keep_order) {
-            CK(cudaMalloc(&c.pv_alt, sizeof(double) * (size_t)N_ATTR * c.cap));
+            CK(cudaMalloc(&c.pv_alt, c.store_bytes()));
             c.nbox = box_count(P);
             CK(cudaMalloc(&c.box_start, sizeof(int) * ((size_t)c.nbox + 1)));
         }
@@ -315,7 +317,7 @@ int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const doub
     if (n > c.cap) throw CudaError(EPIC_ERR_CAPACITY, "set_parcels: more parcels than the device capacity");
     c.n = n;
     c.n_box = 0;
-    CK(cudaMemsetAsync(c.pv.base, 0, sizeof(double) * (size_t)N_ATTR * c.cap, c.stream));
+    CK(cudaMemsetAsync(c.pv.base, 0, c.store_bytes(), c.stream));
     upload_attr(c, pos, 3, A_X);
     upload_attr(c, vor, 3, A_VX);
     upload_attr(c, B, 5, A_B11);

@@ -43,11 +43,48 @@ struct Params {
     double dzi, hdzi, ap;         // inversion_utils.f90:107-113
 };
 
+// Slots held in FP32 by the mixed-precision form: vorticity, B, buoyancy,
+// humidity, delta_vor, delta_b, strain, Veta, Vtau.  Position, volume and
+// delta_pos stay FP64 in both forms.
+EPIC_HD constexpr bool attr_f32(int k) {
+    return (k >= A_VX && k <= A_B23) || k == A_BUOY || k == A_HUM || k >= A_DVX;
+}
+// Byte offset of slot k in units of `cap` in the mixed form (FP32 slots take
+// 4 bytes): the prefix sum of the slot sizes in closed form.
+EPIC_HD constexpr long long mixed_slot_off(int k) {
+    return k <= 3 ? 8LL * k : k <= 11 ? 24 + 4LL * (k - 3) : k <= 12 ? 64 : k <= 14 ? 64 + 4LL * (k - 12)
+         : k <= 17 ? 72 + 8LL * (k - 14) : 96 + 4LL * (k - 17);
+}
+constexpr bool mixed_slot_off_ok() {
+    long long o = 0;
+    for (int j = 0; j <= N_ATTR; ++j) {
+        if (mixed_slot_off(j) != o) return false;
+        if (j < N_ATTR) o += attr_f32(j) ? 4 : 8;
+    }
+    return true;
+}
+static_assert(mixed_slot_off_ok(), "mixed slot offsets");
+constexpr long long PARCEL_BYTES_PLAIN = 8LL * N_ATTR;              // 312
+constexpr long long PARCEL_BYTES_MIXED = mixed_slot_off(N_ATTR);    // 184
+
+// View of the parcel store: slot k of parcel i.  get/set convert between the
+// slot's storage type and double; typed pointers (d, f) serve the kernels that
+// are written for one form.
 struct PView {
-    double* base;
+    double* base;        // start of the store (bytes addressed through off)
     long long cap;
-    EPIC_HD double* a(int k) const { return base + (long long)k * cap; }
-    EPIC_HD double& at(int k, long long i) const { return base[(long long)k * cap + i]; }
+    int mixed;           // 1: FP32 slots as in attr_f32
+    EPIC_HD long long off(int k) const { return (mixed ? mixed_slot_off(k) : 8LL * k) * cap; }
+    EPIC_HD bool f32(int k) const { return mixed && attr_f32(k); }
+    EPIC_HD double* d(int k) const { return reinterpret_cast<double*>(reinterpret_cast<char*>(base) + off(k)); }
+    EPIC_HD float* f(int k) const { return reinterpret_cast<float*>(reinterpret_cast<char*>(base) + off(k)); }
+    template <class R>
+    EPIC_HD R* ptr(int k) const { return reinterpret_cast<R*>(reinterpret_cast<char*>(base) + off(k)); }
+    EPIC_HD double get(int k, long long i) const { return f32(k) ? (double)f(k)[i] : d(k)[i]; }
+    EPIC_HD void set(int k, long long i, double v) const {
+        if (f32(k)) f(k)[i] = (float)v;
+        else d(k)[i] = v;
+    }
 };
 
 // Field index: z fastest with one halo row below, x slowest.
@@ -63,14 +100,23 @@ EPIC_HD int wrapi(int i, int n) {
 // (split test, nearest-parcel distances) round exactly like the oracle's
 // -ffp-contract=off build; FastOps lets the compiler contract.
 struct ExactOps {
+    using T = double;
     static EPIC_DEV double mul(double a, double b) { return __dmul_rn(a, b); }
     static EPIC_DEV double add(double a, double b) { return __dadd_rn(a, b); }
     static EPIC_DEV double sub(double a, double b) { return __dsub_rn(a, b); }
 };
 struct FastOps {
+    using T = double;
     static EPIC_DEV double mul(double a, double b) { return a * b; }
     static EPIC_DEV double add(double a, double b) { return a + b; }
     static EPIC_DEV double sub(double a, double b) { return a - b; }
+};
+// FP32 arithmetic of the mixed-precision form.
+struct F32Ops {
+    using T = float;
+    static EPIC_DEV float mul(float a, float b) { return a * b; }
+    static EPIC_DEV float add(float a, float b) { return a + b; }
+    static EPIC_DEV float sub(float a, float b) { return a - b; }
 };
 
 // Error word bits written by kernels (read once per step by the host).

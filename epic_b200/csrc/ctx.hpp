@@ -84,7 +84,7 @@ struct Ctx {
     // parcels
     long long cap = 0;
     long long n = 0;
-    PView pv{nullptr, 0};
+    PView pv{nullptr, 0, 0};
     // fields: velog 3, vortg 3, vtend 3, velgradg 8, tbuoyg, dbuoyg, humg, volg = 21
     double* fields = nullptr;
     int* nparg = nullptr, *nsparg = nullptr;
@@ -123,6 +123,9 @@ struct Ctx {
     long long n_parcel_splits = 0, n_parcel_merges = 0, n_big_close = 0;
     bool has_parcels = false;
 
+    size_t store_bytes() const {
+        return (size_t)(pv.mixed ? PARCEL_BYTES_MIXED : PARCEL_BYTES_PLAIN) * (size_t)cap;
+    }
     double* field(int id) const { return fields + (long long)id * P.fsz; }
     double* velog(int c) const { return field(EPIC_FIELD_VELOG_X + c); }
     double* vortg(int c) const { return field(EPIC_FIELD_VORTG_X + c); }

@@ -10,56 +10,57 @@ namespace epic {
 // scherzinger.f90:16 -- the single-precision literal 1.0e-12
 #define EPIC_SCHERZINGER_ATOL ((double)1.0e-12f)
 
-template <class O>
-EPIC_DEV double dot3(const double* a, const double* b) {
+template <class O, class T = typename O::T>
+EPIC_DEV T dot3(const T* a, const T* b) {
     return O::add(O::add(O::mul(a[0], b[0]), O::mul(a[1], b[1])), O::mul(a[2], b[2]));
 }
-template <class O>
-EPIC_DEV double nrm3(const double* a) { return sqrt(dot3<O>(a, a)); }
+template <class O, class T = typename O::T>
+EPIC_DEV T nrm3(const T* a) { return sqrt(dot3<O>(a, a)); }
 
-template <class O>
-EPIC_DEV void cross3(const double* a, const double* b, double* c) {
+template <class O, class T = typename O::T>
+EPIC_DEV void cross3(const T* a, const T* b, T* c) {
     c[0] = O::sub(O::mul(a[1], b[2]), O::mul(a[2], b[1]));
     c[1] = O::sub(O::mul(a[2], b[0]), O::mul(a[0], b[2]));
     c[2] = O::sub(O::mul(a[0], b[1]), O::mul(a[1], b[0]));
 }
 
-EPIC_DEV double signum_d(double v) { return v == 0.0 ? 0.0 : copysign(1.0, v); }
+template <class T>
+EPIC_DEV T signum_d(T v) { return v == T(0) ? T(0) : copysign(T(1), v); }
 
 // evaluate_eigenvalues (scherzinger.f90:151-227); A becomes its deviator,
 // r receives s1, s2 (columns 0, 1) and t3 (column 2).
-template <class O>
-EPIC_DEV void sz_evaluate(double* A, double* r, double* eta, double* D) {
-    const double f13 = 1.0 / 3.0;
-    double tr = O::add(O::add(A[0], A[4]), A[8]);
-    double tmp = O::mul(f13, tr);
+template <class O, class T = typename O::T>
+EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
+    const T f13 = T(1.0 / 3.0);
+    T tr = O::add(O::add(A[0], A[4]), A[8]);
+    T tmp = O::mul(f13, tr);
     A[0] = O::sub(A[0], tmp); A[4] = O::sub(A[4], tmp); A[8] = O::sub(A[8], tmp);
     // j2 = 1/2 trace(A A) with dsymm's evaluation (linalg.f90:57-71)
-    double a11 = A[0], a12 = A[3], a13 = A[6], a22 = A[4], a23 = A[7], a33 = A[8];
-    double c11 = O::add(O::add(O::mul(a11, a11), O::mul(a12, a12)), O::mul(a13, a13));
-    double c22 = O::add(O::add(O::mul(a12, a12), O::mul(a22, a22)), O::mul(a23, a23));
-    double c33 = O::add(O::add(O::mul(a13, a13), O::mul(a23, a23)), O::mul(a33, a33));
-    double j2 = O::mul(0.5, O::add(O::add(c11, c22), c33));
+    T a11 = A[0], a12 = A[3], a13 = A[6], a22 = A[4], a23 = A[7], a33 = A[8];
+    T c11 = O::add(O::add(O::mul(a11, a11), O::mul(a12, a12)), O::mul(a13, a13));
+    T c22 = O::add(O::add(O::mul(a12, a12), O::mul(a22, a22)), O::mul(a23, a23));
+    T c33 = O::add(O::add(O::mul(a13, a13), O::mul(a23, a23)), O::mul(a33, a33));
+    T j2 = O::mul(T(0.5), O::add(O::add(c11, c22), c33));
     // determinant (linalg.f90:43-52)
-    double j3 = O::add(O::sub(O::mul(a11, O::sub(O::mul(a22, a33), O::mul(a23, a23))),
+    T j3 = O::add(O::sub(O::mul(a11, O::sub(O::mul(a22, a33), O::mul(a23, a23))),
                               O::mul(a12, O::sub(O::mul(a12, a33), O::mul(a13, a23)))),
                        O::mul(a13, O::sub(O::mul(a12, a23), O::mul(a13, a22))));
-    double smp = O::mul(O::mul(0.5, j3), pow(3.0 / j2, 1.5));
-    smp = fmin(fmax(-1.0, smp), 1.0);
-    double alpha = O::mul(f13, acos(smp));
+    T smp = O::mul(O::mul(T(0.5), j3), pow(T(3) / j2, T(1.5)));
+    smp = fmin(fmax(T(-1), smp), T(1));
+    T alpha = O::mul(f13, acos(smp));
     const double pi = 3.141592653589793;
-    if (alpha > pi / 6.0) alpha = O::add(alpha, O::mul(2.0 / 3.0, pi));
-    eta[0] = O::mul(O::mul(2.0, sqrt(O::mul(f13, j2))), cos(alpha));
+    if (alpha > T(pi / 6.0)) alpha = O::add(alpha, O::mul(T(2.0 / 3.0), T(pi)));
+    eta[0] = O::mul(O::mul(T(2), sqrt(O::mul(f13, j2))), cos(alpha));
     r[0] = O::sub(A[0], eta[0]); r[1] = A[1];                 r[2] = A[2];
     r[3] = A[3];                 r[4] = O::sub(A[4], eta[0]); r[5] = A[5];
     r[6] = A[6];                 r[7] = A[7];                 r[8] = O::sub(A[8], eta[0]);
-    double rl0 = nrm3<O>(&r[0]), rl1 = nrm3<O>(&r[3]), rl2 = nrm3<O>(&r[6]);
+    T rl0 = nrm3<O>(&r[0]), rl1 = nrm3<O>(&r[3]), rl2 = nrm3<O>(&r[6]);
     int i = 0;
-    double rm = rl0;
+    T rm = rl0;
     if (rl1 > rm) { i = 1; rm = rl1; }
     if (rl2 > rm) { i = 2; rm = rl2; }
     // column i of r, selected without a run-time array index (keeps r in registers)
-    double s1[3];
+    T s1[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) / rm;
     if (i == 1) { r[3] = r[0]; r[4] = r[1]; r[5] = r[2]; }
@@ -75,41 +76,42 @@ EPIC_DEV void sz_evaluate(double* A, double* r, double* eta, double* D) {
     rl1 = nrm3<O>(&r[3]);
     rl2 = nrm3<O>(&r[6]);
     int j = (rl2 > rl1) ? 2 : 1;
-    double rj = (j == 2) ? rl2 : rl1;
-    double s2[3];
+    T rj = (j == 2) ? rl2 : rl1;
+    T s2[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) / rj;
     r[3] = s2[0]; r[4] = s2[1]; r[5] = s2[2];
-    double Ar[6];
+    T Ar[6];
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
         for (int row = 0; row < 3; ++row)
             Ar[row + 3 * c] = O::add(O::add(O::mul(A[row], r[3 * c]), O::mul(A[row + 3], r[3 * c + 1])),
                                      O::mul(A[row + 6], r[3 * c + 2]));
-    double s1As1 = dot3<O>(&r[0], &Ar[0]);
-    double s2As1 = dot3<O>(&r[3], &Ar[0]);
-    double s1As2 = s2As1;
-    double s2As2 = dot3<O>(&r[3], &Ar[3]);
+    T s1As1 = dot3<O>(&r[0], &Ar[0]);
+    T s2As1 = dot3<O>(&r[3], &Ar[0]);
+    T s1As2 = s2As1;
+    T s2As2 = dot3<O>(&r[3], &Ar[3]);
     tmp = O::sub(s1As1, s2As2);
     smp = O::add(s1As1, s2As2);
-    double disc = O::add(O::mul(tmp, tmp), O::mul(O::mul(4.0, s1As2), s2As1));
-    eta[1] = O::sub(O::mul(0.5, smp), O::mul(O::mul(0.5, signum_d(tmp)), sqrt(disc)));
+    T disc = O::add(O::mul(tmp, tmp), O::mul(O::mul(T(4), s1As2), s2As1));
+    eta[1] = O::sub(O::mul(T(0.5), smp), O::mul(O::mul(T(0.5), signum_d(tmp)), sqrt(disc)));
     eta[2] = O::sub(smp, eta[1]);
-    double t3 = O::mul(f13, tr);
+    T t3 = O::mul(f13, tr);
     D[0] = O::add(eta[0], t3); D[1] = O::add(eta[1], t3); D[2] = O::add(eta[2], t3);
 }
 
-EPIC_DEV void swapd(double& a, double& b) { double t = a; a = b; b = t; }
+template <class T>
+EPIC_DEV void swapd(T& a, T& b) { T t = a; a = b; b = t; }
 
 // scherzinger_eigenvalues (scherzinger.f90:127-147) + sort_eigenvalues
-template <class O>
-EPIC_DEV void sz_eigenvalues(double* A, double* D) {
-    double off = fabs(A[3]) + fabs(A[6]) + fabs(A[7]);
-    if (off < EPIC_SCHERZINGER_ATOL) {
+template <class O, class T = typename O::T>
+EPIC_DEV void sz_eigenvalues(T* A, T* D) {
+    T off = fabs(A[3]) + fabs(A[6]) + fabs(A[7]);
+    if (off < T(EPIC_SCHERZINGER_ATOL)) {
         D[0] = A[0]; D[1] = A[4]; D[2] = A[8];
     } else {
-        double r[9], eta[3];
+        T r[9], eta[3];
         sz_evaluate<O>(A, r, eta, D);
     }
     if (D[1] > D[0]) swapd(D[0], D[1]);
@@ -117,40 +119,41 @@ EPIC_DEV void sz_eigenvalues(double* A, double* D) {
     if (D[1] > D[0]) swapd(D[0], D[1]);
 }
 
-EPIC_DEV void swapcol(double* V, int a, int b) {
+template <class T>
+EPIC_DEV void swapcol(T* V, int a, int b) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) swapd(V[3 * a + k], V[3 * b + k]);
 }
 
 // scherzinger_diagonalise (scherzinger.f90:31-118)
-template <class O>
-EPIC_DEV void sz_diagonalise(double* A, double* D, double* V) {
-    double off = fabs(A[3]) + fabs(A[6]) + fabs(A[7]);
-    if (off < EPIC_SCHERZINGER_ATOL) {
+template <class O, class T = typename O::T>
+EPIC_DEV void sz_diagonalise(T* A, T* D, T* V) {
+    T off = fabs(A[3]) + fabs(A[6]) + fabs(A[7]);
+    if (off < T(EPIC_SCHERZINGER_ATOL)) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) V[k] = 0.0;
-        V[0] = V[4] = V[8] = 1.0;
+        for (int k = 0; k < 9; ++k) V[k] = T(0);
+        V[0] = V[4] = V[8] = T(1);
         D[0] = A[0]; D[1] = A[4]; D[2] = A[8];
     } else {
-        double r[9], eta[3];
+        T r[9], eta[3];
         sz_evaluate<O>(A, r, eta, D);
         A[0] = O::sub(A[0], eta[1]); A[4] = O::sub(A[4], eta[1]); A[8] = O::sub(A[8], eta[1]);
         cross3<O>(&r[0], &r[3], &V[0]);
-        double Ar[6];
+        T Ar[6];
 #pragma unroll
         for (int c = 0; c < 2; ++c)
 #pragma unroll
             for (int row = 0; row < 3; ++row)
                 Ar[row + 3 * c] = O::add(O::add(O::mul(A[row], r[3 * c]), O::mul(A[row + 3], r[3 * c + 1])),
                                          O::mul(A[row + 6], r[3 * c + 2]));
-        double l0 = nrm3<O>(&Ar[0]), l1 = nrm3<O>(&Ar[3]);
+        T l0 = nrm3<O>(&Ar[0]), l1 = nrm3<O>(&Ar[3]);
         int i = (l1 > l0) ? 1 : 0;
-        double li = i ? l1 : l0;
+        T li = i ? l1 : l0;
 #pragma unroll
         for (int k = 0; k < 3; ++k) V[6 + k] = (i ? Ar[3 + k] : Ar[k]) / li;
         cross3<O>(&V[6], &V[0], &V[3]);
         cross3<O>(&V[0], &V[3], &V[6]);
-        double n0 = nrm3<O>(&V[0]), n1 = nrm3<O>(&V[3]), n2 = nrm3<O>(&V[6]);
+        T n0 = nrm3<O>(&V[0]), n1 = nrm3<O>(&V[3]), n2 = nrm3<O>(&V[6]);
 #pragma unroll
         for (int k = 0; k < 3; ++k) { V[k] /= n0; V[3 + k] /= n1; V[6 + k] /= n2; }
     }
@@ -177,8 +180,8 @@ EPIC_DEV double get_B33(const double* b, double vol, unsigned* err) {
     return num / den;
 }
 
-template <class O>
-EPIC_DEV void full_matrix(const double* b, double B33, double* U) {
+template <class O, class T = typename O::T>
+EPIC_DEV void full_matrix(const T* b, T B33, T* U) {
     U[0] = b[0]; U[3] = b[1]; U[6] = b[2];
     U[1] = b[1]; U[4] = b[3]; U[7] = b[4];
     U[2] = b[2]; U[5] = b[4]; U[8] = B33;
@@ -198,6 +201,20 @@ EPIC_DEV void support_vectors(const double* b, double vol, double* Veta, double*
 #pragma unroll
     for (int k = 0; k < 3; ++k) { Veta[k] = se * V[k]; Vtau[k] = st * V[3 + k]; }
     if (Dout) { Dout[0] = D[0]; Dout[1] = D[1]; Dout[2] = D[2]; }
+}
+
+// Mixed form: B in FP32, B33 recovered in FP64 (get_B33), the eigen-
+// decomposition and the support vectors in FP32.
+EPIC_DEV void support_vectors_f32(const float* b, double vol, float* Veta, float* Vtau, unsigned* err) {
+    double bd[5] = {b[0], b[1], b[2], b[3], b[4]};
+    float U[9], D[3], V[9];
+    full_matrix<F32Ops>(b, (float)get_B33<FastOps>(bd, vol, err), U);
+    sz_diagonalise<F32Ops>(U, D, V);
+    const float rho = 0.6324555320336759f;   // sqrt(2/5)
+    float se = sqrtf(fabsf(D[0] - D[2])) * rho;
+    float st = sqrtf(fabsf(D[1] - D[2])) * rho;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { Veta[k] = se * V[k]; Vtau[k] = st * V[3 + k]; }
 }
 
 // cos/sin of theta_j = (2j-1) pi / 4 evaluated in FP64 from the double

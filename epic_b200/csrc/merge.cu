@@ -87,12 +87,12 @@ EPIC_DEV unsigned boundary_bits(const Params& P, double x, double y) {
 __global__ void k_bin_locals(Params P, Box B, PView pv, int N, int* cell, int* small, unsigned* bits,
                              unsigned* err) {
     MLOOP(N) {
-        double x = pv.at(A_X, i), y = pv.at(A_Y, i), z = pv.at(A_Z, i);
+        double x = pv.get(A_X, i), y = pv.get(A_Y, i), z = pv.get(A_Z, i);
         double x0 = x, y0 = y;
         cell[i] = bin_cell(P, B, x, y, z, err);
-        if (x != x0) pv.at(A_X, i) = x;
-        if (y != y0) pv.at(A_Y, i) = y;
-        int s = pv.at(A_VOL, i) < P.vmin;
+        if (x != x0) pv.set(A_X, i, x);
+        if (y != y0) pv.set(A_Y, i, y);
+        int s = pv.get(A_VOL, i) < P.vmin;
         small[i] = s;
         bits[i] = s ? boundary_bits(P, x, y) : 0u;
     }
@@ -127,7 +127,7 @@ __global__ void k_make_copies(Params P, Box B, PView pv, const int* Ls, int nls,
         int m = (int)(i - (long long)(r - 1) * nls);
         int q = off[i];
         int n = Ls[m];
-        double x = pv.at(A_X, n), y = pv.at(A_Y, n), z = pv.at(A_Z, n);
+        double x = pv.get(A_X, n), y = pv.get(A_Y, n), z = pv.get(A_Z, n);
         int ix = nint_d(ExactOps::mul(P.dxi[0], ExactOps::sub(x, P.lower[0])));
         int iy = nint_d(ExactOps::mul(P.dxi[1], ExactOps::sub(y, P.lower[1])));
         bool xe = (ix <= 0) || (ix >= P.nx), ye = (iy <= 0) || (iy >= P.ny);
@@ -162,7 +162,7 @@ __global__ void k_cell_ranges(const int* keys, long long nt, int* cstart, int* c
 }
 
 EPIC_DEV void entry_pos(const PView& pv, const CopyArgs& C, int N, int j, double& x, double& y, double& z) {
-    if (j < N) { x = pv.at(A_X, j); y = pv.at(A_Y, j); z = pv.at(A_Z, j); }
+    if (j < N) { x = pv.get(A_X, j); y = pv.get(A_Y, j); z = pv.get(A_Z, j); }
     else { x = C.cx[j - N]; y = C.cy[j - N]; z = C.cz[j - N]; }
 }
 
@@ -328,7 +328,7 @@ __global__ void k_set_minv(const int* Ls, int nls, int* minv) { MLOOP(nls) minv[
 
 __global__ void k_big_close(PView pv, const int* icl, int nm, double vmin, unsigned long long* cnt) {
     unsigned long long local = 0;
-    MLOOP(nm) local += pv.at(A_VOL, icl[i]) > vmin;
+    MLOOP(nm) local += pv.get(A_VOL, icl[i]) > vmin;
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffff, local, o);
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(cnt, local);
 }
@@ -349,32 +349,32 @@ __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int
         int s0 = gstart[i];
         int s1 = (i + 1 < ng) ? gstart[i + 1] : nm;
         int ic = skeys[s0];
-        double vic = pv.at(A_VOL, ic);
-        double xic = pv.at(A_X, ic), yic = pv.at(A_Y, ic), zic = pv.at(A_Z, ic);
+        double vic = pv.get(A_VOL, ic);
+        double xic = pv.get(A_X, ic), yic = pv.get(A_Y, ic), zic = pv.get(A_Z, ic);
         double vm = vic, x0 = xic, y0 = yic;
         double pm0 = 0.0, pm1 = 0.0, pm2 = vic * zic;
-        double bm = vic * pv.at(A_BUOY, ic), hm = vic * pv.at(A_HUM, ic);
-        double wm[3] = {vic * pv.at(A_VX, ic), vic * pv.at(A_VY, ic), vic * pv.at(A_VZ, ic)};
+        double bm = vic * pv.get(A_BUOY, ic), hm = vic * pv.get(A_HUM, ic);
+        double wm[3] = {vic * pv.get(A_VX, ic), vic * pv.get(A_VY, ic), vic * pv.get(A_VZ, ic)};
         for (int q = s0; q < s1; ++q) {
             int is = ism[svals[q]];
-            double p[3] = {pv.at(A_X, is), pv.at(A_Y, is), pv.at(A_Z, is)};
+            double p[3] = {pv.get(A_X, is), pv.get(A_Y, is), pv.get(A_Z, is)};
             // apply_periodic_bc on the small parcel (parcel_merge.f90:143)
             p[0] = p[0] - P.extent[0] * (double)(int)((p[0] - P.center[0]) * P.hli[0]);
             p[1] = p[1] - P.extent[1] * (double)(int)((p[1] - P.center[1]) * P.hli[1]);
-            pv.at(A_X, is) = p[0];
-            pv.at(A_Y, is) = p[1];
-            double v = pv.at(A_VOL, is);
+            pv.set(A_X, is, p[0]);
+            pv.set(A_Y, is, p[1]);
+            double v = pv.get(A_VOL, is);
             vm = vm + v;
             double dx = pdelta(p[0] - x0, P.extent[0], P.extenti[0]);
             double dy = pdelta(p[1] - y0, P.extent[1], P.extenti[1]);
             pm0 = pm0 + v * dx;
             pm1 = pm1 + v * dy;
             pm2 = pm2 + v * p[2];
-            bm = bm + v * pv.at(A_BUOY, is);
-            hm = hm + v * pv.at(A_HUM, is);
-            wm[0] = wm[0] + v * pv.at(A_VX, is);
-            wm[1] = wm[1] + v * pv.at(A_VY, is);
-            wm[2] = wm[2] + v * pv.at(A_VZ, is);
+            bm = bm + v * pv.get(A_BUOY, is);
+            hm = hm + v * pv.get(A_HUM, is);
+            wm[0] = wm[0] + v * pv.get(A_VX, is);
+            wm[1] = wm[1] + v * pv.get(A_VY, is);
+            wm[2] = wm[2] + v * pv.get(A_VZ, is);
         }
         double vmerge = 1.0 / vm;
         pm0 = vmerge * pm0;
@@ -389,7 +389,7 @@ __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int
         for (int k = 0; k < 3; ++k) wm[k] = vmerge * wm[k];
         // shape (parcel_merge.f90:263-322)
         double b[5];
-        for (int k = 0; k < 5; ++k) b[k] = pv.at(A_B11 + k, ic);
+        for (int k = 0; k < 5; ++k) b[k] = pv.get(A_B11 + k, ic);
         double B33 = get_B33<FastOps>(b, vic, err);
         double dx = pdelta(xic - pm0, P.extent[0], P.extenti[0]);
         double dy = pdelta(yic - pm1, P.extent[1], P.extenti[1]);
@@ -404,13 +404,13 @@ __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int
         Bm[5] = mu * (5.0 * (dz * dz) + B33);
         for (int q = s0; q < s1; ++q) {
             int is = ism[svals[q]];
-            double px = pv.at(A_X, is), py = pv.at(A_Y, is), pz = pv.at(A_Z, is);
+            double px = pv.get(A_X, is), py = pv.get(A_Y, is), pz = pv.get(A_Z, is);
             double ex = pdelta(px - pm0, P.extent[0], P.extenti[0]);
             double ey = pdelta(py - pm1, P.extent[1], P.extenti[1]);
             double ez = pz - pm2;
             double bs[5];
-            for (int k = 0; k < 5; ++k) bs[k] = pv.at(A_B11 + k, is);
-            double vs = pv.at(A_VOL, is);
+            for (int k = 0; k < 5; ++k) bs[k] = pv.get(A_B11 + k, is);
+            double vs = pv.get(A_VOL, is);
             double B33s = get_B33<FastOps>(bs, vs, err);
             double m2 = vmerge * vs;
             Bm[0] = Bm[0] + m2 * (5.0 * (ex * ex) + bs[0]);
@@ -424,14 +424,14 @@ __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int
                     + Bm[2] * (Bm[1] * Bm[4] - Bm[2] * Bm[3]);
         double abc = get_abc(vm);
         double factor = pow(abc * abc / detB, 1.0 / 3.0);
-        pv.at(A_VOL, ic) = vm;
-        pv.at(A_X, ic) = pm0;
-        pv.at(A_Y, ic) = pm1;
-        pv.at(A_Z, ic) = pm2;
-        pv.at(A_BUOY, ic) = bm;
-        pv.at(A_HUM, ic) = hm;
-        for (int k = 0; k < 3; ++k) pv.at(A_VX + k, ic) = wm[k];
-        for (int k = 0; k < 5; ++k) pv.at(A_B11 + k, ic) = Bm[k] * factor;
+        pv.set(A_VOL, ic, vm);
+        pv.set(A_X, ic, pm0);
+        pv.set(A_Y, ic, pm1);
+        pv.set(A_Z, ic, pm2);
+        pv.set(A_BUOY, ic, bm);
+        pv.set(A_HUM, ic, hm);
+        for (int k = 0; k < 3; ++k) pv.set(A_VX + k, ic, wm[k]);
+        for (int k = 0; k < 5; ++k) pv.set(A_B11 + k, ic, Bm[k] * factor);
     }
 }
 
@@ -448,15 +448,15 @@ __global__ void k_move(PView pv, const int* holes, const int* srcs, int nh, int 
         int a = (int)(i / nh);
         int dst = holes[h];
         int src = newN + srcs[nh - 1 - h];
-        pv.at(a, dst) = pv.at(a, src);
+        pv.set(a, dst, pv.get(a, src));
     }
 }
 
 __global__ void k_periodic_m(Params P, PView pv, long long n) {
     MLOOP(n) {
-        double x = pv.at(A_X, i), y = pv.at(A_Y, i);
-        pv.at(A_X, i) = x - P.extent[0] * (double)(int)((x - P.center[0]) * P.hli[0]);
-        pv.at(A_Y, i) = y - P.extent[1] * (double)(int)((y - P.center[1]) * P.hli[1]);
+        double x = pv.get(A_X, i), y = pv.get(A_Y, i);
+        pv.set(A_X, i, x - P.extent[0] * (double)(int)((x - P.center[0]) * P.hli[0]));
+        pv.set(A_Y, i, y - P.extent[1] * (double)(int)((y - P.center[1]) * P.hli[1]));
     }
 }
 

@@ -68,7 +68,7 @@ EPIC_DEV double csum(const double* f, const Tri& t, const long long a[2][2]) {
 
 EPIC_DEV void load_B(const PView& pv, long long i, double* b) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) b[k] = pv.at(A_B11 + k, i);
+    for (int k = 0; k < 5; ++k) b[k] = pv.get(A_B11 + k, i);
 }
 
 // Support vectors: recomputed, or reused from the parcel store (l_reuse).
@@ -76,15 +76,15 @@ EPIC_DEV void get_vectors(const PView& pv, long long i, bool reuse, bool store, 
                           double* D, unsigned* err) {
     if (reuse) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { eta[k] = pv.at(A_ETA0 + k, i); tau[k] = pv.at(A_TAU0 + k, i); }
+        for (int k = 0; k < 3; ++k) { eta[k] = pv.get(A_ETA0 + k, i); tau[k] = pv.get(A_TAU0 + k, i); }
         return;
     }
     double b[5];
     load_B(pv, i, b);
-    support_vectors<FastOps>(b, pv.at(A_VOL, i), eta, tau, D, err);
+    support_vectors<FastOps>(b, pv.get(A_VOL, i), eta, tau, D, err);
     if (store) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { pv.at(A_ETA0 + k, i) = eta[k]; pv.at(A_TAU0 + k, i) = tau[k]; }
+        for (int k = 0; k < 3; ++k) { pv.set(A_ETA0 + k, i, eta[k]); pv.set(A_TAU0 + k, i, tau[k]); }
     }
 }
 

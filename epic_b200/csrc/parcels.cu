@@ -131,15 +131,15 @@ __global__ void __launch_bounds__(PB) k_g2p(Params P, PView pv, long long n, Gat
     acc[10] = 0.0; acc[11] = 0.0;   // bmin, bmax start at zero (parcel_diagnostics.f90:62-63)
     double dt = sc->dt;
     PLOOP(n) {
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+        double pos[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
         double b[5];
         load_B(pv, i, b);
-        double vol = pv.at(A_VOL, i);
+        double vol = pv.get(A_VOL, i);
         double eta[3], tau[3], D[3];
         support_vectors<FastOps>(b, vol, eta, tau, D, err);
         // grid2par stores the vectors like get_points (parcel_ellipsoid.f90:243-246)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { pv.at(A_ETA0 + k, i) = eta[k]; pv.at(A_TAU0 + k, i) = tau[k]; }
+        for (int k = 0; k < 3; ++k) { pv.set(A_ETA0 + k, i, eta[k]); pv.set(A_TAU0 + k, i, tau[k]); }
         double g[14];
 #pragma unroll
         for (int l = 0; l < 14; ++l) g[l] = 0.0;
@@ -157,17 +157,17 @@ __global__ void __launch_bounds__(PB) k_g2p(Params P, PView pv, long long n, Gat
         double dp[3], dv[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            dp[k] = S.add ? pv.at(A_DX + k, i) + g[k] : g[k];
-            dv[k] = S.add ? pv.at(A_DVX + k, i) + g[11 + k] : g[11 + k];
+            dp[k] = S.add ? pv.get(A_DX + k, i) + g[k] : g[k];
+            dv[k] = S.add ? pv.get(A_DVX + k, i) + g[11 + k] : g[11 + k];
         }
         const double* strain = &g[3];
         if (S.store_strain) {
 #pragma unroll
-            for (int l = 0; l < 8; ++l) pv.at(A_S0 + l, i) = strain[l];
+            for (int l = 0; l < 8; ++l) pv.set(A_S0 + l, i, strain[l]);
         }
         if (S.diag) {
-            double vx = pv.at(A_VX, i), vy = pv.at(A_VY, i), vz = pv.at(A_VZ, i);
-            double bu = pv.at(A_BUOY, i);
+            double vx = pv.get(A_VX, i), vy = pv.get(A_VY, i), vz = pv.get(A_VZ, i);
+            double bu = pv.get(A_BUOY, i);
             acc[0] += (dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]) * vol;
             acc[1] += (vx * vx + vy * vy + vz * vz) * vol;
             double lam = sqrt(D[0] / D[2]);
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(PB) k_g2p(Params P, PView pv, long long n, Gat
         }
         if (S.mode == 0) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { pv.at(A_DX + k, i) = dp[k]; pv.at(A_DVX + k, i) = dv[k]; }
+            for (int k = 0; k < 3; ++k) { pv.set(A_DX + k, i, dp[k]); pv.set(A_DVX + k, i, dv[k]); }
             continue;
         }
         double B33 = get_B33<FastOps>(b, vol, err);
@@ -192,10 +192,10 @@ __global__ void __launch_bounds__(PB) k_g2p(Params P, PView pv, long long n, Gat
         dBdt(strain, b, B33, db);
         if (S.stage > 1) {
 #pragma unroll
-            for (int k = 0; k < 5; ++k) db[k] = pv.at(A_DB0 + k, i) + db[k];
+            for (int k = 0; k < 5; ++k) db[k] = pv.get(A_DB0 + k, i) + db[k];
         }
         double cdt = S.cb * dt;
-        double vor[3] = {pv.at(A_VX, i), pv.at(A_VY, i), pv.at(A_VZ, i)};
+        double vor[3] = {pv.get(A_VX, i), pv.get(A_VY, i), pv.get(A_VZ, i)};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             pos[k] = pos[k] + cdt * dp[k];
@@ -214,15 +214,15 @@ __global__ void __launch_bounds__(PB) k_g2p(Params P, PView pv, long long n, Gat
         }
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            pv.at(A_X + k, i) = pos[k];
-            pv.at(A_VX + k, i) = vor[k];
-            pv.at(A_DX + k, i) = dp[k];
-            pv.at(A_DVX + k, i) = dv[k];
+            pv.set(A_X + k, i, pos[k]);
+            pv.set(A_VX + k, i, vor[k]);
+            pv.set(A_DX + k, i, dp[k]);
+            pv.set(A_DVX + k, i, dv[k]);
         }
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            pv.at(A_B11 + k, i) = b[k];
-            pv.at(A_DB0 + k, i) = db[k];
+            pv.set(A_B11 + k, i, b[k]);
+            pv.set(A_DB0 + k, i, db[k]);
         }
     }
     if (S.diag) {
@@ -332,13 +332,13 @@ __global__ void __launch_bounds__(PB) k_pdiag(Params P, PView pv, long long n, d
     PLOOP(n) {
         double b[5];
         load_B(pv, i, b);
-        double vol = pv.at(A_VOL, i);
+        double vol = pv.get(A_VOL, i);
         double U[9], D[3];
         full_matrix<FastOps>(b, get_B33<FastOps>(b, vol, err), U);
         sz_eigenvalues<FastOps>(U, D);
-        double dp0 = pv.at(A_DX, i), dp1 = pv.at(A_DY, i), dp2 = pv.at(A_DZ, i);
-        double vx = pv.at(A_VX, i), vy = pv.at(A_VY, i), vz = pv.at(A_VZ, i);
-        double bu = pv.at(A_BUOY, i);
+        double dp0 = pv.get(A_DX, i), dp1 = pv.get(A_DY, i), dp2 = pv.get(A_DZ, i);
+        double vx = pv.get(A_VX, i), vy = pv.get(A_VY, i), vz = pv.get(A_VZ, i);
+        double bu = pv.get(A_BUOY, i);
         acc[0] += (dp0 * dp0 + dp1 * dp1 + dp2 * dp2) * vol;
         acc[1] += (vx * vx + vy * vy + vz * vz) * vol;
         double lam = sqrt(D[0] / D[2]);
@@ -497,11 +497,11 @@ void field_diagnostics(Ctx& c, double* st) {
 __global__ void __launch_bounds__(PB) k_vortsum(PView pv, long long n, double* partials) {
     double acc[4] = {0, 0, 0, 0};
     PLOOP(n) {
-        double v = pv.at(A_VOL, i);
+        double v = pv.get(A_VOL, i);
         acc[0] += v;
-        acc[1] += pv.at(A_VX, i) * v;
-        acc[2] += pv.at(A_VY, i) * v;
-        acc[3] += pv.at(A_VZ, i) * v;
+        acc[1] += pv.get(A_VX, i) * v;
+        acc[2] += pv.get(A_VY, i) * v;
+        acc[3] += pv.get(A_VZ, i) * v;
     }
     __shared__ double red[PB / 32][4];
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -531,9 +531,9 @@ __global__ void k_vortsum_final(const double* partials, int nb, const double* vo
 __global__ void k_vortcor_apply(PView pv, long long n, const double* dvor) {
     double d0 = dvor[0], d1 = dvor[1], d2 = dvor[2];
     PLOOP(n) {
-        pv.at(A_VX, i) = pv.at(A_VX, i) - d0;
-        pv.at(A_VY, i) = pv.at(A_VY, i) - d1;
-        pv.at(A_VZ, i) = pv.at(A_VZ, i) - d2;
+        pv.set(A_VX, i, pv.get(A_VX, i) - d0);
+        pv.set(A_VY, i, pv.get(A_VY, i) - d1);
+        pv.set(A_VZ, i, pv.get(A_VZ, i) - d2);
     }
 }
 
@@ -564,7 +564,7 @@ struct Grad3 {
 
 __global__ void k_laplace_move(Params P, PView pv, long long n, Grad3 G, unsigned* err) {
     PLOOP(n) {
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+        double pos[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
         Tri t = trilinear(P, pos);
         long long a[2][2];
         if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
@@ -583,9 +583,9 @@ __global__ void k_laplace_move(Params P, PView pv, long long n, Grad3 G, unsigne
 #pragma unroll
         for (int l = 0; l < 3; ++l) pos[l] = pos[l] + d[l];
         periodic_bc(P, pos);
-        pv.at(A_X, i) = pos[0];
-        pv.at(A_Y, i) = pos[1];
-        pv.at(A_Z, i) = pos[2];
+        pv.set(A_X, i, pos[0]);
+        pv.set(A_Y, i, pos[1]);
+        pv.set(A_Z, i, pos[2]);
     }
 }
 
@@ -606,7 +606,7 @@ void apply_laplace(Ctx& c, bool reuse) {
 __global__ void k_gradient_move(Params P, PView pv, long long n, const double* volg, double pref, double maxc,
                                 unsigned* err) {
     PLOOP(n) {
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+        double pos[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
         Tri t = trilinear(P, pos);
         long long a[2][2];
         if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
@@ -635,9 +635,9 @@ __global__ void k_gradient_move(Params P, PView pv, long long n, const double* v
         pos[1] = pos[1] + ys;
         pos[2] = pos[2] + zs;
         periodic_bc(P, pos);
-        pv.at(A_X, i) = pos[0];
-        pv.at(A_Y, i) = pos[1];
-        pv.at(A_Z, i) = pos[2];
+        pv.set(A_X, i, pos[0]);
+        pv.set(A_Y, i, pos[1]);
+        pv.set(A_Z, i, pos[2]);
     }
 }
 
@@ -650,10 +650,10 @@ void apply_gradient(Ctx& c, bool reuse) {
 
 __global__ void k_periodic(Params P, PView pv, long long n) {
     PLOOP(n) {
-        double p[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+        double p[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
         periodic_bc(P, p);
-        pv.at(A_X, i) = p[0];
-        pv.at(A_Y, i) = p[1];
+        pv.set(A_X, i, p[0]);
+        pv.set(A_Y, i, p[1]);
     }
 }
 
@@ -671,7 +671,7 @@ __global__ void k_split_flag(Params P, PView pv, long long n, int* flag, unsigne
         double b[5];
         load_B(pv, i, b);
         double U[9], D[3];
-        full_matrix<ExactOps>(b, get_B33<ExactOps>(b, pv.at(A_VOL, i), err), U);
+        full_matrix<ExactOps>(b, get_B33<ExactOps>(b, pv.get(A_VOL, i), err), U);
         sz_eigenvalues<ExactOps>(U, D);
         double lam = sqrt(D[0] / D[2]);
         flag[i] = (lam < P.lambda_max && D[0] < P.amax2) ? 0 : 1;
@@ -685,7 +685,7 @@ __global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, 
         long long m = n + offs[i];
         double b[5];
         load_B(pv, i, b);
-        double vol = pv.at(A_VOL, i);
+        double vol = pv.get(A_VOL, i);
         double U[9], D[3], V[9];
         full_matrix<FastOps>(b, get_B33<FastOps>(b, vol, err), U);
         sz_diagonalise<FastOps>(U, D, V);
@@ -697,7 +697,7 @@ __global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, 
         nb[4] = b[4] - 0.75 * D[0] * V[1] * V[2];
         double hv = 0.5 * vol;
         double s = dh * sqrt(D[0]);
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+        double pos[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
         double pc[3], pp[3], bc[5], bp[5];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -713,19 +713,19 @@ __global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, 
         periodic_bc(P, pp);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            pv.at(A_X + k, m) = pc[k];
-            pv.at(A_X + k, i) = pp[k];
-            pv.at(A_VX + k, m) = pv.at(A_VX + k, i);
+            pv.set(A_X + k, m, pc[k]);
+            pv.set(A_X + k, i, pp[k]);
+            pv.set(A_VX + k, m, pv.get(A_VX + k, i));
         }
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            pv.at(A_B11 + k, m) = bc[k];
-            pv.at(A_B11 + k, i) = bp[k];
+            pv.set(A_B11 + k, m, bc[k]);
+            pv.set(A_B11 + k, i, bp[k]);
         }
-        pv.at(A_VOL, m) = hv;
-        pv.at(A_VOL, i) = hv;
-        pv.at(A_BUOY, m) = pv.at(A_BUOY, i);
-        pv.at(A_HUM, m) = pv.at(A_HUM, i);
+        pv.set(A_VOL, m, hv);
+        pv.set(A_VOL, i, hv);
+        pv.set(A_BUOY, m, pv.get(A_BUOY, i));
+        pv.set(A_HUM, m, pv.get(A_HUM, i));
     }
 }
 

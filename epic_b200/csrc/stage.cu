@@ -91,7 +91,7 @@ EPIC_DEV Range cta_range(const Params& P, const PView& pv, const Boxes& B, long 
         R.r1 = min(R.r0 + SCHUNK, n);
         R.ref[0] = R.ref[1] = R.ref[2] = 0;
         if (R.r0 < R.r1) {
-            double p[3] = {pv.at(A_X, R.r0), pv.at(A_Y, R.r0), pv.at(A_Z, R.r0)};
+            double p[3] = {pv.get(A_X, R.r0), pv.get(A_Y, R.r0), pv.get(A_Z, R.r0)};
             cell_of(P, p, R.ref[0], R.ref[1], R.ref[2]);
             R.ref[0] = wrapi(R.ref[0], P.nx);
             R.ref[1] = wrapi(R.ref[1], P.ny);
@@ -183,7 +183,7 @@ EPIC_DEV void win_reduce(WinShared<NF>* ws, WinPart<NF>& wp) {
 
 // Window and fixed-point scales of a round of `count` parcels (one thread).
 template <int NF>
-EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long long count) {
+EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long long count, int max_bits = 50) {
     Window& W = ws->W;
     W.gx0 = R.ref[0] + ws->mn[0] - 1;
     W.gy0 = R.ref[1] + ws->mn[1] - 1;
@@ -196,7 +196,7 @@ EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long 
               (long long)W.WX * W.WY * W.WZ <= WCAP;
     // contributions per grid point <= 4 count <= 2^lg; |window sum| <= 2^(bits + lg) <= 2^62
     int lg = 32 - __clz((unsigned)(4 * count - 1));
-    int bits = min(50, 62 - lg);
+    int bits = min(max_bits, 62 - lg);
     for (int f = 0; f < NF; ++f) {
         double m = __longlong_as_double((long long)ws->vbits[f]);
         if (!(m <= 1.0e300)) ok = false;
@@ -211,6 +211,37 @@ EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long 
 struct Fields7 {
     double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg
 };
+
+// Arithmetic of the two forms: R is the type of the FP32-able attributes,
+// of the gathered values and of the window sums (double: plain, float: mixed).
+template <class R> struct Form {
+    static constexpr bool mixed = false;
+    using Ops = FastOps;
+};
+template <> struct Form<float> {
+    static constexpr bool mixed = true;
+    using Ops = F32Ops;
+};
+
+// Slot k of parcel i: FP64 slots (position, volume, delta_pos) and R slots.
+template <class R>
+EPIC_DEV double& a64(const PView& pv, int k, long long i) {
+    return reinterpret_cast<double*>(reinterpret_cast<char*>(pv.base) +
+                                     (Form<R>::mixed ? mixed_slot_off(k) : 8LL * k) * pv.cap)[i];
+}
+template <class R>
+EPIC_DEV R& aR(const PView& pv, int k, long long i) {
+    return reinterpret_cast<R*>(reinterpret_cast<char*>(pv.base) +
+                                (Form<R>::mixed ? mixed_slot_off(k) : 8LL * k) * pv.cap)[i];
+}
+
+// Window accumulator words per field: three fixed-point limbs (plain, 2^-50
+// resolution) or two (mixed, 2^-36, far below FP32 rounding).
+template <class R> constexpr int win_words() { return Form<R>::mixed ? 2 : NLIMB; }
+template <class R, int NF> constexpr size_t win_bytes() { return sizeof(unsigned) * NF * win_words<R>() * WCAP; }
+// Parcels per round: at most 4 rounds contributions per grid point, 2^14
+// (plain) or 2^13 (mixed: keeps the 19-bit limb sums inside 32 bits).
+template <class R> constexpr int round_max() { return Form<R>::mixed ? 2048 : ROUND; }
 
 // Fixed-point accumulation.  r = wt * vs + 1.5 * 2^52 rounds wt * vs
 // (|wt * vs| <= 2^50) to the integer q once; the low 52 bits of r hold
@@ -232,13 +263,27 @@ EPIC_DEV double fx_value(const unsigned* acc, int w, double inv) {
     return (double)q * inv;
 }
 
+// Two-limb variant (mixed form, |wt * vs| <= 2^36): q = h * 2^19 + l with
+// l = q mod 2^19 and h = floor(q / 2^19), |h| <= 2^17.
+EPIC_DEV void fx2_add(unsigned* acc, int w, double wt, double vs) {
+    double r = fma(wt, vs, FX_MAGIC);
+    long long m = __double_as_longlong(r) & 0xfffffffffffffll;   // 2^51 + q
+    atomicAdd(&acc[w], (unsigned)(m & 0x7ffff));
+    atomicAdd(&acc[WCAP + w], (unsigned)((m >> 19) - (1ll << 32)));
+}
+
+EPIC_DEV double fx2_value(const unsigned* acc, int w, double inv) {
+    long long q = (long long)(int)acc[WCAP + w] * (1ll << 19) + (long long)acc[w];
+    return (double)q * inv;
+}
+
 EPIC_DEV int wrap_to(int l, int n) { return ((unsigned)l < (unsigned)n) ? l : wrapi(l, n); }
 
 // Scatter one support point: vp[f] = value * point weight * volume, vs[f] =
-// vp[f] in fixed-point units.
-template <int NF>
+// vp[f] in fixed-point units (plain form only).
+template <int NF, class R>
 EPIC_DEV void scatter_point(const Params& P, const Window& W, unsigned* acc, const Fields7& F, const double* pt,
-                            const double* vp, const double* vs, unsigned* err) {
+                            const R* vp, const double* vs, unsigned* err) {
     Tri t = trilinear(P, pt);
     if (t.ks < -1 || t.ks > P.nz) { set_err(err, ERRB_ZRANGE); return; }
     int lx = wrap_to(t.is - W.gx0, P.nx), ly = wrap_to(t.js - W.gy0, P.ny), lz = t.ks - W.gz0;
@@ -251,9 +296,15 @@ EPIC_DEV void scatter_point(const Params& P, const Window& W, unsigned* acc, con
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     int w = base + (ii * W.WY + jj) * W.WZ + kk;
-                    double wt = t.w[kk][jj][ii];
+                    if constexpr (Form<R>::mixed) {
+                        const double wt = (double)(float)t.w[kk][jj][ii];
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
+                        for (int f = 0; f < NF; ++f) fx2_add(acc + f * 2 * WCAP, w, wt, vs[f]);
+                    } else {
+                        const double wt = t.w[kk][jj][ii];
+#pragma unroll
+                        for (int f = 0; f < NF; ++f) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
+                    }
                 }
     } else {
         long long a[2][2];
@@ -265,22 +316,22 @@ EPIC_DEV void scatter_point(const Params& P, const Window& W, unsigned* acc, con
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     long long g = a[jj][ii] + kk;
-                    double wt = t.w[kk][jj][ii];
+                    const R wt = (R)t.w[kk][jj][ii];
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) atomicAdd(&F.f[f][g], wt * vp[f]);
+                    for (int f = 0; f < NF; ++f) atomicAdd(&F.f[f][g], (double)(wt * vp[f]));
                 }
     }
 }
 
-template <int NF>
+template <int NF, class R>
 EPIC_DEV void win_zero(unsigned* acc, const Window& W) {
     if (!W.ok) return;
     int n = W.WX * W.WY * W.WZ;
-    for (int f = 0; f < NF * NLIMB; ++f)
+    for (int f = 0; f < NF * win_words<R>(); ++f)
         for (int w = threadIdx.x; w < n; w += blockDim.x) acc[f * WCAP + w] = 0u;
 }
 
-template <int NF>
+template <int NF, class R>
 EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF>* ws, const Fields7& F) {
     const Window W = ws->W;
     if (!W.ok) return;
@@ -293,7 +344,9 @@ EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF
         long long g = fidx(P, W.gz0 + z, wrapi(W.gy0 + y, P.ny), wrapi(W.gx0 + x, P.nx));
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            double v = fx_value(acc + f * NLIMB * WCAP, w, ws->inv[f]);
+            double v;
+            if constexpr (Form<R>::mixed) v = fx2_value(acc + f * 2 * WCAP, w, ws->inv[f]);
+            else v = fx_value(acc + f * NLIMB * WCAP, w, ws->inv[f]);
             if (v != 0.0) atomicAdd(&F.f[f][g], v);
         }
     }
@@ -301,27 +354,27 @@ EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF
 
 // Contributions of one parcel to the par2grid fields (parcel_interpl.f90:177-230):
 // value * point weight (1/4) * volume.
-EPIC_DEV void p2g_values(const Params& P, const double* vor, double z, double vol, double buoy, double hum,
-                         double* vp) {
-    double q_c = hum - P.q_0 * exp(P.lambda_c * (P.lower[2] - z));
-    q_c = fmax(0.0, q_c);
-    double pw = 0.25 * vol;
+template <class R>
+EPIC_DEV void p2g_values(const Params& P, const R* vor, double z, double vol, R buoy, R hum, R* vp) {
+    R q_c = hum - (R)P.q_0 * exp((R)(P.lambda_c * (P.lower[2] - z)));
+    q_c = fmax((R)0, q_c);
+    const R pw = (R)(0.25 * vol);
     vp[0] = pw * vor[0];
     vp[1] = pw * vor[1];
     vp[2] = pw * vor[2];
     vp[3] = pw * buoy;
     vp[4] = pw * hum;
-    vp[5] = pw * (buoy + P.glat * q_c);
+    vp[5] = pw * (buoy + (R)P.glat * q_c);
     vp[6] = pw;
 }
 
-template <int NF>
-EPIC_DEV void load_values(const Params& P, const PView& pv, long long i, double z, double* vp) {
+template <int NF, class R>
+EPIC_DEV void load_values(const Params& P, const PView& pv, long long i, double z, R* vp) {
     if (NF == 7) {
-        double vor[3] = {pv.at(A_VX, i), pv.at(A_VY, i), pv.at(A_VZ, i)};
-        p2g_values(P, vor, z, pv.at(A_VOL, i), pv.at(A_BUOY, i), pv.at(A_HUM, i), vp);
+        R vor[3] = {aR<R>(pv, A_VX, i), aR<R>(pv, A_VY, i), aR<R>(pv, A_VZ, i)};
+        p2g_values<R>(P, vor, z, a64<R>(pv, A_VOL, i), aR<R>(pv, A_BUOY, i), aR<R>(pv, A_HUM, i), vp);
     } else {
-        vp[0] = 0.25 * pv.at(A_VOL, i);
+        vp[0] = (R)(0.25 * a64<R>(pv, A_VOL, i));
     }
 }
 
@@ -334,9 +387,28 @@ EPIC_DEV void count_parcel(const Params& P, const double* pos, double vol, int* 
     if (vol <= P.vmin) atomicAdd(&nsparg[g], 1);
 }
 
+// Support vectors of parcel i: stored ones (reuse) or from B (and stored).
+template <class R>
+EPIC_DEV void vectors(const PView& pv, long long i, bool reuse, bool store, R* eta, R* tau, unsigned* err) {
+    if (reuse) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { eta[k] = aR<R>(pv, A_ETA0 + k, i); tau[k] = aR<R>(pv, A_TAU0 + k, i); }
+        return;
+    }
+    R b[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) b[k] = aR<R>(pv, A_B11 + k, i);
+    if constexpr (Form<R>::mixed) support_vectors_f32(b, a64<R>(pv, A_VOL, i), eta, tau, err);
+    else support_vectors<FastOps>(b, a64<R>(pv, A_VOL, i), eta, tau, nullptr, err);
+    if (store) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { aR<R>(pv, A_ETA0 + k, i) = eta[k]; aR<R>(pv, A_TAU0 + k, i) = tau[k]; }
+    }
+}
+
 // Pass B of a scatter round: support points of parcels [q0, q1) into the
 // window (or the global fields).
-template <int NF>
+template <int NF, class R>
 EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long long q1, const WinShared<NF>* ws,
                             unsigned* acc, const Fields7& F, int* nparg, int* nsparg, bool reuse, bool store,
                             int lg, unsigned* err) {
@@ -359,53 +431,57 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         const int slot = (u << lg) + m;
         if (u >= U || slot >= cnt) continue;
         long long i = q0 + slot;
-        double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
-        double eta[3], tau[3];
-        get_vectors(pv, i, reuse, store, eta, tau, nullptr, err);
-        double vp[NF], vs[NF];
-        load_values<NF>(P, pv, i, pos[2], vp);
+        double pos[3] = {a64<R>(pv, A_X, i), a64<R>(pv, A_Y, i), a64<R>(pv, A_Z, i)};
+        R eta[3], tau[3];
+        vectors<R>(pv, i, reuse, store, eta, tau, err);
+        R vp[NF];
+        double vs[NF];
+        load_values<NF, R>(P, pv, i, pos[2], vp);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) vs[f] = vp[f] * scale[f];
-        if (NF == 7) count_parcel(P, pos, pv.at(A_VOL, i), nparg, nsparg, err);
+        for (int f = 0; f < NF; ++f) vs[f] = (double)vp[f] * scale[f];
+        if (NF == 7) count_parcel(P, pos, a64<R>(pv, A_VOL, i), nparg, nsparg, err);
         for (int p = 0; p < 4; ++p) {
             double cp = support_cos(p), sp = support_sin(p);
             double pt[3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-            scatter_point<NF>(P, W, acc, F, pt, vp, vs, err);
+            for (int k = 0; k < 3; ++k) pt[k] = pos[k] + (double)eta[k] * cp + (double)tau[k] * sp;
+            scatter_point<NF, R>(P, W, acc, F, pt, vp, vs, err);
         }
     }
 }
 
 // par2grid scatter (NF = 7) and vol2grid (NF = 1).
-template <int NF>
+template <int NF, class R>
 __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long long n, Boxes B, Fields7 F,
                                                     int* nparg, int* nsparg, int reuse, int store, int lg,
                                                     unsigned* err) {
     extern __shared__ unsigned acc[];
     __shared__ WinShared<NF> ws;
-    const Range R = cta_range(P, pv, B, n);
-    for (long long q0 = R.r0; q0 < R.r1; q0 += ROUND) {
-        long long q1 = min(q0 + ROUND, R.r1);
+    const Range Rg = cta_range(P, pv, B, n);
+    for (long long q0 = Rg.r0; q0 < Rg.r1; q0 += round_max<R>()) {
+        long long q1 = min(q0 + round_max<R>(), Rg.r1);
         win_begin(&ws);
         __syncthreads();
         WinPart<NF> wp;
         wp.init();
         for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
-            double p[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+            double p[3] = {a64<R>(pv, A_X, i), a64<R>(pv, A_Y, i), a64<R>(pv, A_Z, i)};
+            R vpr[NF];
+            load_values<NF, R>(P, pv, i, p[2], vpr);
             double vp[NF];
-            load_values<NF>(P, pv, i, p[2], vp);
-            wp.add(P, R, p, vp);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) vp[f] = (double)vpr[f];
+            wp.add(P, Rg, p, vp);
         }
         win_reduce(&ws, wp);
         __syncthreads();
-        if (threadIdx.x == 0) win_make(P, R, &ws, q1 - q0);
+        if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 36 : 50);
         __syncthreads();
-        win_zero<NF>(acc, ws.W);
+        win_zero<NF, R>(acc, ws.W);
         __syncthreads();
-        scatter_round<NF>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, lg, err);
+        scatter_round<NF, R>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, lg, err);
         __syncthreads();
-        win_flush<NF>(P, acc, &ws, F);
+        win_flush<NF, R>(P, acc, &ws, F);
         __syncthreads();
     }
 }
@@ -418,18 +494,25 @@ struct FusedArgs {
 };
 
 // The 14 gathered fields (velog 3, velgradg 8, vtend 3) of a grid point as
-// one 128-byte record: a trilinear corner is one cache line, read with 7
-// 16-byte loads at constant offsets.
+// one record of 16 values (128 bytes plain, 64 bytes mixed): a trilinear
+// corner is one record, read with 16-byte loads at constant offsets.
 constexpr int GREC = 16;
 
-__global__ void k_pack_gather(GatherFields G, double* pack, long long fsz) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < fsz * (GREC / 2);
+template <class R>
+__global__ void k_pack_gather(GatherFields G, R* pack, long long fsz) {
+    constexpr int V = 16 / sizeof(R);   // values per 16-byte word
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < fsz * (GREC / V);
          e += (long long)gridDim.x * blockDim.x) {
-        long long g = e >> 3;
-        int l2 = (int)(e & 7);
-        double2 v = make_double2(0.0, 0.0);
-        if (l2 < 7) v = make_double2(G.f[2 * l2][g], G.f[2 * l2 + 1][g]);
-        reinterpret_cast<double2*>(pack)[e] = v;
+        long long g = e / (GREC / V);
+        int q = (int)(e - g * (GREC / V));
+        R v[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            int l = q * V + j;
+            v[j] = l < 14 ? (R)G.f[l][g] : (R)0;
+        }
+        if constexpr (Form<R>::mixed) reinterpret_cast<float4*>(pack)[e] = make_float4(v[0], v[1], v[2], v[3]);
+        else reinterpret_cast<double2*>(pack)[e] = make_double2(v[0], v[1]);
     }
 }
 
@@ -444,7 +527,8 @@ EPIC_DEV int wrap_near(int i, int n) {
 // g[l] += sum over the 8 corners of (w / 4) f_l (interpl.f90:17-56, the
 // point weight 1/4 of parcel_interpl.f90:433).  Returns false when the
 // point leaves the vertical halo.
-EPIC_DEV bool gather_point(const Params& P, const double* __restrict__ pack, const double* pt, double* g) {
+template <class R>
+EPIC_DEV bool gather_point(const Params& P, const R* __restrict__ pack, const double* pt, R* g) {
     Tri t = trilinear(P, pt);
     if (t.ks < -1 || t.ks > P.nz) return false;
     const int i0 = wrap_near(t.is, P.nx), i1 = wrap_near(t.is + 1, P.nx);
@@ -454,25 +538,49 @@ EPIC_DEV bool gather_point(const Params& P, const double* __restrict__ pack, con
 #pragma unroll
         for (int jj = 0; jj < 2; ++jj) {
             const long long a = fidx(P, t.ks, jj ? j1 : j0, ii ? i1 : i0);
-            const double2* q = reinterpret_cast<const double2*>(pack + a * GREC);
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk) {
-                const double w = 0.25 * t.w[kk][jj][ii];
+                const R w = (R)(0.25 * t.w[kk][jj][ii]);
+                if constexpr (Form<R>::mixed) {
+                    const float4* q = reinterpret_cast<const float4*>(pack + (a + kk) * GREC);
 #pragma unroll
-                for (int l2 = 0; l2 < 7; ++l2) {
-                    const double2 v = __ldg(q + kk * (GREC / 2) + l2);
-                    g[2 * l2] = fma(w, v.x, g[2 * l2]);
-                    g[2 * l2 + 1] = fma(w, v.y, g[2 * l2 + 1]);
+                    for (int l4 = 0; l4 < 4; ++l4) {
+                        const float4 v = __ldg(q + l4);
+                        g[4 * l4] = fmaf(w, v.x, g[4 * l4]);
+                        g[4 * l4 + 1] = fmaf(w, v.y, g[4 * l4 + 1]);
+                        if (4 * l4 + 2 < 14) g[4 * l4 + 2] = fmaf(w, v.z, g[4 * l4 + 2]);
+                        if (4 * l4 + 3 < 14) g[4 * l4 + 3] = fmaf(w, v.w, g[4 * l4 + 3]);
+                    }
+                } else {
+                    const double2* q = reinterpret_cast<const double2*>(pack + (a + kk) * GREC);
+#pragma unroll
+                    for (int l2 = 0; l2 < 7; ++l2) {
+                        const double2 v = __ldg(q + l2);
+                        g[2 * l2] = fma(w, v.x, g[2 * l2]);
+                        g[2 * l2 + 1] = fma(w, v.y, g[2 * l2 + 1]);
+                    }
                 }
             }
         }
     return true;
 }
 
-template <bool DIAG, bool SCATTER>
-__global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long n, Boxes B, GatherFields G,
+// get_dBdt (parcel_ellipsoid.f90:466-507) in the attribute type.
+template <class R>
+EPIC_DEV void dBdt_r(const R* s, const R* b, R B33, R* o) {
+    R dwdz = -(s[I_DUDX] + s[I_DVDY]);
+    o[0] = R(2) * (s[I_DUDX] * b[0] + s[I_DUDY] * b[1] + s[I_DUDZ] * b[2]);
+    o[1] = s[I_DVDX] * b[0] - dwdz * b[1] + s[I_DVDZ] * b[2] + s[I_DUDY] * b[3] + s[I_DUDZ] * b[4];
+    o[2] = s[I_DWDX] * b[0] + s[I_DWDY] * b[1] - s[I_DVDY] * b[2] + s[I_DUDY] * b[4] + s[I_DUDZ] * B33;
+    o[3] = R(2) * (s[I_DVDX] * b[1] + s[I_DVDY] * b[3] + s[I_DVDZ] * b[4]);
+    o[4] = s[I_DWDX] * b[1] + s[I_DVDX] * b[2] + s[I_DWDY] * b[3] - s[I_DUDX] * b[4] + s[I_DVDZ] * B33;
+}
+
+template <bool DIAG, bool SCATTER, class R>
+__global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long n, Boxes B, const R* pack,
                                                   Fields7 F, int* nparg, int* nsparg, FusedArgs S,
                                                   const StepScalars* sc, double* partials, unsigned* err) {
+    using Ops = typename Form<R>::Ops;
     extern __shared__ unsigned acc[];
     __shared__ WinShared<7> ws;
     __shared__ double red[PB / 32][NDIAG];
@@ -481,9 +589,9 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
 #pragma unroll
     for (int k = 0; k < ND; ++k) dacc[k] = 0.0;
     const double dt = sc->dt;
-    const Range R = cta_range(P, pv, B, n);
-    for (long long q0 = R.r0; q0 < R.r1; q0 += ROUND) {
-        long long q1 = min(q0 + ROUND, R.r1);
+    const Range Rg = cta_range(P, pv, B, n);
+    for (long long q0 = Rg.r0; q0 < Rg.r1; q0 += round_max<R>()) {
+        long long q1 = min(q0 + round_max<R>(), Rg.r1);
         if (SCATTER) {
             win_begin(&ws);
             __syncthreads();
@@ -492,105 +600,123 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
         wp.init();
         // pass A: grid2par + dB/dt + LS-RK update
         for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
-            double pos[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
-            double g[14];
+            double pos[3] = {a64<R>(pv, A_X, i), a64<R>(pv, A_Y, i), a64<R>(pv, A_Z, i)};
+            R g[14];
 #pragma unroll
-            for (int l = 0; l < 14; ++l) g[l] = 0.0;
+            for (int l = 0; l < 14; ++l) g[l] = (R)0;
             {
-                double eta[3], tau[3];
+                R eta[3], tau[3];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) { eta[k] = pv.at(A_ETA0 + k, i); tau[k] = pv.at(A_TAU0 + k, i); }
+                for (int k = 0; k < 3; ++k) { eta[k] = aR<R>(pv, A_ETA0 + k, i); tau[k] = aR<R>(pv, A_TAU0 + k, i); }
                 for (int p = 0; p < 4; ++p) {
                     double cp = support_cos(p), sp = support_sin(p);
                     double pt[3];
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
-                    if (!gather_point(P, G.pack, pt, g)) set_err(err, ERRB_ZRANGE);
+                    for (int k = 0; k < 3; ++k) pt[k] = pos[k] + (double)eta[k] * cp + (double)tau[k] * sp;
+                    if (!gather_point<R>(P, pack, pt, g)) set_err(err, ERRB_ZRANGE);
                 }
             }
-            double b[5];
-            load_B(pv, i, b);
-            double vol = pv.at(A_VOL, i);
-            double dp[3], dv[3], vor[3] = {pv.at(A_VX, i), pv.at(A_VY, i), pv.at(A_VZ, i)};
+            R b[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) b[k] = aR<R>(pv, A_B11 + k, i);
+            const double vol = a64<R>(pv, A_VOL, i);
+            double dp[3];
+            R dv[3], vor[3] = {aR<R>(pv, A_VX, i), aR<R>(pv, A_VY, i), aR<R>(pv, A_VZ, i)};
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                dp[k] = S.stage > 1 ? pv.at(A_DX + k, i) + g[k] : g[k];
-                dv[k] = S.stage > 1 ? pv.at(A_DVX + k, i) + g[11 + k] : g[11 + k];
+                dp[k] = S.stage > 1 ? a64<R>(pv, A_DX + k, i) + (double)g[k] : (double)g[k];
+                dv[k] = S.stage > 1 ? aR<R>(pv, A_DVX + k, i) + g[11 + k] : g[11 + k];
             }
-            const double* strain = &g[3];
+            const R* strain = &g[3];
+            // B33 from the volume constraint in FP64 (parcel_ellipsoid.f90:383-402)
+            double bd[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) bd[k] = (double)b[k];
+            const double B33d = get_B33<FastOps>(bd, vol, err);
             if (DIAG) {
                 // parcel diagnostics before the update (ls_rk.f90:116, parcel_diagnostics.f90:66-120)
-                double U[9], D[3];
-                full_matrix<FastOps>(b, get_B33<FastOps>(b, vol, err), U);
-                sz_eigenvalues<FastOps>(U, D);
-                double bu = pv.at(A_BUOY, i);
+                R U[9], D[3];
+                full_matrix<Ops>(b, (R)B33d, U);
+                sz_eigenvalues<Ops>(U, D);
+                double bu = (double)aR<R>(pv, A_BUOY, i);
+                double vx = vor[0], vy = vor[1], vz = vor[2];
                 dacc[0] += (dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]) * vol;
-                dacc[1] += (vor[0] * vor[0] + vor[1] * vor[1] + vor[2] * vor[2]) * vol;
-                double lam = sqrt(D[0] / D[2]);
+                dacc[1] += (vx * vx + vy * vy + vz * vz) * vol;
+                double lam = sqrt((double)D[0] / (double)D[2]);
                 dacc[2] += lam;
                 dacc[3] += lam * lam;
                 dacc[4] += vol;
                 dacc[5] += vol * vol;
                 if (vol <= P.vmin) dacc[6] += 1.0;
-                dacc[7] += vol * (vor[0] * vor[0]);
-                dacc[8] += vol * (vor[1] * vor[1]);
-                dacc[9] += vol * (vor[2] * vor[2]);
+                dacc[7] += vol * (vx * vx);
+                dacc[8] += vol * (vy * vy);
+                dacc[9] += vol * (vz * vz);
                 dacc[10] = fmin(dacc[10], bu);
                 dacc[11] = fmax(dacc[11], bu);
             }
-            double B33 = get_B33<FastOps>(b, vol, err);
-            double db[5];
-            dBdt(strain, b, B33, db);
+            R db[5];
+            dBdt_r<R>(strain, b, (R)B33d, db);
             if (S.stage > 1) {
 #pragma unroll
-                for (int k = 0; k < 5; ++k) db[k] = pv.at(A_DB0 + k, i) + db[k];
+                for (int k = 0; k < 5; ++k) db[k] = aR<R>(pv, A_DB0 + k, i) + db[k];
             }
-            double cdt = S.cb * dt;
+            const double cdt = S.cb * dt;
+            const R cdtr = (R)cdt;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 pos[k] = pos[k] + cdt * dp[k];
-                vor[k] = vor[k] + cdt * dv[k];
+                vor[k] = vor[k] + cdtr * dv[k];
             }
 #pragma unroll
-            for (int k = 0; k < 5; ++k) b[k] = b[k] + cdt * db[k];
+            for (int k = 0; k < 5; ++k) b[k] = b[k] + cdtr * db[k];
             periodic_bc(P, pos);
             if (S.last) {
-                reflective_bc(P, pos, b);
+                if (pos[2] > P.upper[2]) {
+                    pos[2] = 2.0 * P.upper[2] - pos[2];
+                    b[2] = -b[2]; b[4] = -b[4];
+                } else if (pos[2] < P.lower[2]) {
+                    pos[2] = 2.0 * P.lower[2] - pos[2];
+                    b[2] = -b[2]; b[4] = -b[4];
+                }
             } else {
+                const R car = (R)S.ca;
 #pragma unroll
-                for (int k = 0; k < 3; ++k) { dp[k] = S.ca * dp[k]; dv[k] = S.ca * dv[k]; }
+                for (int k = 0; k < 3; ++k) { dp[k] = S.ca * dp[k]; dv[k] = car * dv[k]; }
 #pragma unroll
-                for (int k = 0; k < 5; ++k) db[k] = S.ca * db[k];
+                for (int k = 0; k < 5; ++k) db[k] = car * db[k];
             }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                pv.at(A_X + k, i) = pos[k];
-                pv.at(A_VX + k, i) = vor[k];
-                pv.at(A_DX + k, i) = dp[k];
-                pv.at(A_DVX + k, i) = dv[k];
+                a64<R>(pv, A_X + k, i) = pos[k];
+                aR<R>(pv, A_VX + k, i) = vor[k];
+                a64<R>(pv, A_DX + k, i) = dp[k];
+                aR<R>(pv, A_DVX + k, i) = dv[k];
             }
 #pragma unroll
             for (int k = 0; k < 5; ++k) {
-                pv.at(A_B11 + k, i) = b[k];
-                pv.at(A_DB0 + k, i) = db[k];
+                aR<R>(pv, A_B11 + k, i) = b[k];
+                aR<R>(pv, A_DB0 + k, i) = db[k];
             }
             if (SCATTER) {
+                R vpr[7];
+                p2g_values<R>(P, vor, pos[2], vol, aR<R>(pv, A_BUOY, i), aR<R>(pv, A_HUM, i), vpr);
                 double vp[7];
-                p2g_values(P, vor, pos[2], vol, pv.at(A_BUOY, i), pv.at(A_HUM, i), vp);
-                wp.add(P, R, pos, vp);
+#pragma unroll
+                for (int f = 0; f < 7; ++f) vp[f] = (double)vpr[f];
+                wp.add(P, Rg, pos, vp);
             }
         }
         if (SCATTER) {
             win_reduce(&ws, wp);
             __syncthreads();
-            if (threadIdx.x == 0) win_make(P, R, &ws, q1 - q0);
+            if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 36 : 50);
             __syncthreads();
-            win_zero<7>(acc, ws.W);
+            win_zero<7, R>(acc, ws.W);
             __syncthreads();
             // pass B: support vectors of the advanced shape + next par2grid
-            scatter_round<7>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, false, true, S.lg, err);
+            scatter_round<7, R>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, false, true, S.lg, err);
             __syncthreads();
-            win_flush<7>(P, acc, &ws, F);
+            win_flush<7, R>(P, acc, &ws, F);
             __syncthreads();
         }
     }
@@ -663,16 +789,23 @@ static void set_smem(K kernel, size_t bytes) {
     CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
+template <int NF, class R>
+static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int lg) {
+    size_t sm = win_bytes<R, NF>();
+    set_smem(k_scatter<NF, R>, sm);
+    Boxes B = boxes(c);
+    k_scatter<NF, R><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, NF == 7 ? c.nparg : nullptr,
+                                                         NF == 7 ? c.nsparg : nullptr, reuse, store, lg,
+                                                         &c.dsc->err);
+    CKL();
+}
+
 void scatter_p2g(Ctx& c, bool reuse, bool store) {
     zero_p2g_fields(c);
     if (c.n == 0) return;
-    size_t sm = sizeof(unsigned) * 7 * NLIMB * WCAP;
-    set_smem(k_scatter<7>, sm);
-    Boxes B = boxes(c);
     prof_begin(c, "p2g");
-    k_scatter<7><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, fields7(c), c.nparg, c.nsparg, reuse, store,
-                                                     c.scatter_lg[1], &c.dsc->err);
-    CKL();
+    if (c.pv.mixed) launch_scatter<7, float>(c, fields7(c), reuse, store, c.scatter_lg[1]);
+    else launch_scatter<7, double>(c, fields7(c), reuse, store, c.scatter_lg[1]);
     prof_end(c, "p2g");
 }
 
@@ -681,13 +814,43 @@ void scatter_v2g(Ctx& c, bool reuse) {
     if (c.n == 0) return;
     Fields7 F;
     F.f[0] = c.volg();
-    size_t sm = sizeof(unsigned) * 1 * NLIMB * WCAP;
-    Boxes B = boxes(c);
     prof_begin(c, "v2g");
-    k_scatter<1><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, nullptr, nullptr, reuse, 1,
-                                                     c.scatter_lg[0], &c.dsc->err);
-    CKL();
+    if (c.pv.mixed) launch_scatter<1, float>(c, F, reuse, true, c.scatter_lg[0]);
+    else launch_scatter<1, double>(c, F, reuse, true, c.scatter_lg[0]);
     prof_end(c, "v2g");
+}
+
+template <class R>
+static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatter) {
+    GatherFields G;
+    for (int k = 0; k < 3; ++k) G.f[k] = c.velog(k);
+    for (int k = 0; k < 8; ++k) G.f[3 + k] = c.velgrad(k);
+    for (int k = 0; k < 3; ++k) G.f[11 + k] = c.vtend(k);
+    G.pack = nullptr;
+    R* pack = reinterpret_cast<R*>(c.gpack);
+    constexpr int V = 16 / sizeof(R);
+    k_pack_gather<R><<<pgrid(c.P.fsz * (GREC / V)), PB, 0, c.stream>>>(G, pack, c.P.fsz);
+    CKL();
+    if (scatter) zero_p2g_fields(c);
+    Boxes B = boxes(c);
+    int g = sgrid(c, B);
+    if (with_diag) {
+        c.n_partials = g;
+        c.diag_buf = c.stage_partials;
+    }
+    size_t sm = scatter ? win_bytes<R, 7>() : 0;
+    auto launch = [&](auto kernel) {
+        if (sm) set_smem(kernel, sm);
+        prof_begin(c, "stage");
+        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, pack, fields7(c), c.nparg, c.nsparg, S, c.dsc,
+                                        c.stage_partials, &c.dsc->err);
+        CKL();
+        prof_end(c, "stage");
+    };
+    if (with_diag && scatter) launch(k_stage<true, true, R>);
+    else if (with_diag) launch(k_stage<true, false, R>);
+    else if (scatter) launch(k_stage<false, true, R>);
+    else launch(k_stage<false, false, R>);
 }
 
 // One LS-RK stage (grid2par + update) fused with the next stage's par2grid
@@ -700,33 +863,8 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     S.cb = c.cb[stage - 1];
     S.lg = c.scatter_lg[2];
     bool scatter = !S.last;
-    GatherFields G;
-    for (int k = 0; k < 3; ++k) G.f[k] = c.velog(k);
-    for (int k = 0; k < 8; ++k) G.f[3 + k] = c.velgrad(k);
-    for (int k = 0; k < 3; ++k) G.f[11 + k] = c.vtend(k);
-    G.pack = c.gpack;
-    k_pack_gather<<<pgrid(c.P.fsz * (GREC / 2)), PB, 0, c.stream>>>(G, c.gpack, c.P.fsz);
-    CKL();
-    if (scatter) zero_p2g_fields(c);
-    Boxes B = boxes(c);
-    int g = sgrid(c, B);
-    if (with_diag) {
-        c.n_partials = g;
-        c.diag_buf = c.stage_partials;
-    }
-    size_t sm = scatter ? sizeof(unsigned) * 7 * NLIMB * WCAP : 0;
-    auto launch = [&](auto kernel) {
-        if (sm) set_smem(kernel, sm);
-        prof_begin(c, "stage");
-        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, G, fields7(c), c.nparg, c.nsparg, S, c.dsc,
-                                        c.stage_partials, &c.dsc->err);
-        CKL();
-        prof_end(c, "stage");
-    };
-    if (with_diag && scatter) launch(k_stage<true, true>);
-    else if (with_diag) launch(k_stage<true, false>);
-    else if (scatter) launch(k_stage<false, true>);
-    else launch(k_stage<false, false>);
+    if (c.pv.mixed) launch_stage<float>(c, S, with_diag, scatter);
+    else launch_stage<double>(c, S, with_diag, scatter);
 }
 
 // ---------------------------------------------------------------------------
@@ -736,7 +874,7 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
 __global__ void k_sort_keys(Params P, PView pv, long long n, unsigned* key, int* idx) {
     int nby = (P.ny + BOXY - 1) / BOXY, nbz = (P.nz + BOXZ - 1) / BOXZ;
     PLOOP(n) {
-        double p[3] = {pv.at(A_X, i), pv.at(A_Y, i), pv.at(A_Z, i)};
+        double p[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
         int ci, cj, ck;
         cell_of(P, p, ci, cj, ck);
         ci = min(max(ci, 0), P.nx - 1);
@@ -768,7 +906,7 @@ __global__ void k_permute(PView src, PView dst, long long n, const int* perm) {
         int a = (int)(t / n);
         long long i = t - (long long)a * n;
         int k = attrs[a];
-        dst.at(k, i) = src.at(k, perm[i]);
+        dst.set(k, i, src.get(k, perm[i]));
     }
 }
 
@@ -795,7 +933,7 @@ void sort_parcels(Ctx& c) {
     CK(cub::DeviceRadixSort::SortPairs(tmp, cubb, k0, k1, i0, i1, (int)n, 0, endbit, c.stream));
     k_box_start<<<pgrid(n), PB, 0, c.stream>>>(k1, n, c.nbox, c.box_start);
     CKL();
-    PView dst{c.pv_alt, c.cap};
+    PView dst{c.pv_alt, c.cap, c.pv.mixed};
     k_permute<<<pgrid(n * 20), PB, 0, c.stream>>>(c.pv, dst, n, i1);
     CKL();
     std::swap(c.pv.base, c.pv_alt);

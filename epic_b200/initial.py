@@ -174,12 +174,15 @@ def thermal(nx=128, ny=None, nz=None, extent=(6.28, 6.28, 6.28), seed=1234, n_pe
 
 
 def config(name: str, **kw) -> Setup:
-    """Named workloads: 'beltrami-32' (32^3, 262,144 parcels) and
-    'thermal-128' (128^3, 16.8M parcels) plus small test variants."""
+    """Named workloads: 'beltrami-32' (32^3, 262,144 parcels), 'thermal-128'
+    (128^3, 16.8M parcels), 'thermal-256x256x128' (domain 6.28 x 6.28 x 3.14,
+    67.1M parcels: the mixed-precision workload) plus small test variants."""
     if name == "beltrami-32":
         return beltrami(32, **kw)
     if name == "thermal-128":
         return thermal(128, **kw)
+    if name == "thermal-256x256x128":
+        return thermal(256, 256, 128, extent=(6.28, 6.28, 3.14), steps=100, name=name, **kw)
     if name.startswith("beltrami-"):
         return beltrami(int(name.split("-")[1]), **kw)
     if name.startswith("thermal-"):

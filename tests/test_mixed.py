@@ -1,0 +1,84 @@
+"""Mixed-precision form (EPIC_PRECISION_MIXED) against the FP64 oracle and the
+plain FP64 GPU path.
+
+The mixed form keeps vorticity, B, buoyancy, humidity, the RK accumulators of
+vorticity and B and the support vectors in FP32, accumulates par2grid and
+interpolates grid2par in FP32, and keeps positions, volume, delta_pos and the
+B33 volume constraint in FP64.  Tolerances are relative to the field or
+quantity scale.
+"""
+import numpy as np
+import pytest
+
+from epic_b200 import abi, make_context
+from tests.helpers import pair, small_state
+
+pytestmark = pytest.mark.gpu
+
+MIXED = 1
+FIELD_TOL = 2e-6      # one par2grid / vor2vel in FP32 against FP64
+DRIFT_TOL = 1e-5      # energy / enstrophy after many steps, mixed vs plain
+
+
+def _rel(a, b):
+    scale = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / scale
+
+
+def test_mixed_par2grid_vs_oracle(olib, glib):
+    s = small_state("thermal")
+    oc = make_context(s, olib)
+    gc = make_context(s, glib, precision=MIXED)
+    oc.par2grid(False)
+    gc.par2grid(False)
+    for fid in list(abi.VORTG) + [abi.TBUOYG, abi.VOLG]:
+        assert _rel(gc.get_field(fid), oc.get_field(fid)) < FIELD_TOL, fid
+
+
+def test_mixed_rk_step_vs_oracle(olib, glib):
+    s = small_state("thermal")
+    oc = make_context(s, olib)
+    gc = make_context(s, glib, precision=MIXED)
+    _, dto = oc.rk_step(0.0)
+    _, dtg = gc.rk_step(0.0)
+    assert abs(dtg - dto) / dto < 1e-5
+    po, pg = oc.get_parcels(), gc.get_parcels()
+    assert np.abs(pg["pos"] - po["pos"]).max() < 1e-6 * s.dx.min()
+    for key in ("vor", "B"):
+        assert _rel(pg[key], po[key]) < 1e-5, key
+    for fid in list(abi.VELOG):
+        assert _rel(gc.get_field(fid), oc.get_field(fid)) < 1e-5, fid
+
+
+def test_mixed_store_round_trip(glib):
+    """set_parcels / get_parcels of the mixed store: FP64 positions and volume
+    come back exactly, FP32 attributes rounded once."""
+    s = small_state("beltrami")
+    gc = make_context(s, glib, precision=MIXED)
+    p = gc.get_parcels()
+    assert np.array_equal(p["pos"], s.pos)
+    assert np.array_equal(p["vol"], s.vol)
+    assert np.array_equal(p["vor"], s.vor.astype(np.float32).astype(np.float64))
+    assert np.array_equal(p["B"], s.B.astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("kind,steps,dt", [("thermal", 100, 0.05), ("beltrami", 100, 0.02)])
+def test_mixed_drift_vs_plain(glib, kind, steps, dt):
+    """Energy and enstrophy of the mixed form track the plain FP64 run of the
+    same seed within 1e-5 relative after 100 full steps (merge, split and
+    corrections on).  The step is fixed so that both runs compare the same
+    times: with the adaptive step the thermal reaches its turbulent phase,
+    where any rounding difference, FP64 ones included, grows."""
+    s = small_state(kind, small_frac=0.02)
+    runs = {}
+    for prec in (0, MIXED):
+        c = make_context(s, glib, precision=prec, keep_order=0, use_fixed_dt=1, fixed_dt=dt,
+                         capacity=4 * s.n)
+        t = 0.0
+        for _ in range(steps):
+            t, info = c.step(t)
+        runs[prec] = (info.parcel_stats[1], info.parcel_stats[12], c.get_field(abi.VELOG[2]))
+    ke0, en0, w0 = runs[0]
+    ke1, en1, w1 = runs[MIXED]
+    assert abs(ke1 - ke0) / abs(ke0) < DRIFT_TOL
+    assert abs(en1 - en0) / abs(en0) < DRIFT_TOL
