@@ -92,7 +92,9 @@ struct Ctx {
     int n_work = 0;
     double* work = nullptr;
     FFTPlan px, py;
-    bool use_plane_fft = true;   // 2-D plane kernel where the grid allows it
+    // horizontal FFT: 0 = 2-D plane kernel where the grid allows it, else the
+    // tiled line kernel, else Stockham lines; 1 = tiled, else Stockham; 2 = Stockham
+    int fft_path = 0;
     double* gpack = nullptr;     // gathered fields, 16 doubles per grid point
     // log2 of the consecutive parcels a lane group scatters (vol2grid,
     // par2grid, fused stage)

@@ -242,6 +242,7 @@ template <> struct Radix<16> { static constexpr int N1 = 4, N2 = 4; };
 template <> struct Radix<32> { static constexpr int N1 = 8, N2 = 4; };
 template <> struct Radix<64> { static constexpr int N1 = 8, N2 = 8; };
 template <> struct Radix<128> { static constexpr int N1 = 16, N2 = 8; };
+template <> struct Radix<256> { static constexpr int N1 = 16, N2 = 16; };
 
 // Line geometry inside the plane: real element c of line a at P[a0 + c*es],
 // of line b at P[a0 + c*es + bo]; complex scratch element c at P[s0 + c*cs].
@@ -402,6 +403,79 @@ static void launch_plane(Ctx& c, const double* const* in, double* const* out, in
     prof_end(c, "fft");
 }
 
+// Tiled line FFT along x (axis 0) or y (axis 1) for power-of-two lengths
+// n = 16 .. 256: a CTA loads TL = 32 consecutive z-lines (coalesced 256-byte
+// rows) of one (y or x) index into shared memory as rows of n + 2, and
+// transforms them as TL/2 complex line pairs with line_fft.
+constexpr int TL = 32;
+
+template <int N, bool FWD>
+__global__ void __launch_bounds__((TL / 2) * Radix<N>::N2) k_fft_tile(FFTBatch B) {
+    constexpr int S = N + 2, N2 = Radix<N>::N2;
+    extern __shared__ double P[];
+    __shared__ C2 tw[N];
+    const double* in = B.in[blockIdx.z];
+    double* out = B.out[blockIdx.z];
+    const int l0 = blockIdx.x * TL;
+    const long long rowbase = (long long)blockIdx.y * B.row_stride + 1;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = c2(B.tw[i].x, B.tw[i].y);
+    for (int idx = threadIdx.x; idx < TL * N; idx += blockDim.x) {
+        const int l = idx % TL, e = idx / TL;
+        const int line = l0 + l;
+        P[l * S + e] = (line < B.nl) ? in[rowbase + line + (long long)e * B.es] : 0.0;
+    }
+    __syncthreads();
+    const int pair = threadIdx.x / N2, t = threadIdx.x - pair * N2;
+    const LineGeo g = {2 * pair * S, 1, S, 2 * pair * S, 2};
+    line_fft<N, FWD>(P, g, t, tw, B.scale);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < TL * N; idx += blockDim.x) {
+        const int l = idx % TL, e = idx / TL;
+        const int line = l0 + l;
+        if (line < B.nl) out[rowbase + line + (long long)e * B.es] = P[l * S + e];
+    }
+}
+
+template <int N>
+static void launch_tile_axis(Ctx& c, const FFTPlan& pl, int axis, const double* const* in, double* const* out,
+                             int nf, bool forward) {
+    const Params& P = c.P;
+    FFTBatch B;
+    for (int f = 0; f < nf; ++f) { B.in[f] = in[f]; B.out[f] = out[f]; }
+    B.n = N;
+    B.tw = pl.tw;
+    B.nl = P.nz + 1;
+    B.scale = 1.0 / std::sqrt((double)N);
+    int nrows;
+    if (axis == 0) { B.es = (long long)P.ny * P.nzh; B.row_stride = P.nzh; nrows = P.ny; }
+    else { B.es = P.nzh; B.row_stride = (long long)P.ny * P.nzh; nrows = P.nx; }
+    size_t sm = sizeof(double) * (size_t)TL * (N + 2);
+    dim3 grid((B.nl + TL - 1) / TL, nrows, nf);
+    int threads = (TL / 2) * Radix<N>::N2;
+    prof_begin(c, "fft");
+    if (forward) {
+        CK(cudaFuncSetAttribute(k_fft_tile<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fft_tile<N, true><<<grid, threads, sm, c.stream>>>(B);
+    } else {
+        CK(cudaFuncSetAttribute(k_fft_tile<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fft_tile<N, false><<<grid, threads, sm, c.stream>>>(B);
+    }
+    CKL();
+    prof_end(c, "fft");
+}
+
+static bool tile_axis(Ctx& c, const FFTPlan& pl, int axis, const double* const* in, double* const* out, int nf,
+                      bool forward) {
+    switch (pl.n) {
+        case 16: launch_tile_axis<16>(c, pl, axis, in, out, nf, forward); return true;
+        case 32: launch_tile_axis<32>(c, pl, axis, in, out, nf, forward); return true;
+        case 64: launch_tile_axis<64>(c, pl, axis, in, out, nf, forward); return true;
+        case 128: launch_tile_axis<128>(c, pl, axis, in, out, nf, forward); return true;
+        case 256: launch_tile_axis<256>(c, pl, axis, in, out, nf, forward); return true;
+        default: return false;
+    }
+}
+
 // Plane kernel sizes: square n x n grids with n = 16, 32, 64, 128.
 static bool plane_fft(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
     const Params& P = c.P;
@@ -474,13 +548,18 @@ static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* cons
 void fft_xy(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
     for (int f0 = 0; f0 < nf; f0 += MAXF) {
         int k = std::min(MAXF, nf - f0);
-        if (c.use_plane_fft && plane_fft(c, in + f0, out + f0, k, forward)) continue;
+        if (c.fft_path == 0 && plane_fft(c, in + f0, out + f0, k, forward)) continue;
+        // per axis: tiled register FFT for powers of two up to 256, else Stockham lines
+        auto axis = [&](const FFTPlan& pl, int ax, const double* const* src, double* const* dst, bool fwd) {
+            if (c.fft_path <= 1 && tile_axis(c, pl, ax, src, dst, k, fwd)) return;
+            run_fft_axis(c, pl, ax, src, dst, k, fwd);
+        };
         if (forward) {
-            run_fft_axis(c, c.py, 1, in + f0, out + f0, k, true);
-            run_fft_axis(c, c.px, 0, out + f0, out + f0, k, true);
+            axis(c.py, 1, in + f0, out + f0, true);
+            axis(c.px, 0, out + f0, out + f0, true);
         } else {
-            run_fft_axis(c, c.px, 0, in + f0, out + f0, k, false);
-            run_fft_axis(c, c.py, 1, out + f0, out + f0, k, false);
+            axis(c.px, 0, in + f0, out + f0, false);
+            axis(c.py, 1, out + f0, out + f0, false);
         }
     }
 }

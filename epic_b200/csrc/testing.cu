@@ -63,9 +63,10 @@ extern "C" int epic_gpu_test_diverge(epic_ctx* ctx, const double* phi, double* g
     return EPIC_OK;
 }
 
-extern "C" int epic_gpu_test_set_fft_path(epic_ctx* ctx, int plane) {
+extern "C" int epic_gpu_test_set_fft_path(epic_ctx* ctx, int path) {
     if (!ctx) return EPIC_ERR_ARG;
-    ctx->c.use_plane_fft = plane != 0;
+    if (path < 0 || path > 2) return EPIC_ERR_ARG;
+    ctx->c.fft_path = path;
     return EPIC_OK;
 }
 

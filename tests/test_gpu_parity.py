@@ -77,12 +77,14 @@ def test_eigen_exact_matches_oracle_bitwise(glib, olib):
     assert np.abs(D - Do).max() <= 4 * np.spacing(np.abs(Do).max())
 
 
-@pytest.mark.parametrize("shape,plane", [((64, 64, 64), 1), ((64, 64, 64), 0), ((16, 16, 16), 1),
-                                         ((32, 32, 24), 1), ((128, 128, 32), 1), ((48, 32, 16), 1)])
+@pytest.mark.parametrize("shape,plane", [((64, 64, 64), 0), ((64, 64, 64), 1), ((64, 64, 64), 2),
+                                         ((16, 16, 16), 0), ((32, 32, 24), 0), ((128, 128, 32), 0),
+                                         ((48, 32, 16), 0), ((256, 256, 16), 0), ((64, 256, 16), 0)])
 def test_vor2vel_taylor_green_kat(glib, shape, plane):
     """test_mpi_vor2vel.f90: Taylor-Green vorticity on 64^3, max err < 1e-14; the
-    same flow on other grids through both horizontal FFT paths (the 2-D plane
-    kernel for square 16..128 grids, the line kernels otherwise)."""
+    same flow on other grids through the three horizontal FFT paths (2-D plane
+    kernel for square 16..128 grids, tiled register FFT for power-of-two axes
+    up to 256, Stockham lines otherwise)."""
     nx, ny, nz = shape
     lower = (-math.pi, -math.pi, -0.5 * math.pi)
     extent = (2 * math.pi, 2 * math.pi, 2 * math.pi)
@@ -122,7 +124,7 @@ def test_par2grid(olib, glib, kind):
         assert np.array_equal(gc.get_field(fid)[:, :, 1:-2], oc.get_field(fid)[:, :, 1:-2])
 
 
-@pytest.mark.parametrize("kind,plane", [("thermal", 1), ("beltrami", 1), ("thermal", 0)])
+@pytest.mark.parametrize("kind,plane", [("thermal", 0), ("beltrami", 0), ("thermal", 1), ("thermal", 2)])
 def test_vor2vel_vtend_timestep(olib, glib, kind, plane):
     s = small_state(kind)
     oc, gc = pair(s, olib, glib)
