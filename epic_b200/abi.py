@@ -78,6 +78,31 @@ class EpicStepInfo(C.Structure):
     ]
 
 
+INIT_THERMAL, INIT_BELTRAMI = 0, 1
+
+
+class EpicInitSpec(C.Structure):
+    """epic_init_spec of include/epic_gpu.h (device-side initial states)."""
+    _fields_ = [
+        ("kind", C.c_int32), ("n_per_cell", C.c_int32), ("seed", C.c_uint64),
+        ("k", C.c_int32), ("l", C.c_int32), ("m", C.c_int32),
+        ("n_bubbles", C.c_int32), ("bubble", (C.c_double * 4) * 4),
+    ]
+
+
+def init_spec(kind, n_per_cell=8, seed=1234, klm=(1, 1, 1), bubbles=((0.0, 0.0, 1.5, 0.5),)) -> EpicInitSpec:
+    s = EpicInitSpec()
+    s.kind = kind
+    s.n_per_cell = n_per_cell
+    s.seed = seed
+    s.k, s.l, s.m = klm
+    s.n_bubbles = len(bubbles)
+    for b, row in enumerate(bubbles):
+        for q in range(4):
+            s.bubble[b][q] = row[q]
+    return s
+
+
 class EpicError(RuntimeError):
     def __init__(self, code: int, func: str, msg: str):
         self.code = code
@@ -151,6 +176,13 @@ class EpicLib:
             f.argtypes = args
             f.restype = C.c_int
             self.fn[name] = f
+        # entry points only the CUDA library has
+        for name, args in (("init_state", [_VP, C.POINTER(EpicInitSpec)]),):
+            if hasattr(self.lib, prefix + name):
+                f = getattr(self.lib, prefix + name)
+                f.argtypes = args
+                f.restype = C.c_int
+                self.fn[name] = f
         d = getattr(self.lib, prefix + "destroy")
         d.argtypes = [_VP]
         d.restype = None
@@ -288,6 +320,9 @@ class EpicContext:
 
     def grid2par(self, add=False):
         self._call("grid2par", C.c_int(int(add)))
+
+    def init_state(self, spec: "EpicInitSpec"):
+        self._call("init_state", C.byref(spec))
 
     def rk_step(self, t: float):
         tt = C.c_double(t)

@@ -13,9 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libepic_b200.so")
-SOURCES = ["api.cu", "spectral.cu", "parcels.cu", "merge.cu", "testing.cu", "noalloc.cu", "stage.cu"]
+SOURCES = ["api.cu", "spectral.cu", "parcels.cu", "merge.cu", "testing.cu", "noalloc.cu", "stage.cu", "init.cu", "serve.cu"]
 HEADERS = ["common.cuh", "eigen.cuh", "ctx.hpp", "parcel_ops.cuh", os.path.join("..", "..", "include", "epic_gpu.h"),
-           os.path.join("..", "..", "include", "epic_gpu_testing.h")]
+           os.path.join("..", "..", "include", "epic_gpu_testing.h"), os.path.join("..", "..", "include", "epic_serve.h")]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -45,7 +45,7 @@ def build(force: bool = False) -> str:
     with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(lambda s: _compile(s, force), SOURCES))
     if force or _mtime(LIB) < max(_mtime(o) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

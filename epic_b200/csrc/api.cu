@@ -17,6 +17,19 @@ namespace epic {
 
 std::atomic<long long> g_launches{0};
 
+int smem_optin() {
+    static std::atomic<int> cache[64];   // per device, 0 = not queried yet
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) dev = 63;
+    int v = cache[dev].load();
+    if (v == 0) {
+        CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cache[dev].store(v);
+    }
+    return v;
+}
+
 void prof_begin(Ctx& c, const char* name) {
     if (c.prof.target.empty() || c.prof.target != name) return;
     cudaEvent_t e;
@@ -326,6 +339,14 @@ int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const doub
     if (hum) upload_attr(c, hum, 1, A_HUM);
     c.has_parcels = true;
     CK(cudaStreamSynchronize(c.stream));
+    API_END
+}
+
+int epic_gpu_init_state(epic_ctx* ctx, const epic_init_spec* spec) {
+    API_BEGIN
+    if (!spec) throw CudaError(EPIC_ERR_ARG, "init_state: null spec");
+    init_state(ctx->c, *spec);
+    CK(cudaStreamSynchronize(ctx->c.stream));
     API_END
 }
 

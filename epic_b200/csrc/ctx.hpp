@@ -181,8 +181,27 @@ int box_count(const Params& P);
 long long stage_grid_max(const Params& P, long long cap);
 void p2g_tail(Ctx& c);
 
+// init.cu
+void init_state(Ctx& c, const epic_init_spec& s);
+
 // merge.cu
 long long parcel_merge(Ctx& c);
+
+// Largest dynamic shared memory a block may opt in to on the current device.
+int smem_optin();
+// Let `kernel` use up to the device's opt-in maximum of dynamic shared memory
+// and check that a launch's `bytes` fit.  The attribute is process-wide, so
+// it is always set to that same maximum: contexts on other threads launching
+// the kernel with other sizes never see a smaller limit.
+template <typename K>
+void allow_smem(K kernel, size_t bytes) {
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    int mx = smem_optin() - (int)fa.sharedSizeBytes;   // minus the kernel's static shared memory
+    if ((long long)bytes > mx)
+        throw CudaError(EPIC_ERR_CONFIG, "grid too large for the shared-memory tiles of this device");
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+}
 
 // api.cu
 void prof_begin(Ctx& c, const char* name);

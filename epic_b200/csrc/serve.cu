@@ -1,0 +1,237 @@
+// Served ensembles (include/epic_serve.h): a pool of worker threads, one per
+// slot, each running one simulation at a time on its own context and CUDA
+// stream; first-come-first-served admission by slot and by free HBM; idle
+// contexts kept per configuration and reused, so that a steady stream of
+// requests allocates (and frees, which synchronises the whole device) no
+// device memory.
+#include "ctx.hpp"
+#include "../../include/epic_serve.h"
+
+#include <chrono>
+#include <cstdio>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace epic {
+
+// Device bytes of a context created with cfg (the allocations of
+// epic_gpu_create plus the step's stream-ordered scratch), with a margin.
+static double estimate_bytes(const epic_cfg& g) {
+    const double nx = g.nx, ny = g.ny, nz = g.nz;
+    const double ncell = nx * ny * nz;
+    double cap = g.capacity > 0 ? (double)g.capacity : 2.0 * ncell * std::max(1, g.n_per_cell) + 1024.0;
+    const double fsz = nx * ny * (nz + 3);
+    const double store = (g.precision == EPIC_PRECISION_MIXED ? PARCEL_BYTES_MIXED : PARCEL_BYTES_PLAIN) * cap;
+    double b = store * (g.keep_order ? 1.0 : 2.0);
+    b += fsz * 8.0 * (21 + 14 + 16 + 12) + fsz * 8.0;   // fields, work, gather records, tables, counts
+    b += cap * 32.0;                                     // sort keys / merge and split scratch
+    return 1.15 * b + 64.0 * (1 << 20);
+}
+
+struct Job {
+    int64_t id;
+    epic_request req;
+    double t_submit;
+    double bytes;
+};
+
+struct PooledCtx {
+    epic_cfg cfg;
+    epic_ctx* ctx;
+    double bytes;
+};
+
+}  // namespace epic
+
+using namespace epic;
+
+struct epic_server {
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Job> queue;
+    std::map<int64_t, epic_result> results;
+    std::vector<PooledCtx> idle;
+    std::vector<std::thread> workers;
+    int device = 0;
+    double budget = 0.0, in_use = 0.0;   // bytes: running requests + idle contexts
+    int64_t next_id = 1, running = 0;
+    bool stop = false;
+    std::chrono::steady_clock::time_point t0;
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+static bool same_cfg(const epic_cfg& a, const epic_cfg& b) { return std::memcmp(&a, &b, sizeof(epic_cfg)) == 0; }
+
+// Take an idle context of this configuration out of the pool (nullptr if none).
+static epic_ctx* pool_take(epic_server* s, const epic_cfg& cfg, double* bytes) {
+    for (size_t k = 0; k < s->idle.size(); ++k)
+        if (same_cfg(s->idle[k].cfg, cfg)) {
+            epic_ctx* c = s->idle[k].ctx;
+            *bytes = s->idle[k].bytes;
+            s->idle.erase(s->idle.begin() + k);
+            return c;
+        }
+    return nullptr;
+}
+
+static void run_job(epic_server* s, const Job& job, int slot, epic_ctx* ctx, epic_result& r) {
+    int rc = EPIC_OK;
+    if (!ctx) rc = epic_gpu_create(&job.req.cfg, &ctx);
+    double t = job.req.cfg.t_initial;
+    epic_step_info info{};
+    int64_t psteps = 0;
+    if (rc == EPIC_OK) rc = epic_gpu_init_state(ctx, &job.req.init);
+    if (rc == EPIC_OK) rc = epic_gpu_init_correction(ctx);
+    for (int k = 0; rc == EPIC_OK && k < job.req.steps; ++k) {
+        int64_t n0 = 0;
+        epic_gpu_num_parcels(ctx, &n0);
+        rc = epic_gpu_step(ctx, &t, &info);
+        psteps += n0;
+    }
+    r.status = rc;
+    r.slot = slot;
+    if (rc != EPIC_OK) {
+        const char* m = ctx ? epic_gpu_last_error(ctx) : "context creation failed";
+        std::snprintf(r.message, sizeof(r.message), "%s", m ? m : "");
+    }
+    r.parcel_steps = psteps;
+    r.n_parcels = info.n_parcels;
+    r.t_final = t;
+    r.ke = info.parcel_stats[1];
+    r.enstrophy = info.parcel_stats[12];
+    std::lock_guard<std::mutex> lk(s->mu);
+    r.t_done = s->now();
+    if (rc == EPIC_OK) {
+        s->idle.push_back({job.req.cfg, ctx, job.bytes});   // keeps its share of in_use
+    } else {
+        if (ctx) epic_gpu_destroy(ctx);
+        s->in_use -= job.bytes;
+    }
+    --s->running;
+    s->results[job.id] = r;
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+}
+
+static void worker(epic_server* s, int slot) {
+    cudaSetDevice(s->device);
+    for (;;) {
+        Job job;
+        epic_ctx* ctx = nullptr;
+        double pooled_bytes = 0.0;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            for (;;) {
+                if (s->queue.empty()) {
+                    if (s->stop) return;
+                    s->cv_work.wait(lk);
+                    continue;
+                }
+                Job& head = s->queue.front();
+                ctx = pool_take(s, head.req.cfg, &pooled_bytes);
+                if (ctx) break;                                   // its memory is already counted
+                // make room by freeing idle contexts of other configurations
+                while (s->in_use + head.bytes > s->budget && !s->idle.empty()) {
+                    PooledCtx p = s->idle.back();
+                    s->idle.pop_back();
+                    s->in_use -= p.bytes;
+                    epic_gpu_destroy(p.ctx);
+                }
+                if (s->in_use + head.bytes <= s->budget || s->running == 0) break;
+                s->cv_work.wait(lk);                              // wait for a running job to finish
+            }
+            job = s->queue.front();
+            s->queue.pop_front();
+            if (ctx) job.bytes = pooled_bytes;
+            else s->in_use += job.bytes;
+            ++s->running;
+        }
+        epic_result r{};
+        r.id = job.id;
+        r.t_submit = job.t_submit;
+        r.device_bytes = job.bytes;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r.t_start = s->now();
+        }
+        run_job(s, job, slot, ctx, r);
+    }
+}
+
+extern "C" int epic_srv_create(int32_t max_slots, double hbm_fraction, epic_server** out) {
+    if (!out || max_slots < 1 || max_slots > 64 || !(hbm_fraction > 0.0 && hbm_fraction <= 1.0))
+        return EPIC_ERR_ARG;
+    auto* s = new epic_server();
+    s->t0 = std::chrono::steady_clock::now();
+    if (cudaGetDevice(&s->device) != cudaSuccess) { delete s; return EPIC_ERR_CUDA; }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { delete s; return EPIC_ERR_CUDA; }
+    s->budget = hbm_fraction * (double)free_b;
+    for (int k = 0; k < max_slots; ++k) s->workers.emplace_back(worker, s, k);
+    *out = s;
+    return EPIC_OK;
+}
+
+extern "C" int epic_srv_submit(epic_server* s, const epic_request* req, int64_t* id) {
+    if (!s || !req || !id || req->steps < 0) return EPIC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    Job j;
+    j.id = s->next_id++;
+    j.req = *req;
+    j.t_submit = s->now();
+    j.bytes = estimate_bytes(req->cfg);
+    *id = j.id;
+    if (j.bytes > s->budget) {
+        epic_result r{};
+        r.id = j.id;
+        r.status = EPIC_ERR_CAPACITY;
+        r.slot = -1;
+        r.t_submit = r.t_start = r.t_done = j.t_submit;
+        r.device_bytes = j.bytes;
+        std::snprintf(r.message, sizeof(r.message), "request needs %.3g bytes, server budget %.3g", j.bytes, s->budget);
+        s->results[j.id] = r;
+        s->cv_done.notify_all();
+        return EPIC_OK;
+    }
+    s->queue.push_back(j);
+    s->cv_work.notify_all();
+    return EPIC_OK;
+}
+
+extern "C" int epic_srv_wait(epic_server* s, int64_t id, epic_result* out) {
+    if (!s || !out || id < 1) return EPIC_ERR_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (id >= s->next_id) return EPIC_ERR_ARG;
+    s->cv_done.wait(lk, [&] { return s->results.count(id) != 0; });
+    *out = s->results[id];
+    return EPIC_OK;
+}
+
+extern "C" int epic_srv_counts(epic_server* s, int64_t* queued, int64_t* running, int64_t* done) {
+    if (!s) return EPIC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (queued) *queued = (int64_t)s->queue.size();
+    if (running) *running = s->running;
+    if (done) *done = (int64_t)s->results.size();
+    return EPIC_OK;
+}
+
+extern "C" void epic_srv_destroy(epic_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    for (auto& w : s->workers) w.join();
+    for (auto& p : s->idle) epic_gpu_destroy(p.ctx);
+    delete s;
+}

@@ -393,10 +393,10 @@ static void launch_plane(Ctx& c, const double* const* in, double* const* out, in
     int threads = (N / 2) * Radix<N>::N2;
     prof_begin(c, "fft");
     if (forward) {
-        CK(cudaFuncSetAttribute(k_fft_plane<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_fft_plane<N, true>, sm);
         k_fft_plane<N, true><<<grid, threads, sm, c.stream>>>(B);
     } else {
-        CK(cudaFuncSetAttribute(k_fft_plane<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_fft_plane<N, false>, sm);
         k_fft_plane<N, false><<<grid, threads, sm, c.stream>>>(B);
     }
     CKL();
@@ -454,10 +454,10 @@ static void launch_tile_axis(Ctx& c, const FFTPlan& pl, int axis, const double* 
     int threads = (TL / 2) * Radix<N>::N2;
     prof_begin(c, "fft");
     if (forward) {
-        CK(cudaFuncSetAttribute(k_fft_tile<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_fft_tile<N, true>, sm);
         k_fft_tile<N, true><<<grid, threads, sm, c.stream>>>(B);
     } else {
-        CK(cudaFuncSetAttribute(k_fft_tile<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_fft_tile<N, false>, sm);
         k_fft_tile<N, false><<<grid, threads, sm, c.stream>>>(B);
     }
     CKL();
@@ -532,11 +532,11 @@ static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* cons
     dim3 grid((B.nl + B.T - 1) / B.T, nrows, nf);
     prof_begin(c, "fft");
     if (forward) {
-        CK(cudaFuncSetAttribute(k_fft_lines<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_fft_lines<true>, sm);
         k_fft_lines<true><<<grid, 256, sm, c.stream>>>(B);
         CKL();
     } else {
-        CK(cudaFuncSetAttribute(k_fft_lines<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_fft_lines<false>, sm);
         k_fft_lines<false><<<grid, 256, sm, c.stream>>>(B);
         CKL();
     }
@@ -1215,7 +1215,7 @@ static void col_decompose(Ctx& c, const double* const* in, double* const* out, i
     for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
     size_t sm = col_smem(c, 2);
     with_rows(col_rows(c.P), [&](auto R) {
-        CK(cudaFuncSetAttribute(k_col_decompose<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_col_decompose<R>, sm);
         k_col_decompose<R><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A, mode);
         CKL();
     });
@@ -1227,7 +1227,7 @@ static void col_combine(Ctx& c, const double* const* in, double* const* out, int
     for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
     size_t sm = col_smem(c, 2);
     with_rows(col_rows(c.P), [&](auto R) {
-        CK(cudaFuncSetAttribute(k_col_combine<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        allow_smem(k_col_combine<R>, sm);
         k_col_combine<R><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A);
         CKL();
     });
@@ -1283,7 +1283,7 @@ void vor2vel(Ctx& c) {
         A.out[1] = es;
         size_t sm = col_smem(c, 4);
         with_rows(col_rows(c.P), [&](auto R) {
-            CK(cudaFuncSetAttribute(k_col_wsolve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            allow_smem(k_col_wsolve<R>, sm);
             k_col_wsolve<R><<<(A.ncol + CT - 1) / CT, 256, sm, c.stream>>>(A);
             CKL();
         });
@@ -1359,7 +1359,7 @@ void diverge_laplace(Ctx& c, double* phi, double* grad[3]) {
     fft_xy(c, in, out, 1, true);
     int ncol = P.nx * P.ny;
     size_t lsm = col_smem(c, 3);
-    CK(cudaFuncSetAttribute(k_lapinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    allow_smem(k_lapinv, lsm);
     k_lapinv<<<(ncol + CT - 1) / CT, 256, lsm, c.stream>>>(ds, c.T.etdv, c.T.htdv, P.ap, ncol, P.nz, P.nzh);
     CKL();
     SpecArgs S = spec_args(c);

@@ -786,7 +786,7 @@ static void zero_p2g_fields(Ctx& c) {
 
 template <typename K>
 static void set_smem(K kernel, size_t bytes) {
-    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    allow_smem(kernel, bytes);
 }
 
 template <int NF, class R>

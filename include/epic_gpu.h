@@ -132,6 +132,31 @@ int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const doub
 int epic_gpu_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, double* vor,
                          double* B, double* vol, double* buoy, double* hum);
 int epic_gpu_num_parcels(epic_ctx* ctx, int64_t* n);
+
+/* Initial states generated on the device (no host arrays), the parcels of
+ * init_regular_positions / parcel_default (parcel_init.f90:31-152):
+ * n_per_cell = npd^3 parcels per cell at the sub-cell centres, z outermost.
+ *   EPIC_INIT_THERMAL: spheroids of the cell aspect ratio (parcel_default),
+ *     zero vorticity and humidity, buoyancy sum_b amp_b exp(-r_b^2 / 0.25)
+ *     plus seeded U(-1e-3, 1e-3), positions jittered by seeded
+ *     U(-0.1 dx, 0.1 dx) per component (z kept inside the domain);
+ *   EPIC_INIT_BELTRAMI: spheres, vorticity of the Beltrami modes (k, l, m)
+ *     (models/3d/beltrami_3d.f90:103-122), no buoyancy.
+ * Random numbers are SplitMix64 keyed by (seed, parcel index, component), the
+ * generator of the Python package (epic_b200/initial.py), so both produce
+ * the same state (positions bit for bit; exp, sin and cos to their last bit).
+ * Replaces set_parcels + the host generator; call init_correction after. */
+#define EPIC_INIT_THERMAL  0
+#define EPIC_INIT_BELTRAMI 1
+typedef struct epic_init_spec {
+    int32_t  kind;            /* EPIC_INIT_*                                   */
+    int32_t  n_per_cell;      /* a cube: 1, 8, 27, ...                         */
+    uint64_t seed;            /* thermal noise                                 */
+    int32_t  k, l, m;         /* Beltrami modes                                */
+    int32_t  n_bubbles;       /* thermal: 1 .. 4                               */
+    double   bubble[4][4];    /* thermal: centre x, y, z and amplitude         */
+} epic_init_spec;
+int epic_gpu_init_state(epic_ctx* ctx, const epic_init_spec* spec);
 /* LS-RK accumulators (delta_pos(3,n), delta_vor(3,n), strain(8,n), delta_b(5,n)). */
 int epic_gpu_get_parcel_rk(epic_ctx* ctx, int64_t cap, int64_t* n, double* delta_pos,
                            double* delta_vor, double* strain, double* delta_b);

@@ -13,6 +13,7 @@
 #include "oracle_core.hpp"
 #include "../include/epic_gpu.h"
 
+#include <algorithm>
 #include <memory>
 #include <numeric>
 #ifdef _OPENMP
@@ -1716,6 +1717,78 @@ int epic_oracle_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const d
     std::fill(c.dB.begin(), c.dB.end(), 0.0);
     std::fill(c.strain.begin(), c.strain.end(), 0.0);
     return EPIC_OK;
+}
+
+// Initial states of the benchmark workloads (parcel_init.f90:31-152 placement
+// and shapes, beltrami_3d.f90:103-122 vorticity, the rising thermal), the
+// same arithmetic as epic_b200/initial.py, with its SplitMix64 counter RNG.
+static uint64_t sm64(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static double u01(uint64_t seed, uint64_t idx, int comp) {
+    uint64_t key = (seed * 0x9E3779B97F4A7C15ull) ^ (idx * 16ull + (uint64_t)comp);
+    return (double)(sm64(sm64(key)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+int epic_oracle_init_state(epic_ctx* ctx, const epic_init_spec* s) {
+    if (!ctx || !s) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    int npd = (int)std::lround(std::cbrt((double)s->n_per_cell));
+    if (npd < 1 || npd * npd * npd != s->n_per_cell) return EPIC_ERR_CONFIG;
+    if (s->kind != EPIC_INIT_THERMAL && s->kind != EPIC_INIT_BELTRAMI) return EPIC_ERR_CONFIG;
+    long n = (long)c.nx * c.ny * c.nz * s->n_per_cell;
+    std::vector<double> pos(3 * n), vor(3 * n, 0.0), B(5 * n, 0.0), vol(n), buoy(n, 0.0), hum(n, 0.0);
+    const double im = 1.0 / npd;
+    const double v = c.vcell / s->n_per_cell;
+    const double* d = c.dx;
+    double lam = std::max({d[0] / d[1], d[1] / d[0], d[0] / d[2], d[2] / d[0], d[1] / d[2], d[2] / d[1]});
+    if (s->kind == EPIC_INIT_BELTRAMI) lam = 1.0;
+    const double b11 = std::pow(lam * (0.75 * v * (1.0 / M_PI)), 2.0 / 3.0);
+    const double kk = s->k, ll = s->l, mm = s->m;
+    const double alpha = std::sqrt(kk * kk + ll * ll + mm * mm);
+    const double fk2l2 = s->kind == EPIC_INIT_BELTRAMI ? alpha / (double)(s->k * s->k + s->l * s->l) : 0.0;
+    const double zmax = std::nextafter(c.upper[2], c.lower[2]);
+    for (long p = 0; p < n; ++p) {
+        long q = p;
+        int sub[3], cell[3];
+        for (int k = 0; k < 3; ++k) { sub[k] = (int)(q % npd) + 1; q /= npd; }
+        cell[0] = (int)(q % c.nx); q /= c.nx;
+        cell[1] = (int)(q % c.ny); q /= c.ny;
+        cell[2] = (int)q;
+        double x[3];
+        for (int k = 0; k < 3; ++k) {
+            double corner = c.lower[k] + (double)cell[k] * d[k];
+            x[k] = corner + d[k] * ((double)sub[k] - 0.5) * im;
+        }
+        if (s->kind == EPIC_INIT_THERMAL) {
+            for (int k = 0; k < 3; ++k) x[k] += (2.0 * u01(s->seed, (uint64_t)p, k) - 1.0) * 0.1 * d[k];
+            x[2] = std::min(std::max(x[2], c.lower[2]), zmax);
+            double b = 0.0;
+            for (int q2 = 0; q2 < s->n_bubbles; ++q2) {
+                const double* bb = s->bubble[q2];
+                double r2 = (x[0] - bb[0]) * (x[0] - bb[0]) + (x[1] - bb[1]) * (x[1] - bb[1]) +
+                            (x[2] - bb[2]) * (x[2] - bb[2]);
+                b += bb[3] * std::exp(-r2 / 0.25);
+            }
+            b += (2.0 * u01(s->seed, (uint64_t)p, 3) - 1.0) * 1.0e-3;
+            buoy[p] = b;
+        } else {
+            double cosmz = std::cos(mm * x[2]), sinmz = std::sin(mm * x[2]);
+            double sn = std::sin(kk * x[0] + ll * x[1]), cs = std::cos(kk * x[0] + ll * x[1]);
+            vor[3 * p] = fk2l2 * (kk * mm * sinmz - ll * alpha * cosmz) * sn;
+            vor[3 * p + 1] = fk2l2 * (ll * mm * sinmz + kk * alpha * cosmz) * sn;
+            vor[3 * p + 2] = alpha * cosmz * cs;
+        }
+        for (int k = 0; k < 3; ++k) pos[3 * p + k] = x[k];
+        B[5 * p] = b11;
+        B[5 * p + 3] = b11;
+        vol[p] = v;
+    }
+    c.n_parcel_splits = c.n_parcel_merges = c.n_big_close = 0;
+    return epic_oracle_set_parcels(ctx, n, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(), hum.data());
 }
 
 int epic_oracle_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, double* vor, double* B,

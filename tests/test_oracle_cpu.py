@@ -184,3 +184,27 @@ def test_laplace_correction_reduces_volume_error(olib):
         ctx.apply_gradient(True)
     assert errs[-1] < errs[0]
     assert all(b <= a * 1.05 for a, b in zip(errs, errs[1:]))
+
+
+@pytest.mark.parametrize("kind", ["thermal", "beltrami"])
+def test_oracle_init_state_matches_generator(olib, kind):
+    """epic_oracle_init_state builds the same parcels as epic_b200/initial.py
+    (same arithmetic, same counter RNG): positions, shapes and volumes bit for
+    bit; buoyancy and vorticity to the last bit of exp/sin/cos (numpy's
+    vectorised exp is not glibc's)."""
+    from epic_b200 import abi
+    if kind == "thermal":
+        bubbles = ((0.0, 0.0, 1.5, 0.5), (-0.75, 0.3, 2.0, 0.3))
+        s = initial.thermal(8, 8, 6, seed=11, bubbles=bubbles)
+        spec = abi.init_spec(abi.INIT_THERMAL, seed=11, bubbles=bubbles)
+    else:
+        s = initial.beltrami(8, 2, 1, 2)
+        spec = abi.init_spec(abi.INIT_BELTRAMI, klm=(2, 1, 2))
+    cfg = olib.default_config(s.nx, s.ny, s.nz, s.lower, s.extent, **s.options)
+    ctx = abi.EpicContext(olib, cfg)
+    ctx.init_state(spec)
+    p = ctx.get_parcels()
+    for key in ("pos", "B", "vol", "hum"):
+        assert np.array_equal(p[key], getattr(s, key).reshape(p[key].shape)), key
+    for key in ("buoy", "vor"):
+        np.testing.assert_allclose(p[key], getattr(s, key).reshape(p[key].shape), rtol=4e-16, atol=1e-18)
