@@ -325,6 +325,95 @@ def run_ours(args):
 
 
 # ---------------------------------------------------------------------------
+def served_requests(args, lib):
+    """The served ensemble: requests with seeded Poisson arrivals, grids drawn
+    uniformly from {32^3, 48^3, 64^3, 96x96x48}, a Beltrami (k, l, m in {1, 2})
+    or thermal initial state of its own seed, mixed precision."""
+    from epic_b200 import serve
+    rng = np.random.default_rng(args.served_seed)
+    grids = [(32, 32, 32), (48, 48, 48), (64, 64, 64), (96, 96, 48)]
+    reqs, arrivals, meta = [], [], []
+    t = 0.0
+    for r in range(args.served_requests):
+        t += float(rng.exponential(1.0 / args.served_rate))
+        g = grids[int(rng.integers(0, len(grids)))]
+        kind = "beltrami" if rng.random() < 0.5 else "thermal"
+        klm = tuple(int(v) for v in rng.integers(1, 3, size=3))
+        reqs.append(serve.request(kind, g, seed=1000 + r, klm=klm, steps=args.served_steps, precision=1, lib=lib))
+        arrivals.append(t)
+        meta.append({"grid": list(g), "kind": kind, "klm": list(klm) if kind == "beltrami" else None})
+    return reqs, arrivals, meta
+
+
+def run_served(args):
+    import torch
+    import epic_b200
+    from epic_b200 import serve
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local if world > 1 else 0)
+    dev = torch.cuda.current_device()
+    lib = epic_b200.load()
+    reqs, arrivals, meta = served_requests(args, lib)
+    clocks = ClockSampler(dev)
+    srv = serve.Server(slots=args.served_slots, hbm_fraction=0.8, lib=lib)
+    ids = []
+    clocks.start()
+    w0 = time.perf_counter()
+    for req, ta in zip(reqs, arrivals):
+        delay = ta - (time.perf_counter() - w0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(req))
+    res = [srv.wait(i) for i in ids]
+    wall = time.perf_counter() - w0
+    clk = clocks.stop()
+    srv.close()
+    failed = [r for r in res if r["status"] != 0]
+    lat = np.array([r["t_done"] - r["t_submit"] for r in res if r["status"] == 0])
+    ps = sum(r["parcel_steps"] for r in res if r["status"] == 0)
+    span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+    value = ps / span
+    ps_total = value
+    if world > 1:
+        # replicas: every rank serves its own copy of the ensemble
+        _, ps_total = reduce_timing(span * 1e3, float(ps))
+        ps_total = ps_total / span
+    req_bytes = C_sizeof_request()
+    line = {
+        "metric": METRIC, "value": ps_total, "unit": UNIT, "n_gpus": world, "steps": args.served_steps,
+        "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/f64", "data": "synthetic",
+        "config": {"workload": f"served ensemble: {len(reqs)} requests, Poisson arrivals {args.served_rate}/s "
+                               f"(seed {args.served_seed}), grids 32^3/48^3/64^3/96x96x48, Beltrami (k,l,m in 1..2) "
+                               f"or thermal, {args.served_steps} mixed-precision steps each, "
+                               f"{args.served_slots} slots, admission by free HBM",
+                   "form": "served", "requests": len(reqs), "slots": args.served_slots,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "timing": "host steady clock of the server: submit to completion per request; "
+                             "aggregate = parcel-steps / (last completion - first submission)"},
+        "latency": {"p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+                    "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+                    "mean_s": float(lat.mean()) if len(lat) else None,
+                    "max_s": float(lat.max()) if len(lat) else None},
+        "failed": len(failed),
+        "failures": [dict(meta[k], message=r["message"]) for k, r in enumerate(res) if r["status"] != 0][:8],
+        "clocks": clk,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": req_bytes * len(reqs) / max(1, args.served_steps * len(reqs)),
+                "d2h_bytes_per_step": 0, "mode": "requests submitted through the server's C ABI; "
+                "initial states generated on the device; results (diagnostics) read back"},
+        "wall_s": wall, "span_s": span, "parcel_steps": ps,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def C_sizeof_request():
+    import ctypes
+    from epic_b200 import serve
+    return ctypes.sizeof(serve.EpicRequest)
+
+
 def oracle_sample_workload():
     """The bounded CPU sample: the same rising thermal on a 64^3 grid
     (2,097,152 parcels, same parcel density and physics), one step."""
@@ -391,8 +480,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="thermal-128")
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
-                    help="plain FP64, or the mixed-precision form (FP32 attributes and interpolation)")
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed", "served"],
+                    help="plain FP64, the mixed-precision form (FP32 attributes and interpolation), "
+                         "or the served ensemble")
+    ap.add_argument("--served-requests", type=int, default=64)
+    ap.add_argument("--served-rate", type=float, default=4.0, help="mean arrivals per second")
+    ap.add_argument("--served-steps", type=int, default=100)
+    ap.add_argument("--served-slots", type=int, default=8)
+    ap.add_argument("--served-seed", type=int, default=2024)
     ap.add_argument("--roofline-kernel", default="stage", choices=["stage", "p2g", "g2p", "fft"])
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of that kernel")
     ap.add_argument("--profile-kernels", default="", help="comma list of kernels to time over one extra step each")
@@ -404,6 +499,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.form == "served":
+        run_served(args)
     else:
         run_ours(args)
 

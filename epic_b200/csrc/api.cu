@@ -17,6 +17,34 @@ namespace epic {
 
 std::atomic<long long> g_launches{0};
 
+// parcels%resize (parcel_container.f90:273-308): reallocate the store for at
+// least grow_factor x need parcels, keeping parcels [0, n); the sort buffer
+// and the per-CTA partials follow the new capacity.
+void grow_store(Ctx& c, long long need) {
+    long long ncap = std::max(need, (long long)std::llround(c.cfg.grow_factor * (double)need));
+    ncap = (ncap + 63) & ~63LL;
+    PView nv{nullptr, ncap, c.pv.mixed};
+    const size_t nbytes = (size_t)(c.pv.mixed ? PARCEL_BYTES_MIXED : PARCEL_BYTES_PLAIN) * (size_t)ncap;
+    CK(cudaMalloc(&nv.base, nbytes));
+    for (int k = 0; k < N_ATTR; ++k) {
+        const size_t es = c.pv.f32(k) ? 4 : 8;
+        CK(cudaMemcpyAsync(reinterpret_cast<char*>(nv.base) + nv.off(k), reinterpret_cast<char*>(c.pv.base) + c.pv.off(k),
+                           es * (size_t)c.n, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    CK(cudaFree(c.pv.base));
+    c.pv = nv;
+    c.cap = ncap;
+    if (c.pv_alt) {
+        CK(cudaFree(c.pv_alt));
+        c.pv_alt = nullptr;
+        CK(cudaMalloc(&c.pv_alt, nbytes));
+    }
+    CK(cudaFree(c.stage_partials));
+    c.stage_partials = nullptr;
+    CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)stage_grid_max(c.P, c.cap)));
+}
+
 int smem_optin() {
     static std::atomic<int> cache[64];   // per device, 0 = not queried yet
     int dev = 0;

@@ -204,6 +204,7 @@ void allow_smem(K kernel, size_t bytes) {
 }
 
 // api.cu
+void grow_store(Ctx& c, long long need);
 void prof_begin(Ctx& c, const char* name);
 void prof_end(Ctx& c, const char* name);
 void check_device_error(Ctx& c);

@@ -749,9 +749,8 @@ long long parcel_split(Ctx& c) {
     CK(cudaMemcpyAsync(&ns, offs + n, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     if (ns == 0) return 0;
-    if (n + ns > c.cap)
-        throw CudaError(EPIC_ERR_CAPACITY, "parcel_split: parcel container capacity exceeded ("
-                                               + std::to_string(n + ns) + " > " + std::to_string(c.cap) + ")");
+    // parcel_split.f90:91-94: a full container grows to grow_factor x the parcels needed
+    if (n + ns > c.cap) grow_store(c, n + ns);
     k_split_apply<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, flag, offs, &c.dsc->err);
     CKL();
     c.n = n + ns;

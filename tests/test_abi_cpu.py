@@ -25,6 +25,13 @@ def test_library_exports_declared_symbols(header):
     assert not missing, missing
 
 
+def test_library_resolves_every_symbol():
+    """RTLD_NOW: a symbol the library uses but does not define fails here, on
+    the CPU, instead of at first use on a GPU."""
+    import epic_b200
+    ctypes.CDLL(epic_b200.LIB_PATH, mode=os.RTLD_NOW)
+
+
 def test_binding_covers_abi():
     import epic_b200
     lib = epic_b200.load()      # binds every signature of epic_b200/abi.py

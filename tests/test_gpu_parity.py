@@ -194,6 +194,29 @@ def test_split_bit_exact(olib, glib):
     _cmp_parcels(oc, gc)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_split_grows_full_container(olib, glib, precision):
+    """A split that overflows the container grows it (parcel_split.f90:91-94,
+    grow_factor x the parcels needed) and keeps every parcel; steps go on."""
+    s = small_state("thermal", stretch=True)
+    oc = make_context(s, olib)
+    gc = make_context(s, glib, capacity=s.n + 64, precision=precision)
+    so, sg = oc.split(), gc.split()
+    assert sg > 64
+    po, pg = oc.get_parcels(), gc.get_parcels()
+    assert len(pg["vol"]) == s.n + sg
+    if precision == 0:
+        assert so == sg
+        assert np.array_equal(pg["vol"], po["vol"])
+        _cmp_parcels(oc, gc)
+    else:   # FP32 shapes: decisions may differ at the threshold, positions by rounding
+        assert abs(so - sg) <= 2
+        if so == sg:
+            assert np.abs(pg["pos"] - po["pos"]).max() < 1e-5 * s.dx.min()
+    t, _ = gc.step(0.0)
+    assert t > 0
+
+
 @pytest.mark.parametrize("reuse", [False, True])
 def test_corrections(olib, glib, reuse):
     s = small_state("thermal", stretch=True)
