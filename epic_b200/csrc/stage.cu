@@ -13,7 +13,8 @@
 // 4 support points x 8 corners of every parcel into a shared-memory window
 // covering that box plus the support-point reach, and adds the window to the
 // global fields once.  Window sums are fixed point: each contribution is
-// scaled by a power of two so that its magnitude is at most 2^b (b <= 50),
+// scaled by a power of two so that its magnitude is at most 2^(b+2)
+// (b <= 48; the +2 covers the merged weights of up to 4 support points),
 // rounded to an integer, and added as three 32-bit limbs (two unsigned
 // 18-bit limbs and a signed top limb) with integer shared-memory atomics,
 // which run at several times the rate of FP64 shared atomics, do not
@@ -194,7 +195,8 @@ EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long 
     W.WZ = gz1 - W.gz0 + 1;
     bool ok = ws->mn[0] <= ws->mx[0] && W.WX <= P.nx && W.WY <= P.ny && W.WZ > 0 &&
               (long long)W.WX * W.WY * W.WZ <= WCAP;
-    // contributions per grid point <= 4 count <= 2^lg; |window sum| <= 2^(bits + lg) <= 2^62
+    // contributions per grid point <= 4 count <= 2^lg; |window sum| <= 2^(bits + lg) <= 2^62;
+    // one contribution (merged weights of up to 4 points, <= 4) <= 2^(bits + 2)
     int lg = 32 - __clz((unsigned)(4 * count - 1));
     int bits = min(max_bits, 62 - lg);
     for (int f = 0; f < NF; ++f) {
@@ -279,12 +281,30 @@ EPIC_DEV double fx2_value(const unsigned* acc, int w, double inv) {
 
 EPIC_DEV int wrap_to(int l, int n) { return ((unsigned)l < (unsigned)n) ? l : wrapi(l, n); }
 
+// Support points of one parcel that fall into the same cell as the point
+// before them share their 8 corners: their trilinear weights are summed and
+// the corners visited once (sum_p w_p f = (sum_p w_p) f; only the rounding
+// order differs from visiting each point).
+EPIC_DEV bool same_cell(const Tri& a, const Tri& b) { return a.is == b.is && a.js == b.js && a.ks == b.ks; }
+EPIC_DEV void add_weights(Tri& a, const Tri& b) {
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk)
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+            for (int ii = 0; ii < 2; ++ii) a.w[kk][jj][ii] += b.w[kk][jj][ii];
+}
+EPIC_DEV void support_point(const double* pos, const double* eta, const double* tau, int p, double* pt) {
+    const double cp = support_cos(p), sp = support_sin(p);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
+}
+
 // Scatter one support point: vp[f] = value * point weight * volume, vs[f] =
 // vp[f] in fixed-point units (plain form only).
 template <int NF, class R>
-EPIC_DEV void scatter_point(const Params& P, const Window& W, unsigned* acc, const Fields7& F, const double* pt,
-                            const R* vp, const double* vs, unsigned* err) {
-    Tri t = trilinear(P, pt);
+EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const Fields7& F, const Tri& t,
+                          const R* vp, const double* vs, unsigned* err) {
     if (t.ks < -1 || t.ks > P.nz) { set_err(err, ERRB_ZRANGE); return; }
     int lx = wrap_to(t.is - W.gx0, P.nx), ly = wrap_to(t.js - W.gy0, P.ny), lz = t.ks - W.gz0;
     if (W.ok && lx + 1 < W.WX && ly + 1 < W.WY && lz >= 0 && lz + 1 < W.WZ) {
@@ -440,13 +460,22 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
 #pragma unroll
         for (int f = 0; f < NF; ++f) vs[f] = (double)vp[f] * scale[f];
         if (NF == 7) count_parcel(P, pos, a64<R>(pv, A_VOL, i), nparg, nsparg, err);
-        for (int p = 0; p < 4; ++p) {
-            double cp = support_cos(p), sp = support_sin(p);
-            double pt[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) pt[k] = pos[k] + (double)eta[k] * cp + (double)tau[k] * sp;
-            scatter_point<NF, R>(P, W, acc, F, pt, vp, vs, err);
+        const double ed[3] = {(double)eta[0], (double)eta[1], (double)eta[2]};
+        const double td[3] = {(double)tau[0], (double)tau[1], (double)tau[2]};
+        double pt[3];
+        support_point(pos, ed, td, 0, pt);
+        Tri cur = trilinear(P, pt);
+        for (int p = 1; p < 4; ++p) {
+            support_point(pos, ed, td, p, pt);
+            const Tri tp = trilinear(P, pt);
+            if (same_cell(cur, tp)) {
+                add_weights(cur, tp);
+            } else {
+                scatter_tri<NF, R>(P, W, acc, F, cur, vp, vs, err);
+                cur = tp;
+            }
         }
+        scatter_tri<NF, R>(P, W, acc, F, cur, vp, vs, err);
     }
 }
 
@@ -475,7 +504,7 @@ __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long lon
         }
         win_reduce(&ws, wp);
         __syncthreads();
-        if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 36 : 50);
+        if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 34 : 48);
         __syncthreads();
         win_zero<NF, R>(acc, ws.W);
         __syncthreads();
@@ -528,8 +557,7 @@ EPIC_DEV int wrap_near(int i, int n) {
 // point weight 1/4 of parcel_interpl.f90:433).  Returns false when the
 // point leaves the vertical halo.
 template <class R>
-EPIC_DEV bool gather_point(const Params& P, const R* __restrict__ pack, const double* pt, R* g) {
-    Tri t = trilinear(P, pt);
+EPIC_DEV bool gather_tri(const Params& P, const R* __restrict__ pack, const Tri& t, R* g) {
     if (t.ks < -1 || t.ks > P.nz) return false;
     const int i0 = wrap_near(t.is, P.nx), i1 = wrap_near(t.is + 1, P.nx);
     const int j0 = wrap_near(t.js, P.ny), j1 = wrap_near(t.js + 1, P.ny);
@@ -608,13 +636,24 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 R eta[3], tau[3];
 #pragma unroll
                 for (int k = 0; k < 3; ++k) { eta[k] = aR<R>(pv, A_ETA0 + k, i); tau[k] = aR<R>(pv, A_TAU0 + k, i); }
-                for (int p = 0; p < 4; ++p) {
-                    double cp = support_cos(p), sp = support_sin(p);
-                    double pt[3];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) pt[k] = pos[k] + (double)eta[k] * cp + (double)tau[k] * sp;
-                    if (!gather_point<R>(P, pack, pt, g)) set_err(err, ERRB_ZRANGE);
+                const double ed[3] = {(double)eta[0], (double)eta[1], (double)eta[2]};
+                const double td[3] = {(double)tau[0], (double)tau[1], (double)tau[2]};
+                double pt[3];
+                support_point(pos, ed, td, 0, pt);
+                Tri cur = trilinear(P, pt);
+                bool ok = true;
+                for (int p = 1; p < 4; ++p) {
+                    support_point(pos, ed, td, p, pt);
+                    const Tri tp = trilinear(P, pt);
+                    if (same_cell(cur, tp)) {
+                        add_weights(cur, tp);
+                    } else {
+                        ok = gather_tri<R>(P, pack, cur, g) && ok;
+                        cur = tp;
+                    }
                 }
+                ok = gather_tri<R>(P, pack, cur, g) && ok;
+                if (!ok) set_err(err, ERRB_ZRANGE);
             }
             R b[5];
 #pragma unroll
@@ -709,7 +748,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
         if (SCATTER) {
             win_reduce(&ws, wp);
             __syncthreads();
-            if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 36 : 50);
+            if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 34 : 48);
             __syncthreads();
             win_zero<7, R>(acc, ws.W);
             __syncthreads();

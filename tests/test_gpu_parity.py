@@ -303,6 +303,22 @@ def test_nearest_constellations_gpu(olib, glib, case):
     _cmp_parcels(oc, gc)
 
 
+@pytest.mark.parametrize("kind", ["thermal", "beltrami"])
+def test_par2grid_box_windows(olib, glib, kind):
+    """par2grid and vol2grid through the box-ordered store (shared-memory
+    fixed-point windows): after one step with keep_order=0 the parcel set is
+    the oracle's in another order, and the gridded sums must agree."""
+    s = small_state(kind, small_frac=0.02, seed=5)
+    oc = make_context(s, olib)
+    gc = make_context(s, glib, keep_order=0)
+    oc.step(0.0)
+    gc.step(0.0)
+    oc.par2grid(False); gc.par2grid(False)
+    _cmp_fields(oc, gc, list(abi.VORTG) + [abi.TBUOYG, abi.DBUOYG, abi.HUMG, abi.VOLG], tol=1e-9)
+    oc.vol2grid(False); gc.vol2grid(False)
+    _cmp_fields(oc, gc, [abi.VOLG], tol=1e-9)
+
+
 def test_full_steps_reordered_store(olib, glib):
     """keep_order=0: the device reorders parcels by cell tiles each step; the
     parcel set must still equal the oracle's (matched by position)."""

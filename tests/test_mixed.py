@@ -82,3 +82,17 @@ def test_mixed_drift_vs_plain(glib, kind, steps, dt):
     ke1, en1, w1 = runs[MIXED]
     assert abs(ke1 - ke0) / abs(ke0) < DRIFT_TOL
     assert abs(en1 - en0) / abs(en0) < DRIFT_TOL
+
+
+def test_mixed_par2grid_box_windows(olib, glib):
+    """The mixed form's two-limb fixed-point windows (box-ordered store)
+    against the oracle after one full step."""
+    s = small_state("thermal", small_frac=0.02, seed=5)
+    oc = make_context(s, olib)
+    gc = make_context(s, glib, precision=MIXED, keep_order=0)
+    oc.step(0.0)
+    gc.step(0.0)
+    oc.par2grid(False)
+    gc.par2grid(False)
+    for fid in list(abi.VORTG) + [abi.TBUOYG, abi.VOLG]:
+        assert _rel(gc.get_field(fid), oc.get_field(fid)) < 1e-5, fid
