@@ -483,7 +483,7 @@ static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
     // with the following par2grid (stage.cu)
     double tt = t;
     CK(cudaMemcpyAsync(&c.dsc->t, &tt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    par2grid(c, t > c.cfg.t_initial, true);
+    par2grid(c, t > c.cfg.t_initial, true, c.n_stages == 1);
     prof_begin(c, "vor2vel");
     vor2vel(c);
     prof_end(c, "vor2vel");

@@ -99,6 +99,7 @@ struct Ctx {
     // log2 of the consecutive parcels a lane group scatters (vol2grid,
     // par2grid, fused stage)
     int scatter_lg[3] = {1, 1, 0};
+    bool fused_scatter = false;   // stage kernel runs the next par2grid itself (else a separate scatter kernel)
     Tables T;
     StepScalars* dsc = nullptr;     // device
     StepScalars* hsc = nullptr;     // pinned host mirror
@@ -156,7 +157,9 @@ void time_step_reduce(Ctx& c);
 void make_phi(Ctx& c, double* phi);
 
 // parcels.cu
-void par2grid(Ctx& c, bool reuse, bool store_vectors);
+// moist = false skips dbuoyg and humg, which nothing in the step reads before
+// the next par2grid overwrites them (the RK stages before the last)
+void par2grid(Ctx& c, bool reuse, bool store_vectors, bool moist = true);
 void vol2grid(Ctx& c, bool reuse);
 void grid2par(Ctx& c, bool add);
 void g2p_rk_stage(Ctx& c, int stage, bool with_diag);
@@ -173,7 +176,7 @@ void reflective_all(Ctx& c);
 void finish_parcel_diag(Ctx& c, double* out);
 
 // stage.cu
-void scatter_p2g(Ctx& c, bool reuse, bool store);
+void scatter_p2g(Ctx& c, bool reuse, bool store, bool moist = true);
 void scatter_v2g(Ctx& c, bool reuse);
 void fused_stage(Ctx& c, int stage, bool with_diag);
 void sort_parcels(Ctx& c);

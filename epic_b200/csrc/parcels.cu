@@ -103,8 +103,8 @@ void p2g_tail(Ctx& c) {
     CKL();
 }
 
-void par2grid(Ctx& c, bool reuse, bool store_vectors) {
-    scatter_p2g(c, reuse, store_vectors);
+void par2grid(Ctx& c, bool reuse, bool store_vectors, bool moist) {
+    scatter_p2g(c, reuse, store_vectors, moist);
     p2g_tail(c);
 }
 

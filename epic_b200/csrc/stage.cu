@@ -212,7 +212,10 @@ EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long 
 
 struct Fields7 {
     double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg
+    int mask;       // bit f set: field f is accumulated
 };
+constexpr int ALL_FIELDS = 0x7f;
+constexpr int DRY_FIELDS = 0x67;   // without dbuoyg (3) and humg (4)
 
 // Arithmetic of the two forms: R is the type of the FP32-able attributes,
 // of the gathered values and of the window sums (double: plain, float: mixed).
@@ -299,6 +302,25 @@ EPIC_DEV void support_point(const double* pos, const double* eta, const double* 
 #pragma unroll
     for (int k = 0; k < 3; ++k) pt[k] = pos[k] + eta[k] * cp + tau[k] * sp;
 }
+// The points lie on an ellipse in the order 0..3; starting the merge at a
+// point whose predecessor (cyclically) is in another cell also merges a run
+// that wraps from point 3 to point 0.
+EPIC_DEV int merge_start(const Params& P, const double* pos, const double* eta, const double* tau) {
+    int c[4][3];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        double pt[3];
+        support_point(pos, eta, tau, p, pt);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) c[p][k] = (int)floor((pt[k] - P.lower[k]) * P.dxi[k]);
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int q = (p + 3) & 3;
+        if (c[p][0] != c[q][0] || c[p][1] != c[q][1] || c[p][2] != c[q][2]) return p;
+    }
+    return 0;
+}
 
 // Scatter one support point: vp[f] = value * point weight * volume, vs[f] =
 // vp[f] in fixed-point units (plain form only).
@@ -319,11 +341,13 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
                     if constexpr (Form<R>::mixed) {
                         const double wt = (double)(float)t.w[kk][jj][ii];
 #pragma unroll
-                        for (int f = 0; f < NF; ++f) fx2_add(acc + f * 2 * WCAP, w, wt, vs[f]);
+                        for (int f = 0; f < NF; ++f)
+                            if ((F.mask >> f) & 1) fx2_add(acc + f * 2 * WCAP, w, wt, vs[f]);
                     } else {
                         const double wt = t.w[kk][jj][ii];
 #pragma unroll
-                        for (int f = 0; f < NF; ++f) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
+                        for (int f = 0; f < NF; ++f)
+                            if ((F.mask >> f) & 1) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
                     }
                 }
     } else {
@@ -338,7 +362,8 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
                     long long g = a[jj][ii] + kk;
                     const R wt = (R)t.w[kk][jj][ii];
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) atomicAdd(&F.f[f][g], (double)(wt * vp[f]));
+                    for (int f = 0; f < NF; ++f)
+                        if ((F.mask >> f) & 1) atomicAdd(&F.f[f][g], (double)(wt * vp[f]));
                 }
     }
 }
@@ -364,6 +389,7 @@ EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF
         long long g = fidx(P, W.gz0 + z, wrapi(W.gy0 + y, P.ny), wrapi(W.gx0 + x, P.nx));
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
+            if (!((F.mask >> f) & 1)) continue;
             double v;
             if constexpr (Form<R>::mixed) v = fx2_value(acc + f * 2 * WCAP, w, ws->inv[f]);
             else v = fx_value(acc + f * NLIMB * WCAP, w, ws->inv[f]);
@@ -463,10 +489,11 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         const double ed[3] = {(double)eta[0], (double)eta[1], (double)eta[2]};
         const double td[3] = {(double)tau[0], (double)tau[1], (double)tau[2]};
         double pt[3];
-        support_point(pos, ed, td, 0, pt);
+        const int s0 = merge_start(P, pos, ed, td);
+        support_point(pos, ed, td, s0, pt);
         Tri cur = trilinear(P, pt);
-        for (int p = 1; p < 4; ++p) {
-            support_point(pos, ed, td, p, pt);
+        for (int q = 1; q < 4; ++q) {
+            support_point(pos, ed, td, (s0 + q) & 3, pt);
             const Tri tp = trilinear(P, pt);
             if (same_cell(cur, tp)) {
                 add_weights(cur, tp);
@@ -639,11 +666,12 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 const double ed[3] = {(double)eta[0], (double)eta[1], (double)eta[2]};
                 const double td[3] = {(double)tau[0], (double)tau[1], (double)tau[2]};
                 double pt[3];
-                support_point(pos, ed, td, 0, pt);
+                const int s0 = merge_start(P, pos, ed, td);
+                support_point(pos, ed, td, s0, pt);
                 Tri cur = trilinear(P, pt);
                 bool ok = true;
-                for (int p = 1; p < 4; ++p) {
-                    support_point(pos, ed, td, p, pt);
+                for (int q = 1; q < 4; ++q) {
+                    support_point(pos, ed, td, (s0 + q) & 3, pt);
                     const Tri tp = trilinear(P, pt);
                     if (same_cell(cur, tp)) {
                         add_weights(cur, tp);
@@ -782,10 +810,11 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
 }
 
 // ---------------------------------------------------------------------------
-static Fields7 fields7(Ctx& c) {
+static Fields7 fields7(Ctx& c, bool moist = true) {
     Fields7 F;
     F.f[0] = c.vortg(0); F.f[1] = c.vortg(1); F.f[2] = c.vortg(2);
     F.f[3] = c.dbuoyg(); F.f[4] = c.humg(); F.f[5] = c.tbuoyg(); F.f[6] = c.volg();
+    F.mask = moist ? ALL_FIELDS : DRY_FIELDS;
     return F;
 }
 
@@ -839,12 +868,12 @@ static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int
     CKL();
 }
 
-void scatter_p2g(Ctx& c, bool reuse, bool store) {
+void scatter_p2g(Ctx& c, bool reuse, bool store, bool moist) {
     zero_p2g_fields(c);
     if (c.n == 0) return;
     prof_begin(c, "p2g");
-    if (c.pv.mixed) launch_scatter<7, float>(c, fields7(c), reuse, store, c.scatter_lg[1]);
-    else launch_scatter<7, double>(c, fields7(c), reuse, store, c.scatter_lg[1]);
+    if (c.pv.mixed) launch_scatter<7, float>(c, fields7(c, moist), reuse, store, c.scatter_lg[1]);
+    else launch_scatter<7, double>(c, fields7(c, moist), reuse, store, c.scatter_lg[1]);
     prof_end(c, "p2g");
 }
 
@@ -853,6 +882,7 @@ void scatter_v2g(Ctx& c, bool reuse) {
     if (c.n == 0) return;
     Fields7 F;
     F.f[0] = c.volg();
+    F.mask = 1;
     prof_begin(c, "v2g");
     if (c.pv.mixed) launch_scatter<1, float>(c, F, reuse, true, c.scatter_lg[0]);
     else launch_scatter<1, double>(c, F, reuse, true, c.scatter_lg[0]);
@@ -877,12 +907,18 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
         c.n_partials = g;
         c.diag_buf = c.stage_partials;
     }
+    // split form: the stage kernel without its scatter pass, then the scatter
+    // kernel (its own register budget; one more read of the parcels)
+    const bool split = scatter && !c.fused_scatter;
+    const bool moist = S.stage + 1 == c.n_stages;
+    if (split) scatter = false;
     size_t sm = scatter ? win_bytes<R, 7>() : 0;
     auto launch = [&](auto kernel) {
         if (sm) set_smem(kernel, sm);
         prof_begin(c, "stage");
-        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, pack, fields7(c), c.nparg, c.nsparg, S, c.dsc,
-                                        c.stage_partials, &c.dsc->err);
+        // this scatter is the par2grid of stage + 1: dbuoyg and humg only for the last stage
+        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, pack, fields7(c, moist), c.nparg,
+                                        c.nsparg, S, c.dsc, c.stage_partials, &c.dsc->err);
         CKL();
         prof_end(c, "stage");
     };
@@ -890,6 +926,11 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
     else if (with_diag) launch(k_stage<true, false, R>);
     else if (scatter) launch(k_stage<false, true, R>);
     else launch(k_stage<false, false, R>);
+    if (split) {
+        prof_begin(c, "stage");
+        launch_scatter<7, R>(c, fields7(c, moist), false, true, c.scatter_lg[1]);
+        prof_end(c, "stage");
+    }
 }
 
 // One LS-RK stage (grid2par + update) fused with the next stage's par2grid

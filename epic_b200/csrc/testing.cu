@@ -78,3 +78,9 @@ extern "C" int epic_gpu_test_set_scatter_groups(epic_ctx* ctx, int lg_vol2grid, 
     for (int k = 0; k < 3; ++k) ctx->c.scatter_lg[k] = v[k];
     return EPIC_OK;
 }
+
+extern "C" int epic_gpu_test_set_stage_form(epic_ctx* ctx, int fused) {
+    if (!ctx) return EPIC_ERR_ARG;
+    ctx->c.fused_scatter = fused != 0;
+    return EPIC_OK;
+}

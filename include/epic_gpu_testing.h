@@ -38,6 +38,10 @@ int epic_gpu_test_set_fft_path(struct epic_ctx* ctx, int path);
  * setting computes the same sums; it only changes the memory access order. */
 int epic_gpu_test_set_scatter_groups(struct epic_ctx* ctx, int lg_vol2grid, int lg_par2grid, int lg_stage);
 
+/* fused != 0: each LS-RK stage kernel also scatters the next stage's
+ * par2grid; 0: a separate scatter kernel does (same sums). */
+int epic_gpu_test_set_stage_form(struct epic_ctx* ctx, int fused);
+
 #ifdef __cplusplus
 }
 #endif
