@@ -267,6 +267,14 @@ def run_ours(args):
                 "algorithmic_bytes_per_unit": alg}
     if args.traffic is not None:
         roofline["traffic"] = args.traffic
+    elif args.roofline_kernel == "stage" and args.form == "plain":
+        # DRAM bytes of the stage phase from the ncu capture of
+        # profiles/k_stage_k_scatter_thermal64_developed.md (64^3, 2.27M parcels:
+        # 5 x 0.914 GB + 4 x 0.382 GB per step = 2674 B per parcel), scaled by
+        # the parcels of this run (traffic grows with the parcel count)
+        roofline["traffic"] = 2674.0 * avg_n
+        roofline["traffic_source"] = "ncu dram__bytes_read+write of k_stage/k_scatter, 64^3 capture scaled by parcels"
+        roofline["traffic_over_algorithmic"] = roofline["traffic"] / alg
 
     # ---- end-to-end through the C ABI with host buffers (drop-in serial step:
     # the host container owns the parcels; every step copies them in, steps,
