@@ -50,6 +50,7 @@ struct Tables {
     double* rkz = nullptr, *rkzi = nullptr, *gamtop = nullptr, *gambot = nullptr;  // nz+1
     // z-transform matrices, (nz+1) x (nz+1) row-major: DST-I (rows/cols 1..nz-1), DCT-I
     double* mdst = nullptr, *mdct = nullptr;
+    float* mdst32 = nullptr, *mdct32 = nullptr;   // FP32 copies (mixed form)
 };
 
 // Device scalars of one step (kept on the device between kernels).
@@ -149,7 +150,7 @@ constexpr int N_WORK = 14;
 // spectral.cu
 void spectral_init(Ctx& c);
 void spectral_free(Ctx& c);
-void fft_xy(Ctx& c, const double* const* in, double* const* out, int nf, bool forward);
+
 void vor2vel(Ctx& c);
 void vorticity_tendency(Ctx& c);
 void diverge_laplace(Ctx& c, double* phi, double* grad[3]);

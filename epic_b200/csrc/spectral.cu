@@ -33,8 +33,8 @@ namespace epic {
 constexpr int MAXF = 12;
 
 struct FFTBatch {
-    const double* in[MAXF];
-    double* out[MAXF];
+    const void* in[MAXF];   // element type TI of the kernel
+    void* out[MAXF];        // element type TO
     long long es;          // element stride along the transformed axis
     long long row_stride;  // stride between rows of lines
     int nl;                // lines per row (nz + 1, contiguous)
@@ -99,7 +99,7 @@ EPIC_DEV double2* stockham(double2* a, double2* b, int L, int n, int nfac, const
     return a;
 }
 
-template <bool FWD>
+template <bool FWD, class TI, class TO>
 __global__ void __launch_bounds__(256) k_fft_lines(FFTBatch B) {
     extern __shared__ double smem[];
     const int n = B.n, T = B.T, L = T / 2;
@@ -107,8 +107,8 @@ __global__ void __launch_bounds__(256) k_fft_lines(FFTBatch B) {
     double2* cz = reinterpret_cast<double2*>(sx + (long long)T * n);
     double2* cw = cz + (long long)L * n;
     double2* stw = cw + (long long)L * n;
-    const double* in = B.in[blockIdx.z];
-    double* out = B.out[blockIdx.z];
+    const TI* in = static_cast<const TI*>(B.in[blockIdx.z]);
+    TO* out = static_cast<TO*>(B.out[blockIdx.z]);
     const int l0 = blockIdx.x * T;
     const long long rowbase = (long long)blockIdx.y * B.row_stride + 1;
 
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(256) k_fft_lines(FFTBatch B) {
     for (int idx = threadIdx.x; idx < T * n; idx += blockDim.x) {
         int l = idx % T, e = idx / T;
         int line = l0 + l;
-        sx[e * T + l] = (line < B.nl) ? in[rowbase + line + (long long)e * B.es] : 0.0;
+        sx[e * T + l] = (line < B.nl) ? (double)in[rowbase + line + (long long)e * B.es] : 0.0;
     }
     __syncthreads();
     const int h = n / 2;
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256) k_fft_lines(FFTBatch B) {
     for (int idx = threadIdx.x; idx < T * n; idx += blockDim.x) {
         int l = idx % T, e = idx / T;
         int line = l0 + l;
-        if (line < B.nl) out[rowbase + line + (long long)e * B.es] = sx[e * T + l] * B.scale;
+        if (line < B.nl) out[rowbase + line + (long long)e * B.es] = (TO)(sx[e * T + l] * B.scale);
     }
 }
 
@@ -185,13 +185,14 @@ __global__ void __launch_bounds__(256) k_fft_lines(FFTBatch B) {
 // registers over n1 (stride N2), the twiddles W_N^(t k1), an exchange through
 // the line's own storage, and a radix-N2 DFT in registers; only warp-level
 // synchronisation inside a pass.
-struct C2 {
-    double x, y;
+template <class T>
+struct CX {
+    T x, y;
 };
-EPIC_DEV C2 c2(double a, double b) { C2 r; r.x = a; r.y = b; return r; }
-EPIC_DEV C2 operator+(C2 a, C2 b) { return c2(a.x + b.x, a.y + b.y); }
-EPIC_DEV C2 operator-(C2 a, C2 b) { return c2(a.x - b.x, a.y - b.y); }
-EPIC_DEV C2 cmulw(C2 a, C2 w) { return c2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); }
+template <class T> EPIC_DEV CX<T> cx(T a, T b) { CX<T> r; r.x = a; r.y = b; return r; }
+template <class T> EPIC_DEV CX<T> operator+(CX<T> a, CX<T> b) { return cx<T>(a.x + b.x, a.y + b.y); }
+template <class T> EPIC_DEV CX<T> operator-(CX<T> a, CX<T> b) { return cx<T>(a.x - b.x, a.y - b.y); }
+template <class T> EPIC_DEV CX<T> cmulw(CX<T> a, CX<T> w) { return cx<T>(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); }
 
 // exp(-2 pi i j / 16): cos(pi/8), sin(pi/8) and sqrt(1/2) rounded to double
 constexpr double FC1 = 0.92387953251128674, FS1 = 0.38268343236508978, FR2 = 0.70710678118654757;
@@ -200,13 +201,14 @@ EPIC_DEV double w16c(int j) {
     return c[j & 15];
 }
 // a * exp(-2 pi i j / 16) with the quarter turns done exactly
-EPIC_DEV C2 rot16(C2 a, int j) {
+template <class T>
+EPIC_DEV CX<T> rot16(CX<T> a, int j) {
     j &= 15;
     if (j == 0) return a;
-    if (j == 4) return c2(a.y, -a.x);
-    if (j == 8) return c2(-a.x, -a.y);
-    if (j == 12) return c2(-a.y, a.x);
-    return cmulw(a, c2(w16c(j), -w16c((j + 12) & 15)));
+    if (j == 4) return cx<T>(a.y, -a.x);
+    if (j == 8) return cx<T>(-a.x, -a.y);
+    if (j == 12) return cx<T>(-a.y, a.x);
+    return cmulw(a, cx<T>((T)w16c(j), (T)-w16c((j + 12) & 15)));
 }
 
 constexpr int bitrev_c(int i, int n) {
@@ -216,15 +218,15 @@ constexpr int bitrev_c(int i, int n) {
 }
 
 // Forward DFT of N <= 16 values in registers (natural order in and out).
-template <int N>
-EPIC_DEV void fft_reg(C2 (&v)[N]) {
+template <int N, class T>
+EPIC_DEV void fft_reg(CX<T> (&v)[N]) {
 #pragma unroll
     for (int half = N / 2; half >= 1; half >>= 1) {
 #pragma unroll
         for (int blk = 0; blk < N; blk += 2 * half) {
 #pragma unroll
             for (int j = 0; j < half; ++j) {
-                C2 a = v[blk + j], b = v[blk + j + half];
+                CX<T> a = v[blk + j], b = v[blk + j + half];
                 v[blk + j] = a + b;
                 v[blk + j + half] = rot16(a - b, j * (16 / (2 * half)));
             }
@@ -233,7 +235,7 @@ EPIC_DEV void fft_reg(C2 (&v)[N]) {
 #pragma unroll
     for (int i = 0; i < N; ++i) {
         const int r = bitrev_c(i, N);
-        if (r > i) { C2 t = v[i]; v[i] = v[r]; v[r] = t; }
+        if (r > i) { CX<T> t = v[i]; v[i] = v[r]; v[r] = t; }
     }
 }
 
@@ -250,21 +252,21 @@ struct LineGeo {
     int a0, es, bo, s0, cs;
 };
 
-template <int N, bool FWD>
-EPIC_DEV void line_fft(double* P, const LineGeo g, int t, const C2* tw, double scale) {
+template <int N, bool FWD, class T>
+EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
     constexpr int N1 = Radix<N>::N1, N2 = Radix<N>::N2, KPT = N1 / N2, H = N / 2;
-    C2 v[N1];
+    CX<T> v[N1];
 #pragma unroll
     for (int m = 0; m < N1; ++m) {
         const int c = t + N2 * m;
         if (FWD) {
-            v[m] = c2(P[g.a0 + c * g.es], P[g.a0 + c * g.es + g.bo]);
+            v[m] = cx<T>(P[g.a0 + c * g.es], P[g.a0 + c * g.es + g.bo]);
         } else {
             // conj(A + i B) from the Hermitian lines a, b
-            double ra, ia, rb, ib;
+            T ra, ia, rb, ib;
             if (c == 0 || c == H) {
-                ra = P[g.a0 + c * g.es]; ia = 0.0;
-                rb = P[g.a0 + c * g.es + g.bo]; ib = 0.0;
+                ra = P[g.a0 + c * g.es]; ia = T(0);
+                rb = P[g.a0 + c * g.es + g.bo]; ib = T(0);
             } else if (c < H) {
                 ra = P[g.a0 + c * g.es]; ia = P[g.a0 + (N - c) * g.es];
                 rb = P[g.a0 + c * g.es + g.bo]; ib = P[g.a0 + (N - c) * g.es + g.bo];
@@ -272,19 +274,19 @@ EPIC_DEV void line_fft(double* P, const LineGeo g, int t, const C2* tw, double s
                 ra = P[g.a0 + (N - c) * g.es]; ia = -P[g.a0 + c * g.es];
                 rb = P[g.a0 + (N - c) * g.es + g.bo]; ib = -P[g.a0 + c * g.es + g.bo];
             }
-            v[m] = c2(ra - ib, -(ia + rb));
+            v[m] = cx<T>(ra - ib, -(ia + rb));
         }
     }
     fft_reg<N1>(v);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulw(v[k1], tw[t * k1]);
     __syncwarp();
-    C2* sc = reinterpret_cast<C2*>(P + g.s0);
+    CX<T>* sc = reinterpret_cast<CX<T>*>(P + g.s0);
     const int cs2 = g.cs / 2;   // scratch stride in complex elements
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) sc[(k1 * N2 + t) * cs2] = v[k1];
     __syncwarp();
-    C2 y[KPT][N2];
+    CX<T> y[KPT][N2];
 #pragma unroll
     for (int e = 0; e < KPT; ++e)
 #pragma unroll
@@ -300,7 +302,7 @@ EPIC_DEV void line_fft(double* P, const LineGeo g, int t, const C2* tw, double s
             for (int k2 = 0; k2 < N2; ++k2) sc[(t * KPT + e + N1 * k2) * cs2] = y[e][k2];
         __syncwarp();
         constexpr int KU = H / N2 + 1;
-        C2 zk[KU], zn[KU];
+        CX<T> zk[KU], zn[KU];
 #pragma unroll
         for (int j = 0; j < KU; ++j) {
             const int k = t + N2 * j;
@@ -314,11 +316,11 @@ EPIC_DEV void line_fft(double* P, const LineGeo g, int t, const C2* tw, double s
         for (int j = 0; j < KU; ++j) {
             const int k = t + N2 * j;
             if (k <= H) {
-                P[g.a0 + k * g.es] = 0.5 * (zk[j].x + zn[j].x) * scale;
-                P[g.a0 + k * g.es + g.bo] = 0.5 * (zk[j].y + zn[j].y) * scale;
+                P[g.a0 + k * g.es] = T(0.5) * (zk[j].x + zn[j].x) * scale;
+                P[g.a0 + k * g.es + g.bo] = T(0.5) * (zk[j].y + zn[j].y) * scale;
                 if (k > 0 && k < H) {
-                    P[g.a0 + (N - k) * g.es] = 0.5 * (zk[j].y - zn[j].y) * scale;
-                    P[g.a0 + (N - k) * g.es + g.bo] = 0.5 * (zn[j].x - zk[j].x) * scale;
+                    P[g.a0 + (N - k) * g.es] = T(0.5) * (zk[j].y - zn[j].y) * scale;
+                    P[g.a0 + (N - k) * g.es + g.bo] = T(0.5) * (zn[j].x - zk[j].x) * scale;
                 }
             }
         }
@@ -336,8 +338,8 @@ EPIC_DEV void line_fft(double* P, const LineGeo g, int t, const C2* tw, double s
 }
 
 struct PlaneBatch {
-    const double* in[MAXF];
-    double* out[MAXF];
+    const void* in[MAXF];
+    void* out[MAXF];
     const double2* tw;   // exp(-2 pi i m / n)
     int ny, nzh;
     double scale;        // 1 / sqrt(n), applied per pass
@@ -345,42 +347,50 @@ struct PlaneBatch {
 
 // fftxyp2s (FWD: y then x) / fftxys2p (x then y) of plane z = blockIdx.x of
 // field blockIdx.y, rows z = 0 .. nz.
-template <int N, bool FWD>
+template <int N, bool FWD, class TI, class TO, class TC>
 __global__ void __launch_bounds__((N / 2) * Radix<N>::N2) k_fft_plane(PlaneBatch B) {
     constexpr int S = N + 2, N2 = Radix<N>::N2;
-    extern __shared__ double P[];
-    __shared__ C2 tw[N];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TC* P = reinterpret_cast<TC*>(smraw);
+    __shared__ CX<TC> tw[N];
     const int z = blockIdx.x;
-    const double* in = B.in[blockIdx.y];
-    double* out = B.out[blockIdx.y];
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = c2(B.tw[i].x, B.tw[i].y);
+    const TI* in = static_cast<const TI*>(B.in[blockIdx.y]);
+    TO* out = static_cast<TO*>(B.out[blockIdx.y]);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = cx<TC>((TC)B.tw[i].x, (TC)B.tw[i].y);
     for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
         const int ix = idx / N, iy = idx - ix * N;
-        P[ix * S + iy] = in[((long long)ix * B.ny + iy) * B.nzh + 1 + z];
+        P[ix * S + iy] = (TC)in[((long long)ix * B.ny + iy) * B.nzh + 1 + z];
     }
     __syncthreads();
     const int line = threadIdx.x / N2, t = threadIdx.x - line * N2;
     // y lines: rows 2p, 2p+1; x lines: columns 2q, 2q+1 (complex pairs)
     const LineGeo gy = {2 * line * S, 1, S, 2 * line * S, 2};
     const LineGeo gx = {2 * line, S, 1, 2 * line, S};
+    const TC scale = (TC)B.scale;
     if (FWD) {
-        line_fft<N, true>(P, gy, t, tw, B.scale);
+        line_fft<N, true, TC>(P, gy, t, tw, scale);
         __syncthreads();
-        line_fft<N, true>(P, gx, t, tw, B.scale);
+        line_fft<N, true, TC>(P, gx, t, tw, scale);
     } else {
-        line_fft<N, false>(P, gx, t, tw, B.scale);
+        line_fft<N, false, TC>(P, gx, t, tw, scale);
         __syncthreads();
-        line_fft<N, false>(P, gy, t, tw, B.scale);
+        line_fft<N, false, TC>(P, gy, t, tw, scale);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
         const int ix = idx / N, iy = idx - ix * N;
-        out[((long long)ix * B.ny + iy) * B.nzh + 1 + z] = P[ix * S + iy];
+        out[((long long)ix * B.ny + iy) * B.nzh + 1 + z] = (TO)P[ix * S + iy];
     }
 }
 
-template <int N>
-static void launch_plane(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
+// Compute type of a transform: FP32 when either side is FP32 (mixed form).
+template <class TI, class TO>
+using TCmp = typename std::conditional<std::is_same<TI, float>::value || std::is_same<TO, float>::value, float,
+                                       double>::type;
+
+template <int N, class TI, class TO>
+static void launch_plane(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
+    using TC = TCmp<TI, TO>;
     constexpr int S = N + 2;
     PlaneBatch B;
     for (int f = 0; f < nf; ++f) { B.in[f] = in[f]; B.out[f] = out[f]; }
@@ -388,16 +398,16 @@ static void launch_plane(Ctx& c, const double* const* in, double* const* out, in
     B.ny = c.P.ny;
     B.nzh = c.P.nzh;
     B.scale = 1.0 / std::sqrt((double)N);
-    size_t sm = sizeof(double) * (size_t)N * S;
+    size_t sm = sizeof(TC) * (size_t)N * S;
     dim3 grid(c.P.nz + 1, nf);
     int threads = (N / 2) * Radix<N>::N2;
     prof_begin(c, "fft");
     if (forward) {
-        allow_smem(k_fft_plane<N, true>, sm);
-        k_fft_plane<N, true><<<grid, threads, sm, c.stream>>>(B);
+        allow_smem(k_fft_plane<N, true, TI, TO, TC>, sm);
+        k_fft_plane<N, true, TI, TO, TC><<<grid, threads, sm, c.stream>>>(B);
     } else {
-        allow_smem(k_fft_plane<N, false>, sm);
-        k_fft_plane<N, false><<<grid, threads, sm, c.stream>>>(B);
+        allow_smem(k_fft_plane<N, false, TI, TO, TC>, sm);
+        k_fft_plane<N, false, TI, TO, TC><<<grid, threads, sm, c.stream>>>(B);
     }
     CKL();
     prof_end(c, "fft");
@@ -409,36 +419,38 @@ static void launch_plane(Ctx& c, const double* const* in, double* const* out, in
 // transforms them as TL/2 complex line pairs with line_fft.
 constexpr int TL = 32;
 
-template <int N, bool FWD>
+template <int N, bool FWD, class TI, class TO, class TC>
 __global__ void __launch_bounds__((TL / 2) * Radix<N>::N2) k_fft_tile(FFTBatch B) {
     constexpr int S = N + 2, N2 = Radix<N>::N2;
-    extern __shared__ double P[];
-    __shared__ C2 tw[N];
-    const double* in = B.in[blockIdx.z];
-    double* out = B.out[blockIdx.z];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TC* P = reinterpret_cast<TC*>(smraw);
+    __shared__ CX<TC> tw[N];
+    const TI* in = static_cast<const TI*>(B.in[blockIdx.z]);
+    TO* out = static_cast<TO*>(B.out[blockIdx.z]);
     const int l0 = blockIdx.x * TL;
     const long long rowbase = (long long)blockIdx.y * B.row_stride + 1;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = c2(B.tw[i].x, B.tw[i].y);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = cx<TC>((TC)B.tw[i].x, (TC)B.tw[i].y);
     for (int idx = threadIdx.x; idx < TL * N; idx += blockDim.x) {
         const int l = idx % TL, e = idx / TL;
         const int line = l0 + l;
-        P[l * S + e] = (line < B.nl) ? in[rowbase + line + (long long)e * B.es] : 0.0;
+        P[l * S + e] = (line < B.nl) ? (TC)in[rowbase + line + (long long)e * B.es] : TC(0);
     }
     __syncthreads();
     const int pair = threadIdx.x / N2, t = threadIdx.x - pair * N2;
     const LineGeo g = {2 * pair * S, 1, S, 2 * pair * S, 2};
-    line_fft<N, FWD>(P, g, t, tw, B.scale);
+    line_fft<N, FWD, TC>(P, g, t, tw, (TC)B.scale);
     __syncthreads();
     for (int idx = threadIdx.x; idx < TL * N; idx += blockDim.x) {
         const int l = idx % TL, e = idx / TL;
         const int line = l0 + l;
-        if (line < B.nl) out[rowbase + line + (long long)e * B.es] = P[l * S + e];
+        if (line < B.nl) out[rowbase + line + (long long)e * B.es] = (TO)P[l * S + e];
     }
 }
 
-template <int N>
-static void launch_tile_axis(Ctx& c, const FFTPlan& pl, int axis, const double* const* in, double* const* out,
+template <int N, class TI, class TO>
+static void launch_tile_axis(Ctx& c, const FFTPlan& pl, int axis, const TI* const* in, TO* const* out,
                              int nf, bool forward) {
+    using TC = TCmp<TI, TO>;
     const Params& P = c.P;
     FFTBatch B;
     for (int f = 0; f < nf; ++f) { B.in[f] = in[f]; B.out[f] = out[f]; }
@@ -449,22 +461,23 @@ static void launch_tile_axis(Ctx& c, const FFTPlan& pl, int axis, const double* 
     int nrows;
     if (axis == 0) { B.es = (long long)P.ny * P.nzh; B.row_stride = P.nzh; nrows = P.ny; }
     else { B.es = P.nzh; B.row_stride = (long long)P.ny * P.nzh; nrows = P.nx; }
-    size_t sm = sizeof(double) * (size_t)TL * (N + 2);
+    size_t sm = sizeof(TC) * (size_t)TL * (N + 2);
     dim3 grid((B.nl + TL - 1) / TL, nrows, nf);
     int threads = (TL / 2) * Radix<N>::N2;
     prof_begin(c, "fft");
     if (forward) {
-        allow_smem(k_fft_tile<N, true>, sm);
-        k_fft_tile<N, true><<<grid, threads, sm, c.stream>>>(B);
+        allow_smem(k_fft_tile<N, true, TI, TO, TC>, sm);
+        k_fft_tile<N, true, TI, TO, TC><<<grid, threads, sm, c.stream>>>(B);
     } else {
-        allow_smem(k_fft_tile<N, false>, sm);
-        k_fft_tile<N, false><<<grid, threads, sm, c.stream>>>(B);
+        allow_smem(k_fft_tile<N, false, TI, TO, TC>, sm);
+        k_fft_tile<N, false, TI, TO, TC><<<grid, threads, sm, c.stream>>>(B);
     }
     CKL();
     prof_end(c, "fft");
 }
 
-static bool tile_axis(Ctx& c, const FFTPlan& pl, int axis, const double* const* in, double* const* out, int nf,
+template <class TI, class TO>
+static bool tile_axis(Ctx& c, const FFTPlan& pl, int axis, const TI* const* in, TO* const* out, int nf,
                       bool forward) {
     switch (pl.n) {
         case 16: launch_tile_axis<16>(c, pl, axis, in, out, nf, forward); return true;
@@ -477,7 +490,8 @@ static bool tile_axis(Ctx& c, const FFTPlan& pl, int axis, const double* const* 
 }
 
 // Plane kernel sizes: square n x n grids with n = 16, 32, 64, 128.
-static bool plane_fft(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
+template <class TI, class TO>
+static bool plane_fft(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
     const Params& P = c.P;
     if (P.nx != P.ny) return false;
     switch (P.nx) {
@@ -512,8 +526,9 @@ static int tile_lines(int n) {
     return T & ~1;
 }
 
-static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* const* in,
-                         double* const* out, int nf, bool forward) {
+template <class TI, class TO>
+static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const TI* const* in,
+                         TO* const* out, int nf, bool forward) {
     const Params& P = c.P;
     FFTBatch B;
     for (int f = 0; f < nf; ++f) { B.in[f] = in[f]; B.out[f] = out[f]; }
@@ -532,12 +547,12 @@ static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* cons
     dim3 grid((B.nl + B.T - 1) / B.T, nrows, nf);
     prof_begin(c, "fft");
     if (forward) {
-        allow_smem(k_fft_lines<true>, sm);
-        k_fft_lines<true><<<grid, 256, sm, c.stream>>>(B);
+        allow_smem(k_fft_lines<true, TI, TO>, sm);
+        k_fft_lines<true, TI, TO><<<grid, 256, sm, c.stream>>>(B);
         CKL();
     } else {
-        allow_smem(k_fft_lines<false>, sm);
-        k_fft_lines<false><<<grid, 256, sm, c.stream>>>(B);
+        allow_smem(k_fft_lines<false, TI, TO>, sm);
+        k_fft_lines<false, TI, TO><<<grid, 256, sm, c.stream>>>(B);
         CKL();
     }
     prof_end(c, "fft");
@@ -545,21 +560,24 @@ static void run_fft_axis(Ctx& c, const FFTPlan& pl, int axis, const double* cons
 
 // fftxyp2s: y then x (forward); fftxys2p: x then y (reverse).  Only rows
 // z = 0 .. nz are read and written.
-void fft_xy(Ctx& c, const double* const* in, double* const* out, int nf, bool forward) {
+// The first pass reads TI and writes TO; the second runs in place on TO.
+template <class TI, class TO>
+void fft_xy(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
     for (int f0 = 0; f0 < nf; f0 += MAXF) {
         int k = std::min(MAXF, nf - f0);
         if (c.fft_path == 0 && plane_fft(c, in + f0, out + f0, k, forward)) continue;
         // per axis: tiled register FFT for powers of two up to 256, else Stockham lines
-        auto axis = [&](const FFTPlan& pl, int ax, const double* const* src, double* const* dst, bool fwd) {
+        auto axis = [&](const FFTPlan& pl, int ax, auto src, TO* const* dst, bool fwd) {
             if (c.fft_path <= 1 && tile_axis(c, pl, ax, src, dst, k, fwd)) return;
             run_fft_axis(c, pl, ax, src, dst, k, fwd);
         };
+        const TO* const* oc = const_cast<const TO* const*>(out + f0);
         if (forward) {
             axis(c.py, 1, in + f0, out + f0, true);
-            axis(c.px, 0, out + f0, out + f0, true);
+            axis(c.px, 0, oc, out + f0, true);
         } else {
             axis(c.px, 0, in + f0, out + f0, false);
-            axis(c.py, 1, out + f0, out + f0, false);
+            axis(c.py, 1, oc, out + f0, false);
         }
     }
 }
@@ -574,25 +592,27 @@ constexpr int CP = 33;
 
 struct ColArgs {
     const double* tab[8];
-    const double* in[4];
-    double* out[4];
-    const double* mdst;
-    const double* mdct;
+    const void* in[4];      // element type T of the kernel
+    void* out[4];
+    const void* mdst;       // (nz+1)^2 matrices in T
+    const void* mdct;
     int ncol;      // nx * ny
     int nz;
     int nzh;
     double dzi, hdzi;
 };
 
-EPIC_DEV void col_load(const double* f, double* xs, int c0, const ColArgs& A) {
+template <class T>
+EPIC_DEV void col_load(const T* f, T* xs, int c0, const ColArgs& A) {
     int nzp = A.nz + 1;
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx / nzp, j = idx - col * nzp;
         int c = c0 + col;
-        xs[j * CP + col] = (c < A.ncol) ? f[(long long)c * A.nzh + 1 + j] : 0.0;
+        xs[j * CP + col] = (c < A.ncol) ? f[(long long)c * A.nzh + 1 + j] : T(0);
     }
 }
-EPIC_DEV void col_store(double* f, const double* xs, int c0, const ColArgs& A) {
+template <class T>
+EPIC_DEV void col_store(T* f, const T* xs, int c0, const ColArgs& A) {
     int nzp = A.nz + 1;
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx / nzp, j = idx - col * nzp;
@@ -608,24 +628,24 @@ EPIC_DEV double tabv(const double* t, int c, int j, const ColArgs& A) {
 // all 32 columns of a CTA (256 threads), register tiled: thread (rg, cg)
 // computes rows lo + rg + 32 r (r < R) of columns 4 cg .. 4 cg + 3, 20 FMAs
 // per 9 loads.  ADD accumulates into ys instead of overwriting.
-template <int R, bool ADD>
-EPIC_DEV void col_matvec_t(const double* __restrict__ M, int lo, int hi, const double* xs, double* ys, int nz) {
+template <int R, bool ADD, class T>
+EPIC_DEV void col_matvec_t(const T* __restrict__ M, int lo, int hi, const T* xs, T* ys, int nz) {
     const int nzp = nz + 1;
     const int cg = threadIdx.x & 7, rg = threadIdx.x >> 3;
-    double acc[R][4];
+    T acc[R][4];
     int krow[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         krow[r] = min(lo + rg + 32 * r, hi) * nzp;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
+        for (int q = 0; q < 4; ++q) acc[r][q] = T(0);
     }
     for (int j = lo; j <= hi; ++j) {
-        const double* xr = xs + j * CP + 4 * cg;
-        double x0 = xr[0], x1 = xr[1], x2 = xr[2], x3 = xr[3];
+        const T* xr = xs + j * CP + 4 * cg;
+        T x0 = xr[0], x1 = xr[1], x2 = xr[2], x3 = xr[3];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            double m = __ldg(M + krow[r] + j);
+            T m = __ldg(M + krow[r] + j);
             acc[r][0] = fma(m, x0, acc[r][0]);
             acc[r][1] = fma(m, x1, acc[r][1]);
             acc[r][2] = fma(m, x2, acc[r][2]);
@@ -638,7 +658,7 @@ EPIC_DEV void col_matvec_t(const double* __restrict__ M, int lo, int hi, const d
         if (k <= hi) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                double* o = ys + k * CP + 4 * cg + q;
+                T* o = ys + k * CP + 4 * cg + q;
                 *o = ADD ? *o + acc[r][q] : acc[r][q];
             }
         }
@@ -648,25 +668,26 @@ EPIC_DEV void col_matvec_t(const double* __restrict__ M, int lo, int hi, const d
 // field_decompose_semi_spectral (inversion_utils.f90:370-401), optionally
 // followed by the Hou-Li filter and/or preceded by central_diffz_semi_spectral
 // (inversion_utils.f90:460-480).  mode bit 1: filter, bit 2: central diff.
-template <int R>
+template <int R, class T>
 __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
     int nzp = A.nz + 1, nz = A.nz;
-    double* xs = sm;
-    double* ys = sm + nzp * CP;
+    T* xs = sm;
+    T* ys = sm + nzp * CP;
     int c0 = blockIdx.x * CT;
     const double* phim = A.tab[0];
     const double* phip = A.tab[1];
     const double* filt = A.tab[2];
-    col_load(A.in[blockIdx.y], xs, c0, A);
+    col_load(static_cast<const T*>(A.in[blockIdx.y]), xs, c0, A);
     __syncthreads();
     if (mode & 2) {
         for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
             int col = idx % CT, j = idx / CT;
-            double v;
-            if (j == 0) v = A.dzi * (xs[1 * CP + col] - xs[col]);
-            else if (j == nz) v = A.dzi * (xs[nz * CP + col] - xs[(nz - 1) * CP + col]);
-            else v = (xs[(j + 1) * CP + col] - xs[(j - 1) * CP + col]) * A.hdzi;
+            T v;
+            if (j == 0) v = (T)A.dzi * (xs[1 * CP + col] - xs[col]);
+            else if (j == nz) v = (T)A.dzi * (xs[nz * CP + col] - xs[(nz - 1) * CP + col]);
+            else v = (xs[(j + 1) * CP + col] - xs[(j - 1) * CP + col]) * (T)A.hdzi;
             ys[j * CP + col] = v;
         }
         __syncthreads();
@@ -677,10 +698,10 @@ __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
     for (int idx = threadIdx.x; idx < CT * (nz - 1); idx += blockDim.x) {
         int col = idx % CT, j = 1 + idx / CT;
         int c = min(c0 + col, A.ncol - 1);
-        xs[j * CP + col] = xs[j * CP + col] - (xs[col] * tabv(phim, c, j, A) + xs[nz * CP + col] * tabv(phip, c, j, A));
+        xs[j * CP + col] = xs[j * CP + col] - (xs[col] * (T)tabv(phim, c, j, A) + xs[nz * CP + col] * (T)tabv(phip, c, j, A));
     }
     __syncthreads();
-    col_matvec_t<R, false>(A.mdst, 1, nz - 1, xs, ys, nz);
+    col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
     for (int col = threadIdx.x; col < CT; col += blockDim.x) {
         ys[col] = xs[col];
         ys[nz * CP + col] = xs[nz * CP + col];
@@ -690,50 +711,52 @@ __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
         for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
             int col = idx % CT, j = idx / CT;
             int c = min(c0 + col, A.ncol - 1);
-            ys[j * CP + col] = tabv(filt, c, j, A) * ys[j * CP + col];
+            ys[j * CP + col] = (T)tabv(filt, c, j, A) * ys[j * CP + col];
         }
         __syncthreads();
     }
-    col_store(A.out[blockIdx.y], ys, c0, A);
+    col_store(static_cast<T*>(A.out[blockIdx.y]), ys, c0, A);
 }
 
 // field_combine_semi_spectral (inversion_utils.f90:421-456)
-template <int R>
+template <int R, class T>
 __global__ void __launch_bounds__(256) k_col_combine(ColArgs A) {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
     int nzp = A.nz + 1, nz = A.nz;
-    double* xs = sm;
-    double* ys = sm + nzp * CP;
+    T* xs = sm;
+    T* ys = sm + nzp * CP;
     int c0 = blockIdx.x * CT;
     const double* phim = A.tab[0];
     const double* phip = A.tab[1];
-    col_load(A.in[blockIdx.y], xs, c0, A);
+    col_load(static_cast<const T*>(A.in[blockIdx.y]), xs, c0, A);
     __syncthreads();
-    col_matvec_t<R, false>(A.mdst, 1, nz - 1, xs, ys, nz);
+    col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx % CT, j = idx / CT;
         int c = min(c0 + col, A.ncol - 1);
-        double v;
+        T v;
         if (j == 0) v = xs[col];
         else if (j == nz) v = xs[nz * CP + col];
-        else v = ys[j * CP + col] + xs[col] * tabv(phim, c, j, A) + xs[nz * CP + col] * tabv(phip, c, j, A);
+        else v = ys[j * CP + col] + xs[col] * (T)tabv(phim, c, j, A) + xs[nz * CP + col] * (T)tabv(phip, c, j, A);
         xs[j * CP + col] = v;
     }
     __syncthreads();
-    col_store(A.out[blockIdx.y], xs, c0, A);
+    col_store(static_cast<T*>(A.out[blockIdx.y]), xs, c0, A);
 }
 
 // Vertical-velocity solve of vor2vel (inversion.f90:97-150): in[0] = D
 // (source) -> out[0] = w (semi-spectral), out[1] = dw/dz part es.
-template <int R>
+template <int R, class T>
 __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
     int nzp = A.nz + 1, nz = A.nz;
-    double* ds = sm;
-    double* as = sm + nzp * CP;
-    double* bs = sm + 2 * nzp * CP;
-    double* es = sm + 3 * nzp * CP;
+    T* ds = sm;
+    T* as = sm + nzp * CP;
+    T* bs = sm + 2 * nzp * CP;
+    T* es = sm + 3 * nzp * CP;
     int c0 = blockIdx.x * CT;
     const double* thetam = A.tab[0];
     const double* thetap = A.tab[1];
@@ -741,51 +764,51 @@ __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
     const double* dthetap = A.tab[3];
     const double* green = A.tab[4];
     const double* rkz = A.tab[5];
-    col_load(A.in[0], ds, c0, A);
+    col_load(static_cast<const T*>(A.in[0]), ds, c0, A);
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx % CT, j = idx / CT;
         int c = min(c0 + col, A.ncol - 1);
-        double d0 = ds[col], dn = ds[nz * CP + col];
-        if (j >= 1 && j <= nz - 1) bs[j * CP + col] = d0 * tabv(thetam, c, j, A) + dn * tabv(thetap, c, j, A);
-        es[j * CP + col] = d0 * tabv(dthetam, c, j, A) + dn * tabv(dthetap, c, j, A);
+        T d0 = ds[col], dn = ds[nz * CP + col];
+        if (j >= 1 && j <= nz - 1) bs[j * CP + col] = d0 * (T)tabv(thetam, c, j, A) + dn * (T)tabv(thetap, c, j, A);
+        es[j * CP + col] = d0 * (T)tabv(dthetam, c, j, A) + dn * (T)tabv(dthetap, c, j, A);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx % CT, j = idx / CT;
         int c = min(c0 + col, A.ncol - 1);
         if (j >= 1 && j <= nz - 1) {
-            double g = tabv(green, c, j, A) * ds[j * CP + col];
+            T g = (T)tabv(green, c, j, A) * ds[j * CP + col];
             ds[j * CP + col] = g;
-            as[j * CP + col] = rkz[j] * g;
+            as[j * CP + col] = (T)rkz[j] * g;
         } else {
-            as[j * CP + col] = 0.0;
+            as[j * CP + col] = T(0);
         }
     }
     __syncthreads();
     // es += DCT(as); then as(1:nz-1) = DST(ds(1:nz-1))
-    col_matvec_t<R, true>(A.mdct, 0, nz, as, es, nz);
+    col_matvec_t<R, true, T>(static_cast<const T*>(A.mdct), 0, nz, as, es, nz);
     __syncthreads();
-    col_matvec_t<R, false>(A.mdst, 1, nz - 1, ds, as, nz);
+    col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, ds, as, nz);
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx % CT, j = idx / CT;
-        ds[j * CP + col] = (j >= 1 && j <= nz - 1) ? as[j * CP + col] + bs[j * CP + col] : 0.0;
+        ds[j * CP + col] = (j >= 1 && j <= nz - 1) ? as[j * CP + col] + bs[j * CP + col] : T(0);
     }
     __syncthreads();
-    col_store(A.out[0], ds, c0, A);
-    col_store(A.out[1], es, c0, A);
+    col_store(static_cast<T*>(A.out[0]), ds, c0, A);
+    col_store(static_cast<T*>(A.out[1]), es, c0, A);
 }
 
 // ---------------------------------------------------------------------------
 // Pointwise spectral kernels.  Element (kx, ky, iz), iz = 0 .. nz.
 struct SpecArgs {
-    const double* in[6];
-    double* out[6];
+    const void* in[6];      // element type T of the kernel
+    void* out[6];
     const double* k2l2i;
     const double* fdx;
     const double* fdy;
-    const double* zbuf;    // (0,0)-column replacement values (2 x (nz+1))
+    const void* zbuf;      // (0,0)-column replacement values (2 x (nz+1)), T
     int nx, ny, nz, nzh;
     long long nel;         // nx * ny * (nz + 1)
 };
@@ -812,89 +835,102 @@ EPIC_DEV SpecIdx spec_idx(const SpecArgs& S, long long i) {
     return r;
 }
 
+// typed views of the kernel's untyped in/out pointers
+#define IN(k) static_cast<const T*>(S.in[k])
+#define OUT(k) static_cast<T*>(S.out[k])
+
 #define SPEC_LOOP(S) for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (S).nel; \
                           i += (long long)gridDim.x * blockDim.x)
 
 // out0 = Dx(in0) - Dy(in1)  (used for D = B_x - A_y and for the w source
 // Dy(A) - Dx(B) with swapped signs via `sign`)
+template <class T>
 __global__ void k_spec_dxdy(SpecArgs S, double sx, double sy) {
     SPEC_LOOP(S) {
         SpecIdx q = spec_idx(S, i);
-        S.out[0][q.a] = sx * S.fdx[q.kx] * S.in[0][q.ax] + sy * S.fdy[q.ky] * S.in[1][q.ay];
+        OUT(0)[q.a] = (T)(sx * S.fdx[q.kx]) * IN(0)[q.ax] + (T)(sy * S.fdy[q.ky]) * IN(1)[q.ay];
     }
 }
 
 // svor_x = k2l2i (Dx(es) + Dy(ds)); svor_y = k2l2i (Dy(es) - Dx(ds));
 // (0,0) column unchanged (inversion.f90:76-87).  in0 = es, in1 = ds.
+template <class T>
 __global__ void k_spec_project(SpecArgs S) {
     SPEC_LOOP(S) {
         SpecIdx q = spec_idx(S, i);
         if (q.kx == 0 && q.ky == 0) continue;
-        double k2 = S.k2l2i[(long long)q.kx * S.ny + q.ky];
-        double ex = S.fdx[q.kx] * S.in[0][q.ax], ey = S.fdy[q.ky] * S.in[0][q.ay];
-        double dx = S.fdx[q.kx] * S.in[1][q.ax], dy = S.fdy[q.ky] * S.in[1][q.ay];
-        S.out[0][q.a] = k2 * (ex + dy);
-        S.out[1][q.a] = k2 * (ey - dx);
+        T k2 = (T)S.k2l2i[(long long)q.kx * S.ny + q.ky];
+        T fx = (T)S.fdx[q.kx], fy = (T)S.fdy[q.ky];
+        T ex = fx * IN(0)[q.ax], ey = fy * IN(0)[q.ay];
+        T dx = fx * IN(1)[q.ax], dy = fy * IN(1)[q.ay];
+        OUT(0)[q.a] = k2 * (ex + dy);
+        OUT(1)[q.a] = k2 * (ey - dx);
     }
 }
 
 // u = k2l2i (Dx(es) + Dy(cs)), v = k2l2i (Dy(es) - Dx(cs)); (0,0) = ubar, vbar
 // (inversion.f90:180-226).  in0 = es, in1 = cs.
+template <class T>
 __global__ void k_spec_uv(SpecArgs S) {
     SPEC_LOOP(S) {
         SpecIdx q = spec_idx(S, i);
         if (q.kx == 0 && q.ky == 0) {
-            S.out[0][q.a] = S.zbuf[q.iz];
-            S.out[1][q.a] = S.zbuf[S.nz + 1 + q.iz];
+            OUT(0)[q.a] = static_cast<const T*>(S.zbuf)[q.iz];
+            OUT(1)[q.a] = static_cast<const T*>(S.zbuf)[S.nz + 1 + q.iz];
             continue;
         }
-        double k2 = S.k2l2i[(long long)q.kx * S.ny + q.ky];
-        double ex = S.fdx[q.kx] * S.in[0][q.ax], ey = S.fdy[q.ky] * S.in[0][q.ay];
-        double cx = S.fdx[q.kx] * S.in[1][q.ax], cy = S.fdy[q.ky] * S.in[1][q.ay];
-        S.out[0][q.a] = k2 * (ex + cy);
-        S.out[1][q.a] = k2 * (ey - cx);
+        T k2 = (T)S.k2l2i[(long long)q.kx * S.ny + q.ky];
+        T fx = (T)S.fdx[q.kx], fy = (T)S.fdy[q.ky];
+        T ex = fx * IN(0)[q.ax], ey = fy * IN(0)[q.ay];
+        T cx = fx * IN(1)[q.ax], cy = fy * IN(1)[q.ay];
+        OUT(0)[q.a] = k2 * (ex + cy);
+        OUT(1)[q.a] = k2 * (ey - cx);
     }
 }
 
 // velocity gradients (inversion.f90:259-290): in = u, v, w ->
 // out = du/dx, du/dy, dw/dx, dv/dy, dw/dy
+template <class T>
 __global__ void k_spec_grad(SpecArgs S) {
     SPEC_LOOP(S) {
         SpecIdx q = spec_idx(S, i);
-        double fx = S.fdx[q.kx], fy = S.fdy[q.ky];
-        S.out[0][q.a] = fx * S.in[0][q.ax];
-        S.out[1][q.a] = fy * S.in[0][q.ay];
-        S.out[2][q.a] = fx * S.in[2][q.ax];
-        S.out[3][q.a] = fy * S.in[1][q.ay];
-        S.out[4][q.a] = fy * S.in[2][q.ay];
+        T fx = (T)S.fdx[q.kx], fy = (T)S.fdy[q.ky];
+        OUT(0)[q.a] = fx * IN(0)[q.ax];
+        OUT(1)[q.a] = fy * IN(0)[q.ay];
+        OUT(2)[q.a] = fx * IN(2)[q.ax];
+        OUT(3)[q.a] = fy * IN(1)[q.ay];
+        OUT(4)[q.a] = fy * IN(2)[q.ay];
     }
 }
 
 // vorticity tendency: out_c = Dx(Fx_c) + Dy(Fy_c), in = Fx0, Fy0, Fx1, Fy1, Fx2, Fy2
+template <class T>
 __global__ void k_spec_divxy(SpecArgs S) {
     SPEC_LOOP(S) {
         SpecIdx q = spec_idx(S, i);
-        double fx = S.fdx[q.kx], fy = S.fdy[q.ky];
+        T fx = (T)S.fdx[q.kx], fy = (T)S.fdy[q.ky];
         for (int c = 0; c < 3; ++c)
-            S.out[c][q.a] = fx * S.in[2 * c][q.ax] + fy * S.in[2 * c + 1][q.ay];
+            OUT(c)[q.a] = fx * IN(2 * c)[q.ax] + fy * IN(2 * c + 1)[q.ay];
     }
 }
 
 // diverge (inversion.f90:431-451): us = Dx(ds), vs = Dy(ds),
 // ws = central_diffz_semi_spectral(ds) with ws(0) = ws(nz) = 0.
+template <class T>
 __global__ void k_spec_lapgrad(SpecArgs S, double hdzi) {
     SPEC_LOOP(S) {
         SpecIdx q = spec_idx(S, i);
-        const double* d = S.in[0];
-        S.out[0][q.a] = S.fdx[q.kx] * d[q.ax];
-        S.out[1][q.a] = S.fdy[q.ky] * d[q.ay];
-        S.out[2][q.a] = (q.iz == 0 || q.iz == S.nz) ? 0.0 : (d[q.a + 1] - d[q.a - 1]) * hdzi;
+        const T* d = IN(0);
+        OUT(0)[q.a] = (T)S.fdx[q.kx] * d[q.ax];
+        OUT(1)[q.a] = (T)S.fdy[q.ky] * d[q.ay];
+        OUT(2)[q.a] = (q.iz == 0 || q.iz == S.nz) ? T(0) : (d[q.a + 1] - d[q.a - 1]) * (T)hdzi;
     }
 }
 
 // Mean flow (inversion.f90:158-176), one CTA: zbuf = (ubar, vbar).
-__global__ void k_mean_flow(const double* svx, const double* svy, const double* rkzi, const double* gamtop,
-                            const double* gambot, const double* mdct, double* zbuf, int nz) {
+template <class T>
+__global__ void k_mean_flow(const T* svx, const T* svy, const double* rkzi, const double* gamtop,
+                            const double* gambot, const double* mdct, T* zbuf, int nz) {
     extern __shared__ double sm[];
     double* u = sm;
     double* v = sm + nz + 1;
@@ -908,8 +944,8 @@ __global__ void k_mean_flow(const double* svx, const double* svy, const double* 
         const double* row = mdct + (long long)k * (nz + 1);
         double su = 0.0, sv = 0.0;
         for (int j = 0; j <= nz; ++j) { su = fma(row[j], u[j], su); sv = fma(row[j], v[j], sv); }
-        zbuf[k] = su + svy[1 + nz] * gamtop[k] - svy[1] * gambot[k];
-        zbuf[nz + 1 + k] = sv - svx[1 + nz] * gamtop[k] + svx[1] * gambot[k];
+        zbuf[k] = (T)(su + (double)svy[1 + nz] * gamtop[k] - (double)svy[1] * gambot[k]);
+        zbuf[nz + 1 + k] = (T)(sv - (double)svx[1 + nz] * gamtop[k] + (double)svx[1] * gambot[k]);
     }
 }
 
@@ -962,13 +998,14 @@ struct FluxArgs {
     const double* vort[3];
     const double* vel[3];
     const double* b;
-    double* f[6];
+    void* f[6];             // work arrays, element type T of the kernel
     double fc[3];
     int nx, ny, nz, nzh;
     long long nel;   // nx * ny * (nz+1)
 };
 
 // Flux products of vorticity_tendency (inversion.f90:327-348), rows 0..nz.
+template <class T>
 __global__ void k_flux(FluxArgs A) {
     int nzp = A.nz + 1;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.nel;
@@ -978,17 +1015,19 @@ __global__ void k_flux(FluxArgs A) {
         double wx = A.vort[0][a] + A.fc[0], wy = A.vort[1][a] + A.fc[1];
         double b = A.b[a];
         double u = A.vel[0][a], v = A.vel[1][a], w = A.vel[2][a];
-        A.f[0][a] = wx * u;
-        A.f[1][a] = wy * u + b;
-        A.f[2][a] = wx * v - b;
-        A.f[3][a] = wy * v;
-        A.f[4][a] = wx * w;
-        A.f[5][a] = wy * w;
+        T* const* f = reinterpret_cast<T* const*>(A.f);
+        f[0][a] = (T)(wx * u);
+        f[1][a] = (T)(wy * u + b);
+        f[2][a] = (T)(wx * v - b);
+        f[3][a] = (T)(wy * v);
+        f[4][a] = (T)(wx * w);
+        f[5][a] = (T)(wy * w);
     }
 }
 
 // vtend_c(0:nz) = divxy_c + central_diffz((zeta + f_z) u_c), with the zeta
 // boundary zeroing (inversion.f90:374-384, inversion_utils.f90:485-510).
+template <class T>
 __global__ void k_vtend_rows(FluxArgs A, Ptr8 divxy, MPtr8 vt, double dzi, double hdzi, int z0, int z1) {
     int nzp = A.nz + 1, nz = A.nz;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.nel;
@@ -1004,7 +1043,7 @@ __global__ void k_vtend_rows(FluxArgs A, Ptr8 divxy, MPtr8 vt, double dzi, doubl
             if (iz == 0) dz = dzi * ((wz[a + 1] + fz) * u[a + 1] - (wz[a] + fz) * u[a]);
             else if (iz == nz) dz = dzi * ((wz[a] + fz) * u[a] - (wz[a - 1] + fz) * u[a - 1]);
             else dz = ((wz[a + 1] + fz) * u[a + 1] - (wz[a - 1] + fz) * u[a - 1]) * hdzi;
-            double v = divxy.p[k][a] + dz;
+            double v = (double)reinterpret_cast<const T*>(divxy.p[k])[a] + dz;
             if (k == 2 && ((iz == 0 && z0) || (iz == nz && z1))) v = 0.0;
             vt.p[k][a] = v;
         }
@@ -1015,7 +1054,8 @@ __global__ void k_vtend_rows(FluxArgs A, Ptr8 divxy, MPtr8 vt, double dzi, doubl
 // the (0,0) column is zero (inversion.f90:423-426, inversion_utils.f90:584-587).
 // A CTA stages 32 columns of f and of the two tables in shared memory with
 // coalesced loads; one warp then solves its 32 columns, one lane each.
-EPIC_DEV void cols_load(const double* f, double* xs, int c0, int ncol, int nzp, int nzh) {
+template <class T>
+EPIC_DEV void cols_load(const T* f, double* xs, int c0, int ncol, int nzp, int nzh) {
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx / nzp, j = idx - col * nzp;
         int c = c0 + col;
@@ -1023,7 +1063,8 @@ EPIC_DEV void cols_load(const double* f, double* xs, int c0, int ncol, int nzp, 
     }
 }
 
-__global__ void __launch_bounds__(256) k_lapinv(double* fs, const double* etdv, const double* htdv, double ap,
+template <class T>
+__global__ void __launch_bounds__(256) k_lapinv(T* fs, const double* etdv, const double* htdv, double ap,
                                                int ncol, int nz, int nzh) {
     extern __shared__ double sm[];
     const int nzp = nz + 1;
@@ -1054,7 +1095,7 @@ __global__ void __launch_bounds__(256) k_lapinv(double* fs, const double* etdv, 
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx / nzp, j = idx - col * nzp;
         int c = c0 + col;
-        if (c < ncol) fs[(long long)c * nzh + 1 + j] = f[j * CP + col];
+        if (c < ncol) fs[(long long)c * nzh + 1 + j] = (T)f[j * CP + col];
     }
 }
 
@@ -1147,11 +1188,17 @@ static int nblocks(long long n, int bs = 256) {
     return (int)std::min<long long>(b, 148LL * 64);
 }
 
+// Work arrays of the spectral part in the form's type T (the mixed form's
+// are FP32, packed at k * fsz floats of the work block).
+template <class T>
+static T* wk(Ctx& c, int k) { return reinterpret_cast<T*>(c.work) + (long long)k * c.P.fsz; }
+
+template <class T>
 static ColArgs col_args(Ctx& c) {
     ColArgs A;
     std::memset(&A, 0, sizeof(A));
-    A.mdst = c.T.mdst;
-    A.mdct = c.T.mdct;
+    if (std::is_same<T, float>::value) { A.mdst = c.T.mdst32; A.mdct = c.T.mdct32; }
+    else { A.mdst = c.T.mdst; A.mdct = c.T.mdct; }
     A.ncol = c.P.nx * c.P.ny;
     A.nz = c.P.nz;
     A.nzh = c.P.nzh;
@@ -1184,7 +1231,8 @@ static void halo(Ctx& c, std::initializer_list<std::pair<double*, int>> list) {
     CKL();
 }
 
-static size_t col_smem(const Ctx& c, int arrays) { return sizeof(double) * (size_t)arrays * (c.P.nz + 1) * CP; }
+template <class T = double>
+static size_t col_smem(const Ctx& c, int arrays) { return sizeof(T) * (size_t)arrays * (c.P.nz + 1) * CP; }
 
 // Rows per thread of the tiled column matvec: ceil((nz + 1) / 32), nz <= 511.
 static int col_rows(const Params& P) {
@@ -1209,102 +1257,107 @@ static void with_rows(int R, F&& f) {
     }
 }
 
-static void col_decompose(Ctx& c, const double* const* in, double* const* out, int nf, int mode) {
-    ColArgs A = col_args(c);
+template <class T>
+static void col_decompose(Ctx& c, const T* const* in, T* const* out, int nf, int mode) {
+    ColArgs A = col_args<T>(c);
     A.tab[0] = c.T.phim; A.tab[1] = c.T.phip; A.tab[2] = c.T.filt;
     for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
-    size_t sm = col_smem(c, 2);
+    size_t sm = col_smem<T>(c, 2);
     with_rows(col_rows(c.P), [&](auto R) {
-        allow_smem(k_col_decompose<R>, sm);
-        k_col_decompose<R><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A, mode);
+        allow_smem(k_col_decompose<R, T>, sm);
+        k_col_decompose<R, T><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A, mode);
         CKL();
     });
 }
 
-static void col_combine(Ctx& c, const double* const* in, double* const* out, int nf) {
-    ColArgs A = col_args(c);
+template <class T>
+static void col_combine(Ctx& c, const T* const* in, T* const* out, int nf) {
+    ColArgs A = col_args<T>(c);
     A.tab[0] = c.T.phim; A.tab[1] = c.T.phip;
     for (int f = 0; f < nf; ++f) { A.in[f] = in[f]; A.out[f] = out[f]; }
-    size_t sm = col_smem(c, 2);
+    size_t sm = col_smem<T>(c, 2);
     with_rows(col_rows(c.P), [&](auto R) {
-        allow_smem(k_col_combine<R>, sm);
-        k_col_combine<R><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A);
+        allow_smem(k_col_combine<R, T>, sm);
+        k_col_combine<R, T><<<dim3((A.ncol + CT - 1) / CT, nf), 256, sm, c.stream>>>(A);
         CKL();
     });
 }
 
-void vor2vel(Ctx& c) {
+template <class T>
+static void vor2vel_t(Ctx& c) {
     const Params& P = c.P;
     SpecArgs S = spec_args(c);
     int sb = nblocks(S.nel);
-    double* sv[3] = {c.w(0), c.w(1), c.w(2)};
-    double *ds = c.w(3), *es = c.w(4), *cs = c.w(5);
+    T* sv[3] = {wk<T>(c, 0), wk<T>(c, 1), wk<T>(c, 2)};
+    T *ds = wk<T>(c, 3), *es = wk<T>(c, 4), *cs = wk<T>(c, 5);
     // decompose and filter (inversion.f90:36-40)
     {
         const double* in[3] = {c.vortg(0), c.vortg(1), c.vortg(2)};
         fft_xy(c, in, sv, 3, true);
-        col_decompose(c, sv, sv, 3, 1);
+        col_decompose<T>(c, sv, sv, 3, 1);
     }
     // solenoidal projection (inversion.f90:43-87)
     S.in[0] = sv[1]; S.in[1] = sv[0]; S.out[0] = ds;
-    k_spec_dxdy<<<sb, 256, 0, c.stream>>>(S, 1.0, -1.0);
+    k_spec_dxdy<T><<<sb, 256, 0, c.stream>>>(S, 1.0, -1.0);
     CKL();
     {
-        const double* in[1] = {sv[2]};
-        double* out[1] = {cs};
-        col_combine(c, in, out, 1);
-        const double* in2[1] = {cs};
-        double* out2[1] = {es};
-        col_decompose(c, in2, out2, 1, 2);
+        const T* in[1] = {sv[2]};
+        T* out[1] = {cs};
+        col_combine<T>(c, in, out, 1);
+        const T* in2[1] = {cs};
+        T* out2[1] = {es};
+        col_decompose<T>(c, in2, out2, 1, 2);
     }
     S.in[0] = es; S.in[1] = ds; S.out[0] = sv[0]; S.out[1] = sv[1];
-    k_spec_project<<<sb, 256, 0, c.stream>>>(S);
+    k_spec_project<T><<<sb, 256, 0, c.stream>>>(S);
     CKL();
     // vorticity in physical space (inversion.f90:91-93); halo rows keep the
     // par2grid extrapolation, as in the reference
     // (combine(svor_z) is cs from above: svor_z is unchanged since)
     {
-        double* tmp[2] = {c.w(10), c.w(11)};
-        col_combine(c, sv, tmp, 2);
-        const double* inv[3] = {tmp[0], tmp[1], cs};
+        T* tmp[2] = {wk<T>(c, 10), wk<T>(c, 11)};
+        col_combine<T>(c, sv, tmp, 2);
+        const T* inv[3] = {tmp[0], tmp[1], cs};
         double* outv[3] = {c.vortg(0), c.vortg(1), c.vortg(2)};
         fft_xy(c, inv, outv, 3, false);
     }
     // vertical velocity (inversion.f90:97-150)
     S.in[0] = sv[1]; S.in[1] = sv[0]; S.out[0] = ds;
-    k_spec_dxdy<<<sb, 256, 0, c.stream>>>(S, -1.0, 1.0);
+    k_spec_dxdy<T><<<sb, 256, 0, c.stream>>>(S, -1.0, 1.0);
     CKL();
     {
-        ColArgs A = col_args(c);
+        ColArgs A = col_args<T>(c);
         A.tab[0] = c.T.thetam; A.tab[1] = c.T.thetap; A.tab[2] = c.T.dthetam; A.tab[3] = c.T.dthetap;
         A.tab[4] = c.T.green; A.tab[5] = c.T.rkz;
         A.in[0] = ds;
-        A.out[0] = c.w(9);
+        A.out[0] = wk<T>(c, 9);
         A.out[1] = es;
-        size_t sm = col_smem(c, 4);
+        size_t sm = col_smem<T>(c, 4);
         with_rows(col_rows(c.P), [&](auto R) {
-            allow_smem(k_col_wsolve<R>, sm);
-            k_col_wsolve<R><<<(A.ncol + CT - 1) / CT, 256, sm, c.stream>>>(A);
+            allow_smem(k_col_wsolve<R, T>, sm);
+            k_col_wsolve<R, T><<<(A.ncol + CT - 1) / CT, 256, sm, c.stream>>>(A);
             CKL();
         });
         // cs = combine(svor_z) still holds (inversion.f90:150)
     }
     // mean flow (inversion.f90:158-176)
-    double* zbuf = c.w(13);   // first 2 (nz+1) entries used as scratch
-    k_mean_flow<<<1, 256, 2 * sizeof(double) * (P.nz + 1), c.stream>>>(
+    T* zbuf = wk<T>(c, 13);   // first 2 (nz+1) entries used as scratch
+    k_mean_flow<T><<<1, 256, 2 * sizeof(double) * (P.nz + 1), c.stream>>>(
         sv[0], sv[1], c.T.rkzi, c.T.gamtop, c.T.gambot, c.T.mdct, zbuf, P.nz);
     CKL();
     // u, v (inversion.f90:180-226)
-    S.in[0] = es; S.in[1] = cs; S.out[0] = c.w(7); S.out[1] = c.w(8); S.zbuf = zbuf;
-    k_spec_uv<<<sb, 256, 0, c.stream>>>(S);
+    S.in[0] = es; S.in[1] = cs; S.out[0] = wk<T>(c, 7); S.out[1] = wk<T>(c, 8); S.zbuf = zbuf;
+    k_spec_uv<T><<<sb, 256, 0, c.stream>>>(S);
     CKL();
     // velocity gradients (inversion.f90:259-300)
-    S.in[0] = c.w(7); S.in[1] = c.w(8); S.in[2] = c.w(9);
-    S.out[0] = c.w(10); S.out[1] = c.w(11); S.out[2] = c.w(12); S.out[3] = c.w(3); S.out[4] = c.w(6);
-    k_spec_grad<<<sb, 256, 0, c.stream>>>(S);
+    S.in[0] = wk<T>(c, 7); S.in[1] = wk<T>(c, 8); S.in[2] = wk<T>(c, 9);
+    S.out[0] = wk<T>(c, 10); S.out[1] = wk<T>(c, 11); S.out[2] = wk<T>(c, 12); S.out[3] = wk<T>(c, 3);
+    S.out[4] = wk<T>(c, 6);
+    k_spec_grad<T><<<sb, 256, 0, c.stream>>>(S);
     CKL();
     {
-        const double* in[8] = {c.w(7), c.w(8), c.w(9), c.w(10), c.w(11), c.w(12), c.w(3), c.w(6)};
+        const T* in[8] = {wk<T>(c, 7), wk<T>(c, 8), wk<T>(c, 9), wk<T>(c, 10), wk<T>(c, 11), wk<T>(c, 12),
+                          wk<T>(c, 3), wk<T>(c, 6)};
         double* out[8] = {c.velog(0), c.velog(1), c.velog(2), c.velgrad(I_DUDX), c.velgrad(I_DUDY),
                           c.velgrad(I_DWDX), c.velgrad(I_DVDY), c.velgrad(I_DWDY)};
         fft_xy(c, in, out, 8, false);
@@ -1320,56 +1373,73 @@ void vor2vel(Ctx& c) {
     CKL();
 }
 
-void vorticity_tendency(Ctx& c) {
+template <class T>
+static void vorticity_tendency_t(Ctx& c) {
     const Params& P = c.P;
     FluxArgs F;
     std::memset(&F, 0, sizeof(F));
     for (int k = 0; k < 3; ++k) { F.vort[k] = c.vortg(k); F.vel[k] = c.velog(k); F.fc[k] = P.f_cor[k]; }
     F.b = c.tbuoyg();
-    for (int k = 0; k < 6; ++k) F.f[k] = c.w(k);
+    for (int k = 0; k < 6; ++k) F.f[k] = wk<T>(c, k);
     F.nx = P.nx; F.ny = P.ny; F.nz = P.nz; F.nzh = P.nzh;
     F.nel = (long long)P.nx * P.ny * (P.nz + 1);
     int nb = nblocks(F.nel);
-    k_flux<<<nb, 256, 0, c.stream>>>(F);
+    k_flux<T><<<nb, 256, 0, c.stream>>>(F);
     CKL();
-    double* fl[6] = {c.w(0), c.w(1), c.w(2), c.w(3), c.w(4), c.w(5)};
+    T* fl[6] = {wk<T>(c, 0), wk<T>(c, 1), wk<T>(c, 2), wk<T>(c, 3), wk<T>(c, 4), wk<T>(c, 5)};
     fft_xy(c, fl, fl, 6, true);
     SpecArgs S = spec_args(c);
-    for (int k = 0; k < 6; ++k) S.in[k] = c.w(k);
-    S.out[0] = c.w(6); S.out[1] = c.w(7); S.out[2] = c.w(8);
-    k_spec_divxy<<<nblocks(S.nel), 256, 0, c.stream>>>(S);
+    for (int k = 0; k < 6; ++k) S.in[k] = wk<T>(c, k);
+    S.out[0] = wk<T>(c, 6); S.out[1] = wk<T>(c, 7); S.out[2] = wk<T>(c, 8);
+    k_spec_divxy<T><<<nblocks(S.nel), 256, 0, c.stream>>>(S);
     CKL();
-    double* dv[3] = {c.w(6), c.w(7), c.w(8)};
+    T* dv[3] = {wk<T>(c, 6), wk<T>(c, 7), wk<T>(c, 8)};
     fft_xy(c, dv, dv, 3, false);
     Ptr8 d;
     MPtr8 vt;
-    for (int k = 0; k < 3; ++k) { d.p[k] = c.w(6 + k); vt.p[k] = c.vtend(k); }
-    k_vtend_rows<<<nb, 256, 0, c.stream>>>(F, d, vt, P.dzi, P.hdzi, P.zeta_zero[0], P.zeta_zero[1]);
+    for (int k = 0; k < 3; ++k) { d.p[k] = reinterpret_cast<const double*>(wk<T>(c, 6 + k)); vt.p[k] = c.vtend(k); }
+    k_vtend_rows<T><<<nb, 256, 0, c.stream>>>(F, d, vt, P.dzi, P.hdzi, P.zeta_zero[0], P.zeta_zero[1]);
     CKL();
     halo(c, {{c.vtend(0), 0}, {c.vtend(1), 0}, {c.vtend(2), 0}});
 }
 
 // phi -> grad = gradient of the solution of Lap(psi) = phi (diverge,
 // inversion.f90:410-455), grad halo rows extrapolated (parcel_correction.f90:163-165)
-void diverge_laplace(Ctx& c, double* phi, double* grad[3]) {
+template <class T>
+static void diverge_laplace_t(Ctx& c, double* phi, double* grad[3]) {
     const Params& P = c.P;
-    double* ds = c.w(0);
+    T* ds = wk<T>(c, 0);
     const double* in[1] = {phi};
-    double* out[1] = {ds};
+    T* out[1] = {ds};
     fft_xy(c, in, out, 1, true);
     int ncol = P.nx * P.ny;
-    size_t lsm = col_smem(c, 3);
-    allow_smem(k_lapinv, lsm);
-    k_lapinv<<<(ncol + CT - 1) / CT, 256, lsm, c.stream>>>(ds, c.T.etdv, c.T.htdv, P.ap, ncol, P.nz, P.nzh);
+    size_t lsm = col_smem<double>(c, 3);
+    allow_smem(k_lapinv<T>, lsm);
+    k_lapinv<T><<<(ncol + CT - 1) / CT, 256, lsm, c.stream>>>(ds, c.T.etdv, c.T.htdv, P.ap, ncol, P.nz, P.nzh);
     CKL();
     SpecArgs S = spec_args(c);
     S.in[0] = ds;
-    S.out[0] = c.w(1); S.out[1] = c.w(2); S.out[2] = c.w(3);
-    k_spec_lapgrad<<<nblocks(S.nel), 256, 0, c.stream>>>(S, P.hdzi);
+    S.out[0] = wk<T>(c, 1); S.out[1] = wk<T>(c, 2); S.out[2] = wk<T>(c, 3);
+    k_spec_lapgrad<T><<<nblocks(S.nel), 256, 0, c.stream>>>(S, P.hdzi);
     CKL();
-    const double* gi[3] = {c.w(1), c.w(2), c.w(3)};
+    const T* gi[3] = {wk<T>(c, 1), wk<T>(c, 2), wk<T>(c, 3)};
     fft_xy(c, gi, grad, 3, false);
     halo(c, {{grad[0], 0}, {grad[1], 0}, {grad[2], 0}});
+}
+
+// Dispatch by form: the mixed form's spectral temporaries and arithmetic are
+// FP32 (the physical fields stay FP64; lapinv solves in FP64).
+void vor2vel(Ctx& c) {
+    if (c.pv.mixed) vor2vel_t<float>(c);
+    else vor2vel_t<double>(c);
+}
+void vorticity_tendency(Ctx& c) {
+    if (c.pv.mixed) vorticity_tendency_t<float>(c);
+    else vorticity_tendency_t<double>(c);
+}
+void diverge_laplace(Ctx& c, double* phi, double* grad[3]) {
+    if (c.pv.mixed) diverge_laplace_t<float>(c, phi, grad);
+    else diverge_laplace_t<double>(c, phi, grad);
 }
 
 void make_phi(Ctx& c, double* phi) {
@@ -1538,6 +1608,11 @@ void spectral_init(Ctx& c) {
     up(&c.T.etdv, etdv); up(&c.T.htdv, htdv);
     up(&c.T.rkz, rkz); up(&c.T.rkzi, rkzi); up(&c.T.gamtop, gamtop); up(&c.T.gambot, gambot);
     up(&c.T.mdst, mdst); up(&c.T.mdct, mdct);
+    std::vector<float> mdst32(mdst.begin(), mdst.end()), mdct32(mdct.begin(), mdct.end());
+    CK(cudaMalloc(&c.T.mdst32, sizeof(float) * mdst32.size()));
+    CK(cudaMalloc(&c.T.mdct32, sizeof(float) * mdct32.size()));
+    CK(cudaMemcpyAsync(c.T.mdst32, mdst32.data(), sizeof(float) * mdst32.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c.T.mdct32, mdct32.data(), sizeof(float) * mdct32.size(), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
 }
 
@@ -1549,6 +1624,9 @@ void spectral_free(Ctx& c) {
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
+    if (c.T.mdst32) cudaFree(c.T.mdst32);
+    if (c.T.mdct32) cudaFree(c.T.mdct32);
+    c.T.mdst32 = c.T.mdct32 = nullptr;
     if (c.px.tw) cudaFree(c.px.tw);
     if (c.py.tw) cudaFree(c.py.tw);
     c.px.tw = c.py.tw = nullptr;
