@@ -171,12 +171,21 @@ def run_ours(args):
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
 
-    setup = initial.config(args.workload)
     lib = epic_b200.load()
     # the device keeps parcels ordered by boxes of cells (keep_order=0); the
     # parcel set is the reference's, its storage order is not
     mixed = args.form == "mixed"
-    ctx = epic_b200.make_context(setup, lib, keep_order=0, precision=1 if mixed else 0)
+    large = args.workload == "thermal2-512x512x256"
+    if args.device_init or large:
+        # parcels generated on the device (the same state as the host generator)
+        setup = initial.device_spec(args.workload)
+        extra = dict(capacity=int(1.15 * setup.n)) if large else {}
+        ctx = epic_b200.make_context_device(setup, lib, keep_order=0, precision=1 if mixed else 0, **extra)
+        if large:
+            args.no_e2e = True
+    else:
+        setup = initial.config(args.workload)
+        ctx = epic_b200.make_context(setup, lib, keep_order=0, precision=1 if mixed else 0)
     import ctypes as C
     sp = C.c_void_p()
     lib.lib.epic_gpu_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
@@ -525,6 +534,8 @@ def main():
     ap.add_argument("--profile-kernels", default="", help="comma list of kernels to time over one extra step each")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--spinup", type=int, default=0, help="untimed steps before the warm-up (developed flow)")
+    ap.add_argument("--device-init", action="store_true",
+                    help="generate the initial parcels on the device (always for thermal2-512x512x256)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -38,3 +38,16 @@ def make_context(setup, lib: EpicLib | None = None, **overrides) -> EpicContext:
     ctx.set_parcels(*setup.arrays())
     ctx.init_correction()
     return ctx
+
+
+def make_context_device(spec, lib: EpicLib | None = None, **overrides) -> EpicContext:
+    """Create a context for an initial.DeviceSpec: the parcels are generated on
+    the device (epic_gpu_init_state), then init_correction."""
+    lib = lib or load()
+    opts = dict(spec.options)
+    opts.update(overrides)
+    cfg = lib.default_config(spec.nx, spec.ny, spec.nz, spec.lower, spec.extent, **opts)
+    ctx = EpicContext(lib, cfg)
+    ctx.init_state(spec.init_spec())
+    ctx.init_correction()
+    return ctx

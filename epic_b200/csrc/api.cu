@@ -315,11 +315,17 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         CK(cudaMallocHost(&c.hsc, sizeof(StepScalars)));
         CK(cudaMalloc(&c.partials, sizeof(double) * 148 * 8 * 64));
         CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)stage_grid_max(P, c.cap)));
-        CK(cudaMalloc(&c.gpack, sizeof(double) * 16 * (size_t)P.fsz));
+        // gather records: 16 values per grid point (FP32 in the mixed form)
+        CK(cudaMalloc(&c.gpack, (c.pv.mixed ? sizeof(float) : sizeof(double)) * 16 * (size_t)P.fsz));
         if (!cfg->keep_order) {
-            CK(cudaMalloc(&c.pv_alt, c.store_bytes()));
             c.nbox = box_count(P);
             CK(cudaMalloc(&c.box_start, sizeof(int) * ((size_t)c.nbox + 1)));
+            // a second store lets the sort permute in one pass; without room
+            // for it the sort permutes slot by slot through a scratch array
+            if (cudaMalloc(&c.pv_alt, c.store_bytes()) != cudaSuccess) {
+                cudaGetLastError();
+                c.pv_alt = nullptr;
+            }
         }
         CK(cudaMalloc(&c.dvor_bar, sizeof(double) * 8));
         CK(cudaMemsetAsync(c.dvor_bar, 0, sizeof(double) * 8, c.stream));

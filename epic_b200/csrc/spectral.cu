@@ -194,21 +194,24 @@ template <class T> EPIC_DEV CX<T> operator+(CX<T> a, CX<T> b) { return cx<T>(a.x
 template <class T> EPIC_DEV CX<T> operator-(CX<T> a, CX<T> b) { return cx<T>(a.x - b.x, a.y - b.y); }
 template <class T> EPIC_DEV CX<T> cmulw(CX<T> a, CX<T> w) { return cx<T>(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); }
 
-// exp(-2 pi i j / 16): cos(pi/8), sin(pi/8) and sqrt(1/2) rounded to double
-constexpr double FC1 = 0.92387953251128674, FS1 = 0.38268343236508978, FR2 = 0.70710678118654757;
-EPIC_DEV double w16c(int j) {
-    const double c[16] = {1.0, FC1, FR2, FS1, 0.0, -FS1, -FR2, -FC1, -1.0, -FC1, -FR2, -FS1, 0.0, FS1, FR2, FC1};
-    return c[j & 15];
+// cos(2 pi j / 32) = cos(j pi / 16), j = 0..8, rounded to double
+constexpr double K1 = 0.98078528040323043, K2 = 0.92387953251128674, K3 = 0.83146961230254524,
+                 K4 = 0.70710678118654757, K5 = 0.55557023301960218, K6 = 0.38268343236508978,
+                 K7 = 0.19509032201612825;
+EPIC_DEV double w32c(int j) {
+    const double c[32] = {1.0, K1, K2, K3, K4, K5, K6, K7, 0.0, -K7, -K6, -K5, -K4, -K3, -K2, -K1,
+                          -1.0, -K1, -K2, -K3, -K4, -K5, -K6, -K7, 0.0, K7, K6, K5, K4, K3, K2, K1};
+    return c[j & 31];
 }
-// a * exp(-2 pi i j / 16) with the quarter turns done exactly
+// a * exp(-2 pi i j / 32) with the quarter turns done exactly
 template <class T>
-EPIC_DEV CX<T> rot16(CX<T> a, int j) {
-    j &= 15;
+EPIC_DEV CX<T> rot32(CX<T> a, int j) {
+    j &= 31;
     if (j == 0) return a;
-    if (j == 4) return cx<T>(a.y, -a.x);
-    if (j == 8) return cx<T>(-a.x, -a.y);
-    if (j == 12) return cx<T>(-a.y, a.x);
-    return cmulw(a, cx<T>((T)w16c(j), (T)-w16c((j + 12) & 15)));
+    if (j == 8) return cx<T>(a.y, -a.x);
+    if (j == 16) return cx<T>(-a.x, -a.y);
+    if (j == 24) return cx<T>(-a.y, a.x);
+    return cmulw(a, cx<T>((T)w32c(j), (T)-w32c((j + 24) & 31)));
 }
 
 constexpr int bitrev_c(int i, int n) {
@@ -217,7 +220,7 @@ constexpr int bitrev_c(int i, int n) {
     return r;
 }
 
-// Forward DFT of N <= 16 values in registers (natural order in and out).
+// Forward DFT of N <= 32 values in registers (natural order in and out).
 template <int N, class T>
 EPIC_DEV void fft_reg(CX<T> (&v)[N]) {
 #pragma unroll
@@ -228,7 +231,7 @@ EPIC_DEV void fft_reg(CX<T> (&v)[N]) {
             for (int j = 0; j < half; ++j) {
                 CX<T> a = v[blk + j], b = v[blk + j + half];
                 v[blk + j] = a + b;
-                v[blk + j + half] = rot16(a - b, j * (16 / (2 * half)));
+                v[blk + j + half] = rot32(a - b, j * (32 / (2 * half)));
             }
         }
     }
@@ -245,6 +248,7 @@ template <> struct Radix<32> { static constexpr int N1 = 8, N2 = 4; };
 template <> struct Radix<64> { static constexpr int N1 = 8, N2 = 8; };
 template <> struct Radix<128> { static constexpr int N1 = 16, N2 = 8; };
 template <> struct Radix<256> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Radix<512> { static constexpr int N1 = 32, N2 = 16; };
 
 // Line geometry inside the plane: real element c of line a at P[a0 + c*es],
 // of line b at P[a0 + c*es + bo]; complex scratch element c at P[s0 + c*cs].
@@ -414,7 +418,7 @@ static void launch_plane(Ctx& c, const TI* const* in, TO* const* out, int nf, bo
 }
 
 // Tiled line FFT along x (axis 0) or y (axis 1) for power-of-two lengths
-// n = 16 .. 256: a CTA loads TL = 32 consecutive z-lines (coalesced 256-byte
+// n = 16 .. 512: a CTA loads TL = 32 consecutive z-lines (coalesced 256-byte
 // rows) of one (y or x) index into shared memory as rows of n + 2, and
 // transforms them as TL/2 complex line pairs with line_fft.
 constexpr int TL = 32;
@@ -485,6 +489,7 @@ static bool tile_axis(Ctx& c, const FFTPlan& pl, int axis, const TI* const* in, 
         case 64: launch_tile_axis<64>(c, pl, axis, in, out, nf, forward); return true;
         case 128: launch_tile_axis<128>(c, pl, axis, in, out, nf, forward); return true;
         case 256: launch_tile_axis<256>(c, pl, axis, in, out, nf, forward); return true;
+        case 512: launch_tile_axis<512>(c, pl, axis, in, out, nf, forward); return true;
         default: return false;
     }
 }
@@ -1253,6 +1258,9 @@ static void with_rows(int R, F&& f) {
         case 6: f(std::integral_constant<int, 6>{}); break;
         case 7: f(std::integral_constant<int, 7>{}); break;
         case 8: f(std::integral_constant<int, 8>{}); break;
+        case 9: f(std::integral_constant<int, 9>{}); break;
+        case 10: f(std::integral_constant<int, 10>{}); break;
+        case 11: case 12: f(std::integral_constant<int, 12>{}); break;
         default: f(std::integral_constant<int, 16>{}); break;
     }
 }

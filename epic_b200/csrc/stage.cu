@@ -990,10 +990,16 @@ __global__ void k_permute(PView src, PView dst, long long n, const int* perm) {
     }
 }
 
+// One slot gathered through the permutation into a scratch array.
+template <class E>
+__global__ void k_gather_slot(const E* src, E* tmp, long long n, const int* perm) {
+    PLOOP(n) tmp[i] = src[perm[i]];
+}
+
 void sort_parcels(Ctx& c) {
     long long n = c.n;
     c.n_box = 0;
-    if (n < 2 || c.pv_alt == nullptr || c.box_start == nullptr) return;
+    if (n < 2 || c.box_start == nullptr) return;
     size_t cubb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cubb, (unsigned*)0, (unsigned*)0, (int*)0, (int*)0, (int)n, 0, 32,
                                     c.stream);
@@ -1013,10 +1019,28 @@ void sort_parcels(Ctx& c) {
     CK(cub::DeviceRadixSort::SortPairs(tmp, cubb, k0, k1, i0, i1, (int)n, 0, endbit, c.stream));
     k_box_start<<<pgrid(n), PB, 0, c.stream>>>(k1, n, c.nbox, c.box_start);
     CKL();
-    PView dst{c.pv_alt, c.cap, c.pv.mixed};
-    k_permute<<<pgrid(n * 20), PB, 0, c.stream>>>(c.pv, dst, n, i1);
-    CKL();
-    std::swap(c.pv.base, c.pv_alt);
+    if (c.pv_alt) {
+        PView dst{c.pv_alt, c.cap, c.pv.mixed};
+        k_permute<<<pgrid(n * 20), PB, 0, c.stream>>>(c.pv, dst, n, i1);
+        CKL();
+        std::swap(c.pv.base, c.pv_alt);
+    } else {
+        // no second store: slot by slot through the (now free) key arrays k0, k1
+        const int live[20] = {A_X, A_Y, A_Z, A_VX, A_VY, A_VZ, A_B11, A_B12, A_B13, A_B22, A_B23, A_VOL, A_BUOY,
+                              A_HUM, A_ETA0, A_ETA0 + 1, A_ETA0 + 2, A_TAU0, A_TAU0 + 1, A_TAU0 + 2};
+        void* tmp8 = k0;   // k0 and k1 are contiguous: >= 8 n bytes
+        for (int a : live) {
+            if (c.pv.f32(a)) {
+                k_gather_slot<float><<<pgrid(n), PB, 0, c.stream>>>(c.pv.f(a), static_cast<float*>(tmp8), n, i1);
+                CKL();
+                CK(cudaMemcpyAsync(c.pv.f(a), tmp8, sizeof(float) * n, cudaMemcpyDeviceToDevice, c.stream));
+            } else {
+                k_gather_slot<double><<<pgrid(n), PB, 0, c.stream>>>(c.pv.d(a), static_cast<double*>(tmp8), n, i1);
+                CKL();
+                CK(cudaMemcpyAsync(c.pv.d(a), tmp8, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.stream));
+            }
+        }
+    }
     c.n_box = n;
 }
 

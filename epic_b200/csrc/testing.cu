@@ -84,3 +84,13 @@ extern "C" int epic_gpu_test_set_stage_form(epic_ctx* ctx, int fused) {
     ctx->c.fused_scatter = fused != 0;
     return EPIC_OK;
 }
+
+extern "C" int epic_gpu_test_drop_sort_store(epic_ctx* ctx) {
+    if (!ctx) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (c.pv_alt) {
+        if (cudaStreamSynchronize(c.stream) != cudaSuccess || cudaFree(c.pv_alt) != cudaSuccess) return EPIC_ERR_CUDA;
+        c.pv_alt = nullptr;
+    }
+    return EPIC_OK;
+}

@@ -188,3 +188,64 @@ def config(name: str, **kw) -> Setup:
     if name.startswith("thermal-"):
         return thermal(int(name.split("-")[1]), **kw)
     raise KeyError(name)
+
+
+@dataclass
+class DeviceSpec:
+    """A workload whose parcels are generated on the device (epic_gpu_init_state):
+    grid, domain, options and the generator's parameters, no host arrays."""
+    name: str
+    nx: int
+    ny: int
+    nz: int
+    lower: tuple
+    extent: tuple
+    options: dict
+    kind: str                 # "thermal" or "beltrami"
+    seed: int = 1234
+    bubbles: tuple = ((0.0, 0.0, 1.5, 0.5),)
+    klm: tuple = (1, 1, 1)
+    n_per_cell: int = 8
+    steps: int = 1
+
+    @property
+    def n(self) -> int:
+        return self.nx * self.ny * self.nz * self.n_per_cell
+
+    @property
+    def dx(self):
+        return np.array(self.extent) / np.array([self.nx, self.ny, self.nz])
+
+    def init_spec(self):
+        from . import abi
+        if self.kind == "thermal":
+            return abi.init_spec(abi.INIT_THERMAL, self.n_per_cell, self.seed, bubbles=self.bubbles)
+        return abi.init_spec(abi.INIT_BELTRAMI, self.n_per_cell, klm=self.klm)
+
+
+def device_spec(name: str) -> DeviceSpec:
+    """Device-generated versions of the named workloads, plus
+    'thermal2-512x512x256': two Gaussian thermals (b = 0.5 and 0.3 at
+    x = -0.75 and +0.75, z = 1.5) on 512x512x256 cells of 6.28 x 6.28 x 3.14,
+    536,870,912 parcels (the large mixed-precision run)."""
+    def thermal_spec(nx, ny, nz, extent, bubbles, steps):
+        lower = (-0.5 * extent[0], -0.5 * extent[1], 0.0)
+        return DeviceSpec(name, nx, ny, nz, lower, extent,
+                          dict(min_vratio=40.0, lambda_max=4.0, bndry_zeta_zero=(1, 1)),
+                          "thermal", bubbles=bubbles, steps=steps)
+    if name == "thermal2-512x512x256":
+        return thermal_spec(512, 512, 256, (6.28, 6.28, 3.14), ((-0.75, 0.0, 1.5, 0.5), (0.75, 0.0, 1.5, 0.3)), 50)
+    if name == "thermal-256x256x128":
+        return thermal_spec(256, 256, 128, (6.28, 6.28, 3.14), ((0.0, 0.0, 1.5, 0.5),), 100)
+    if name.startswith("thermal-"):
+        n = int(name.split("-")[1])
+        return thermal_spec(n, n, n, (6.28, 6.28, 6.28), ((0.0, 0.0, 1.5, 0.5),), 200)
+    if name.startswith("beltrami-"):
+        n = int(name.split("-")[1])
+        lower = (-math.pi, -math.pi, -0.5 * math.pi)
+        extent = (2 * math.pi, 2 * math.pi, math.pi)
+        from .serve import beltrami_zeta_flags
+        return DeviceSpec(name, n, n, n, lower, extent,
+                          dict(min_vratio=40.0, lambda_max=4.0, bndry_zeta_zero=beltrami_zeta_flags((n, n, n), (1, 1, 1))),
+                          "beltrami", steps=50)
+    raise KeyError(name)

@@ -42,6 +42,10 @@ int epic_gpu_test_set_scatter_groups(struct epic_ctx* ctx, int lg_vol2grid, int 
  * par2grid; 0: a separate scatter kernel does (same sums). */
 int epic_gpu_test_set_stage_form(struct epic_ctx* ctx, int fused);
 
+/* Free the second parcel store, as when the device had no room for it: the
+ * box sort then permutes slot by slot through scratch memory. */
+int epic_gpu_test_drop_sort_store(struct epic_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,7 +79,8 @@ def test_eigen_exact_matches_oracle_bitwise(glib, olib):
 
 @pytest.mark.parametrize("shape,plane", [((64, 64, 64), 0), ((64, 64, 64), 1), ((64, 64, 64), 2),
                                          ((16, 16, 16), 0), ((32, 32, 24), 0), ((128, 128, 32), 0),
-                                         ((48, 32, 16), 0), ((256, 256, 16), 0), ((64, 256, 16), 0)])
+                                         ((48, 32, 16), 0), ((256, 256, 16), 0), ((64, 256, 16), 0),
+                                         ((512, 512, 8), 0)])
 def test_vor2vel_taylor_green_kat(glib, shape, plane):
     """test_mpi_vor2vel.f90: Taylor-Green vorticity on 64^3, max err < 1e-14; the
     same flow on other grids through the three horizontal FFT paths (2-D plane
@@ -319,14 +320,18 @@ def test_par2grid_box_windows(olib, glib, kind):
     _cmp_fields(oc, gc, [abi.VOLG], tol=1e-9)
 
 
-def test_full_steps_reordered_store(olib, glib):
-    """keep_order=0: the device reorders parcels by cell tiles each step; the
-    parcel set must still equal the oracle's (matched by position)."""
+@pytest.mark.parametrize("in_place", [False, True])
+def test_full_steps_reordered_store(olib, glib, in_place):
+    """keep_order=0: the device reorders parcels by boxes of cells each step
+    (through a second store, or slot by slot in place); the parcel set must
+    still equal the oracle's (matched by position)."""
     from scipy.spatial import cKDTree
     s = small_state("thermal", small_frac=0.02, seed=4)
     from epic_b200 import make_context
     oc = make_context(s, olib)
     gc = make_context(s, glib, keep_order=0)
+    if in_place:
+        assert glib.lib.epic_gpu_test_drop_sort_store(gc.h) == 0
     to = tg = 0.0
     for k in range(2):
         to, io = oc.step(to)
