@@ -251,6 +251,8 @@ def run_ours(args):
         kernel_times[kname] = {"ms_per_step": km.value, "launches_per_step": kn.value}
     lib.lib.epic_gpu_profile_kernel(ctx.h, b"")
 
+    free_b, total_b = torch.cuda.mem_get_info()
+    used_gb = (total_b - free_b) / 1e9
     # max over ranks, sum of work
     ms_max, ps_total = reduce_timing(ms, float(psteps))
     value = ps_total / (ms_max * 1e-3)
@@ -346,6 +348,7 @@ def run_ours(args):
                    "grid": [setup.nx, setup.ny, setup.nz], "parcels_at_start": int(setup.n),
                    "parcels_range_timed": [int(nmin), int(nmax)], "precision": precision,
                    "spinup_steps": args.spinup,
+                   "device_memory_used_gb": round(used_gb, 2), "device_memory_total_gb": round(total_b / 1e9, 2),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"inputs larger than L2 (parcel state {store_gb:.2f} GB, fields {field_gb:.2f} GB)"},
         "roofline": roofline,
