@@ -186,6 +186,7 @@ def run_ours(args):
     else:
         setup = initial.config(args.workload)
         ctx = epic_b200.make_context(setup, lib, keep_order=0, precision=1 if mixed else 0)
+    tuning = ctx.autotune() if not args.no_autotune else None
     import ctypes as C
     sp = C.c_void_p()
     lib.lib.epic_gpu_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
@@ -347,7 +348,7 @@ def run_ours(args):
                    "form": args.form,
                    "grid": [setup.nx, setup.ny, setup.nz], "parcels_at_start": int(setup.n),
                    "parcels_range_timed": [int(nmin), int(nmax)], "precision": precision,
-                   "spinup_steps": args.spinup,
+                   "spinup_steps": args.spinup, "autotune": tuning,
                    "device_memory_used_gb": round(used_gb, 2), "device_memory_total_gb": round(total_b / 1e9, 2),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"inputs larger than L2 (parcel state {store_gb:.2f} GB, fields {field_gb:.2f} GB)"},
@@ -537,6 +538,7 @@ def main():
     ap.add_argument("--profile-kernels", default="", help="comma list of kernels to time over one extra step each")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--spinup", type=int, default=0, help="untimed steps before the warm-up (developed flow)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--device-init", action="store_true",
                     help="generate the initial parcels on the device (always for thermal2-512x512x256)")
     ap.add_argument("--no-e2e", action="store_true")

@@ -103,6 +103,13 @@ def init_spec(kind, n_per_cell=8, seed=1234, klm=(1, 1, 1), bubbles=((0.0, 0.0, 
     return s
 
 
+class EpicTuning(C.Structure):
+    """epic_tuning of include/epic_gpu.h (autotuner choices and times)."""
+    _fields_ = [("lg_par2grid", C.c_int32), ("lg_vol2grid", C.c_int32), ("fft_path", C.c_int32),
+                ("reserved", C.c_int32), ("ms_par2grid", C.c_double), ("ms_vol2grid", C.c_double),
+                ("ms_fft", C.c_double)]
+
+
 class EpicError(RuntimeError):
     def __init__(self, code: int, func: str, msg: str):
         self.code = code
@@ -177,7 +184,8 @@ class EpicLib:
             f.restype = C.c_int
             self.fn[name] = f
         # entry points only the CUDA library has
-        for name, args in (("init_state", [_VP, C.POINTER(EpicInitSpec)]),):
+        for name, args in (("init_state", [_VP, C.POINTER(EpicInitSpec)]),
+                           ("autotune", [_VP, C.POINTER(EpicTuning)])):
             if hasattr(self.lib, prefix + name):
                 f = getattr(self.lib, prefix + name)
                 f.argtypes = args
@@ -323,6 +331,11 @@ class EpicContext:
 
     def init_state(self, spec: "EpicInitSpec"):
         self._call("init_state", C.byref(spec))
+
+    def autotune(self) -> dict:
+        t = EpicTuning()
+        self._call("autotune", C.byref(t))
+        return {name: getattr(t, name) for name, _ in t._fields_ if name != "reserved"}
 
     def rk_step(self, t: float):
         tt = C.c_double(t)

@@ -384,6 +384,13 @@ int epic_gpu_init_state(epic_ctx* ctx, const epic_init_spec* spec) {
     API_END
 }
 
+int epic_gpu_autotune(epic_ctx* ctx, epic_tuning* out) {
+    API_BEGIN
+    autotune(ctx->c, out);
+    check_device_error(ctx->c);
+    API_END
+}
+
 int epic_gpu_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, double* vor, double* B,
                          double* vol, double* buoy, double* hum) {
     API_BEGIN

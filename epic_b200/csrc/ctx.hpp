@@ -188,6 +188,11 @@ void p2g_tail(Ctx& c);
 // init.cu
 void init_state(Ctx& c, const epic_init_spec& s);
 
+// tune.cu
+void autotune(Ctx& c, epic_tuning* out);
+// spectral.cu: a forward horizontal FFT of one field into work arrays (timing probe)
+void fft_forward_probe(Ctx& c);
+
 // merge.cu
 long long parcel_merge(Ctx& c);
 

@@ -84,11 +84,14 @@ static epic_ctx* pool_take(epic_server* s, const epic_cfg& cfg, double* bytes) {
 
 static void run_job(epic_server* s, const Job& job, int slot, epic_ctx* ctx, epic_result& r) {
     int rc = EPIC_OK;
+    const bool fresh = ctx == nullptr;
     if (!ctx) rc = epic_gpu_create(&job.req.cfg, &ctx);
     double t = job.req.cfg.t_initial;
     epic_step_info info{};
     int64_t psteps = 0;
     if (rc == EPIC_OK) rc = epic_gpu_init_state(ctx, &job.req.init);
+    // a new context tunes its launch shapes once; pooled ones keep theirs
+    if (rc == EPIC_OK && fresh) rc = epic_gpu_autotune(ctx, nullptr);
     if (rc == EPIC_OK) rc = epic_gpu_init_correction(ctx);
     for (int k = 0; rc == EPIC_OK && k < job.req.steps; ++k) {
         int64_t n0 = 0;

@@ -1435,6 +1435,17 @@ static void diverge_laplace_t(Ctx& c, double* phi, double* grad[3]) {
     halo(c, {{grad[0], 0}, {grad[1], 0}, {grad[2], 0}});
 }
 
+void fft_forward_probe(Ctx& c) {
+    const double* in[3] = {c.tbuoyg(), c.velog(0), c.velog(1)};
+    if (c.pv.mixed) {
+        float* out[3] = {wk<float>(c, 0), wk<float>(c, 1), wk<float>(c, 2)};
+        fft_xy(c, in, out, 3, true);
+    } else {
+        double* out[3] = {wk<double>(c, 0), wk<double>(c, 1), wk<double>(c, 2)};
+        fft_xy(c, in, out, 3, true);
+    }
+}
+
 // Dispatch by form: the mixed form's spectral temporaries and arithmetic are
 // FP32 (the physical fields stay FP64; lapinv solves in FP64).
 void vor2vel(Ctx& c) {

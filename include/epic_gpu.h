@@ -157,6 +157,19 @@ typedef struct epic_init_spec {
     double   bubble[4][4];    /* thermal: centre x, y, z and amplitude         */
 } epic_init_spec;
 int epic_gpu_init_state(epic_ctx* ctx, const epic_init_spec* spec);
+
+/* Autotuner (no counterpart in the reference): times the candidate launch
+ * shapes of this context on its own parcels and grid -- the lane grouping of
+ * the par2grid / vol2grid scatters and the horizontal FFT path -- and keeps
+ * the fastest.  Every candidate computes the same result; only calls that
+ * leave the state unchanged are timed (par2grid, vol2grid, FFTs into work
+ * arrays).  Call after set_parcels / init_state; out may be NULL. */
+typedef struct epic_tuning {
+    int32_t lg_par2grid, lg_vol2grid, fft_path;
+    int32_t reserved;
+    double  ms_par2grid, ms_vol2grid, ms_fft;   /* best times */
+} epic_tuning;
+int epic_gpu_autotune(epic_ctx* ctx, epic_tuning* out);
 /* LS-RK accumulators (delta_pos(3,n), delta_vor(3,n), strain(8,n), delta_b(5,n)). */
 int epic_gpu_get_parcel_rk(epic_ctx* ctx, int64_t cap, int64_t* n, double* delta_pos,
                            double* delta_vor, double* strain, double* delta_b);

@@ -41,7 +41,7 @@ def test_binding_covers_abi():
 def test_oracle_exports_same_abi(olib):
     names = [n.replace("epic_gpu_", "epic_oracle_") for n in _declared("epic_gpu.h")
              if not n.startswith(("epic_gpu_get_stream", "epic_gpu_profile", "epic_gpu_kernel_time",
-                                  "epic_gpu_launch_count", "epic_gpu_apply_vortcor_noalloc"))]
+                                  "epic_gpu_launch_count", "epic_gpu_apply_vortcor_noalloc", "epic_gpu_autotune"))]
     missing = [n for n in names if not hasattr(olib.lib, n)]
     assert not missing, missing
 

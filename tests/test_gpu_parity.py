@@ -345,3 +345,20 @@ def test_full_steps_reordered_store(olib, glib, in_place):
     assert d.max() < 1e-9 and len(set(j.tolist())) == len(j)
     for k in ("vor", "B", "vol", "buoy"):
         assert rel_err(a[k][j], b[k]) < 1e-9, k
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autotune_keeps_results(glib, precision):
+    """The autotuner only changes launch shapes: a step after tuning equals a
+    step of an untuned context on the same state."""
+    s = small_state("thermal", small_frac=0.02, seed=6)
+    a = make_context(s, glib, keep_order=0, precision=precision)
+    b = make_context(s, glib, keep_order=0, precision=precision)
+    tune = a.autotune()
+    assert 0 <= tune["lg_par2grid"] <= 3 and 0 <= tune["lg_vol2grid"] <= 3 and 0 <= tune["fft_path"] <= 2
+    assert tune["ms_par2grid"] > 0 and tune["ms_fft"] > 0
+    ta, ia = a.step(0.0)
+    tb, ib = b.step(0.0)
+    assert ia.n_parcels == ib.n_parcels
+    assert rel_err(ta, tb) < 1e-10
+    assert rel_err(np.array(ia.parcel_stats), np.array(ib.parcel_stats)) < 1e-9
