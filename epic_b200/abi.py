@@ -66,6 +66,12 @@ class EpicCfg(C.Structure):
         ("capacity", C.c_int64),
         ("precision", C.c_int32),
         ("keep_order", C.c_int32),
+        ("damping_vorticity_prefactor", C.c_double),
+        ("damping_scalars_prefactor", C.c_double),
+        ("damping_vorticity", C.c_int32),
+        ("damping_surface_vorticity", C.c_int32),
+        ("damping_scalars", C.c_int32),
+        ("damping_surface_scalars", C.c_int32),
     ]
 
 
@@ -150,6 +156,9 @@ _SIGNATURES = {
     "parcel_diagnostics": [_VP, _D],
     "field_diagnostics": [_VP, _D],
     "step": [_VP, _D, C.POINTER(EpicStepInfo)],
+    "parcel_damp": [_VP, C.c_double],
+    "set_bndry_fluxes": [_VP, _D, _D],
+    "apply_bndry_fluxes": [_VP, C.c_double],
 }
 
 
@@ -378,6 +387,20 @@ class EpicContext:
         st = np.zeros(11)
         self._call("field_diagnostics", _ptr(st))
         return st
+
+    def parcel_damp(self, dt: float):
+        self._call("parcel_damp", C.c_double(dt))
+
+    def set_bndry_fluxes(self, bflux=None, hflux=None):
+        """bflux, hflux: (nx, ny) arrays (= the reference's (ny, nx) Fortran
+        datasets); bflux None turns the fluxes off."""
+        shape = (self.nx, self.ny)
+        b = _f64(bflux, shape) if bflux is not None else None
+        h = _f64(hflux, shape) if hflux is not None else None
+        self._call("set_bndry_fluxes", _ptr(b), _ptr(h))
+
+    def apply_bndry_fluxes(self, dt: float):
+        self._call("apply_bndry_fluxes", C.c_double(dt))
 
     def step(self, t: float):
         tt = C.c_double(t)

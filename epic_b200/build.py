@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libepic_b200.so")
-SOURCES = ["api.cu", "spectral.cu", "parcels.cu", "merge.cu", "testing.cu", "noalloc.cu", "stage.cu", "init.cu", "serve.cu", "tune.cu"]
+SOURCES = ["api.cu", "spectral.cu", "parcels.cu", "merge.cu", "testing.cu", "noalloc.cu", "stage.cu", "init.cu", "serve.cu", "tune.cu", "damping.cu"]
 HEADERS = ["common.cuh", "eigen.cuh", "ctx.hpp", "parcel_ops.cuh", os.path.join("..", "..", "include", "epic_gpu.h"),
            os.path.join("..", "..", "include", "epic_gpu_testing.h"), os.path.join("..", "..", "include", "epic_serve.h")]
 

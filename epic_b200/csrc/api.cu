@@ -238,7 +238,7 @@ static void free_ctx(Ctx& c) {
     c.prof.ev.clear();
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
-                    c.dvor_bar, c.box_start, c.gpack};
+                    c.dvor_bar, c.box_start, c.gpack, c.binc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.scratch) cudaFree(c.scratch);
@@ -277,6 +277,7 @@ int epic_gpu_default_config(epic_cfg* g) {
     g->q_0 = 0.015; g->height_c = 1000.0; g->ang_vel = 0.000072921; g->lat_degrees = 45.0;
     g->l_planetary_vorticity = 0;
     g->capacity = 0; g->precision = EPIC_PRECISION_FP64; g->keep_order = 1;
+    g->damping_vorticity_prefactor = 1.0; g->damping_scalars_prefactor = 1.0;
     return EPIC_OK;
 }
 
@@ -285,6 +286,7 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
     if (cfg->nx < 4 || cfg->ny < 4 || cfg->nz < 2 || cfg->nx % 2 || cfg->ny % 2) return EPIC_ERR_CONFIG;
     if (cfg->extent[0] <= 0 || cfg->extent[1] <= 0 || cfg->extent[2] <= 0) return EPIC_ERR_CONFIG;
     if (cfg->precision != EPIC_PRECISION_FP64 && cfg->precision != EPIC_PRECISION_MIXED) return EPIC_ERR_CONFIG;
+    if (check_damping_flags(*cfg, nullptr) != EPIC_OK) return EPIC_ERR_CONFIG;
     auto* ctx = new epic_ctx();
     Ctx& c = ctx->c;
     c.cfg = *cfg;
@@ -504,7 +506,7 @@ static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
     vorticity_tendency(c);
     prof_end(c, "vtend");
     prof_begin(c, "timestep");
-    time_step_reduce(c);
+    time_step_reduce(c, flux_dt_bound(c));
     prof_end(c, "timestep");
     if (fstats) field_diagnostics(c, fstats);
     for (int s = 1; s <= c.n_stages; ++s) {
@@ -523,6 +525,11 @@ static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
             prof_end(c, "p2g_tail");
         }
     }
+    if (damping_on(c.cfg)) {
+        prof_begin(c, "damping");
+        parcel_damp(c);
+        prof_end(c, "damping");
+    }
     if (pstats) finish_parcel_diag(c, pstats);
     double dt = 0.0;
     CK(cudaMemcpyAsync(&dt, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -537,6 +544,32 @@ int epic_gpu_rk_step(epic_ctx* ctx, double* t, double* dt) {
     if (!t) throw CudaError(EPIC_ERR_ARG, "null t");
     double d = rk_step(ctx->c, *t, nullptr, nullptr);
     if (dt) *dt = d;
+    API_END
+}
+
+int epic_gpu_parcel_damp(epic_ctx* ctx, double dt) {
+    API_BEGIN
+    NEED_PARCELS
+    Ctx& c = ctx->c;
+    std::string msg;
+    if (check_damping_flags(c.cfg, &msg) != EPIC_OK) throw CudaError(EPIC_ERR_CONFIG, msg);
+    CK(cudaMemcpyAsync(&c.dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    parcel_damp(c);
+    check_device_error(c);
+    API_END
+}
+
+int epic_gpu_set_bndry_fluxes(epic_ctx* ctx, const double* bflux, const double* hflux) {
+    API_BEGIN set_bndry_fluxes(ctx->c, bflux, hflux); API_END
+}
+
+int epic_gpu_apply_bndry_fluxes(epic_ctx* ctx, double dt) {
+    API_BEGIN
+    NEED_PARCELS
+    Ctx& c = ctx->c;
+    CK(cudaMemcpyAsync(&c.dsc->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    apply_bndry_fluxes(c);
+    check_device_error(c);
     API_END
 }
 

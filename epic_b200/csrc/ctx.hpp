@@ -4,6 +4,7 @@
 #include "common.cuh"
 
 #include <atomic>
+#include <limits>
 #include <string>
 #include <vector>
 #include <stdexcept>
@@ -126,6 +127,12 @@ struct Ctx {
     std::vector<int> last_isma, last_iclo;
     long long n_parcel_splits = 0, n_parcel_merges = 0, n_big_close = 0;
     bool has_parcels = false;
+    // surface fluxes (bndry_fluxes.f90:25-36): binc, hinc are (ny, nx), y
+    // fastest, scaled by 2 / dz; hinc = binc + nx * ny
+    double* binc = nullptr, *hinc = nullptr;
+    bool flux_on = false;
+    double flux_dt = 0.0;   // alpha (dz / max|binc|)^(1/3)
+    double zdepth = 0.0;
 
     size_t store_bytes() const {
         return (size_t)(pv.mixed ? PARCEL_BYTES_MIXED : PARCEL_BYTES_PLAIN) * (size_t)cap;
@@ -154,7 +161,9 @@ void spectral_free(Ctx& c);
 void vor2vel(Ctx& c);
 void vorticity_tendency(Ctx& c);
 void diverge_laplace(Ctx& c, double* phi, double* grad[3]);
-void time_step_reduce(Ctx& c);
+// dt_cap bounds the step's dt after the reference's checks (the surface-flux
+// bound of ls_rk_step; infinite for get_time_step alone)
+void time_step_reduce(Ctx& c, double dt_cap = std::numeric_limits<double>::infinity());
 void make_phi(Ctx& c, double* phi);
 
 // parcels.cu
@@ -187,6 +196,14 @@ void p2g_tail(Ctx& c);
 
 // init.cu
 void init_state(Ctx& c, const epic_init_spec& s);
+
+// damping.cu
+bool damping_on(const epic_cfg& g);
+int check_damping_flags(const epic_cfg& g, std::string* msg);
+void parcel_damp(Ctx& c);
+void set_bndry_fluxes(Ctx& c, const double* bflux, const double* hflux);
+double flux_dt_bound(const Ctx& c);
+void apply_bndry_fluxes(Ctx& c);
 
 // tune.cu
 void autotune(Ctx& c, epic_tuning* out);

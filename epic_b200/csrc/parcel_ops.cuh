@@ -132,6 +132,36 @@ EPIC_DEV void reflective_bc(const Params& P, double* p, double* b) {
     }
 }
 
+// apply_bndry_fluxes (bndry_fluxes.f90:209-247) for one parcel: below
+// zdepth = lower + dz the parcel gains fb = fac * bilinear(binc) of buoyancy
+// and fh = fac * bilinear(hinc) of humidity, fac = (zdepth - z) dxi dt;
+// binc, hinc are (ny, nx), y fastest; bilinear weights ww[j][i]
+// (interpl.f90:65-90).  Returns false (no change) above zdepth.
+EPIC_DEV bool surface_flux(const Params& P, const double* pos, const double* binc, const double* hinc,
+                           double zdepth, double dt, double& fb, double& fh) {
+    const double z = pos[2];
+    if (!(z < zdepth)) return false;
+    const double x = (pos[0] - P.lower[0]) * P.dxi[0];
+    const double y = (pos[1] - P.lower[1]) * P.dxi[1];
+    const int is = (int)floor(x), js = (int)floor(y);
+    const double px = x - (double)is, pxc = 1.0 - px;
+    const double py = y - (double)js, pyc = 1.0 - py;
+    const double ww[2][2] = {{pyc * pxc, pyc * px}, {py * pxc, py * px}};
+    const double fac = (zdepth - z) * P.dxi[2] * dt;
+    double sb = 0.0, sh = 0.0;
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const long long h = (long long)wrapi(is + ii, P.nx) * P.ny + wrapi(js + j, P.ny);
+            sb = sb + __dmul_rn(ww[j][ii], binc[h]);
+            sh = sh + __dmul_rn(ww[j][ii], hinc[h]);
+        }
+    fb = fac * sb;
+    fh = fac * sh;
+    return true;
+}
+
 constexpr int NDIAG = 12;   // KE ENS LAM LAM2 VOL VOL2 NSMALL XI2 ETA2 ZETA2 BMIN BMAX
 
 

@@ -1174,7 +1174,7 @@ __global__ void k_timestep_reduce(Params P, Ptr8 vg, const double* b, StepScalar
 // dt = min(alpha / gmax, alpha / bmax) with the reference's guards
 // (rk_utils.f90:96-99, 133-182); t is read from the device scalars.
 __global__ void k_timestep_final(StepScalars* sc, double alpha, int fixed, double fixed_dt, int precise,
-                                 double t_limit) {
+                                 double t_limit, double dt_cap) {
     const double eps = 2.220446049250313e-16;
     double gmax = fmax(eps, __longlong_as_double((long long)sc->gmax_bits));
     double bmax = sqrt(sqrt(__longlong_as_double((long long)sc->bmax_bits)));
@@ -1182,7 +1182,7 @@ __global__ void k_timestep_final(StepScalars* sc, double alpha, int fixed, doubl
     double dt = fixed ? fixed_dt : fmin(alpha / gmax, alpha / bmax);
     if (precise && (sc->t + dt > t_limit)) dt = t_limit - sc->t;
     if (!(dt > 0.0)) sc->err |= ERRB_DT;
-    sc->dt = dt;
+    sc->dt = fmin(dt, dt_cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -1466,7 +1466,7 @@ void make_phi(Ctx& c, double* phi) {
     CKL();
 }
 
-void time_step_reduce(Ctx& c) {
+void time_step_reduce(Ctx& c, double dt_cap) {
     CK(cudaMemsetAsync(&c.dsc->gmax_bits, 0, 2 * sizeof(unsigned long long), c.stream));
     Ptr8 vg;
     for (int k = 0; k < 8; ++k) vg.p[k] = c.velgrad(k);
@@ -1474,7 +1474,8 @@ void time_step_reduce(Ctx& c) {
     k_timestep_reduce<<<nblocks(nel), 256, 0, c.stream>>>(c.P, vg, c.tbuoyg(), c.dsc);
     CKL();
     const epic_cfg& g = c.cfg;
-    k_timestep_final<<<1, 1, 0, c.stream>>>(c.dsc, g.alpha, g.use_fixed_dt, g.fixed_dt, g.precise_stop, g.t_limit);
+    k_timestep_final<<<1, 1, 0, c.stream>>>(c.dsc, g.alpha, g.use_fixed_dt, g.fixed_dt, g.precise_stop, g.t_limit,
+                                            dt_cap);
     CKL();
 }
 

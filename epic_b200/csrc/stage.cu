@@ -547,6 +547,10 @@ __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long lon
 struct FusedArgs {
     int stage, last, lg;
     double ca, cb;
+    // surface fluxes of stage 1 (null: none)
+    const double* binc;
+    const double* hinc;
+    double zdepth;
 };
 
 // The 14 gathered fields (velog 3, velgradg 8, vtend 3) of a grid point as
@@ -720,6 +724,15 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 dacc[9] += vol * (vz * vz);
                 dacc[10] = fmin(dacc[10], bu);
                 dacc[11] = fmax(dacc[11], bu);
+            }
+            if (DIAG && S.binc) {
+                // apply_bndry_fluxes after the diagnostics, before the first
+                // substep moves the parcel (ls_rk.f90:113-119)
+                double fb, fh;
+                if (surface_flux(P, pos, S.binc, S.hinc, S.zdepth, dt, fb, fh)) {
+                    aR<R>(pv, A_BUOY, i) = (R)((double)aR<R>(pv, A_BUOY, i) + fb);
+                    aR<R>(pv, A_HUM, i) = (R)((double)aR<R>(pv, A_HUM, i) + fh);
+                }
             }
             R db[5];
             dBdt_r<R>(strain, b, (R)B33d, db);
@@ -942,6 +955,13 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     S.ca = c.ca[stage - 1];
     S.cb = c.cb[stage - 1];
     S.lg = c.scatter_lg[2];
+    // surface fluxes: inside the stage-1 kernel after its diagnostics, or
+    // (no diagnostics) by their own kernel before it
+    const bool flux = stage == 1 && c.flux_on;
+    if (flux && !with_diag) apply_bndry_fluxes(c);
+    S.binc = flux && with_diag ? c.binc : nullptr;
+    S.hinc = flux && with_diag ? c.hinc : nullptr;
+    S.zdepth = c.zdepth;
     bool scatter = !S.last;
     if (c.pv.mixed) launch_stage<float>(c, S, with_diag, scatter);
     else launch_stage<double>(c, S, with_diag, scatter);

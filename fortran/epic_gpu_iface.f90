@@ -27,6 +27,10 @@ module epic_gpu_iface
         integer(c_int64_t) :: capacity
         integer(c_int32_t) :: precision
         integer(c_int32_t) :: keep_order
+        ! damping (options.f90:112-122): the reference's logicals as 0 / 1
+        real(c_double)     :: damping_vorticity_prefactor, damping_scalars_prefactor
+        integer(c_int32_t) :: damping_vorticity, damping_surface_vorticity
+        integer(c_int32_t) :: damping_scalars, damping_surface_scalars
     end type epic_cfg
 
     type, bind(C) :: epic_step_info
@@ -85,6 +89,14 @@ module epic_gpu_iface
             type(c_ptr), value   :: ctx
             real(c_double)       :: t
             type(epic_step_info) :: info
+        end function
+
+        ! read_bndry_fluxes: binc, hinc as read from the flux file (y, x)
+        integer(c_int) function epic_gpu_set_bndry_fluxes(ctx, bflux, hflux) &
+                bind(C, name="epic_gpu_set_bndry_fluxes")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value         :: ctx
+            real(c_double), intent(in) :: bflux(*), hflux(*)
         end function
 
         integer(c_int) function epic_gpu_get_field(ctx, field_id, out) bind(C, name="epic_gpu_get_field")

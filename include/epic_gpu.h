@@ -96,6 +96,15 @@ typedef struct epic_cfg {
     int64_t capacity;
     int32_t precision;              /* EPIC_PRECISION_*                         */
     int32_t keep_order;             /* 1: keep the reference's parcel order     */
+    /* damping (options.f90:112-122, parcel_damping.f90:43-225); at most one
+       of damping_vorticity / damping_surface_vorticity and of
+       damping_scalars / damping_surface_scalars */
+    double  damping_vorticity_prefactor;   /* 1.0                            */
+    double  damping_scalars_prefactor;     /* 1.0                            */
+    int32_t damping_vorticity;             /* 0                              */
+    int32_t damping_surface_vorticity;     /* 0                              */
+    int32_t damping_scalars;               /* 0                              */
+    int32_t damping_surface_scalars;       /* 0                              */
 } epic_cfg;
 
 /* Per-step report (epic3d.f90:135-153 plus the statistics the reference
@@ -213,6 +222,23 @@ int epic_gpu_vol2grid(epic_ctx* ctx, int reuse);
  * (parcel_diagnostics.f90:51-159, field_diagnostics.f90:40-154). */
 int epic_gpu_parcel_diagnostics(epic_ctx* ctx, double stats[18]);
 int epic_gpu_field_diagnostics(epic_ctx* ctx, double stats[11]);
+/* parcel_damp (parcel_damping.f90:43-78): par2grid, vor2vel, z-halo
+ * reflection, get_strain_magnitude_field (rk_utils.f90:186-214) and
+ * perturbation_damping (parcel_damping.f90:82-222) with the support points of
+ * that par2grid.  ls_rk_step calls it after the last stage when any damping
+ * flag of the configuration is set; a no-op otherwise. */
+int epic_gpu_parcel_damp(epic_ctx* ctx, double dt);
+/* Surface fluxes of buoyancy and humidity (bndry_fluxes.f90:100-175): bflux
+ * and hflux are ny x nx arrays, y fastest (the 'bflux' / 'hflux' datasets of
+ * the reference's flux file, m^2/s^3 and 1/s times m).  Stored scaled by
+ * 2 / dz; from then on ls_rk_step bounds dt by alpha (dz / max|binc|)^(1/3)
+ * (bndry_fluxes_time_step, :180-205; not with a fixed dt) and adds the fluxes
+ * to the parcels below lower + dz before the first stage (apply_bndry_fluxes,
+ * :209-247).  hflux may be NULL (zero humidity flux); bflux == NULL turns the
+ * fluxes off (the reference's empty flux_file). */
+int epic_gpu_set_bndry_fluxes(epic_ctx* ctx, const double* bflux, const double* hflux);
+/* apply_bndry_fluxes (bndry_fluxes.f90:209-247) alone, for a given dt. */
+int epic_gpu_apply_bndry_fluxes(epic_ctx* ctx, double dt);
 /* One iteration of the run loop (epic3d.f90:135-153): apply_vortcor,
  * ls_rk_step, parcel_merge, parcel_split, correction_iters x
  * (apply_laplace, apply_gradient). */

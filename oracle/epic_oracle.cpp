@@ -68,6 +68,12 @@ struct Ctx {
     // counters for diagnostics
     long n_parcel_splits = 0, n_parcel_merges = 0, n_big_close = 0;
     double t = 0.0;
+    // surface fluxes (bndry_fluxes.f90:25-36): (ny, nx), y fastest, scaled by 2/dz
+    bool l_enable_flux = false;
+    std::vector<double> binc, hinc;
+    double zdepth = 0.0;
+    // strain magnitude of parcel_damp (fields.f90 strain_mag)
+    std::vector<double> strain_mag;
 
     long fi(int iz, int iy, int ix) const { return ((long)ix * ny + iy) * nzh + (iz + 1); }
     long si(int iz, int ky, int kx) const { return ((long)kx * ny + ky) * (nz + 1) + iz; }
@@ -1117,6 +1123,204 @@ void apply_gradient(Ctx& c, double prefactor, double max_compression, bool reuse
 }
 
 // ---------------------------------------------------------------------------
+// Surface fluxes (bndry_fluxes.f90)
+
+// read_bndry_fluxes (:100-175) given the two datasets: binc = 2 dxi(3) bflux.
+void set_bndry_fluxes(Ctx& c, const double* bflux, const double* hflux) {
+    c.l_enable_flux = bflux != nullptr;
+    if (!c.l_enable_flux) return;
+    const long m = (long)c.nx * c.ny;
+    c.binc.assign(bflux, bflux + m);
+    c.hinc.assign(m, zero);
+    if (hflux) c.hinc.assign(hflux, hflux + m);
+    c.zdepth = c.lower[2] + c.dx[2];
+    for (long i = 0; i < m; ++i) {
+        c.binc[i] = two * c.dxi[2] * c.binc[i];
+        c.hinc[i] = two * c.dxi[2] * c.hinc[i];
+    }
+}
+
+// bndry_fluxes_time_step (:180-205)
+void bndry_fluxes_time_step(Ctx& c, double& dt) {
+    if (!c.l_enable_flux) return;
+    double abs_max = 0.0;
+    for (double v : c.binc) abs_max = std::max(abs_max, std::fabs(v));
+    abs_max = std::pow(c.dx[2] / abs_max, f13);
+    dt = std::min(dt, c.cfg.alpha * abs_max);
+}
+
+// apply_bndry_fluxes (:209-247) with bilinear (interpl.f90:65-90); ww[j][i]
+void apply_bndry_fluxes(Ctx& c, double dt) {
+    if (!c.l_enable_flux) return;
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < c.n; ++n) {
+        const double z = c.pos[3 * n + 2];
+        if (!(z < c.zdepth)) continue;
+        double xy0 = (c.pos[3 * n] - c.lower[0]) * c.dxi[0];
+        double xy1 = (c.pos[3 * n + 1] - c.lower[1]) * c.dxi[1];
+        int is = ffloor(xy0), js = ffloor(xy1);
+        double px = xy0 - (double)is, pxc = one - px;
+        double py = xy1 - (double)js, pyc = one - py;
+        double ww[2][2] = {{pyc * pxc, pyc * px}, {py * pxc, py * px}};
+        double fac = (c.zdepth - z) * c.dxi[2] * dt;
+        double sb = 0.0, sh = 0.0;
+        for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j) {
+                long h = c.hi2(c.wrapy(js + j), c.wrapx(is + i));
+                sb += ww[j][i] * c.binc[h];
+                sh += ww[j][i] * c.hinc[h];
+            }
+        c.buoy[n] = c.buoy[n] + fac * sb;
+        c.hum[n] = c.hum[n] + fac * sh;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Damping (parcel_damping.f90)
+
+// get_strain_magnitude_field (rk_utils.f90:186-214): sqrt(2 S:S) of the
+// symmetrised strain, z halo reflected (the x/y halo is the periodic wrap).
+void strain_magnitude_field(Ctx& c) {
+    c.strain_mag.assign(c.fsz, 0.0);
+    for (int ix = 0; ix < c.nx; ++ix)
+        for (int iy = 0; iy < c.ny; ++iy) {
+            long t = c.fi(0, iy, ix);
+            for (int iz = 0; iz <= c.nz; ++iz) {
+                double v[8];
+                for (int l = 0; l < 8; ++l) v[l] = c.velgradg[l][t + iz];
+                double S[9];
+                M3(S, 0, 0) = v[I_DUDX];
+                M3(S, 0, 1) = f12 * (v[I_DUDY] + v[I_DVDX]);
+                M3(S, 0, 2) = f12 * (v[I_DUDZ] + v[I_DWDX]);
+                M3(S, 1, 0) = M3(S, 0, 1);
+                M3(S, 1, 1) = v[I_DVDY];
+                M3(S, 1, 2) = f12 * (v[I_DVDZ] + v[I_DWDY]);
+                M3(S, 2, 0) = M3(S, 0, 2);
+                M3(S, 2, 1) = M3(S, 1, 2);
+                M3(S, 2, 2) = -(v[I_DUDX] + v[I_DVDY]);
+                double q = M3(S, 0, 0) * M3(S, 0, 0) + M3(S, 0, 1) * M3(S, 0, 1);
+                q = q + M3(S, 0, 2) * M3(S, 0, 2);
+                q = q + M3(S, 1, 0) * M3(S, 1, 0);
+                q = q + M3(S, 1, 1) * M3(S, 1, 1);
+                q = q + M3(S, 1, 2) * M3(S, 1, 2);
+                q = q + M3(S, 2, 0) * M3(S, 2, 0);
+                q = q + M3(S, 2, 1) * M3(S, 2, 1);
+                q = q + M3(S, 2, 2) * M3(S, 2, 2);
+                c.strain_mag[t + iz] = std::sqrt(two * q);
+            }
+            c.strain_mag[t - 1] = c.strain_mag[t + 1];
+            c.strain_mag[t + c.nz + 1] = c.strain_mag[t + c.nz - 1];
+        }
+}
+
+void check_damping_flags(const epic_cfg& g) {
+    if (g.damping_vorticity && g.damping_surface_vorticity)
+        throw OracleError(EPIC_ERR_CONFIG,
+                          "damping%l_vorticity and  damping%l_surface_vorticity both activated, only one allowed");
+    if (g.damping_scalars && g.damping_surface_scalars)
+        throw OracleError(EPIC_ERR_CONFIG,
+                          "damping%l_scalars and  damping%l_surface_scalars both activated, only one allowed");
+}
+
+// perturbation_damping (:82-222), moist build (humidity and dry buoyancy).
+// sum(weight * time_fact * (g - a)) over the 2x2x2 corners in Fortran order
+// (k fastest); the surface forms sum over the (j, i) slice of level ks + si.
+void perturbation_damping(Ctx& c, double dt, bool reuse) {
+    const epic_cfg& g = c.cfg;
+    const bool lv = g.damping_vorticity, ls = g.damping_scalars;
+    const bool lsv = g.damping_surface_vorticity, lss = g.damping_surface_scalars;
+    const double pv = g.damping_vorticity_prefactor, ps = g.damping_scalars_prefactor;
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < c.n; ++n) {
+        if (!(lv || ls)) {
+            const double z = c.pos[3 * n + 2];
+            if (z > c.lower[2] + 2 * c.dx[2] && z < c.upper[2] - 2 * c.dx[2]) continue;
+        }
+        double pts[4][3], ww[2][2][2], wt[2][2][2], tf[2][2][2];
+        int is, js, ks;
+        get_points(c, n, reuse, pts);
+        double vortend[3] = {zero, zero, zero}, humtend = zero, dbuoytend = zero;
+        const double* vor = &c.vor[3 * n];
+        const double hum = c.hum[n], buoy = c.buoy[n];
+        auto idx = [&](int k, int j, int i) { return c.fi(ks + k, c.wrapy(js + j), c.wrapx(is + i)); };
+        auto time_fact = [&](double pref) {
+            for (int i = 0; i < 2; ++i)
+                for (int j = 0; j < 2; ++j)
+                    for (int k = 0; k < 2; ++k) tf[k][j][i] = one - std::exp(-pref * c.strain_mag[idx(k, j, i)] * dt);
+        };
+        auto full = [&](const Arr& f, double a) {
+            double s = 0.0;
+            for (int i = 0; i < 2; ++i)
+                for (int j = 0; j < 2; ++j)
+                    for (int k = 0; k < 2; ++k) s += wt[k][j][i] * tf[k][j][i] * (f[idx(k, j, i)] - a);
+            return s;
+        };
+        auto slice = [&](const Arr& f, double a, int si) {
+            double s = 0.0;
+            for (int i = 0; i < 2; ++i)
+                for (int j = 0; j < 2; ++j) s += wt[si][j][i] * tf[si][j][i] * (f[idx(si, j, i)] - a);
+            return s;
+        };
+        for (int p = 0; p < 4; ++p) {
+            trilinear(c, pts[p], is, js, ks, ww);
+            check_k(c, ks);
+            for (int i = 0; i < 2; ++i)
+                for (int j = 0; j < 2; ++j)
+                    for (int k = 0; k < 2; ++k) wt[k][j][i] = f14 * ww[k][j][i];
+            if (lv) {
+                time_fact(pv);
+                for (int l = 0; l < 3; ++l) vortend[l] = vortend[l] + full(c.vortg[l], vor[l]);
+            }
+            if (ls) {
+                time_fact(ps);
+                humtend = humtend + full(c.humg, hum);
+                dbuoytend = dbuoytend + full(c.dbuoyg, buoy);
+            }
+            if (!(lsv || lss)) continue;
+            int si;
+            if (ks == -1 || ks == c.nz - 1) si = 1;
+            else if (ks == 0 || ks == c.nz) si = 0;
+            else continue;
+            if (lsv) {
+                time_fact(pv);
+                for (int l = 0; l < 3; ++l) vortend[l] = vortend[l] + slice(c.vortg[l], vor[l], si);
+            }
+            if (lss) {
+                time_fact(ps);
+                humtend = humtend + slice(c.humg, hum, si);
+                dbuoytend = dbuoytend + slice(c.dbuoyg, buoy, si);
+            }
+        }
+        if (lv || lsv)
+            for (int l = 0; l < 3; ++l) c.vor[3 * n + l] = c.vor[3 * n + l] + vortend[l];
+        if (ls || lss) {
+            c.hum[n] = c.hum[n] + humtend;
+            c.buoy[n] = c.buoy[n] + dbuoytend;
+        }
+    }
+}
+
+// parcel_damp (:43-78)
+void parcel_damp(Ctx& c, double dt) {
+    const epic_cfg& g = c.cfg;
+    check_damping_flags(g);
+    if (!(g.damping_vorticity || g.damping_scalars || g.damping_surface_vorticity || g.damping_surface_scalars))
+        return;
+    par2grid(c, false);
+    vor2vel(c);
+    for (int ix = 0; ix < c.nx; ++ix)
+        for (int iy = 0; iy < c.ny; ++iy) {
+            long t = c.fi(0, iy, ix);
+            for (Arr* f : {&c.vortg[0], &c.vortg[1], &c.vortg[2], &c.humg, &c.dbuoyg}) {
+                (*f)[t - 1] = (*f)[t + 1];
+                (*f)[t + c.nz + 1] = (*f)[t + c.nz - 1];
+            }
+        }
+    strain_magnitude_field(c);
+    perturbation_damping(c, dt, true);
+}
+
+// ---------------------------------------------------------------------------
 // LS-RK (ls_rk.f90:88-217)
 void ensure_parcel_capacity(Ctx& c, long need) {
     if ((long)c.vol.size() >= need) return;
@@ -1170,11 +1374,14 @@ double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
     vor2vel(c);
     vorticity_tendency(c);
     double dt = get_time_step(c, t);
+    if (!c.cfg.use_fixed_dt) bndry_fluxes_time_step(c, dt);
     grid2par(c, false);
     if (pstats) parcel_diagnostics(c, pstats);
     if (fstats) field_diagnostics(c, fstats);
+    apply_bndry_fluxes(c, dt);
     for (int n = 1; n <= c.n_stages; ++n) rk_substep(c, dt, n);
     for (long n = 0; n < c.n; ++n) apply_reflective_bc(c, &c.pos[3 * n], &c.B[5 * n]);
+    parcel_damp(c, dt);
     t = t + dt;
     return dt;
 }
@@ -1674,6 +1881,7 @@ int epic_oracle_default_config(epic_cfg* g) {
     g->l_planetary_vorticity = 0;
     g->bndry_zeta_zero[0] = g->bndry_zeta_zero[1] = 0;
     g->capacity = 0; g->precision = EPIC_PRECISION_FP64; g->keep_order = 1;
+    g->damping_vorticity_prefactor = 1.0; g->damping_scalars_prefactor = 1.0;
     return EPIC_OK;
 }
 
@@ -1683,6 +1891,7 @@ int epic_oracle_create(const epic_cfg* cfg, epic_ctx** out) {
     auto* ctx = new epic_ctx();
     ctx->c.cfg = *cfg;
     try {
+        check_damping_flags(*cfg);
         update_parameters(ctx->c);
         alloc_fields(ctx->c);
         init_inversion(ctx->c);
@@ -1892,6 +2101,11 @@ int epic_oracle_apply_gradient(epic_ctx* ctx, int reuse) {
     GUARD_BEGIN apply_gradient(ctx->c, ctx->c.cfg.gradient_pref, ctx->c.cfg.max_compression, reuse != 0); GUARD_END
 }
 int epic_oracle_vol2grid(epic_ctx* ctx, int reuse) { GUARD_BEGIN vol2grid(ctx->c, reuse != 0); GUARD_END }
+int epic_oracle_parcel_damp(epic_ctx* ctx, double dt) { GUARD_BEGIN parcel_damp(ctx->c, dt); GUARD_END }
+int epic_oracle_set_bndry_fluxes(epic_ctx* ctx, const double* bflux, const double* hflux) {
+    GUARD_BEGIN set_bndry_fluxes(ctx->c, bflux, hflux); GUARD_END
+}
+int epic_oracle_apply_bndry_fluxes(epic_ctx* ctx, double dt) { GUARD_BEGIN apply_bndry_fluxes(ctx->c, dt); GUARD_END }
 int epic_oracle_parcel_diagnostics(epic_ctx* ctx, double* st) { GUARD_BEGIN parcel_diagnostics(ctx->c, st); GUARD_END }
 int epic_oracle_field_diagnostics(epic_ctx* ctx, double* st) { GUARD_BEGIN field_diagnostics(ctx->c, st); GUARD_END }
 
