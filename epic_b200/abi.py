@@ -84,7 +84,7 @@ class EpicStepInfo(C.Structure):
     ]
 
 
-INIT_THERMAL, INIT_BELTRAMI = 0, 1
+INIT_THERMAL, INIT_BELTRAMI, INIT_DEFAULT = 0, 1, 2
 
 
 class EpicInitSpec(C.Structure):
@@ -159,6 +159,7 @@ _SIGNATURES = {
     "parcel_damp": [_VP, C.c_double],
     "set_bndry_fluxes": [_VP, _D, _D],
     "apply_bndry_fluxes": [_VP, C.c_double],
+    "init_from_grids": [_VP, _D, _D, _D, _I32],
 }
 
 
@@ -390,6 +391,17 @@ class EpicContext:
 
     def parcel_damp(self, dt: float):
         self._call("parcel_damp", C.c_double(dt))
+
+    def init_from_grids(self, vortg, tbuoyg, humg=None):
+        """parcel_default + init_refine + init_parcels_from_grids +
+        set_zeta_boundary_flag; vortg (3, nx, ny, nz+3), tbuoyg and humg
+        (nx, ny, nz+3).  Returns the zeta boundary flags."""
+        v = _f64(vortg, (3,) + self.field_shape)
+        b = _f64(tbuoyg, self.field_shape)
+        h = _f64(humg, self.field_shape) if humg is not None else None
+        flags = np.zeros(2, dtype=np.int32)
+        self._call("init_from_grids", _ptr(v), _ptr(b), _ptr(h), flags.ctypes.data_as(_I32))
+        return int(flags[0]), int(flags[1])
 
     def set_bndry_fluxes(self, bflux=None, hflux=None):
         """bflux, hflux: (nx, ny) arrays (= the reference's (ny, nx) Fortran

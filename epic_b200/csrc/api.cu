@@ -386,6 +386,17 @@ int epic_gpu_init_state(epic_ctx* ctx, const epic_init_spec* spec) {
     API_END
 }
 
+int epic_gpu_init_from_grids(epic_ctx* ctx, const double* vortg, const double* tbuoyg, const double* humg,
+                             int32_t zeta_flags[2]) {
+    API_BEGIN
+    if (!vortg || !tbuoyg) throw CudaError(EPIC_ERR_ARG, "init_from_grids: null field");
+    int f[2];
+    init_from_grids(ctx->c, vortg, tbuoyg, humg, f);
+    if (zeta_flags) { zeta_flags[0] = f[0]; zeta_flags[1] = f[1]; }
+    check_device_error(ctx->c);
+    API_END
+}
+
 int epic_gpu_autotune(epic_ctx* ctx, epic_tuning* out) {
     API_BEGIN
     autotune(ctx->c, out);

@@ -196,6 +196,7 @@ void p2g_tail(Ctx& c);
 
 // init.cu
 void init_state(Ctx& c, const epic_init_spec& s);
+void init_from_grids(Ctx& c, const double* vortg, const double* tbuoyg, const double* humg, int* zeta_flags);
 
 // damping.cu
 bool damping_on(const epic_cfg& g);

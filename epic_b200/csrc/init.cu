@@ -3,7 +3,7 @@
 // the benchmark workloads).  The arithmetic follows epic_b200/initial.py
 // operation by operation (non-contracted products and sums), so positions
 // and volumes match it bit for bit; exp/sin/cos may differ in the last bit.
-#include "ctx.hpp"
+#include "parcel_ops.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -60,7 +60,9 @@ __global__ void k_init_state(InitArgs A, PView pv) {
             pos[c] = __dadd_rn(corner, __dmul_rn(__dmul_rn(P.dx[c], (double)sub[c] - 0.5), A.im));
         }
         double vor[3] = {0.0, 0.0, 0.0}, buoy = 0.0;
-        if (A.kind == EPIC_INIT_THERMAL) {
+        if (A.kind == EPIC_INIT_DEFAULT) {
+            // parcel_default: regular positions, zero attributes
+        } else if (A.kind == EPIC_INIT_THERMAL) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 double u = uniform01(A.seed, (unsigned long long)p, c);
@@ -102,13 +104,19 @@ __global__ void k_init_state(InitArgs A, PView pv) {
     }
 }
 
+static void launch_init(Ctx& c, const epic_init_spec& s, int npd);
+
 void init_state(Ctx& c, const epic_init_spec& s) {
-    const Params& P = c.P;
     int npd = (int)std::lround(std::cbrt((double)s.n_per_cell));
     if (npd < 1 || npd * npd * npd != s.n_per_cell)
         throw CudaError(EPIC_ERR_CONFIG, "init_state: n_per_cell must be a cube");
     if (s.kind != EPIC_INIT_THERMAL && s.kind != EPIC_INIT_BELTRAMI)
         throw CudaError(EPIC_ERR_CONFIG, "init_state: unknown kind");
+    launch_init(c, s, npd);
+}
+
+static void launch_init(Ctx& c, const epic_init_spec& s, int npd) {
+    const Params& P = c.P;
     if (s.kind == EPIC_INIT_THERMAL && (s.n_bubbles < 0 || s.n_bubbles > 4))
         throw CudaError(EPIC_ERR_CONFIG, "init_state: 0 .. 4 bubbles");
     long long n = (long long)P.nx * P.ny * P.nz * s.n_per_cell;
@@ -142,6 +150,91 @@ void init_state(Ctx& c, const epic_init_spec& s) {
     k_init_state<<<grid, 256, 0, c.stream>>>(A, c.pv);
     CKL();
     c.has_parcels = true;
+}
+
+// ---------------------------------------------------------------------------
+// The start of a run from a field file (utils.f90:223-234).
+
+// lam = sqrt(a^2 / c^2) of parcel 0 (get_eigenvalues, parcel_ellipsoid.f90:288-305)
+__global__ void k_first_lambda(PView pv, double* out, unsigned* err) {
+    double b[5], U[9], D[3];
+    load_B(pv, 0, b);
+    full_matrix<ExactOps>(b, get_B33<ExactOps>(b, pv.get(A_VOL, 0), err), U);
+    sz_eigenvalues<ExactOps>(U, D);
+    *out = sqrt(D[0] / D[2]);
+}
+
+// init_parcels_from_grids (parcel_init.f90:170-203): each parcel adds the
+// trilinear interpolation of the gridded vorticity, buoyancy and humidity
+// at its centre (x/y halo = periodic wrap).
+__global__ void k_from_grids(Params P, PView pv, long long n, const double* vx, const double* vy, const double* vz,
+                             const double* b, const double* h, unsigned* err) {
+    PLOOP(n) {
+        const double pos[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
+        const Tri t = trilinear(P, pos);
+        long long a[2][2];
+        if (!corners(P, t, a)) { set_err(err, ERRB_ZRANGE); continue; }
+        pv.set(A_VX, i, pv.get(A_VX, i) + csum(vx, t, a));
+        pv.set(A_VY, i, pv.get(A_VY, i) + csum(vy, t, a));
+        pv.set(A_VZ, i, pv.get(A_VZ, i) + csum(vz, t, a));
+        pv.set(A_BUOY, i, pv.get(A_BUOY, i) + csum(b, t, a));
+        pv.set(A_HUM, i, pv.get(A_HUM, i) + csum(h, t, a));
+    }
+}
+
+void init_from_grids(Ctx& c, const double* vortg, const double* tbuoyg, const double* humg, int* zeta_flags) {
+    const Params& P = c.P;
+    // parcel_default + init_regular_positions (parcel_init.f90:31-152)
+    const int npc = c.cfg.n_per_cell;
+    const int npd = (int)std::pow((double)npc, 1.0 / 3.0);
+    if (npd < 1 || npd * npd * npd != npc) throw CudaError(EPIC_ERR_CONFIG, "Number of parcels per cell not a cubic.");
+    epic_init_spec s{};
+    s.kind = EPIC_INIT_DEFAULT;
+    s.n_per_cell = npc;
+    launch_init(c, s, npd);
+    // init_refine (:156-166): split until parcel 1 is less elongated than lambda_max
+    const double* d = P.dx;
+    double lam = std::max({d[0] / d[1], d[1] / d[0], d[0] / d[2], d[2] / d[0], d[1] / d[2], d[2] / d[1]});
+    while (lam >= c.cfg.lambda_max) {
+        parcel_split(c);
+        k_first_lambda<<<1, 1, 0, c.stream>>>(c.pv, c.partials, &c.dsc->err);
+        CKL();
+        CK(cudaMemcpyAsync(&lam, c.partials, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+    }
+    c.n_parcel_splits = c.n_parcel_merges = c.n_big_close = 0;
+    // the gridded fields into vortg, tbuoyg, humg (overwritten by the next par2grid)
+    const size_t fb = sizeof(double) * (size_t)P.fsz;
+    CK(cudaMemcpyAsync(c.vortg(0), vortg, 3 * fb, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.tbuoyg(), tbuoyg, fb, cudaMemcpyHostToDevice, c.stream));
+    if (humg) CK(cudaMemcpyAsync(c.humg(), humg, fb, cudaMemcpyHostToDevice, c.stream));
+    else CK(cudaMemsetAsync(c.humg(), 0, fb, c.stream));
+    k_from_grids<<<pgrid(c.n), PB, 0, c.stream>>>(P, c.pv, c.n, c.vortg(0), c.vortg(1), c.vortg(2), c.tbuoyg(),
+                                                  c.humg(), &c.dsc->err);
+    CKL();
+    // set_zeta_boundary_flag (parameters.f90:168-217) on the host copy of zeta,
+    // summed in the reference's column-major order
+    const double* zeta = vortg + 2 * P.fsz;
+    auto z = [&](int iz, int iy, int ix) { return zeta[fidx(P, iz, iy, ix)]; };
+    double val[3] = {0.0, 0.0, 0.0};
+    for (int ix = 0; ix < P.nx; ++ix)
+        for (int iy = 0; iy < P.ny; ++iy)
+            for (int iz = 1; iz <= P.nz - 1; ++iz) val[0] += z(iz, iy, ix) * z(iz, iy, ix);
+    for (int ix = 0; ix < P.nx; ++ix)
+        for (int iy = 0; iy < P.ny; ++iy) {
+            val[1] += z(0, iy, ix) * z(0, iy, ix);
+            val[2] += z(P.nz, iy, ix) * z(P.nz, iy, ix);
+        }
+    const double nhcelli = 1.0 / (double)((long long)P.nx * P.ny);
+    const double rms_interior = std::sqrt(val[0] * nhcelli / (double)(P.nz - 1));
+    const double thres = (double)1.0e-3f * rms_interior + 2.220446049250313e-16;   // zeta_tol, epsilon
+    for (int b = 0; b < 2; ++b) {
+        const bool z0 = std::sqrt(val[1 + b] * nhcelli) < thres;
+        c.cfg.bndry_zeta_zero[b] = z0 ? 1 : 0;
+        c.P.zeta_zero[b] = z0 ? 1 : 0;
+        if (zeta_flags) zeta_flags[b] = z0 ? 1 : 0;
+    }
+    CK(cudaStreamSynchronize(c.stream));
 }
 
 }  // namespace epic

@@ -91,6 +91,16 @@ module epic_gpu_iface
             type(epic_step_info) :: info
         end function
 
+        ! setup_fields_and_parcels from a field file: parcel_default,
+        ! init_parcels_from_grids, set_zeta_boundary_flag (vortg(:,:,:,1:3))
+        integer(c_int) function epic_gpu_init_from_grids(ctx, vortg, tbuoyg, humg, zeta_flags) &
+                bind(C, name="epic_gpu_init_from_grids")
+            import :: c_int, c_int32_t, c_ptr, c_double
+            type(c_ptr), value          :: ctx
+            real(c_double), intent(in)  :: vortg(*), tbuoyg(*), humg(*)
+            integer(c_int32_t)          :: zeta_flags(2)
+        end function
+
         ! read_bndry_fluxes: binc, hinc as read from the flux file (y, x)
         integer(c_int) function epic_gpu_set_bndry_fluxes(ctx, bflux, hflux) &
                 bind(C, name="epic_gpu_set_bndry_fluxes")

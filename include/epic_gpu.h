@@ -157,6 +157,7 @@ int epic_gpu_num_parcels(epic_ctx* ctx, int64_t* n);
  * Replaces set_parcels + the host generator; call init_correction after. */
 #define EPIC_INIT_THERMAL  0
 #define EPIC_INIT_BELTRAMI 1
+#define EPIC_INIT_DEFAULT  2   /* parcel_default alone (epic_gpu_init_from_grids) */
 typedef struct epic_init_spec {
     int32_t  kind;            /* EPIC_INIT_*                                   */
     int32_t  n_per_cell;      /* a cube: 1, 8, 27, ...                         */
@@ -166,6 +167,19 @@ typedef struct epic_init_spec {
     double   bubble[4][4];    /* thermal: centre x, y, z and amplitude         */
 } epic_init_spec;
 int epic_gpu_init_state(epic_ctx* ctx, const epic_init_spec* spec);
+
+/* The start of a run from a field file (utils.f90:223-234): parcel_default
+ * with init_regular_positions and init_refine (parcel_init.f90:31-166; cfg
+ * n_per_cell parcels per cell, split until lambda < lambda_max),
+ * init_parcels_from_grids (:170-203: every parcel takes the trilinear
+ * interpolation of the fields at its centre) and set_zeta_boundary_flag
+ * (parameters.f90:168-217), whose result replaces the configuration's
+ * bndry_zeta_zero and is returned in zeta_flags (may be NULL).  vortg holds
+ * the x, y, z components one after the other, each a field in the layout of
+ * epic_gpu_set_field like tbuoyg and humg (NULL: zero humidity); rows 0..nz
+ * are read.  Call init_correction after. */
+int epic_gpu_init_from_grids(epic_ctx* ctx, const double* vortg, const double* tbuoyg, const double* humg,
+                             int32_t zeta_flags[2]);
 
 /* Autotuner (no counterpart in the reference): times the candidate launch
  * shapes of this context on its own parcels and grid -- the lane grouping of

@@ -2000,6 +2000,92 @@ int epic_oracle_init_state(epic_ctx* ctx, const epic_init_spec* s) {
     return epic_oracle_set_parcels(ctx, n, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(), hum.data());
 }
 
+// The start of a run from a field file (utils.f90:223-234): parcel_default
+// with init_regular_positions and init_refine (parcel_init.f90:31-166),
+// init_parcels_from_grids (:170-203) and set_zeta_boundary_flag
+// (parameters.f90:168-217).  Fields as in epic_oracle_set_field; rows 0..nz.
+int epic_oracle_init_from_grids(epic_ctx* ctx, const double* vortg, const double* tbuoyg, const double* humg,
+                                int32_t* zeta_flags) {
+    if (!ctx || !vortg || !tbuoyg) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    GUARD_BEGIN
+    const int npc = c.cfg.n_per_cell;
+    const int npd = (int)std::pow((double)npc, f13);
+    if (npd * npd * npd != npc) throw OracleError(EPIC_ERR_CONFIG, "Number of parcels per cell not a cubic.");
+    const long n = (long)npc * c.nx * c.ny * c.nz;
+    std::vector<double> pos(3 * n), zero3(3 * n, 0.0), B(5 * n, 0.0), vol(n), zero1(n, 0.0);
+    const double im = one / (double)npd;
+    long l = 0;
+    for (int iz = 0; iz < c.nz; ++iz)
+        for (int iy = 0; iy < c.ny; ++iy)
+            for (int ix = 0; ix < c.nx; ++ix) {
+                const double corner[3] = {c.lower[0] + (double)ix * c.dx[0], c.lower[1] + (double)iy * c.dx[1],
+                                          c.lower[2] + (double)iz * c.dx[2]};
+                for (int k = 1; k <= npd; ++k)
+                    for (int j = 1; j <= npd; ++j)
+                        for (int i = 1; i <= npd; ++i) {
+                            pos[3 * l] = corner[0] + c.dx[0] * ((double)i - f12) * im;
+                            pos[3 * l + 1] = corner[1] + c.dx[1] * ((double)j - f12) * im;
+                            pos[3 * l + 2] = corner[2] + c.dx[2] * ((double)k - f12) * im;
+                            ++l;
+                        }
+            }
+    const double* d = c.dx;
+    double lam = std::max({d[0] / d[1], d[1] / d[0], d[0] / d[2], d[2] / d[0], d[1] / d[2], d[2] / d[1]});
+    for (long q = 0; q < n; ++q) {
+        vol[q] = c.vcell / (double)npc;
+        const double l23 = std::pow(lam * get_abc(vol[q]), f23);
+        B[5 * q] = l23;
+        B[5 * q + 3] = l23;
+    }
+    int rc = epic_oracle_set_parcels(ctx, n, pos.data(), zero3.data(), B.data(), vol.data(), zero1.data(),
+                                     zero1.data());
+    if (rc != EPIC_OK) return rc;
+    // init_refine: split until parcel 1 is less elongated than lambda_max
+    while (lam >= c.cfg.lambda_max) {
+        parcel_split(c);
+        double D[3];
+        get_eigenvalues(c, 0, D);
+        lam = std::sqrt(D[0] / D[2]);
+    }
+    c.n_parcel_splits = c.n_parcel_merges = c.n_big_close = 0;
+    // init_parcels_from_grids: the x/y halo is the periodic wrap
+    Arr vg[3], bg(tbuoyg, tbuoyg + c.fsz), hg(c.fsz, 0.0);
+    for (int k = 0; k < 3; ++k) vg[k].assign(vortg + k * c.fsz, vortg + (k + 1) * c.fsz);
+    if (humg) hg.assign(humg, humg + c.fsz);
+    for (long q = 0; q < c.n; ++q) {
+        int is, js, ks;
+        double ww[2][2][2];
+        trilinear(c, &c.pos[3 * q], is, js, ks, ww);
+        check_k(c, ks);
+        for (int k = 0; k < 3; ++k) c.vor[3 * q + k] = c.vor[3 * q + k] + corner_sum(c, vg[k], is, js, ks, ww);
+        c.buoy[q] = c.buoy[q] + corner_sum(c, bg, is, js, ks, ww);
+        c.hum[q] = c.hum[q] + corner_sum(c, hg, is, js, ks, ww);
+    }
+    // set_zeta_boundary_flag on the gridded vertical vorticity
+    const Arr& zeta = vg[2];
+    double val[3] = {0.0, 0.0, 0.0};
+    for (int ix = 0; ix < c.nx; ++ix)
+        for (int iy = 0; iy < c.ny; ++iy)
+            for (int iz = 1; iz <= c.nz - 1; ++iz) val[0] += zeta[c.fi(iz, iy, ix)] * zeta[c.fi(iz, iy, ix)];
+    for (int ix = 0; ix < c.nx; ++ix)
+        for (int iy = 0; iy < c.ny; ++iy) {
+            val[1] += zeta[c.fi(0, iy, ix)] * zeta[c.fi(0, iy, ix)];
+            val[2] += zeta[c.fi(c.nz, iy, ix)] * zeta[c.fi(c.nz, iy, ix)];
+        }
+    const double nhcelli = one / (double)((long)c.nx * c.ny);
+    const double rms_interior = std::sqrt(val[0] * nhcelli / (double)(c.nz - 1));
+    const double zeta_tol = (double)1.0e-3f;
+    const double thres = zeta_tol * rms_interior + 2.220446049250313e-16;
+    for (int b = 0; b < 2; ++b) {
+        const bool z0 = std::sqrt(val[1 + b] * nhcelli) < thres;
+        c.bndry_zeta_zero[b] = z0;
+        c.cfg.bndry_zeta_zero[b] = z0 ? 1 : 0;
+        if (zeta_flags) zeta_flags[b] = z0 ? 1 : 0;
+    }
+    GUARD_END
+}
+
 int epic_oracle_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, double* vor, double* B,
                             double* vol, double* buoy, double* hum) {
     if (!ctx || !n) return EPIC_ERR_ARG;
