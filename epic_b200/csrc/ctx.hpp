@@ -52,6 +52,11 @@ struct Tables {
     // z-transform matrices, (nz+1) x (nz+1) row-major: DST-I (rows/cols 1..nz-1), DCT-I
     double* mdst = nullptr, *mdct = nullptr;
     float* mdst32 = nullptr, *mdct32 = nullptr;   // FP32 copies (mixed form)
+    // quarter tables of the symmetric z transforms (even nz): rows k < nz/2
+    // grouped by parity, columns j = j0 .. nz/2; qld entries per j
+    double* qdst = nullptr, *qdct = nullptr;
+    float* qdst32 = nullptr, *qdct32 = nullptr;
+    int qld_dst = 0, qld_dct = 0;
 };
 
 // Device scalars of one step (kept on the device between kernels).
@@ -102,6 +107,9 @@ struct Ctx {
     // par2grid, fused stage)
     int scatter_lg[3] = {1, 1, 0};
     bool fused_scatter = false;   // stage kernel runs the next par2grid itself (else a separate scatter kernel)
+    bool vectors_kernel = true;   // support vectors by their own kernel before a scatter that recomputes them
+    int stage_recwin = 1;         // split-form stage kernel gathers from records staged in shared memory
+    bool p2g_counted = true;      // the last par2grid scatter counted parcels per cell (nparg, nsparg)
     Tables T;
     StepScalars* dsc = nullptr;     // device
     StepScalars* hsc = nullptr;     // pinned host mirror

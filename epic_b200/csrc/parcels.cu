@@ -93,10 +93,15 @@ void p2g_tail(Ctx& c) {
     F.f[0] = c.vortg(0); F.f[1] = c.vortg(1); F.f[2] = c.vortg(2);
     F.f[3] = c.dbuoyg(); F.f[4] = c.humg(); F.f[5] = c.tbuoyg(); F.f[6] = c.volg();
     long long ncol = (long long)P.nx * P.ny;
-    k_p2g_fold<<<(int)((ncol + 255) / 256), 256, 0, c.stream>>>(P, F, 7, c.nparg, c.nsparg, &c.dsc->count);
+    // the parcel-count check (parcel_interpl.f90:245-250) where the scatter counted
+    const bool counted = c.p2g_counted;
+    k_p2g_fold<<<(int)((ncol + 255) / 256), 256, 0, c.stream>>>(P, F, 7, counted ? c.nparg : nullptr,
+                                                                  c.nsparg, &c.dsc->count);
     CKL();
-    k_count_check<<<1, 1, 0, c.stream>>>(c.dsc, c.n);
-    CKL();
+    if (counted) {
+        k_count_check<<<1, 1, 0, c.stream>>>(c.dsc, c.n);
+        CKL();
+    }
     k_p2g_divide<<<pgrid((long long)P.nx * P.ny * (P.nz + 1)), PB, 0, c.stream>>>(P, F);
     CKL();
     k_p2g_halo<<<(int)((ncol + 255) / 256), 256, 0, c.stream>>>(P, F);

@@ -589,11 +589,11 @@ void fft_xy(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
 
 // ---------------------------------------------------------------------------
 // Vertical (column) kernels.  A CTA holds 32 columns (kx, ky) of nz+1 values
-// in shared memory as x[j * 33 + col]; matrix-vector products with the DST-I /
-// DCT-I matrices read each matrix entry once per warp (broadcast) and keep
-// all 32 lanes busy on different columns.
+// in shared memory as x[j * 34 + col] (rows 16-byte aligned); matrix-vector
+// products with the DST-I / DCT-I matrices keep all 32 lanes busy on
+// different columns.
 constexpr int CT = 32;
-constexpr int CP = 33;
+constexpr int CP = 34;
 
 struct ColArgs {
     const double* tab[8];
@@ -601,11 +601,144 @@ struct ColArgs {
     void* out[4];
     const void* mdst;       // (nz+1)^2 matrices in T
     const void* mdct;
+    const void* qdst;       // quarter tables in T (even nz), null: full matrices
+    const void* qdct;
+    int qld_dst, qld_dct;
     int ncol;      // nx * ny
     int nz;
     int nzh;
     double dzi, hdzi;
+    double sn;     // sqrt(2 / nz)
 };
+
+// Symmetric z transforms (even n = nz, h = n / 2).  The DST-I matrix
+// M[k][j] = sn sin(pi k j / n) (rows, columns 1 .. n-1) and the DCT-I matrix
+// C[k][j] = sn w_j cos(pi k j / n) (0 .. n, w_0 = w_n = 1/2) satisfy
+//   M[k][n-j] = (-1)^(k+1) M[k][j],  M[n-k][j] = (-1)^(j+1) M[k][j],
+//   C[k][n-j] = (-1)^k C[k][j],      C[n-k][j] = (-1)^j C[k][j].
+// So with S[j] = x[j] + x[n-j], D[j] = x[j] - x[n-j] (j < h), for k < h
+//   Y[k]   = E + O + mid,   E, O = sums over even, odd j < h of Q[k][j] V[j],
+//   Y[n-k] = O - E + (-1)^(h+1) mid (DST),  E - O + (-1)^h mid (DCT),
+// mid = Q[k][h] x[h] and V = S for odd k (DST) / even k (DCT), else D; row h
+// is a signed sum of every other x.  A quarter of the multiply-adds of the
+// full matrix, from a table Q of (h - j0 + 1) x qld values: rows of the
+// S-parity first (padded to 8), then the others (padded to 8).
+// KIND 0: DST over rows 1 .. n-1; KIND 1: DCT over rows 0 .. n.  The pairs
+// of x are formed in place (x is consumed; rows 0 and n of a DST input and
+// row h are kept); ADD accumulates into y.  All threads of the CTA call it.
+template <int KIND>
+struct ZT {
+    static constexpr int j0 = KIND == 0 ? 1 : 0;
+    // rows of the two parity blocks below h and their k
+    static EPIC_HD int nA(int h) { return KIND == 0 ? h / 2 : (h + 1) / 2; }
+    static EPIC_HD int nB(int h) { return KIND == 0 ? (h - 1) / 2 : h / 2; }
+    static EPIC_HD int kA(int i) { return KIND == 0 ? 2 * i + 1 : 2 * i; }
+    static EPIC_HD int kB(int i) { return KIND == 0 ? 2 * i + 2 : 2 * i + 1; }
+    static EPIC_HD int qld(int h) { return 8 * ((nA(h) + 7) / 8 + (nB(h) + 7) / 8); }
+};
+
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+template <int KIND, bool ADD, class T>
+EPIC_DEV void col_ztransform(const T* __restrict__ Q, int qld, T* xs, T* ys, int n, T sn) {
+    using Z = ZT<KIND>;
+    using V2 = typename Vec2<T>::type;
+    constexpr int j0 = Z::j0;
+    const int h = n / 2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    // row h: a signed sum of every other x (one thread per column)
+    T yh = T(0);
+    if (tid < CT) {
+        if (KIND == 0) {
+            for (int j = 1; j < n; j += 2) yh += ((j >> 1) & 1) ? -xs[j * CP + tid] : xs[j * CP + tid];
+        } else {
+            yh = T(0.5) * (xs[tid] + (((n >> 1) & 1) ? -xs[n * CP + tid] : xs[n * CP + tid]));
+            for (int j = 2; j < n; j += 2) yh += ((j >> 1) & 1) ? -xs[j * CP + tid] : xs[j * CP + tid];
+        }
+        yh *= sn;
+    }
+    __syncthreads();
+    // pairs in place: S[j] at row j, D[j] at row n - j
+    const int np = h - j0;
+    for (int idx = tid; idx < CT * np; idx += blockDim.x) {
+        const int col = idx & (CT - 1), j = j0 + (idx >> 5);
+        const T a = xs[j * CP + col], b = xs[(n - j) * CP + col];
+        xs[j * CP + col] = a + b;
+        xs[(n - j) * CP + col] = a - b;
+    }
+    __syncthreads();
+    if (tid < CT) {
+        T* o = ys + h * CP + tid;
+        *o = ADD ? *o + yh : yh;
+    }
+    // octets of rows: 8 rows x 32 columns per warp; a lane owns 2 rows and
+    // the columns {2c, 2c+1, 16+2c, 17+2c}, so that each 2-wide load of the
+    // 8 lanes of a row group covers 128 contiguous bytes
+    const int nA = Z::nA(h), nB = Z::nB(h), oA = (nA + 7) / 8, oB = (nB + 7) / 8;
+    const int rl = lane >> 3, cl = lane & 7;
+    const int c0 = 2 * cl, c1 = 16 + 2 * cl;
+    const T sE = KIND == 0 ? T(-1) : T(1), sO = -sE;
+    const T sM = ((h & 1) ^ (KIND == 0 ? 1 : 0)) ? T(-1) : T(1);   // (-1)^(h+1) DST, (-1)^h DCT
+    for (int oct = warp; oct < oA + oB; oct += nwarp) {
+        const bool blockA = oct < oA;
+        const int ib = 8 * (blockA ? oct : oct - oA) + 2 * rl;          // row in its block
+        const int iq = blockA ? ib : 8 * oA + ib;                      // row in Q
+        const int nrows = blockA ? nA : nB;
+        // V rows: S at j (block A), D at n - j (block B)
+        const T* v = xs + (blockA ? j0 : n - j0) * CP;
+        const int vstep = blockA ? CP : -CP;
+        const T* q = Q + iq;
+        T e[2][4], o[2][4];
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) { e[r][c] = T(0); o[r][c] = T(0); }
+        auto step = [&](T (&acc)[2][4]) {
+            const V2 qq = *reinterpret_cast<const V2*>(q);
+            const V2 va = *reinterpret_cast<const V2*>(v + c0);
+            const V2 vb = *reinterpret_cast<const V2*>(v + c1);
+            const T vv[4] = {va.x, va.y, vb.x, vb.y};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                acc[0][c] = fma(qq.x, vv[c], acc[0][c]);
+                acc[1][c] = fma(qq.y, vv[c], acc[1][c]);
+            }
+            q += qld;
+            v += vstep;
+        };
+        int j = j0;
+#pragma unroll 2
+        for (; j + 1 < h; j += 2) {
+            if (j0 & 1) { step(o); step(e); }
+            else { step(e); step(o); }
+        }
+        if (j < h) {
+            if (j0 & 1) step(o);
+            else step(e);
+        }
+        // q now points at row j = h: the coefficients of x[h]
+        const V2 qm = *reinterpret_cast<const V2*>(Q + (h - j0) * qld + iq);
+        const T cm[2] = {qm.x, qm.y};
+        const int cols[4] = {c0, c0 + 1, c1, c1 + 1};
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            if (ib + r >= nrows) continue;
+            const int k = blockA ? Z::kA(ib + r) : Z::kB(ib + r);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const T mid = cm[r] * xs[h * CP + cols[c]];
+                const T y1 = e[r][c] + o[r][c] + mid;
+                const T y2 = sE * e[r][c] + sO * o[r][c] + sM * mid;
+                T* p1 = ys + k * CP + cols[c];
+                T* p2 = ys + (n - k) * CP + cols[c];
+                *p1 = ADD ? *p1 + y1 : y1;
+                *p2 = ADD ? *p2 + y2 : y2;
+            }
+        }
+    }
+}
 
 template <class T>
 EPIC_DEV void col_load(const T* f, T* xs, int c0, const ColArgs& A) {
@@ -699,14 +832,15 @@ __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
         for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) xs[idx % CT + (idx / CT) * CP] = ys[idx % CT + (idx / CT) * CP];
         __syncthreads();
     }
-    // subtract harmonic part
+    // subtract harmonic part (lanes along z: the per-column tables are read coalesced)
     for (int idx = threadIdx.x; idx < CT * (nz - 1); idx += blockDim.x) {
-        int col = idx % CT, j = 1 + idx / CT;
+        int col = idx / (nz - 1), j = 1 + idx - col * (nz - 1);
         int c = min(c0 + col, A.ncol - 1);
         xs[j * CP + col] = xs[j * CP + col] - (xs[col] * (T)tabv(phim, c, j, A) + xs[nz * CP + col] * (T)tabv(phip, c, j, A));
     }
     __syncthreads();
-    col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
+    if (A.qdst) col_ztransform<0, false, T>(static_cast<const T*>(A.qdst), A.qld_dst, xs, ys, nz, (T)A.sn);
+    else col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
     for (int col = threadIdx.x; col < CT; col += blockDim.x) {
         ys[col] = xs[col];
         ys[nz * CP + col] = xs[nz * CP + col];
@@ -714,7 +848,7 @@ __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
     __syncthreads();
     if (mode & 1) {
         for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-            int col = idx % CT, j = idx / CT;
+            int col = idx / nzp, j = idx - col * nzp;
             int c = min(c0 + col, A.ncol - 1);
             ys[j * CP + col] = (T)tabv(filt, c, j, A) * ys[j * CP + col];
         }
@@ -736,10 +870,11 @@ __global__ void __launch_bounds__(256) k_col_combine(ColArgs A) {
     const double* phip = A.tab[1];
     col_load(static_cast<const T*>(A.in[blockIdx.y]), xs, c0, A);
     __syncthreads();
-    col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
+    if (A.qdst) col_ztransform<0, false, T>(static_cast<const T*>(A.qdst), A.qld_dst, xs, ys, nz, (T)A.sn);
+    else col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx % CT, j = idx / CT;
+        int col = idx / nzp, j = idx - col * nzp;
         int c = min(c0 + col, A.ncol - 1);
         T v;
         if (j == 0) v = xs[col];
@@ -772,7 +907,7 @@ __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
     col_load(static_cast<const T*>(A.in[0]), ds, c0, A);
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx % CT, j = idx / CT;
+        int col = idx / nzp, j = idx - col * nzp;
         int c = min(c0 + col, A.ncol - 1);
         T d0 = ds[col], dn = ds[nz * CP + col];
         if (j >= 1 && j <= nz - 1) bs[j * CP + col] = d0 * (T)tabv(thetam, c, j, A) + dn * (T)tabv(thetap, c, j, A);
@@ -780,7 +915,7 @@ __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx % CT, j = idx / CT;
+        int col = idx / nzp, j = idx - col * nzp;
         int c = min(c0 + col, A.ncol - 1);
         if (j >= 1 && j <= nz - 1) {
             T g = (T)tabv(green, c, j, A) * ds[j * CP + col];
@@ -792,9 +927,11 @@ __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
     }
     __syncthreads();
     // es += DCT(as); then as(1:nz-1) = DST(ds(1:nz-1))
-    col_matvec_t<R, true, T>(static_cast<const T*>(A.mdct), 0, nz, as, es, nz);
+    if (A.qdct) col_ztransform<1, true, T>(static_cast<const T*>(A.qdct), A.qld_dct, as, es, nz, (T)A.sn);
+    else col_matvec_t<R, true, T>(static_cast<const T*>(A.mdct), 0, nz, as, es, nz);
     __syncthreads();
-    col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, ds, as, nz);
+    if (A.qdst) col_ztransform<0, false, T>(static_cast<const T*>(A.qdst), A.qld_dst, ds, as, nz, (T)A.sn);
+    else col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, ds, as, nz);
     __syncthreads();
     for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
         int col = idx % CT, j = idx / CT;
@@ -1202,8 +1339,14 @@ template <class T>
 static ColArgs col_args(Ctx& c) {
     ColArgs A;
     std::memset(&A, 0, sizeof(A));
-    if (std::is_same<T, float>::value) { A.mdst = c.T.mdst32; A.mdct = c.T.mdct32; }
-    else { A.mdst = c.T.mdst; A.mdct = c.T.mdct; }
+    if (std::is_same<T, float>::value) {
+        A.mdst = c.T.mdst32; A.mdct = c.T.mdct32; A.qdst = c.T.qdst32; A.qdct = c.T.qdct32;
+    } else {
+        A.mdst = c.T.mdst; A.mdct = c.T.mdct; A.qdst = c.T.qdst; A.qdct = c.T.qdct;
+    }
+    A.qld_dst = c.T.qld_dst;
+    A.qld_dct = c.T.qld_dct;
+    A.sn = std::sqrt(2.0 / (double)c.P.nz);
     A.ncol = c.P.nx * c.P.ny;
     A.nz = c.P.nz;
     A.nzh = c.P.nzh;
@@ -1633,6 +1776,26 @@ void spectral_init(Ctx& c) {
     CK(cudaMalloc(&c.T.mdct32, sizeof(float) * mdct32.size()));
     CK(cudaMemcpyAsync(c.T.mdst32, mdst32.data(), sizeof(float) * mdst32.size(), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c.T.mdct32, mdct32.data(), sizeof(float) * mdct32.size(), cudaMemcpyHostToDevice, st));
+    // quarter tables of the symmetric transforms (col_ztransform), even nz
+    if (nz % 2 == 0 && nz >= 4) {
+        auto quarter = [&](auto Z, const std::vector<double>& m, double** qd, float** qf, int* qld) {
+            using ZK = decltype(Z);
+            const int h = nz / 2, j0 = ZK::j0, nA = ZK::nA(h), nB = ZK::nB(h), offB = 8 * ((nA + 7) / 8);
+            *qld = ZK::qld(h);
+            std::vector<double> q((size_t)(h - j0 + 1) * *qld, 0.0);
+            for (int j = j0; j <= h; ++j) {
+                for (int i = 0; i < nA; ++i) q[(size_t)(j - j0) * *qld + i] = m[(size_t)ZK::kA(i) * (nz + 1) + j];
+                for (int i = 0; i < nB; ++i) q[(size_t)(j - j0) * *qld + offB + i] = m[(size_t)ZK::kB(i) * (nz + 1) + j];
+            }
+            up(qd, q);
+            std::vector<float> q32(q.begin(), q.end());
+            CK(cudaMalloc(qf, sizeof(float) * q32.size()));
+            CK(cudaMemcpyAsync(*qf, q32.data(), sizeof(float) * q32.size(), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        };
+        quarter(ZT<0>{}, mdst, &c.T.qdst, &c.T.qdst32, &c.T.qld_dst);
+        quarter(ZT<1>{}, mdct, &c.T.qdct, &c.T.qdct32, &c.T.qld_dct);
+    }
     CK(cudaStreamSynchronize(st));
 }
 
@@ -1647,6 +1810,14 @@ void spectral_free(Ctx& c) {
     if (c.T.mdst32) cudaFree(c.T.mdst32);
     if (c.T.mdct32) cudaFree(c.T.mdct32);
     c.T.mdst32 = c.T.mdct32 = nullptr;
+    for (double** p : {&c.T.qdst, &c.T.qdct}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    for (float** p : {&c.T.qdst32, &c.T.qdct32}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
     if (c.px.tw) cudaFree(c.px.tw);
     if (c.py.tw) cudaFree(c.py.tw);
     c.px.tw = c.py.tw = nullptr;

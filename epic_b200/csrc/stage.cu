@@ -212,10 +212,21 @@ EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long 
 
 struct Fields7 {
     double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg
-    int mask;       // bit f set: field f is accumulated
+    int mask;       // bit f set: field f is accumulated (NF = 7)
 };
 constexpr int ALL_FIELDS = 0x7f;
 constexpr int DRY_FIELDS = 0x67;   // without dbuoyg (3) and humg (4)
+
+// Field set of a scatter kernel: NF = 7 (all, masked by Fields7.mask), 5 (the
+// dry set: vorticity, tbuoyg, volg) or 1 (one field, vol2grid).
+template <int NF>
+EPIC_HD constexpr int field_slot(int f) {
+    return NF == 5 ? (f < 3 ? f : f + 2) : f;
+}
+template <int NF>
+EPIC_DEV bool field_on(const Fields7& F, int f) {
+    return NF != 7 || ((F.mask >> f) & 1);
+}
 
 // Arithmetic of the two forms: R is the type of the FP32-able attributes,
 // of the gathered values and of the window sums (double: plain, float: mixed).
@@ -342,12 +353,12 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
                         const double wt = (double)(float)t.w[kk][jj][ii];
 #pragma unroll
                         for (int f = 0; f < NF; ++f)
-                            if ((F.mask >> f) & 1) fx2_add(acc + f * 2 * WCAP, w, wt, vs[f]);
+                            if (field_on<NF>(F, f)) fx2_add(acc + f * 2 * WCAP, w, wt, vs[f]);
                     } else {
                         const double wt = t.w[kk][jj][ii];
 #pragma unroll
                         for (int f = 0; f < NF; ++f)
-                            if ((F.mask >> f) & 1) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
+                            if (field_on<NF>(F, f)) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
                     }
                 }
     } else {
@@ -363,7 +374,7 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
                     const R wt = (R)t.w[kk][jj][ii];
 #pragma unroll
                     for (int f = 0; f < NF; ++f)
-                        if ((F.mask >> f) & 1) atomicAdd(&F.f[f][g], (double)(wt * vp[f]));
+                        if (field_on<NF>(F, f)) atomicAdd(&F.f[field_slot<NF>(f)][g], (double)(wt * vp[f]));
                 }
     }
 }
@@ -389,11 +400,11 @@ EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF
         long long g = fidx(P, W.gz0 + z, wrapi(W.gy0 + y, P.ny), wrapi(W.gx0 + x, P.nx));
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            if (!((F.mask >> f) & 1)) continue;
+            if (!field_on<NF>(F, f)) continue;
             double v;
             if constexpr (Form<R>::mixed) v = fx2_value(acc + f * 2 * WCAP, w, ws->inv[f]);
             else v = fx_value(acc + f * NLIMB * WCAP, w, ws->inv[f]);
-            if (v != 0.0) atomicAdd(&F.f[f][g], v);
+            if (v != 0.0) atomicAdd(&F.f[field_slot<NF>(f)][g], v);
         }
     }
 }
@@ -416,11 +427,14 @@ EPIC_DEV void p2g_values(const Params& P, const R* vor, double z, double vol, R 
 
 template <int NF, class R>
 EPIC_DEV void load_values(const Params& P, const PView& pv, long long i, double z, R* vp) {
-    if (NF == 7) {
-        R vor[3] = {aR<R>(pv, A_VX, i), aR<R>(pv, A_VY, i), aR<R>(pv, A_VZ, i)};
-        p2g_values<R>(P, vor, z, a64<R>(pv, A_VOL, i), aR<R>(pv, A_BUOY, i), aR<R>(pv, A_HUM, i), vp);
-    } else {
+    if (NF == 1) {
         vp[0] = (R)(0.25 * a64<R>(pv, A_VOL, i));
+    } else {
+        R vor[3] = {aR<R>(pv, A_VX, i), aR<R>(pv, A_VY, i), aR<R>(pv, A_VZ, i)};
+        R v7[7];
+        p2g_values<R>(P, vor, z, a64<R>(pv, A_VOL, i), aR<R>(pv, A_BUOY, i), aR<R>(pv, A_HUM, i), v7);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) vp[f] = v7[field_slot<NF>(f)];
     }
 }
 
@@ -454,7 +468,7 @@ EPIC_DEV void vectors(const PView& pv, long long i, bool reuse, bool store, R* e
 
 // Pass B of a scatter round: support points of parcels [q0, q1) into the
 // window (or the global fields).
-template <int NF, class R>
+template <int NF, class R, bool VEC = true>
 EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long long q1, const WinShared<NF>* ws,
                             unsigned* acc, const Fields7& F, int* nparg, int* nsparg, bool reuse, bool store,
                             int lg, unsigned* err) {
@@ -479,13 +493,14 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         long long i = q0 + slot;
         double pos[3] = {a64<R>(pv, A_X, i), a64<R>(pv, A_Y, i), a64<R>(pv, A_Z, i)};
         R eta[3], tau[3];
-        vectors<R>(pv, i, reuse, store, eta, tau, err);
+        // VEC: the support vectors may be recomputed here; else they are stored
+        vectors<R>(pv, i, VEC ? reuse : true, store, eta, tau, err);
         R vp[NF];
         double vs[NF];
         load_values<NF, R>(P, pv, i, pos[2], vp);
 #pragma unroll
         for (int f = 0; f < NF; ++f) vs[f] = (double)vp[f] * scale[f];
-        if (NF == 7) count_parcel(P, pos, a64<R>(pv, A_VOL, i), nparg, nsparg, err);
+        if (NF != 1 && nparg) count_parcel(P, pos, a64<R>(pv, A_VOL, i), nparg, nsparg, err);
         const double ed[3] = {(double)eta[0], (double)eta[1], (double)eta[2]};
         const double td[3] = {(double)tau[0], (double)tau[1], (double)tau[2]};
         double pt[3];
@@ -506,12 +521,24 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
     }
 }
 
+// Support vectors of every parcel from B (get_points, parcel_ellipsoid.f90:
+// 216-260), stored for the scatter that follows: the eigen-solver and the
+// scatter run as separate kernels, each with a small instruction footprint.
+template <class R>
+__global__ void __launch_bounds__(PB) k_vectors(PView pv, long long n, unsigned* err) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        R eta[3], tau[3];
+        vectors<R>(pv, i, false, true, eta, tau, err);
+    }
+}
+
 // par2grid scatter (NF = 7) and vol2grid (NF = 1).
-template <int NF, class R>
+template <int NF, class R, bool VEC>
 __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long long n, Boxes B, Fields7 F,
                                                     int* nparg, int* nsparg, int reuse, int store, int lg,
                                                     unsigned* err) {
-    extern __shared__ unsigned acc[];
+    extern __shared__ __align__(16) unsigned acc[];
     __shared__ WinShared<NF> ws;
     const Range Rg = cta_range(P, pv, B, n);
     for (long long q0 = Rg.r0; q0 < Rg.r1; q0 += round_max<R>()) {
@@ -535,7 +562,7 @@ __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long lon
         __syncthreads();
         win_zero<NF, R>(acc, ws.W);
         __syncthreads();
-        scatter_round<NF, R>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, lg, err);
+        scatter_round<NF, R, VEC>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, lg, err);
         __syncthreads();
         win_flush<NF, R>(P, acc, &ws, F);
         __syncthreads();
@@ -546,6 +573,7 @@ __global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long lon
 // Fused stage kernel.
 struct FusedArgs {
     int stage, last, lg;
+    int recwin;   // gathers from the box's records staged in shared memory (split form)
     double ca, cb;
     // surface fluxes of stage 1 (null: none)
     const double* binc;
@@ -624,6 +652,87 @@ EPIC_DEV bool gather_tri(const Params& P, const R* __restrict__ pack, const Tri&
     return true;
 }
 
+// Gather records of the grid points around a box, staged in shared memory by
+// the stage kernel: the cells of the box and one cell on every side, so the
+// corners of every support point within a cell of the box are on chip.
+// Records are stored whole (16 values); the 16-byte words of record r are
+// permuted by r (word w at w ^ (r mod 8), plain; w ^ (r mod 4), mixed) so
+// that the lanes of a warp, each reading word w of its own record, spread
+// over all banks.
+constexpr int RWM = 0;   // cells of margin around the box
+constexpr int RWX = BOXX + 1 + 2 * RWM, RWY = BOXY + 1 + 2 * RWM, RWZ = BOXZ + 1 + 2 * RWM;
+template <class R> constexpr int rec_words() { return (int)(GREC * sizeof(R) / 16); }   // 8 plain, 4 mixed
+template <class R> constexpr size_t recwin_bytes() { return sizeof(R) * GREC * RWX * RWY * RWZ; }
+
+struct RecWin {
+    int gx0, gy0, gz0, WZ;
+    int ok;
+};
+
+template <class R>
+EPIC_DEV RecWin recwin_load(const Params& P, const Range& Rg, bool box, const R* __restrict__ pack, R* srec) {
+    constexpr int V = rec_words<R>();
+    RecWin W;
+    W.gx0 = Rg.ref[0] - RWM;
+    W.gy0 = Rg.ref[1] - RWM;
+    W.gz0 = Rg.ref[2] - RWM;
+    W.WZ = min(RWZ, P.nz + 2 - W.gz0);
+    W.ok = box && RWX <= P.nx && RWY <= P.ny;
+    if (!W.ok) return W;
+    const int nrec = RWX * RWY * W.WZ;
+    const uint4* src = reinterpret_cast<const uint4*>(pack);
+    uint4* dst = reinterpret_cast<uint4*>(srec);
+    for (int e = threadIdx.x; e < nrec * V; e += blockDim.x) {
+        const int r = e / V, w = e - r * V;
+        const int z = r % W.WZ, xy = r / W.WZ, y = xy % RWY, x = xy / RWY;
+        const long long g = fidx(P, W.gz0 + z, wrap_near(W.gy0 + y, P.ny), wrap_near(W.gx0 + x, P.nx));
+        dst[r * V + (w ^ (r & (V - 1)))] = __ldg(src + g * V + w);
+    }
+    return W;
+}
+
+// gather_tri from the staged records when the point's corners are in the
+// window, else from global memory; the same sums in the same order.
+template <class R>
+EPIC_DEV bool gather_tri_win(const Params& P, const R* __restrict__ pack, const R* srec, const RecWin& W,
+                             const Tri& t, R* g) {
+    constexpr int V = rec_words<R>();
+    const int lx = wrap_to(t.is - W.gx0, P.nx), ly = wrap_to(t.js - W.gy0, P.ny), lz = t.ks - W.gz0;
+    if (!(W.ok && lx + 1 < RWX && ly + 1 < RWY && lz >= 0 && lz + 1 < W.WZ && t.ks >= -1 && t.ks <= P.nz))
+        return gather_tri<R>(P, pack, t, g);
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+            const int rb = ((lx + ii) * RWY + ly + jj) * W.WZ + lz;
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {
+                const int r = rb + kk;
+                const R w = (R)(0.25 * t.w[kk][jj][ii]);
+                if constexpr (Form<R>::mixed) {
+                    const float4* q = reinterpret_cast<const float4*>(srec) + r * V;
+#pragma unroll
+                    for (int l4 = 0; l4 < 4; ++l4) {
+                        const float4 v = q[l4 ^ (r & 3)];
+                        g[4 * l4] = fmaf(w, v.x, g[4 * l4]);
+                        g[4 * l4 + 1] = fmaf(w, v.y, g[4 * l4 + 1]);
+                        if (4 * l4 + 2 < 14) g[4 * l4 + 2] = fmaf(w, v.z, g[4 * l4 + 2]);
+                        if (4 * l4 + 3 < 14) g[4 * l4 + 3] = fmaf(w, v.w, g[4 * l4 + 3]);
+                    }
+                } else {
+                    const double2* q = reinterpret_cast<const double2*>(srec) + r * V;
+#pragma unroll
+                    for (int l2 = 0; l2 < 7; ++l2) {
+                        const double2 v = q[l2 ^ (r & 7)];
+                        g[2 * l2] = fma(w, v.x, g[2 * l2]);
+                        g[2 * l2 + 1] = fma(w, v.y, g[2 * l2 + 1]);
+                    }
+                }
+            }
+        }
+    return true;
+}
+
 // get_dBdt (parcel_ellipsoid.f90:466-507) in the attribute type.
 template <class R>
 EPIC_DEV void dBdt_r(const R* s, const R* b, R B33, R* o) {
@@ -640,7 +749,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                                                   Fields7 F, int* nparg, int* nsparg, FusedArgs S,
                                                   const StepScalars* sc, double* partials, unsigned* err) {
     using Ops = typename Form<R>::Ops;
-    extern __shared__ unsigned acc[];
+    extern __shared__ __align__(16) unsigned acc[];
     __shared__ WinShared<7> ws;
     __shared__ double red[PB / 32][NDIAG];
     constexpr int ND = DIAG ? NDIAG : 1;
@@ -649,6 +758,13 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
     for (int k = 0; k < ND; ++k) dacc[k] = 0.0;
     const double dt = sc->dt;
     const Range Rg = cta_range(P, pv, B, n);
+    // without the scatter pass, the dynamic shared memory holds the box's gather records
+    RecWin RW;
+    RW.ok = 0;
+    if (!SCATTER && S.recwin) {
+        RW = recwin_load<R>(P, Rg, blockIdx.x < B.nbox, pack, reinterpret_cast<R*>(acc));
+        __syncthreads();
+    }
     for (long long q0 = Rg.r0; q0 < Rg.r1; q0 += round_max<R>()) {
         long long q1 = min(q0 + round_max<R>(), Rg.r1);
         if (SCATTER) {
@@ -680,11 +796,13 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                     if (same_cell(cur, tp)) {
                         add_weights(cur, tp);
                     } else {
-                        ok = gather_tri<R>(P, pack, cur, g) && ok;
+                        ok = (SCATTER ? gather_tri<R>(P, pack, cur, g)
+                                      : gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g)) && ok;
                         cur = tp;
                     }
                 }
-                ok = gather_tri<R>(P, pack, cur, g) && ok;
+                ok = (SCATTER ? gather_tri<R>(P, pack, cur, g)
+                              : gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g)) && ok;
                 if (!ok) set_err(err, ERRB_ZRANGE);
             }
             R b[5];
@@ -870,23 +988,40 @@ static void set_smem(K kernel, size_t bytes) {
     allow_smem(kernel, bytes);
 }
 
+// count: par2grid's parcel counts nparg / nsparg (NF = 7 or 5)
 template <int NF, class R>
-static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int lg) {
+static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int lg, bool count) {
+    if (!reuse && store && c.vectors_kernel) {
+        k_vectors<R><<<pgrid(c.n), PB, 0, c.stream>>>(c.pv, c.n, &c.dsc->err);
+        CKL();
+        reuse = true;
+    }
     size_t sm = win_bytes<R, NF>();
-    set_smem(k_scatter<NF, R>, sm);
     Boxes B = boxes(c);
-    k_scatter<NF, R><<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, NF == 7 ? c.nparg : nullptr,
-                                                         NF == 7 ? c.nsparg : nullptr, reuse, store, lg,
-                                                         &c.dsc->err);
-    CKL();
+    auto run = [&](auto kernel) {
+        set_smem(kernel, sm);
+        kernel<<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, count ? c.nparg : nullptr,
+                                                  count ? c.nsparg : nullptr, reuse, store, lg, &c.dsc->err);
+        CKL();
+    };
+    if (reuse) run(k_scatter<NF, R, false>);
+    else run(k_scatter<NF, R, true>);
+}
+
+// par2grid fields: all 7 (moist) or the dry set
+template <class R>
+static void launch_p2g(Ctx& c, bool moist, bool reuse, bool store, bool count) {
+    c.p2g_counted = count;
+    if (moist) launch_scatter<7, R>(c, fields7(c, true), reuse, store, c.scatter_lg[1], count);
+    else launch_scatter<5, R>(c, fields7(c, false), reuse, store, c.scatter_lg[1], count);
 }
 
 void scatter_p2g(Ctx& c, bool reuse, bool store, bool moist) {
     zero_p2g_fields(c);
     if (c.n == 0) return;
     prof_begin(c, "p2g");
-    if (c.pv.mixed) launch_scatter<7, float>(c, fields7(c, moist), reuse, store, c.scatter_lg[1]);
-    else launch_scatter<7, double>(c, fields7(c, moist), reuse, store, c.scatter_lg[1]);
+    if (c.pv.mixed) launch_p2g<float>(c, moist, reuse, store, true);
+    else launch_p2g<double>(c, moist, reuse, store, true);
     prof_end(c, "p2g");
 }
 
@@ -897,8 +1032,8 @@ void scatter_v2g(Ctx& c, bool reuse) {
     F.f[0] = c.volg();
     F.mask = 1;
     prof_begin(c, "v2g");
-    if (c.pv.mixed) launch_scatter<1, float>(c, F, reuse, true, c.scatter_lg[0]);
-    else launch_scatter<1, double>(c, F, reuse, true, c.scatter_lg[0]);
+    if (c.pv.mixed) launch_scatter<1, float>(c, F, reuse, true, c.scatter_lg[0], false);
+    else launch_scatter<1, double>(c, F, reuse, true, c.scatter_lg[0], false);
     prof_end(c, "v2g");
 }
 
@@ -925,7 +1060,7 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
     const bool split = scatter && !c.fused_scatter;
     const bool moist = S.stage + 1 == c.n_stages;
     if (split) scatter = false;
-    size_t sm = scatter ? win_bytes<R, 7>() : 0;
+    size_t sm = scatter ? win_bytes<R, 7>() : S.recwin ? recwin_bytes<R>() : 0;
     auto launch = [&](auto kernel) {
         if (sm) set_smem(kernel, sm);
         prof_begin(c, "stage");
@@ -941,7 +1076,9 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
     else launch(k_stage<false, false, R>);
     if (split) {
         prof_begin(c, "stage");
-        launch_scatter<7, R>(c, fields7(c, moist), false, true, c.scatter_lg[1]);
+        // the parcel counts of the intermediate stages are not read (field
+        // diagnostics use the step's first par2grid); the last one keeps them
+        launch_p2g<R>(c, moist, false, true, moist);
         prof_end(c, "stage");
     }
 }
@@ -955,6 +1092,7 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     S.ca = c.ca[stage - 1];
     S.cb = c.cb[stage - 1];
     S.lg = c.scatter_lg[2];
+    S.recwin = c.stage_recwin;
     // surface fluxes: inside the stage-1 kernel after its diagnostics, or
     // (no diagnostics) by their own kernel before it
     const bool flux = stage == 1 && c.flux_on;

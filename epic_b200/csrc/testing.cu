@@ -85,6 +85,18 @@ extern "C" int epic_gpu_test_set_stage_form(epic_ctx* ctx, int fused) {
     return EPIC_OK;
 }
 
+extern "C" int epic_gpu_test_set_vectors_kernel(epic_ctx* ctx, int on) {
+    if (!ctx) return EPIC_ERR_ARG;
+    ctx->c.vectors_kernel = on != 0;
+    return EPIC_OK;
+}
+
+extern "C" int epic_gpu_test_set_stage_window(epic_ctx* ctx, int on) {
+    if (!ctx) return EPIC_ERR_ARG;
+    ctx->c.stage_recwin = on != 0;
+    return EPIC_OK;
+}
+
 extern "C" int epic_gpu_test_drop_sort_store(epic_ctx* ctx) {
     if (!ctx) return EPIC_ERR_ARG;
     Ctx& c = ctx->c;

@@ -44,6 +44,12 @@ int epic_gpu_test_set_stage_form(struct epic_ctx* ctx, int fused);
 
 /* Free the second parcel store, as when the device had no room for it: the
  * box sort then permutes slot by slot through scratch memory. */
+/* Support vectors by a kernel of their own before a scatter that recomputes
+ * them (1, default) or inside the scatter kernel (0); same results. */
+int epic_gpu_test_set_vectors_kernel(struct epic_ctx* ctx, int on);
+/* Stage kernel (split form) gathers from the box's records staged in shared
+ * memory (1, default) or from global memory (0); same results. */
+int epic_gpu_test_set_stage_window(struct epic_ctx* ctx, int on);
 int epic_gpu_test_drop_sort_store(struct epic_ctx* ctx);
 
 #ifdef __cplusplus
