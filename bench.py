@@ -384,7 +384,8 @@ def served_requests(args, lib):
         g = grids[int(rng.integers(0, len(grids)))]
         kind = "beltrami" if rng.random() < 0.5 else "thermal"
         klm = tuple(int(v) for v in rng.integers(1, 3, size=3))
-        reqs.append(serve.request(kind, g, seed=1000 + r, klm=klm, steps=args.served_steps, precision=1, lib=lib))
+        reqs.append(serve.request(kind, g, seed=1000 + r, klm=klm, steps=args.served_steps, precision=1, lib=lib,
+                                  tune=not args.no_autotune))
         arrivals.append(t)
         meta.append({"grid": list(g), "kind": kind, "klm": list(klm) if kind == "beltrami" else None})
     return reqs, arrivals, meta

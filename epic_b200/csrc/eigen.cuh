@@ -5,6 +5,8 @@
 #pragma once
 #include "common.cuh"
 
+#include <type_traits>
+
 namespace epic {
 
 // scherzinger.f90:16 -- the single-precision literal 1.0e-12
@@ -45,12 +47,33 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
     T j3 = O::add(O::sub(O::mul(a11, O::sub(O::mul(a22, a33), O::mul(a23, a23))),
                               O::mul(a12, O::sub(O::mul(a12, a33), O::mul(a13, a23)))),
                        O::mul(a13, O::sub(O::mul(a12, a23), O::mul(a13, a22))));
-    T smp = O::mul(O::mul(T(0.5), j3), pow(T(3) / j2, T(1.5)));
-    smp = fmin(fmax(T(-1), smp), T(1));
-    T alpha = O::mul(f13, acos(smp));
     const double pi = 3.141592653589793;
-    if (alpha > T(pi / 6.0)) alpha = O::add(alpha, O::mul(T(2.0 / 3.0), T(pi)));
-    eta[0] = O::mul(O::mul(T(2), sqrt(O::mul(f13, j2))), cos(alpha));
+    T cal;   // cos(alpha)
+    T smp;
+    if constexpr (std::is_same<O, FastOps>::value) {
+        // (3/j2)^1.5 as q sqrt(q); cos(acos(s) / 3 [+ 2 pi / 3]) as the root
+        // of the triple-angle cubic 4 y^3 - 3 y = s next to an FP32 estimate,
+        // refined by Newton in FP64 (|y| >= cos(pi/6), so 12 y^2 - 3 >= 6)
+        const double q = 3.0 / j2;
+        smp = 0.5 * j3 * (q * sqrt(q));
+        smp = fmin(fmax(-1.0, smp), 1.0);
+        float af = acosf((float)smp) * (1.0f / 3.0f);
+        if (af > (float)(pi / 6.0)) af += (float)(2.0 * pi / 3.0);
+        double y = (double)cosf(af);
+#pragma unroll
+        for (int it = 0; it < 3; ++it) {
+            const double y2 = y * y;
+            y = y - (y * (4.0 * y2 - 3.0) - smp) / (12.0 * y2 - 3.0);
+        }
+        cal = y;
+    } else {
+        smp = O::mul(O::mul(T(0.5), j3), pow(T(3) / j2, T(1.5)));
+        smp = fmin(fmax(T(-1), smp), T(1));
+        T alpha = O::mul(f13, acos(smp));
+        if (alpha > T(pi / 6.0)) alpha = O::add(alpha, O::mul(T(2.0 / 3.0), T(pi)));
+        cal = cos(alpha);
+    }
+    eta[0] = O::mul(O::mul(T(2), sqrt(O::mul(f13, j2))), cal);
     r[0] = O::sub(A[0], eta[0]); r[1] = A[1];                 r[2] = A[2];
     r[3] = A[3];                 r[4] = O::sub(A[4], eta[0]); r[5] = A[5];
     r[6] = A[6];                 r[7] = A[7];                 r[8] = O::sub(A[8], eta[0]);
@@ -61,8 +84,14 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
     if (rl2 > rm) { i = 2; rm = rl2; }
     // column i of r, selected without a run-time array index (keeps r in registers)
     T s1[3];
+    if constexpr (std::is_same<O, FastOps>::value) {
+        const T ir = T(1) / rm;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) / rm;
+        for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) * ir;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) / rm;
+    }
     if (i == 1) { r[3] = r[0]; r[4] = r[1]; r[5] = r[2]; }
     else if (i == 2) { r[6] = r[0]; r[7] = r[1]; r[8] = r[2]; }
     r[0] = s1[0]; r[1] = s1[1]; r[2] = s1[2];
@@ -78,8 +107,14 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
     int j = (rl2 > rl1) ? 2 : 1;
     T rj = (j == 2) ? rl2 : rl1;
     T s2[3];
+    if constexpr (std::is_same<O, FastOps>::value) {
+        const T ir = T(1) / rj;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) / rj;
+        for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) * ir;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) / rj;
+    }
     r[3] = s2[0]; r[4] = s2[1]; r[5] = s2[2];
     T Ar[6];
 #pragma unroll
@@ -146,16 +181,31 @@ EPIC_DEV void sz_diagonalise(T* A, T* D, T* V) {
             for (int row = 0; row < 3; ++row)
                 Ar[row + 3 * c] = O::add(O::add(O::mul(A[row], r[3 * c]), O::mul(A[row + 3], r[3 * c + 1])),
                                          O::mul(A[row + 6], r[3 * c + 2]));
-        T l0 = nrm3<O>(&Ar[0]), l1 = nrm3<O>(&Ar[3]);
-        int i = (l1 > l0) ? 1 : 0;
-        T li = i ? l1 : l0;
+        if constexpr (std::is_same<O, FastOps>::value) {
+            // normalisations by reciprocal square roots
+            const T q0 = dot3<O>(&Ar[0], &Ar[0]), q1 = dot3<O>(&Ar[3], &Ar[3]);
+            const int i = (q1 > q0) ? 1 : 0;
+            const T il = rsqrt(i ? q1 : q0);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) V[6 + k] = (i ? Ar[3 + k] : Ar[k]) / li;
-        cross3<O>(&V[6], &V[0], &V[3]);
-        cross3<O>(&V[0], &V[3], &V[6]);
-        T n0 = nrm3<O>(&V[0]), n1 = nrm3<O>(&V[3]), n2 = nrm3<O>(&V[6]);
+            for (int k = 0; k < 3; ++k) V[6 + k] = (i ? Ar[3 + k] : Ar[k]) * il;
+            cross3<O>(&V[6], &V[0], &V[3]);
+            cross3<O>(&V[0], &V[3], &V[6]);
+            const T n0 = rsqrt(dot3<O>(&V[0], &V[0])), n1 = rsqrt(dot3<O>(&V[3], &V[3]));
+            const T n2 = rsqrt(dot3<O>(&V[6], &V[6]));
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { V[k] /= n0; V[3 + k] /= n1; V[6 + k] /= n2; }
+            for (int k = 0; k < 3; ++k) { V[k] *= n0; V[3 + k] *= n1; V[6 + k] *= n2; }
+        } else {
+            T l0 = nrm3<O>(&Ar[0]), l1 = nrm3<O>(&Ar[3]);
+            int i = (l1 > l0) ? 1 : 0;
+            T li = i ? l1 : l0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) V[6 + k] = (i ? Ar[3 + k] : Ar[k]) / li;
+            cross3<O>(&V[6], &V[0], &V[3]);
+            cross3<O>(&V[0], &V[3], &V[6]);
+            T n0 = nrm3<O>(&V[0]), n1 = nrm3<O>(&V[3]), n2 = nrm3<O>(&V[6]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { V[k] /= n0; V[3 + k] /= n1; V[6 + k] /= n2; }
+        }
     }
     if (D[1] > D[0]) { swapd(D[0], D[1]); swapcol(V, 0, 1); }
     if (D[2] > D[1]) { swapd(D[1], D[2]); swapcol(V, 1, 2); }

@@ -90,8 +90,8 @@ static void run_job(epic_server* s, const Job& job, int slot, epic_ctx* ctx, epi
     epic_step_info info{};
     int64_t psteps = 0;
     if (rc == EPIC_OK) rc = epic_gpu_init_state(ctx, &job.req.init);
-    // a new context tunes its launch shapes once; pooled ones keep theirs
-    if (rc == EPIC_OK && fresh) rc = epic_gpu_autotune(ctx, nullptr);
+    // a new context tunes its launch shapes once if asked; pooled ones keep theirs
+    if (rc == EPIC_OK && fresh && job.req.tune) rc = epic_gpu_autotune(ctx, nullptr);
     if (rc == EPIC_OK) rc = epic_gpu_init_correction(ctx);
     for (int k = 0; rc == EPIC_OK && k < job.req.steps; ++k) {
         int64_t n0 = 0;

@@ -16,7 +16,7 @@ from . import abi, initial, load
 
 
 class EpicRequest(C.Structure):
-    _fields_ = [("cfg", abi.EpicCfg), ("init", abi.EpicInitSpec), ("steps", C.c_int32), ("reserved", C.c_int32)]
+    _fields_ = [("cfg", abi.EpicCfg), ("init", abi.EpicInitSpec), ("steps", C.c_int32), ("tune", C.c_int32)]
 
 
 class EpicResult(C.Structure):
@@ -48,9 +48,10 @@ def _bind(lib):
 
 
 def request(kind: str, n: tuple, seed: int = 1, klm=(1, 1, 1), steps: int = 100, precision: int = 1,
-            lib=None, **options) -> EpicRequest:
+            lib=None, tune: bool = False, **options) -> EpicRequest:
     """A request for a thermal or Beltrami simulation on an n = (nx, ny, nz)
-    grid with the benchmark workloads' domains and options."""
+    grid with the benchmark workloads' domains and options; tune lets a new
+    context pick its launch shapes by timing (epic_gpu_autotune)."""
     lib = lib or load()
     nx, ny, nz = n
     if kind == "thermal":
@@ -72,6 +73,7 @@ def request(kind: str, n: tuple, seed: int = 1, klm=(1, 1, 1), steps: int = 100,
     r.cfg = lib.default_config(nx, ny, nz, lower, extent, **opts)
     r.init = spec
     r.steps = steps
+    r.tune = int(tune)
     return r
 
 

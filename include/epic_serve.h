@@ -25,7 +25,10 @@ typedef struct epic_request {
     epic_cfg       cfg;       /* grid, options, precision form            */
     epic_init_spec init;      /* initial state, generated on the device    */
     int32_t        steps;     /* full steps (epic_gpu_step) to run         */
-    int32_t        reserved;
+    int32_t        tune;      /* 1: a new context runs epic_gpu_autotune first
+                                 (timing-based launch shapes: fastest, but
+                                 results then depend on the choice to the
+                                 last bits); 0: fixed shapes, reproducible  */
 } epic_request;
 
 typedef struct epic_result {
