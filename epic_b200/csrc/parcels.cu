@@ -675,10 +675,20 @@ __global__ void k_split_flag(Params P, PView pv, long long n, int* flag, unsigne
     PLOOP(n) {
         double b[5];
         load_B(pv, i, b);
+        const double vol = pv.get(A_VOL, i);
         double U[9], D[3];
-        full_matrix<ExactOps>(b, get_B33<ExactOps>(b, pv.get(A_VOL, i), err), U);
-        sz_eigenvalues<ExactOps>(U, D);
+        // The fast eigenvalues decide where both tests are clear of their
+        // thresholds by 1e-9 (they agree with the non-contracted ones to a few
+        // ulps); near a threshold the decision is the oracle's arithmetic.
+        full_matrix<FastOps>(b, get_B33<FastOps>(b, vol, err), U);
+        sz_eigenvalues<FastOps>(U, D);
         double lam = sqrt(D[0] / D[2]);
+        const bool clear = fabs(lam - P.lambda_max) > 1e-9 * P.lambda_max && fabs(D[0] - P.amax2) > 1e-9 * P.amax2;
+        if (!clear) {
+            full_matrix<ExactOps>(b, get_B33<ExactOps>(b, vol, err), U);
+            sz_eigenvalues<ExactOps>(U, D);
+            lam = sqrt(D[0] / D[2]);
+        }
         flag[i] = (lam < P.lambda_max && D[0] < P.amax2) ? 0 : 1;
     }
 }
