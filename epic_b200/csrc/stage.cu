@@ -486,7 +486,7 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
     const int cols = 32 >> lg;                          // groups side by side in a warp
     const int S = (U + cols - 1) / cols;                // groups per column
     const int lane = threadIdx.x & 31, gi = lane >> lg, m = lane & ((1 << lg) - 1);
-    for (int r = threadIdx.x >> 5; r < S; r += PB / 32) {
+    for (int r = threadIdx.x >> 5; r < S; r += blockDim.x >> 5) {
         const int u = gi * S + r;
         const int slot = (u << lg) + m;
         if (u >= U || slot >= cnt) continue;
@@ -998,10 +998,11 @@ static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int
     }
     size_t sm = win_bytes<R, NF>();
     Boxes B = boxes(c);
+    int* np = count ? c.nparg : nullptr;
+    int* nsp = count ? c.nsparg : nullptr;
     auto run = [&](auto kernel) {
         set_smem(kernel, sm);
-        kernel<<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, count ? c.nparg : nullptr,
-                                                  count ? c.nsparg : nullptr, reuse, store, lg, &c.dsc->err);
+        kernel<<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, np, nsp, reuse, store, lg, &c.dsc->err);
         CKL();
     };
     if (reuse) run(k_scatter<NF, R, false>);
@@ -1139,12 +1140,10 @@ __global__ void k_box_start(const unsigned* key, long long n, int nbox, int* sta
 __global__ void k_permute(PView src, PView dst, long long n, const int* perm) {
     const int attrs[20] = {A_X, A_Y, A_Z, A_VX, A_VY, A_VZ, A_B11, A_B12, A_B13, A_B22, A_B23, A_VOL, A_BUOY, A_HUM,
                            A_ETA0, A_ETA0 + 1, A_ETA0 + 2, A_TAU0, A_TAU0 + 1, A_TAU0 + 2};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * 20;
-         t += (long long)gridDim.x * blockDim.x) {
-        int a = (int)(t / n);
-        long long i = t - (long long)a * n;
-        int k = attrs[a];
-        dst.set(k, i, src.get(k, perm[i]));
+    PLOOP(n) {
+        const long long p = perm[i];
+#pragma unroll
+        for (int a = 0; a < 20; ++a) dst.set(attrs[a], i, src.get(attrs[a], p));
     }
 }
 
@@ -1179,7 +1178,7 @@ void sort_parcels(Ctx& c) {
     CKL();
     if (c.pv_alt) {
         PView dst{c.pv_alt, c.cap, c.pv.mixed};
-        k_permute<<<pgrid(n * 20), PB, 0, c.stream>>>(c.pv, dst, n, i1);
+        k_permute<<<pgrid(n), PB, 0, c.stream>>>(c.pv, dst, n, i1);
         CKL();
         std::swap(c.pv.base, c.pv_alt);
     } else {
