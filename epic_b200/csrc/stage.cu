@@ -1137,13 +1137,24 @@ __global__ void k_box_start(const unsigned* key, long long n, int nbox, int* sta
     }
 }
 
+// The 20 live slots of parcel perm[i] into slot i of the other store: all
+// loads of a parcel are issued before its stores (the slot types are known at
+// compile time, MIXED: the FP32 slots of the mixed form).
+template <bool MIXED>
 __global__ void k_permute(PView src, PView dst, long long n, const int* perm) {
-    const int attrs[20] = {A_X, A_Y, A_Z, A_VX, A_VY, A_VZ, A_B11, A_B12, A_B13, A_B22, A_B23, A_VOL, A_BUOY, A_HUM,
-                           A_ETA0, A_ETA0 + 1, A_ETA0 + 2, A_TAU0, A_TAU0 + 1, A_TAU0 + 2};
+    constexpr int attrs[20] = {A_X, A_Y, A_Z, A_VX, A_VY, A_VZ, A_B11, A_B12, A_B13, A_B22, A_B23, A_VOL, A_BUOY,
+                               A_HUM, A_ETA0, A_ETA0 + 1, A_ETA0 + 2, A_TAU0, A_TAU0 + 1, A_TAU0 + 2};
     PLOOP(n) {
         const long long p = perm[i];
+        double v[20];
 #pragma unroll
-        for (int a = 0; a < 20; ++a) dst.set(attrs[a], i, src.get(attrs[a], p));
+        for (int a = 0; a < 20; ++a)
+            v[a] = (MIXED && attr_f32(attrs[a])) ? (double)src.f(attrs[a])[p] : src.d(attrs[a])[p];
+#pragma unroll
+        for (int a = 0; a < 20; ++a) {
+            if (MIXED && attr_f32(attrs[a])) dst.f(attrs[a])[i] = (float)v[a];
+            else dst.d(attrs[a])[i] = v[a];
+        }
     }
 }
 
@@ -1178,7 +1189,8 @@ void sort_parcels(Ctx& c) {
     CKL();
     if (c.pv_alt) {
         PView dst{c.pv_alt, c.cap, c.pv.mixed};
-        k_permute<<<pgrid(n), PB, 0, c.stream>>>(c.pv, dst, n, i1);
+        if (c.pv.mixed) k_permute<true><<<pgrid(n), PB, 0, c.stream>>>(c.pv, dst, n, i1);
+        else k_permute<false><<<pgrid(n), PB, 0, c.stream>>>(c.pv, dst, n, i1);
         CKL();
         std::swap(c.pv.base, c.pv_alt);
     } else {
