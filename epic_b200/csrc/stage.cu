@@ -776,6 +776,21 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
         // pass A: grid2par + dB/dt + LS-RK update
         for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
             double pos[3] = {a64<R>(pv, A_X, i), a64<R>(pv, A_Y, i), a64<R>(pv, A_Z, i)};
+            // the attributes of the update are loaded before the gathers, so
+            // that their latency overlaps the interpolation
+            R b[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) b[k] = aR<R>(pv, A_B11 + k, i);
+            const double vol = a64<R>(pv, A_VOL, i);
+            R vor[3] = {aR<R>(pv, A_VX, i), aR<R>(pv, A_VY, i), aR<R>(pv, A_VZ, i)};
+            double dpo[3] = {0.0, 0.0, 0.0};
+            R dvo[3] = {(R)0, (R)0, (R)0}, dbo[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+            if (S.stage > 1) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { dpo[k] = a64<R>(pv, A_DX + k, i); dvo[k] = aR<R>(pv, A_DVX + k, i); }
+#pragma unroll
+                for (int k = 0; k < 5; ++k) dbo[k] = aR<R>(pv, A_DB0 + k, i);
+            }
             R g[14];
 #pragma unroll
             for (int l = 0; l < 14; ++l) g[l] = (R)0;
@@ -805,16 +820,12 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                               : gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g)) && ok;
                 if (!ok) set_err(err, ERRB_ZRANGE);
             }
-            R b[5];
-#pragma unroll
-            for (int k = 0; k < 5; ++k) b[k] = aR<R>(pv, A_B11 + k, i);
-            const double vol = a64<R>(pv, A_VOL, i);
             double dp[3];
-            R dv[3], vor[3] = {aR<R>(pv, A_VX, i), aR<R>(pv, A_VY, i), aR<R>(pv, A_VZ, i)};
+            R dv[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                dp[k] = S.stage > 1 ? a64<R>(pv, A_DX + k, i) + (double)g[k] : (double)g[k];
-                dv[k] = S.stage > 1 ? aR<R>(pv, A_DVX + k, i) + g[11 + k] : g[11 + k];
+                dp[k] = S.stage > 1 ? dpo[k] + (double)g[k] : (double)g[k];
+                dv[k] = S.stage > 1 ? dvo[k] + g[11 + k] : g[11 + k];
             }
             const R* strain = &g[3];
             // B33 from the volume constraint in FP64 (parcel_ellipsoid.f90:383-402)
@@ -856,7 +867,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
             dBdt_r<R>(strain, b, (R)B33d, db);
             if (S.stage > 1) {
 #pragma unroll
-                for (int k = 0; k < 5; ++k) db[k] = aR<R>(pv, A_DB0 + k, i) + db[k];
+                for (int k = 0; k < 5; ++k) db[k] = dbo[k] + db[k];
             }
             const double cdt = S.cb * dt;
             const R cdtr = (R)cdt;
