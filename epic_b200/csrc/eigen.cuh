@@ -60,11 +60,11 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
         float af = acosf((float)smp) * (1.0f / 3.0f);
         if (af > (float)(pi / 6.0)) af += (float)(2.0 * pi / 3.0);
         double y = (double)cosf(af);
+        // chord steps with the derivative at the FP32 estimate (relative
+        // change of f' ~ 1e-7 per step: three steps reach FP64 rounding)
+        const double idf = 1.0 / (12.0 * y * y - 3.0);
 #pragma unroll
-        for (int it = 0; it < 3; ++it) {
-            const double y2 = y * y;
-            y = y - (y * (4.0 * y2 - 3.0) - smp) / (12.0 * y2 - 3.0);
-        }
+        for (int it = 0; it < 3; ++it) y = y - (y * (4.0 * y * y - 3.0) - smp) * idf;
         cal = y;
     } else {
         smp = O::mul(O::mul(T(0.5), j3), pow(T(3) / j2, T(1.5)));
@@ -77,18 +77,23 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
     r[0] = O::sub(A[0], eta[0]); r[1] = A[1];                 r[2] = A[2];
     r[3] = A[3];                 r[4] = O::sub(A[4], eta[0]); r[5] = A[5];
     r[6] = A[6];                 r[7] = A[7];                 r[8] = O::sub(A[8], eta[0]);
-    T rl0 = nrm3<O>(&r[0]), rl1 = nrm3<O>(&r[3]), rl2 = nrm3<O>(&r[6]);
     int i = 0;
-    T rm = rl0;
-    if (rl1 > rm) { i = 1; rm = rl1; }
-    if (rl2 > rm) { i = 2; rm = rl2; }
-    // column i of r, selected without a run-time array index (keeps r in registers)
     T s1[3];
     if constexpr (std::is_same<O, FastOps>::value) {
-        const T ir = T(1) / rm;
+        // the longest column by squared norms, normalised by a reciprocal square root
+        const T q0 = dot3<O>(&r[0], &r[0]), q1 = dot3<O>(&r[3], &r[3]), q2 = dot3<O>(&r[6], &r[6]);
+        T qm = q0;
+        if (q1 > qm) { i = 1; qm = q1; }
+        if (q2 > qm) { i = 2; qm = q2; }
+        const T ir = rsqrt(qm);
 #pragma unroll
         for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) * ir;
     } else {
+        T rl0 = nrm3<O>(&r[0]), rl1 = nrm3<O>(&r[3]), rl2 = nrm3<O>(&r[6]);
+        T rm = rl0;
+        if (rl1 > rm) { i = 1; rm = rl1; }
+        if (rl2 > rm) { i = 2; rm = rl2; }
+        // column i of r, selected without a run-time array index (keeps r in registers)
 #pragma unroll
         for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) / rm;
     }
@@ -102,16 +107,18 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
         r[3 + k] = O::sub(r[3 + k], O::mul(tmp, r[k]));
         r[6 + k] = O::sub(r[6 + k], O::mul(smp, r[k]));
     }
-    rl1 = nrm3<O>(&r[3]);
-    rl2 = nrm3<O>(&r[6]);
-    int j = (rl2 > rl1) ? 2 : 1;
-    T rj = (j == 2) ? rl2 : rl1;
     T s2[3];
     if constexpr (std::is_same<O, FastOps>::value) {
-        const T ir = T(1) / rj;
+        const T q1 = dot3<O>(&r[3], &r[3]), q2 = dot3<O>(&r[6], &r[6]);
+        const int j = (q2 > q1) ? 2 : 1;
+        const T ir = rsqrt(j == 2 ? q2 : q1);
 #pragma unroll
         for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) * ir;
     } else {
+        T rl1 = nrm3<O>(&r[3]);
+        T rl2 = nrm3<O>(&r[6]);
+        int j = (rl2 > rl1) ? 2 : 1;
+        T rj = (j == 2) ? rl2 : rl1;
 #pragma unroll
         for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) / rj;
     }
