@@ -775,6 +775,19 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
         wp.init();
         // pass A: grid2par + dB/dt + LS-RK update
         for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
+            // bring the next parcel's attribute lines into L2 (one lane per 128-byte line)
+            if (!SCATTER && (threadIdx.x & 15) == 0 && i + blockDim.x < q1) {
+                const long long j = i + blockDim.x;
+#pragma unroll
+                for (int k = 0; k < 29; ++k) {
+                    const int slot = k < 3 ? A_X + k : k < 6 ? A_ETA0 + (k - 3) : k < 9 ? A_TAU0 + (k - 6)
+                                   : k < 14 ? A_B11 + (k - 9) : k == 14 ? A_VOL : k < 18 ? A_VX + (k - 15)
+                                   : k < 21 ? A_DX + (k - 18) : k < 24 ? A_DVX + (k - 21) : A_DB0 + (k - 24);
+                    if (k >= 18 && S.stage == 1) continue;
+                    const void* a = Form<R>::mixed ? (const void*)&aR<R>(pv, slot, j) : (const void*)&a64<R>(pv, slot, j);
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+                }
+            }
             double pos[3] = {a64<R>(pv, A_X, i), a64<R>(pv, A_Y, i), a64<R>(pv, A_Z, i)};
             // the attributes of the update are loaded before the gathers, so
             // that their latency overlaps the interpolation
