@@ -100,7 +100,8 @@ struct Ctx {
     double* work = nullptr;
     FFTPlan px, py;
     // horizontal FFT: 0 = 2-D plane kernel where the grid allows it, else the
-    // tiled line kernel, else Stockham lines; 1 = tiled, else Stockham; 2 = Stockham
+    // tiled line kernel, else Stockham lines; 1 = tiled, else Stockham; 2 = Stockham;
+    // 3 = half-plane cluster kernel (square 64, 128), else as 0
     int fft_path = 0;
     double* gpack = nullptr;     // gathered fields, 16 doubles per grid point
     // log2 of the consecutive parcels a lane group scatters (vol2grid,

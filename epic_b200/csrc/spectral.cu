@@ -22,6 +22,8 @@
 #include <utility>
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 namespace epic {
 
 // ---------------------------------------------------------------------------
@@ -252,31 +254,38 @@ template <> struct Radix<512> { static constexpr int N1 = 32, N2 = 16; };
 
 // Line geometry inside the plane: real element c of line a at P[a0 + c*es],
 // of line b at P[a0 + c*es + bo]; complex scratch element c at P[s0 + c*cs].
+// A line split over two blocks of rows (the half-plane kernel) puts element
+// c at a0 + (c & msk)*es + (c >> sh)*es2 (the scratch likewise with cs).
 struct LineGeo {
     int a0, es, bo, s0, cs;
+    int msk = -1, sh = 30, es2 = 0;
 };
 
 template <int N, bool FWD, class T>
 EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
     constexpr int N1 = Radix<N>::N1, N2 = Radix<N>::N2, KPT = N1 / N2, H = N / 2;
+    auto EL = [&](int c) { return g.a0 + (c & g.msk) * g.es + (c >> g.sh) * g.es2; };
+    auto SC = [&](int k) -> CX<T>& {
+        return *reinterpret_cast<CX<T>*>(P + g.s0 + (k & g.msk) * g.cs + (k >> g.sh) * g.es2);
+    };
     CX<T> v[N1];
 #pragma unroll
     for (int m = 0; m < N1; ++m) {
         const int c = t + N2 * m;
         if (FWD) {
-            v[m] = cx<T>(P[g.a0 + c * g.es], P[g.a0 + c * g.es + g.bo]);
+            v[m] = cx<T>(P[EL(c)], P[EL(c) + g.bo]);
         } else {
             // conj(A + i B) from the Hermitian lines a, b
             T ra, ia, rb, ib;
             if (c == 0 || c == H) {
-                ra = P[g.a0 + c * g.es]; ia = T(0);
-                rb = P[g.a0 + c * g.es + g.bo]; ib = T(0);
+                ra = P[EL(c)]; ia = T(0);
+                rb = P[EL(c) + g.bo]; ib = T(0);
             } else if (c < H) {
-                ra = P[g.a0 + c * g.es]; ia = P[g.a0 + (N - c) * g.es];
-                rb = P[g.a0 + c * g.es + g.bo]; ib = P[g.a0 + (N - c) * g.es + g.bo];
+                ra = P[EL(c)]; ia = P[EL(N - c)];
+                rb = P[EL(c) + g.bo]; ib = P[EL(N - c) + g.bo];
             } else {
-                ra = P[g.a0 + (N - c) * g.es]; ia = -P[g.a0 + c * g.es];
-                rb = P[g.a0 + (N - c) * g.es + g.bo]; ib = -P[g.a0 + c * g.es + g.bo];
+                ra = P[EL(N - c)]; ia = -P[EL(c)];
+                rb = P[EL(N - c) + g.bo]; ib = -P[EL(c) + g.bo];
             }
             v[m] = cx<T>(ra - ib, -(ia + rb));
         }
@@ -285,16 +294,14 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulw(v[k1], tw[t * k1]);
     __syncwarp();
-    CX<T>* sc = reinterpret_cast<CX<T>*>(P + g.s0);
-    const int cs2 = g.cs / 2;   // scratch stride in complex elements
 #pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) sc[(k1 * N2 + t) * cs2] = v[k1];
+    for (int k1 = 0; k1 < N1; ++k1) SC(k1 * N2 + t) = v[k1];
     __syncwarp();
     CX<T> y[KPT][N2];
 #pragma unroll
     for (int e = 0; e < KPT; ++e)
 #pragma unroll
-        for (int t2 = 0; t2 < N2; ++t2) y[e][t2] = sc[((t * KPT + e) * N2 + t2) * cs2];
+        for (int t2 = 0; t2 < N2; ++t2) y[e][t2] = SC((t * KPT + e) * N2 + t2);
 #pragma unroll
     for (int e = 0; e < KPT; ++e) fft_reg<N2>(y[e]);
     __syncwarp();
@@ -303,7 +310,7 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
 #pragma unroll
         for (int e = 0; e < KPT; ++e)
 #pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) sc[(t * KPT + e + N1 * k2) * cs2] = y[e][k2];
+            for (int k2 = 0; k2 < N2; ++k2) SC(t * KPT + e + N1 * k2) = y[e][k2];
         __syncwarp();
         constexpr int KU = H / N2 + 1;
         CX<T> zk[KU], zn[KU];
@@ -311,8 +318,8 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
         for (int j = 0; j < KU; ++j) {
             const int k = t + N2 * j;
             if (k <= H) {
-                zk[j] = sc[k * cs2];
-                zn[j] = sc[((N - k) & (N - 1)) * cs2];
+                zk[j] = SC(k);
+                zn[j] = SC((N - k) & (N - 1));
             }
         }
         __syncwarp();
@@ -320,11 +327,11 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
         for (int j = 0; j < KU; ++j) {
             const int k = t + N2 * j;
             if (k <= H) {
-                P[g.a0 + k * g.es] = T(0.5) * (zk[j].x + zn[j].x) * scale;
-                P[g.a0 + k * g.es + g.bo] = T(0.5) * (zk[j].y + zn[j].y) * scale;
+                P[EL(k)] = T(0.5) * (zk[j].x + zn[j].x) * scale;
+                P[EL(k) + g.bo] = T(0.5) * (zk[j].y + zn[j].y) * scale;
                 if (k > 0 && k < H) {
-                    P[g.a0 + (N - k) * g.es] = T(0.5) * (zk[j].y - zn[j].y) * scale;
-                    P[g.a0 + (N - k) * g.es + g.bo] = T(0.5) * (zn[j].x - zk[j].x) * scale;
+                    P[EL(N - k)] = T(0.5) * (zk[j].y - zn[j].y) * scale;
+                    P[EL(N - k) + g.bo] = T(0.5) * (zn[j].x - zk[j].x) * scale;
                 }
             }
         }
@@ -334,8 +341,8 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
 #pragma unroll
             for (int k2 = 0; k2 < N2; ++k2) {
                 const int k = t * KPT + e + N1 * k2;
-                P[g.a0 + k * g.es] = y[e][k2].x * scale;
-                P[g.a0 + k * g.es + g.bo] = -y[e][k2].y * scale;
+                P[EL(k)] = y[e][k2].x * scale;
+                P[EL(k) + g.bo] = -y[e][k2].y * scale;
             }
     }
     __syncwarp();
@@ -494,6 +501,126 @@ static bool tile_axis(Ctx& c, const FFTPlan& pl, int axis, const TI* const* in, 
     }
 }
 
+// Half-plane 2-D FFT: a cluster of two CTAs per (z plane, field), each with
+// half of the plane in shared memory (n/2 rows of n + 2), so that two or
+// three planes are in flight per SM.  Forward: CTA r loads the rows
+// x in [r n/2, (r+1) n/2), transforms its y lines, then the two CTAs swap
+// the off-diagonal quarter blocks through distributed shared memory, after
+// which CTA r holds every x of the spectral columns ky in [r n/2, (r+1) n/2)
+// -- element (x, ky) at row x mod n/2, column (x / (n/2)) n/2 + ky mod n/2 --
+// and transforms its x lines.  Inverse: the same steps in reverse order (the
+// swap is its own inverse).
+namespace cgr = cooperative_groups;
+
+template <int N, bool FWD, class TI, class TO, class TC>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__((N / 4) * Radix<N>::N2) k_fft_half(PlaneBatch B) {
+    constexpr int H = N / 2, S = N + 2, N2 = Radix<N>::N2, NT = (H / 2) * N2;
+    constexpr int LH = H == 64 ? 6 : H == 32 ? 5 : H == 16 ? 4 : 3;
+    static_assert((1 << LH) == H, "half size");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TC* P = reinterpret_cast<TC*>(smraw);
+    __shared__ CX<TC> tw[N];
+    cgr::cluster_group cl = cgr::this_cluster();
+    const int r = (int)cl.block_rank();
+    const int z = blockIdx.x >> 1;
+    const TI* in = static_cast<const TI*>(B.in[blockIdx.y]);
+    TO* out = static_cast<TO*>(B.out[blockIdx.y]);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = cx<TC>((TC)B.tw[i].x, (TC)B.tw[i].y);
+    const int line = threadIdx.x / N2, t = threadIdx.x - line * N2;
+    const LineGeo gy = {2 * line * S, 1, S, 2 * line * S, 2};
+    LineGeo gx = {2 * line, S, 1, 2 * line, S};
+    gx.msk = H - 1;
+    gx.sh = LH;
+    gx.es2 = H;
+    const TC scale = (TC)B.scale;
+    auto swap_quarters = [&]() {
+        constexpr int PER = H * H / NT;
+        cl.sync();   // both CTAs finished the first pass
+        const TC* peer = cl.map_shared_rank(P, r ^ 1);
+        TC v[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int idx = threadIdx.x + k * NT;
+            const int xl = idx >> LH, c = idx & (H - 1);
+            v[k] = peer[xl * S + H * r + c];
+        }
+        cl.sync();   // both CTAs read their peer's block
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int idx = threadIdx.x + k * NT;
+            const int xl = idx >> LH, c = idx & (H - 1);
+            P[xl * S + H * (1 - r) + c] = v[k];
+        }
+        __syncthreads();
+    };
+    if (FWD) {
+        for (int idx = threadIdx.x; idx < H * N; idx += NT) {
+            const int xl = idx / N, y = idx - xl * N;
+            P[xl * S + y] = (TC)in[((long long)(H * r + xl) * B.ny + y) * B.nzh + 1 + z];
+        }
+        __syncthreads();
+        line_fft<N, true, TC>(P, gy, t, tw, scale);
+        swap_quarters();
+        line_fft<N, true, TC>(P, gx, t, tw, scale);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < N * H; idx += NT) {
+            const int x = idx >> LH, c = idx & (H - 1);
+            out[((long long)x * B.ny + H * r + c) * B.nzh + 1 + z] = (TO)P[(x & (H - 1)) * S + H * (x >> LH) + c];
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < N * H; idx += NT) {
+            const int x = idx >> LH, c = idx & (H - 1);
+            P[(x & (H - 1)) * S + H * (x >> LH) + c] = (TC)in[((long long)x * B.ny + H * r + c) * B.nzh + 1 + z];
+        }
+        __syncthreads();
+        line_fft<N, false, TC>(P, gx, t, tw, scale);
+        swap_quarters();
+        line_fft<N, false, TC>(P, gy, t, tw, scale);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < H * N; idx += NT) {
+            const int xl = idx / N, y = idx - xl * N;
+            out[((long long)(H * r + xl) * B.ny + y) * B.nzh + 1 + z] = (TO)P[xl * S + y];
+        }
+    }
+}
+
+template <int N, class TI, class TO>
+static void launch_half(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
+    using TC = TCmp<TI, TO>;
+    constexpr int S = N + 2;
+    PlaneBatch B;
+    for (int f = 0; f < nf; ++f) { B.in[f] = in[f]; B.out[f] = out[f]; }
+    B.tw = c.px.tw;
+    B.ny = c.P.ny;
+    B.nzh = c.P.nzh;
+    B.scale = 1.0 / std::sqrt((double)N);
+    size_t sm = sizeof(TC) * (size_t)(N / 2) * S;
+    dim3 grid(2 * (c.P.nz + 1), nf);
+    int threads = (N / 4) * Radix<N>::N2;
+    prof_begin(c, "fft");
+    if (forward) {
+        allow_smem(k_fft_half<N, true, TI, TO, TC>, sm);
+        k_fft_half<N, true, TI, TO, TC><<<grid, threads, sm, c.stream>>>(B);
+    } else {
+        allow_smem(k_fft_half<N, false, TI, TO, TC>, sm);
+        k_fft_half<N, false, TI, TO, TC><<<grid, threads, sm, c.stream>>>(B);
+    }
+    CKL();
+    prof_end(c, "fft");
+}
+
+// Half-plane cluster kernel sizes: square n x n grids with n = 64, 128.
+template <class TI, class TO>
+static bool half_fft(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
+    const Params& P = c.P;
+    if (P.nx != P.ny) return false;
+    switch (P.nx) {
+        case 64: launch_half<64>(c, in, out, nf, forward); return true;
+        case 128: launch_half<128>(c, in, out, nf, forward); return true;
+        default: return false;
+    }
+}
+
 // Plane kernel sizes: square n x n grids with n = 16, 32, 64, 128.
 template <class TI, class TO>
 static bool plane_fft(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
@@ -570,7 +697,8 @@ template <class TI, class TO>
 void fft_xy(Ctx& c, const TI* const* in, TO* const* out, int nf, bool forward) {
     for (int f0 = 0; f0 < nf; f0 += MAXF) {
         int k = std::min(MAXF, nf - f0);
-        if (c.fft_path == 0 && plane_fft(c, in + f0, out + f0, k, forward)) continue;
+        if (c.fft_path == 3 && half_fft(c, in + f0, out + f0, k, forward)) continue;
+        if ((c.fft_path == 0 || c.fft_path == 3) && plane_fft(c, in + f0, out + f0, k, forward)) continue;
         // per axis: tiled register FFT for powers of two up to 256, else Stockham lines
         auto axis = [&](const FFTPlan& pl, int ax, auto src, TO* const* dst, bool fwd) {
             if (c.fft_path <= 1 && tile_axis(c, pl, ax, src, dst, k, fwd)) return;

@@ -65,7 +65,7 @@ extern "C" int epic_gpu_test_diverge(epic_ctx* ctx, const double* phi, double* g
 
 extern "C" int epic_gpu_test_set_fft_path(epic_ctx* ctx, int path) {
     if (!ctx) return EPIC_ERR_ARG;
-    if (path < 0 || path > 2) return EPIC_ERR_ARG;
+    if (path < 0 || path > 3) return EPIC_ERR_ARG;
     ctx->c.fft_path = path;
     return EPIC_OK;
 }

@@ -48,10 +48,11 @@ void autotune(Ctx& c, epic_tuning* out) {
     }
     c.scatter_lg[1] = c.scatter_lg[2] = best_p;
     c.scatter_lg[0] = best_v;
-    // horizontal FFT path: plane kernel (square grids up to 128), tiled lines, Stockham lines
+    // horizontal FFT path: plane kernel (square grids up to 128), tiled lines, Stockham lines,
+    // half-plane cluster kernel (square 64 and 128)
     int best_f = c.fft_path;
     float tf = FLT_MAX;
-    for (int path = 0; path <= 2; ++path) {
+    for (int path = 0; path <= 3; ++path) {
         c.fft_path = path;
         float t = time_ms(c, [&] { fft_forward_probe(c); });
         if (t < tf) { tf = t; best_f = path; }

@@ -28,7 +28,8 @@ int epic_gpu_test_diverge(struct epic_ctx* ctx, const double* phi, double* grad)
 /* Selects the horizontal FFT implementation of the context: 0 (default) the
  * 2-D plane kernel for square grids of 16, 32, 64 or 128 points, else the
  * tiled line kernel; 1 the tiled line kernel (power-of-two axes 16 .. 256);
- * 2 the batched Stockham line kernels (any even size with factors 2, 3, 5).
+ * 2 the batched Stockham line kernels (any even size with factors 2, 3, 5);
+ * 3 the half-plane kernel (a cluster of two CTAs per plane, square 64 or 128).
  * Each falls back to the next where it does not apply; all compute
  * fftxyp2s / fftxys2p (sta3dfft.f90:134-257). */
 int epic_gpu_test_set_fft_path(struct epic_ctx* ctx, int path);

@@ -78,14 +78,16 @@ def test_eigen_exact_matches_oracle_bitwise(glib, olib):
 
 
 @pytest.mark.parametrize("shape,plane", [((64, 64, 64), 0), ((64, 64, 64), 1), ((64, 64, 64), 2),
+                                         ((64, 64, 64), 3), ((128, 128, 32), 3),
                                          ((16, 16, 16), 0), ((32, 32, 24), 0), ((128, 128, 32), 0),
                                          ((48, 32, 16), 0), ((256, 256, 16), 0), ((64, 256, 16), 0),
                                          ((512, 512, 8), 0)])
 def test_vor2vel_taylor_green_kat(glib, shape, plane):
     """test_mpi_vor2vel.f90: Taylor-Green vorticity on 64^3, max err < 1e-14; the
-    same flow on other grids through the three horizontal FFT paths (2-D plane
+    same flow on other grids through the horizontal FFT paths (2-D plane
     kernel for square 16..128 grids, tiled register FFT for power-of-two axes
-    up to 256, Stockham lines otherwise)."""
+    up to 256, Stockham lines otherwise, half-plane cluster kernel for square
+    64 and 128)."""
     nx, ny, nz = shape
     lower = (-math.pi, -math.pi, -0.5 * math.pi)
     extent = (2 * math.pi, 2 * math.pi, 2 * math.pi)
@@ -125,9 +127,10 @@ def test_par2grid(olib, glib, kind):
         assert np.array_equal(gc.get_field(fid)[:, :, 1:-2], oc.get_field(fid)[:, :, 1:-2])
 
 
-@pytest.mark.parametrize("kind,plane", [("thermal", 0), ("beltrami", 0), ("thermal", 1), ("thermal", 2)])
+@pytest.mark.parametrize("kind,plane", [("thermal", 0), ("beltrami", 0), ("thermal", 1), ("thermal", 2),
+                                        ("thermal", 3)])
 def test_vor2vel_vtend_timestep(olib, glib, kind, plane):
-    s = small_state(kind)
+    s = small_state(kind, n=64 if plane == 3 else 16)
     oc, gc = pair(s, olib, glib)
     glib.lib.epic_gpu_test_set_fft_path(gc.h, plane)
     for c in (oc, gc):
