@@ -120,16 +120,20 @@ def reduce_timing(ms: float, work: float, device: str = "cuda"):
     return float(mx[0]), float(sm[1])
 
 
-def stage_phase_bytes(n: int, nx: int, ny: int, nz: int, form: str = "plain") -> float:
-    """Minimal DRAM bytes of the RK stage phase of one step: 5 x (read state
-    and accumulators, read the 14 gathered fields, write state and
-    accumulators) + 4 x (write the 7 par2grid fields and 2 counts)."""
+def stage_launch_bytes(n: int, nx: int, ny: int, nz: int, form: str = "plain") -> float:
+    """Minimal DRAM bytes of one stage-kernel launch (grid2par + LS-RK update),
+    averaged over the 5 stages of a step: per parcel the attributes read
+    (position, Veta, Vtau, B, volume, vorticity; stages 2-5 also delta_pos,
+    delta_vor, delta_b; stage 1 the buoyancy for the diagnostics) and written
+    (position, vorticity, B, delta_pos, delta_vor, delta_b), plus one read of
+    the gather records (16 values per grid point)."""
     gh = nx * ny * (nz + 3)
     if form == "mixed":
-        per_stage = (72 + 56 + 56 + 56) * n + 14 * 8.0 * gh
+        # FP64: position, volume, delta_pos; FP32: the rest
+        first, later, rec = 96 + 112, 144 + 112, 64.0
     else:
-        per_stage = 47 * 8.0 * n + 14 * 8.0 * gh
-    return 5 * per_stage + 4 * (7 * 8.0 * gh + 2 * 4.0 * gh)
+        first, later, rec = (19 + 22) * 8, (29 + 22) * 8, 128.0
+    return (first + 4 * later) / 5.0 * n + rec * gh
 
 
 def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int, form: str = "plain") -> float:
@@ -258,15 +262,14 @@ def run_ours(args):
     ms_max, ps_total = reduce_timing(ms, float(psteps))
     value = ps_total / (ms_max * 1e-3)
 
-    # roofline of the dominant phase: for "stage" the RK stage phase of a step
-    # (5 grid2par + update launches and the 4 par2grid scatters of stages 2-5);
-    # for the other kernels one launch
+    # roofline of the dominant kernel: one launch of the stage kernel (grid2par +
+    # LS-RK update, 5 per step), or of the kernel named
     peak, peak_kind = peaks()
     avg_n = psteps / args.steps
     if args.roofline_kernel == "stage":
-        unit_ms = kms.value / args.steps
-        alg = stage_phase_bytes(int(avg_n), setup.nx, setup.ny, setup.nz, args.form)
-        what = "RK stage phase per step: k_stage x5 + k_scatter x4 (grid2par, RK update, next par2grid)"
+        unit_ms = kms.value / max(kl.value, 1)
+        alg = stage_launch_bytes(int(avg_n), setup.nx, setup.ny, setup.nz, args.form)
+        what = "one k_stage launch (grid2par + LS-RK update of every parcel), averaged over the 5 stages"
     else:
         unit_ms = kms.value / max(kl.value, 1)
         alg = algorithmic_bytes(args.roofline_kernel, int(avg_n), setup.nx, setup.ny, setup.nz, args.form)
@@ -280,12 +283,18 @@ def run_ours(args):
     if args.traffic is not None:
         roofline["traffic"] = args.traffic
     elif args.roofline_kernel == "stage" and args.form == "plain":
-        # DRAM bytes of the stage phase from the ncu capture of
-        # profiles/k_stage_k_scatter_thermal64_developed.md (64^3, 2.27M parcels:
-        # 5 x 0.914 GB + 4 x 0.382 GB per step = 2674 B per parcel), scaled by
-        # the parcels of this run (traffic grows with the parcel count)
-        roofline["traffic"] = 2674.0 * avg_n
-        roofline["traffic_source"] = "ncu dram__bytes_read+write of k_stage/k_scatter, 64^3 capture scaled by parcels"
+        # DRAM bytes of one k_stage<0,0> launch from the ncu capture of
+        # profiles/k_stage_k_scatter_k_vectors_thermal64.md (64^3, 2,097,152
+        # parcels: 524.1 MB read + 347.0 MB written = 415 B per parcel),
+        # scaled by the parcels of this run (the traffic grows with them)
+        roofline["traffic"] = 415.4 * avg_n
+        roofline["traffic_source"] = "ncu dram__bytes_read+write of k_stage<0,0,double>, 64^3 capture scaled by parcels"
+        roofline["traffic_over_algorithmic"] = roofline["traffic"] / alg
+    elif args.roofline_kernel == "stage" and args.form == "mixed":
+        # the same for the mixed form (338.8 MB read + 182.1 MB written for
+        # 2,097,152 parcels = 248 B per parcel)
+        roofline["traffic"] = 248.4 * avg_n
+        roofline["traffic_source"] = "ncu dram__bytes_read+write of k_stage<0,0,float>, 64^3 capture scaled by parcels"
         roofline["traffic_over_algorithmic"] = roofline["traffic"] / alg
 
     # ---- end-to-end through the C ABI with host buffers (drop-in serial step:

@@ -1100,11 +1100,11 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
     else if (scatter) launch(k_stage<false, true, R>);
     else launch(k_stage<false, false, R>);
     if (split) {
-        prof_begin(c, "stage");
+        prof_begin(c, "stage_p2g");
         // the parcel counts of the intermediate stages are not read (field
         // diagnostics use the step's first par2grid); the last one keeps them
         launch_p2g<R>(c, moist, false, true, moist);
-        prof_end(c, "stage");
+        prof_end(c, "stage_p2g");
     }
 }
 

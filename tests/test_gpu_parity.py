@@ -358,7 +358,7 @@ def test_autotune_keeps_results(glib, precision):
     a = make_context(s, glib, keep_order=0, precision=precision)
     b = make_context(s, glib, keep_order=0, precision=precision)
     tune = a.autotune()
-    assert 0 <= tune["lg_par2grid"] <= 3 and 0 <= tune["lg_vol2grid"] <= 3 and 0 <= tune["fft_path"] <= 2
+    assert 0 <= tune["lg_par2grid"] <= 3 and 0 <= tune["lg_vol2grid"] <= 3 and 0 <= tune["fft_path"] <= 3
     assert tune["ms_par2grid"] > 0 and tune["ms_fft"] > 0
     ta, ia = a.step(0.0)
     tb, ib = b.step(0.0)
