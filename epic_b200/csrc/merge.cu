@@ -483,6 +483,13 @@ static int read_int(Ctx& c, const int* d) {
 
 static size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// Scratch bytes of the merge's binning phase for n parcels.
+size_t merge_scratch_bytes(long long n) {
+    size_t cub1 = 0;
+    cub::DeviceSelect::Flagged(nullptr, cub1, (int*)0, (int*)0, (int*)0, (int*)0, (int)n);
+    return al(sizeof(int) * (size_t)n) * 5 + al(cub1) + 4096;
+}
+
 long long parcel_merge(Ctx& c) {
     const Params& P = c.P;
     const int N = (int)c.n;
@@ -499,7 +506,7 @@ long long parcel_merge(Ctx& c) {
     // ---- phase 1: binning and the local small list (parcel_nearest.f90:416-431)
     size_t cub1 = 0;
     cub::DeviceSelect::Flagged(nullptr, cub1, (int*)0, (int*)0, (int*)0, (int*)0, N, st);
-    size_t bytes1 = al(sizeof(int) * (size_t)N) * 5 + al(cub1) + 4096;
+    size_t bytes1 = merge_scratch_bytes(N);
     Arena a1{reinterpret_cast<char*>(c.get_scratch2(bytes1)), 0, bytes1};
     int* cell0 = a1.take<int>(N);
     int* small = a1.take<int>(N);

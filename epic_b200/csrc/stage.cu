@@ -744,7 +744,7 @@ EPIC_DEV void dBdt_r(const R* s, const R* b, R B33, R* o) {
     o[4] = s[I_DWDX] * b[1] + s[I_DVDX] * b[2] + s[I_DWDY] * b[3] - s[I_DUDX] * b[4] + s[I_DVDZ] * B33;
 }
 
-template <bool DIAG, bool SCATTER, class R>
+template <bool DIAG, bool SCATTER, class R, bool VOUT = false>
 __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long n, Boxes B, const R* pack,
                                                   Fields7 F, int* nparg, int* nsparg, FusedArgs S,
                                                   const StepScalars* sc, double* partials, unsigned* err) {
@@ -918,6 +918,18 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
             for (int k = 0; k < 5; ++k) {
                 aR<R>(pv, A_B11 + k, i) = b[k];
                 aR<R>(pv, A_DB0 + k, i) = db[k];
+            }
+            if (VOUT) {
+                // support vectors of the advanced shape for the next par2grid
+                R eta[3], tau[3];
+                if constexpr (Form<R>::mixed) {
+                    support_vectors_f32(b, vol, eta, tau, err);
+                } else {
+                    double bdn[5] = {(double)b[0], (double)b[1], (double)b[2], (double)b[3], (double)b[4]};
+                    support_vectors<FastOps>(bdn, vol, eta, tau, nullptr, err);
+                }
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { aR<R>(pv, A_ETA0 + k, i) = eta[k]; aR<R>(pv, A_TAU0 + k, i) = tau[k]; }
             }
             if (SCATTER) {
                 R vpr[7];
@@ -1095,15 +1107,18 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
         CKL();
         prof_end(c, "stage");
     };
+    // in the split form the stage kernel may also compute the support vectors
+    // of the advanced shapes, which the scatter then reads
+    const bool vout = split && c.stage_vectors;
     if (with_diag && scatter) launch(k_stage<true, true, R>);
-    else if (with_diag) launch(k_stage<true, false, R>);
+    else if (with_diag) vout ? launch(k_stage<true, false, R, true>) : launch(k_stage<true, false, R>);
     else if (scatter) launch(k_stage<false, true, R>);
-    else launch(k_stage<false, false, R>);
+    else vout ? launch(k_stage<false, false, R, true>) : launch(k_stage<false, false, R>);
     if (split) {
         prof_begin(c, "stage_p2g");
         // the parcel counts of the intermediate stages are not read (field
         // diagnostics use the step's first par2grid); the last one keeps them
-        launch_p2g<R>(c, moist, false, true, moist);
+        launch_p2g<R>(c, moist, vout, true, moist);
         prof_end(c, "stage_p2g");
     }
 }
@@ -1188,6 +1203,13 @@ __global__ void k_gather_slot(const E* src, E* tmp, long long n, const int* perm
     PLOOP(n) tmp[i] = src[perm[i]];
 }
 
+// Scratch bytes of sort_parcels for n parcels: keys and indices twice, CUB.
+size_t sort_scratch_bytes(long long n) {
+    size_t cubb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, cubb, (unsigned*)0, (unsigned*)0, (int*)0, (int*)0, (int)n, 0, 32);
+    return 4 * ((sizeof(unsigned) * n + 255) & ~(size_t)255) + cubb + 1024;
+}
+
 void sort_parcels(Ctx& c) {
     long long n = c.n;
     c.n_box = 0;
@@ -1195,7 +1217,7 @@ void sort_parcels(Ctx& c) {
     size_t cubb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cubb, (unsigned*)0, (unsigned*)0, (int*)0, (int*)0, (int)n, 0, 32,
                                     c.stream);
-    size_t bytes = 4 * ((sizeof(unsigned) * n + 255) & ~(size_t)255) + cubb + 1024;
+    size_t bytes = sort_scratch_bytes(n);
     char* base = reinterpret_cast<char*>(c.get_scratch(bytes));
     auto take = [&](size_t b) { char* p = base; base += (b + 255) & ~(size_t)255; return p; };
     unsigned* k0 = reinterpret_cast<unsigned*>(take(sizeof(unsigned) * n));

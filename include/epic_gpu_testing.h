@@ -51,6 +51,15 @@ int epic_gpu_test_set_vectors_kernel(struct epic_ctx* ctx, int on);
 /* Stage kernel (split form) gathers from the box's records staged in shared
  * memory (1, default) or from global memory (0); same results. */
 int epic_gpu_test_set_stage_window(struct epic_ctx* ctx, int on);
+/* Split-form stage kernel computes the support vectors of the advanced shapes
+ * for the next par2grid (1, default) or a separate kernel does (0). */
+int epic_gpu_test_set_stage_vectors(struct epic_ctx* ctx, int on);
+/* Online choice of those two variants during the steps (1, default): in every
+ * 64 steps, steps 2 .. 9 time each combination twice and keep the fastest.  0 keeps
+ * the variants as set.  epic_gpu_test_stage_variant returns the choice
+ * (bit 0: vectors in the stage kernel, bit 1: record window; -1: none yet). */
+int epic_gpu_test_set_online_tune(struct epic_ctx* ctx, int on);
+int epic_gpu_test_stage_variant(struct epic_ctx* ctx, int* best);
 int epic_gpu_test_drop_sort_store(struct epic_ctx* ctx);
 
 #ifdef __cplusplus
