@@ -209,15 +209,8 @@ def run_ours(args):
     # optional untimed spin-up to a developed flow (deformed parcels, splits)
     for _ in range(args.spinup):
         t, _info = ctx.step(t)
-    # warm-up: at least W steps, and at least the library's first trial of
-    # its stage-phase variants (steps 2 .. 9), so that the timed steps run the
-    # variant it kept
-    args.warmup = max(args.warmup, 10)
     for _ in range(args.warmup):
         t, _info = ctx.step(t)
-    variant = C.c_int(-1)
-    if hasattr(lib.lib, "epic_gpu_test_stage_variant"):
-        lib.lib.epic_gpu_test_stage_variant(ctx.h, C.byref(variant))
     # ---- device-resident timed region
     lib.lib.epic_gpu_profile_kernel(ctx.h, args.roofline_kernel.encode())
     clocks = ClockSampler(dev if world == 1 else local)
@@ -365,9 +358,6 @@ def run_ours(args):
                    "grid": [setup.nx, setup.ny, setup.nz], "parcels_at_start": int(setup.n),
                    "parcels_range_timed": [int(nmin), int(nmax)], "precision": precision,
                    "spinup_steps": args.spinup, "autotune": tuning,
-                   "stage_variant": {"choice": variant.value,
-                                     "meaning": "bit 0: support vectors in the stage kernel, bit 1: record window "
-                                                "(chosen online by the library, results bitwise identical)"},
                    "device_memory_used_gb": round(used_gb, 2), "device_memory_total_gb": round(total_b / 1e9, 2),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"inputs larger than L2 (parcel state {store_gb:.2f} GB, fields {field_gb:.2f} GB)"},
@@ -542,7 +532,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="thermal-128")
     ap.add_argument("--form", default="plain", choices=["plain", "mixed", "served"],

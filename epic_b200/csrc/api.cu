@@ -238,10 +238,6 @@ static void free_ctx(Ctx& c) {
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto e : c.prof.ev) cudaEventDestroy(e);
     c.prof.ev.clear();
-    for (auto& e : c.stage_ev) {
-        if (e) cudaEventDestroy(e);
-        e = nullptr;
-    }
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
                     c.dvor_bar, c.box_start, c.gpack, c.binc};
@@ -516,38 +512,9 @@ int epic_gpu_grid2par(epic_ctx* ctx, int add) {
     API_BEGIN NEED_PARCELS grid2par(ctx->c, add != 0); check_device_error(ctx->c); API_END
 }
 
-// Online choice of the stage phase's variants: the record window of the
-// stage kernel (on / off) and where the next par2grid's support vectors are
-// computed (the stage kernel / their own kernel).  All four give bitwise the
-// same results; which is fastest depends on the flow (compact early shapes
-// or deformed ones).  In every period of TUNE_PERIOD steps, the TUNE_TRIAL
-// steps from TUNE_SKIP on try each combination twice, in the order
-// 0 1 2 3 3 2 1 0 (a steady drift of the step cost over the trial cancels in
-// the means), timing the stage kernels and their scatters with CUDA events;
-// the fastest mean is kept until the next trial (the first steps of a run,
-// from near-diagonal shapes, are cheaper than the ones that follow).
-constexpr int TUNE_PERIOD = 64, TUNE_SKIP = 2, TUNE_TRIAL = 8;
-
-static void stage_variant(Ctx& c, int v) {
-    c.stage_vectors = (v & 1) != 0;
-    c.stage_recwin = (v >> 1) & 1;
-}
-
 static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
     // ls_rk_step (ls_rk.f90:88-136); each stage's grid2par + update is fused
     // with the following par2grid (stage.cu)
-    const int kt = (int)(c.rk_steps % TUNE_PERIOD) - TUNE_SKIP;
-    const bool trial = c.online_tune && kt >= 0 && kt < TUNE_TRIAL && c.n_stages <= 5;
-    if (trial) {
-        if (kt == 0) {
-            for (int v = 0; v < 4; ++v) { c.tune_ms[v] = 0.0f; c.tune_n[v] = 0; }
-            if (!c.stage_ev[0])
-                for (auto& e : c.stage_ev) CK(cudaEventCreate(&e));
-        }
-        stage_variant(c, kt < 4 ? kt : 7 - kt);
-    } else if (c.online_tune && c.tune_best >= 0) {
-        stage_variant(c, c.tune_best);
-    }
     double tt = t;
     CK(cudaMemcpyAsync(&c.dsc->t, &tt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
     par2grid(c, t > c.cfg.t_initial, true, c.n_stages == 1);
@@ -570,9 +537,7 @@ static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
             vorticity_tendency(c);
             prof_end(c, "vtend");
         }
-        if (trial) CK(cudaEventRecord(c.stage_ev[2 * (s - 1)], c.stream));
         fused_stage(c, s, s == 1 && pstats != nullptr);
-        if (trial) CK(cudaEventRecord(c.stage_ev[2 * (s - 1) + 1], c.stream));
         if (s < c.n_stages) {
             prof_begin(c, "p2g_tail");
             p2g_tail(c);
@@ -588,24 +553,6 @@ static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
     double dt = 0.0;
     CK(cudaMemcpyAsync(&dt, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     check_device_error(c);
-    if (trial) {
-        float tot = 0.0f;
-        for (int s = 0; s < c.n_stages; ++s) {
-            float ms = 0.0f;
-            CK(cudaEventElapsedTime(&ms, c.stage_ev[2 * s], c.stage_ev[2 * s + 1]));
-            tot += ms;
-        }
-        const int v = kt < 4 ? kt : 7 - kt;
-        c.tune_ms[v] += tot;
-        c.tune_n[v] += 1;
-        if (kt == TUNE_TRIAL - 1) {
-            int best = 0;
-            for (int w = 1; w < 4; ++w)
-                if (c.tune_ms[w] / c.tune_n[w] < c.tune_ms[best] / c.tune_n[best]) best = w;
-            c.tune_best = best;
-        }
-    }
-    ++c.rk_steps;
     t = t + dt;
     return dt;
 }

@@ -109,16 +109,8 @@ struct Ctx {
     int scatter_lg[3] = {1, 1, 0};
     bool fused_scatter = false;   // stage kernel runs the next par2grid itself (else a separate scatter kernel)
     bool vectors_kernel = true;   // support vectors by their own kernel before a scatter that recomputes them
-    int stage_recwin = 1;         // split-form stage kernel gathers from records staged in shared memory
+    int stage_recwin = 0;         // split-form stage kernel gathers from records staged in shared memory
     bool stage_vectors = false;   // split-form stage kernel computes the next par2grid's support vectors
-    // online choice of the stage-phase variants (record window, vector output):
-    // results are bitwise the same, only the time differs
-    bool online_tune = true;
-    long long rk_steps = 0;
-    int tune_best = -1;
-    float tune_ms[4] = {0, 0, 0, 0};
-    int tune_n[4] = {0, 0, 0, 0};
-    cudaEvent_t stage_ev[10] = {};
     bool p2g_counted = true;      // the last par2grid scatter counted parcels per cell (nparg, nsparg)
     Tables T;
     StepScalars* dsc = nullptr;     // device

@@ -103,18 +103,6 @@ extern "C" int epic_gpu_test_set_stage_vectors(epic_ctx* ctx, int on) {
     return EPIC_OK;
 }
 
-extern "C" int epic_gpu_test_set_online_tune(epic_ctx* ctx, int on) {
-    if (!ctx) return EPIC_ERR_ARG;
-    ctx->c.online_tune = on != 0;
-    return EPIC_OK;
-}
-
-extern "C" int epic_gpu_test_stage_variant(epic_ctx* ctx, int* best) {
-    if (!ctx || !best) return EPIC_ERR_ARG;
-    *best = ctx->c.tune_best;
-    return EPIC_OK;
-}
-
 extern "C" int epic_gpu_test_drop_sort_store(epic_ctx* ctx) {
     if (!ctx) return EPIC_ERR_ARG;
     Ctx& c = ctx->c;

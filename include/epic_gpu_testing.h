@@ -49,17 +49,13 @@ int epic_gpu_test_set_stage_form(struct epic_ctx* ctx, int fused);
  * them (1, default) or inside the scatter kernel (0); same results. */
 int epic_gpu_test_set_vectors_kernel(struct epic_ctx* ctx, int on);
 /* Stage kernel (split form) gathers from the box's records staged in shared
- * memory (1, default) or from global memory (0); same results. */
+ * memory (1) or from global memory (0, default); same results. */
 int epic_gpu_test_set_stage_window(struct epic_ctx* ctx, int on);
 /* Split-form stage kernel computes the support vectors of the advanced shapes
- * for the next par2grid (1, default) or a separate kernel does (0). */
+ * for the next par2grid (1) or a separate kernel does (0, default); same
+ * results.  Both non-default variants measured slower on the B200 (plain and
+ * mixed, early and developed flows) and are kept for the parity tests. */
 int epic_gpu_test_set_stage_vectors(struct epic_ctx* ctx, int on);
-/* Online choice of those two variants during the steps (1, default): in every
- * 64 steps, steps 2 .. 9 time each combination twice and keep the fastest.  0 keeps
- * the variants as set.  epic_gpu_test_stage_variant returns the choice
- * (bit 0: vectors in the stage kernel, bit 1: record window; -1: none yet). */
-int epic_gpu_test_set_online_tune(struct epic_ctx* ctx, int on);
-int epic_gpu_test_stage_variant(struct epic_ctx* ctx, int* best);
 int epic_gpu_test_drop_sort_store(struct epic_ctx* ctx);
 
 #ifdef __cplusplus

@@ -369,18 +369,15 @@ def test_autotune_keeps_results(glib, precision):
 
 def test_stage_variants_agree(glib):
     """The four variants of the stage phase (record window on / off, support
-    vectors in the stage kernel or their own) give the same steps; the online
-    choice among them only changes the time."""
+    vectors in the stage kernel or their own) give the same steps."""
     import ctypes as C
     s = small_state("thermal", small_frac=0.02, seed=8)
     L = glib.lib
-    L.epic_gpu_test_set_online_tune.argtypes = [C.c_void_p, C.c_int]
     L.epic_gpu_test_set_stage_window.argtypes = [C.c_void_p, C.c_int]
     L.epic_gpu_test_set_stage_vectors.argtypes = [C.c_void_p, C.c_int]
     out = []
     for v in range(4):
         ctx = make_context(s, glib, keep_order=0)
-        L.epic_gpu_test_set_online_tune(ctx.h, 0)
         L.epic_gpu_test_set_stage_vectors(ctx.h, v & 1)
         L.epic_gpu_test_set_stage_window(ctx.h, (v >> 1) & 1)
         t = 0.0
@@ -392,11 +389,3 @@ def test_stage_variants_agree(glib):
         assert n == out[0][1] and rel_err(t, out[0][0]) < 1e-12
         for k in p:
             assert rel_err(p[k], out[0][2][k]) < 1e-11, k
-    # the online choice settles on one of them after its first trial
-    ctx = make_context(s, glib, keep_order=0)
-    t = 0.0
-    for _ in range(10):
-        t, _ = ctx.step(t)
-    best = C.c_int(-1)
-    L.epic_gpu_test_stage_variant(ctx.h, C.byref(best))
-    assert 0 <= best.value <= 3
