@@ -120,19 +120,22 @@ def reduce_timing(ms: float, work: float, device: str = "cuda"):
     return float(mx[0]), float(sm[1])
 
 
-def stage_launch_bytes(n: int, nx: int, ny: int, nz: int, form: str = "plain") -> float:
+def stage_launch_bytes(n: int, nx: int, ny: int, nz: int, form: str = "plain", later_only: bool = False) -> float:
     """Minimal DRAM bytes of one stage-kernel launch (grid2par + LS-RK update),
-    averaged over the 5 stages of a step: per parcel the attributes read
-    (position, Veta, Vtau, B, volume, vorticity; stages 2-5 also delta_pos,
-    delta_vor, delta_b; stage 1 the buoyancy for the diagnostics) and written
-    (position, vorticity, B, delta_pos, delta_vor, delta_b), plus one read of
-    the gather records (16 values per grid point)."""
+    averaged over the 5 stages of a step (later_only: of one of stages 2-5):
+    per parcel the attributes read (position, Veta, Vtau, B, volume,
+    vorticity; stages 2-5 also delta_pos, delta_vor, delta_b; stage 1 the
+    buoyancy for the diagnostics) and written (position, vorticity, B,
+    delta_pos, delta_vor, delta_b), plus one read of the gather records (16
+    values per grid point)."""
     gh = nx * ny * (nz + 3)
     if form == "mixed":
         # FP64: position, volume, delta_pos; FP32: the rest
         first, later, rec = 96 + 112, 144 + 112, 64.0
     else:
         first, later, rec = (19 + 22) * 8, (29 + 22) * 8, 128.0
+    if later_only:
+        return later * n + rec * gh
     return (first + 4 * later) / 5.0 * n + rec * gh
 
 
@@ -282,20 +285,21 @@ def run_ours(args):
                 "algorithmic_bytes_per_unit": alg}
     if args.traffic is not None:
         roofline["traffic"] = args.traffic
-    elif args.roofline_kernel == "stage" and args.form == "plain":
-        # DRAM bytes of one k_stage<0,0> launch from the ncu capture of
-        # profiles/k_stage_k_scatter_k_vectors_thermal64.md (64^3, 2,097,152
-        # parcels: 524.1 MB read + 347.0 MB written = 415 B per parcel),
-        # scaled by the parcels of this run (the traffic grows with them)
-        roofline["traffic"] = 415.4 * avg_n
-        roofline["traffic_source"] = "ncu dram__bytes_read+write of k_stage<0,0,double>, 64^3 capture scaled by parcels"
-        roofline["traffic_over_algorithmic"] = roofline["traffic"] / alg
-    elif args.roofline_kernel == "stage" and args.form == "mixed":
-        # the same for the mixed form (338.8 MB read + 182.1 MB written for
-        # 2,097,152 parcels = 248 B per parcel)
-        roofline["traffic"] = 248.4 * avg_n
-        roofline["traffic_source"] = "ncu dram__bytes_read+write of k_stage<0,0,float>, 64^3 capture scaled by parcels"
-        roofline["traffic_over_algorithmic"] = roofline["traffic"] / alg
+    elif args.roofline_kernel == "stage":
+        # DRAM bytes of one k_stage<0,0> launch (stages 2-5) from the ncu
+        # captures in profiles/k_stage_thermal64.md (64^3, 2,097,152 parcels,
+        # early flow: plain 548.0 MB read + 349.2 MB written = 427.8 B per
+        # parcel; mixed 338.6 + 185.4 MB = 249.9 B), scaled by the parcels of
+        # this run (the traffic grows with them), against the algorithmic
+        # bytes of the same stages.  Lines still dirty in L2 when the launch
+        # ends (up to its 126 MB) are not in the count, which puts the mixed
+        # capture a little below its algorithmic bytes.
+        per_parcel = 249.9 if args.form == "mixed" else 427.8
+        roofline["traffic"] = per_parcel * avg_n
+        roofline["traffic_source"] = (f"ncu dram__bytes_read+write of k_stage<0,0,{'float' if args.form == 'mixed' else 'double'}> "
+                                      "(stages 2-5), 64^3 capture scaled by parcels")
+        roofline["traffic_over_algorithmic"] = roofline["traffic"] / stage_launch_bytes(
+            int(avg_n), setup.nx, setup.ny, setup.nz, args.form, later_only=True)
 
     # ---- end-to-end through the C ABI with host buffers (drop-in serial step:
     # the host container owns the parcels; every step copies them in, steps,
