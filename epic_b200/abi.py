@@ -23,6 +23,7 @@ ERROR_NAMES = {
     6: "EPIC_ERR_ARG",
     7: "EPIC_ERR_STATE",
     8: "EPIC_ERR_PARCEL_COUNT",
+    9: "EPIC_ERR_IO",
 }
 
 # field ids (enum epic_field_id)
@@ -195,7 +196,11 @@ class EpicLib:
             self.fn[name] = f
         # entry points only the CUDA library has
         for name, args in (("init_state", [_VP, C.POINTER(EpicInitSpec)]),
-                           ("autotune", [_VP, C.POINTER(EpicTuning)])):
+                           ("autotune", [_VP, C.POINTER(EpicTuning)]),
+                           ("write_parcels_nc", [_VP, C.c_char_p, C.c_double]),
+                           ("read_parcels_nc", [_VP, C.c_char_p, _D]),
+                           ("write_fields_nc", [_VP, C.c_char_p, C.c_double]),
+                           ("init_from_field_file", [_VP, C.c_char_p, _I32])):
             if hasattr(self.lib, prefix + name):
                 f = getattr(self.lib, prefix + name)
                 f.argtypes = args
@@ -401,6 +406,26 @@ class EpicContext:
         h = _f64(humg, self.field_shape) if humg is not None else None
         flags = np.zeros(2, dtype=np.int32)
         self._call("init_from_grids", _ptr(v), _ptr(b), _ptr(h), flags.ctypes.data_as(_I32))
+        return int(flags[0]), int(flags[1])
+
+    # -- files in the reference's netCDF layout (include/epic_nc.h) --------
+    def write_parcels_nc(self, path, t: float):
+        self._call("write_parcels_nc", os.fsencode(path), C.c_double(t))
+
+    def read_parcels_nc(self, path) -> float:
+        """Parcels (and zeta flags) from a parcel file; returns its time."""
+        t = C.c_double()
+        self._call("read_parcels_nc", os.fsencode(path), C.byref(t))
+        return t.value
+
+    def write_fields_nc(self, path, t: float):
+        self._call("write_fields_nc", os.fsencode(path), C.c_double(t))
+
+    def init_from_field_file(self, path):
+        """init_from_grids on the vorticity, buoyancy and humidity of a field
+        file's last record; returns the zeta boundary flags."""
+        flags = np.zeros(2, dtype=np.int32)
+        self._call("init_from_field_file", os.fsencode(path), flags.ctypes.data_as(_I32))
         return int(flags[0]), int(flags[1])
 
     def set_bndry_fluxes(self, bflux=None, hflux=None):

@@ -13,8 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libepic_b200.so")
-SOURCES = ["api.cu", "spectral.cu", "parcels.cu", "merge.cu", "testing.cu", "noalloc.cu", "stage.cu", "init.cu", "serve.cu", "tune.cu", "damping.cu"]
-HEADERS = ["common.cuh", "eigen.cuh", "ctx.hpp", "parcel_ops.cuh", os.path.join("..", "..", "include", "epic_gpu.h"),
+SOURCES = ["api.cu", "spectral.cu", "parcels.cu", "merge.cu", "testing.cu", "noalloc.cu", "stage.cu", "init.cu", "serve.cu", "tune.cu", "damping.cu", "ncfile.cpp"]
+HEADERS = ["common.cuh", "eigen.cuh", "ctx.hpp", "parcel_ops.cuh", "ncfile.hpp", os.path.join("..", "..", "include", "epic_nc.h"), os.path.join("..", "..", "include", "epic_gpu.h"),
            os.path.join("..", "..", "include", "epic_gpu_testing.h"), os.path.join("..", "..", "include", "epic_serve.h")]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -28,7 +28,7 @@ def _mtime(p):
 
 
 def _compile(src: str, force: bool) -> str:
-    obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+    obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
     deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS]
     if force or _mtime(obj) < max(_mtime(d) for d in deps):
         cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]

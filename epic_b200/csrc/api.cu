@@ -2,6 +2,8 @@
 // host <-> device parcel/field exchange and the step driver
 // (epic3d.f90:135-153, ls_rk.f90:88-217).
 #include "ctx.hpp"
+#include "ncfile.hpp"
+#include "../../include/epic_nc.h"
 
 #include <cmath>
 #include <cstring>
@@ -709,6 +711,135 @@ int epic_gpu_launch_count(int64_t* n) {
     if (!n) return EPIC_ERR_ARG;
     *n = g_launches.load();
     return EPIC_OK;
+}
+
+
+// ---- parcel and field files (include/epic_nc.h) ----------------------------
+static ncio::Box ctx_box(const Ctx& c) {
+    ncio::Box b;
+    const int32_t n[3] = {c.cfg.nx, c.cfg.ny, c.cfg.nz};
+    for (int k = 0; k < 3; ++k) {
+        b.ncells[k] = n[k];
+        b.origin[k] = c.cfg.lower[k];
+        b.extent[k] = c.cfg.extent[k];
+    }
+    return b;
+}
+
+#define NC_TRY(stmt)                                                    \
+    try {                                                               \
+        stmt;                                                           \
+    } catch (const ncio::Error& e) {                                    \
+        throw CudaError(EPIC_ERR_IO, e.what());                         \
+    }
+
+int epic_gpu_write_parcels_nc(epic_ctx* ctx, const char* path, double t) {
+    API_BEGIN
+    NEED_PARCELS
+    Ctx& c = ctx->c;
+    if (!path) throw CudaError(EPIC_ERR_ARG, "write_parcels_nc: null path");
+    const int64_t n = c.n;
+    std::vector<double> pos(3 * n), vor(3 * n), B(5 * n), vol(n), buoy(n), hum(n);
+    int64_t m = 0;
+    const int rc = epic_gpu_get_parcels(ctx, n, &m, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(),
+                                        hum.data());
+    if (rc != EPIC_OK) throw CudaError(rc, c.err);
+    NC_TRY(ncio::write_parcels(path, ctx_box(c), c.cfg.bndry_zeta_zero, t, n, pos.data(), vor.data(), B.data(),
+                               vol.data(), buoy.data(), hum.data()))
+    API_END
+}
+
+int epic_gpu_read_parcels_nc(epic_ctx* ctx, const char* path, double* t) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!path) throw CudaError(EPIC_ERR_ARG, "read_parcels_nc: null path");
+    ncio::Info in;
+    NC_TRY(in = ncio::info(path))
+    if (in.file_type != "parcels") throw CudaError(EPIC_ERR_IO, std::string(path) + " is not a parcel file");
+    NC_TRY(ncio::check_box(in.box, ctx_box(c), path))
+    const int64_t n = in.n_parcels;
+    if (n > c.cap) throw CudaError(EPIC_ERR_CAPACITY, "read_parcels_nc: more parcels than the device capacity");
+    std::vector<double> pos(3 * n), vor(3 * n), B(5 * n), vol(n), buoy(n), hum(n);
+    int64_t m = 0;
+    NC_TRY(ncio::read_parcels(path, n, &m, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(), hum.data()))
+    const int rc = epic_gpu_set_parcels(ctx, n, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(),
+                                        hum.data());
+    if (rc != EPIC_OK) throw CudaError(rc, c.err);
+    if (in.has_zeta)   // read_zeta_boundary_flag (parameters.f90:220-250)
+        for (int b = 0; b < 2; ++b) {
+            c.cfg.bndry_zeta_zero[b] = in.zeta[b];
+            c.P.zeta_zero[b] = in.zeta[b];
+        }
+    if (t) *t = in.t;
+    API_END
+}
+
+int epic_gpu_write_fields_nc(epic_ctx* ctx, const char* path, double t) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!path) throw CudaError(EPIC_ERR_ARG, "write_fields_nc: null path");
+    const size_t fsz = (size_t)c.P.fsz;
+    struct Item { int id; const char *name, *long_name, *unit; bool integer; };
+    // field_netcdf.f90:460-560 (names, long names and units), in the order of
+    // write_netcdf_fields (:214-248)
+    const Item items[] = {
+        {EPIC_FIELD_VELOG_X, "x_velocity", "x velocity component", "m/s", false},
+        {EPIC_FIELD_VELOG_Y, "y_velocity", "y velocity component", "m/s", false},
+        {EPIC_FIELD_VELOG_Z, "z_velocity", "z velocity component", "m/s", false},
+        {EPIC_FIELD_VTEND_X, "x_vorticity_tendency", "x vorticity tendency", "1/s", false},
+        {EPIC_FIELD_VTEND_Y, "y_vorticity_tendency", "y vorticity tendency", "1/s", false},
+        {EPIC_FIELD_VTEND_Z, "z_vorticity_tendency", "z vorticity tendency", "1/s", false},
+        {EPIC_FIELD_NPARG, "nparg", "number of parcels per cell", "1", true},
+        {EPIC_FIELD_NSPARG, "nsparg", "number of small parcels per cell", "1", true},
+        {EPIC_FIELD_VORTG_X, "x_vorticity", "x vorticity component", "1/s", false},
+        {EPIC_FIELD_VORTG_Y, "y_vorticity", "y vorticity component", "1/s", false},
+        {EPIC_FIELD_VORTG_Z, "z_vorticity", "z vorticity component", "1/s", false},
+        {EPIC_FIELD_TBUOYG, "buoyancy", "total buoyancy", "m/s^2", false},
+        {EPIC_FIELD_DBUOYG, "dry_buoyancy", "dry buoyancy", "m/s^2", false},
+        {-1, "liquid_water_content", "liquid-water content", "1", false},
+        {EPIC_FIELD_HUMG, "humidity", "specific humidity", "kg/kg", false},
+        {EPIC_FIELD_VOLG, "volume", "volume", "m^3", false},
+    };
+    const int nitems = (int)(sizeof(items) / sizeof(items[0]));
+    std::vector<std::vector<double>> data(nitems, std::vector<double>(fsz));
+    int it_t = -1, it_d = -1, it_l = -1;
+    for (int k = 0; k < nitems; ++k) {
+        if (items[k].id == EPIC_FIELD_TBUOYG) it_t = k;
+        if (items[k].id == EPIC_FIELD_DBUOYG) it_d = k;
+        if (items[k].id < 0) { it_l = k; continue; }
+        const int rc = epic_gpu_get_field(ctx, items[k].id, data[k].data());
+        if (rc != EPIC_OK) throw CudaError(rc, c.err);
+    }
+    // glati * (tbuoyg - dbuoyg) (field_netcdf.f90:244)
+    const double glati = c.P.glat != 0.0 ? 1.0 / c.P.glat : 0.0;
+    for (size_t g = 0; g < fsz; ++g) data[it_l][g] = glati * (data[it_t][g] - data[it_d][g]);
+    std::vector<ncio::FieldOut> out;
+    for (int k = 0; k < nitems; ++k)
+        out.push_back({items[k].name, items[k].long_name, items[k].unit, data[k].data(), items[k].integer});
+    NC_TRY(ncio::write_fields(path, ctx_box(c), c.cfg.bndry_zeta_zero, t, out))
+    API_END
+}
+
+int epic_gpu_init_from_field_file(epic_ctx* ctx, const char* path, int32_t zeta_flags[2]) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!path) throw CudaError(EPIC_ERR_ARG, "init_from_field_file: null path");
+    ncio::Info in;
+    NC_TRY(in = ncio::info(path))
+    if (in.file_type != "fields") throw CudaError(EPIC_ERR_IO, std::string(path) + " is not a field file");
+    const ncio::Box box = ctx_box(c);
+    NC_TRY(ncio::check_box(in.box, box, path))
+    const size_t fsz = (size_t)c.P.fsz;
+    std::vector<double> vort(3 * fsz, 0.0), buoy(fsz, 0.0), hum(fsz, 0.0);
+    // read_netcdf_fields(field_file, -1) (field_netcdf.f90:306-389): the last
+    // record; datasets the file lacks stay zero
+    const char* vn[3] = {"x_vorticity", "y_vorticity", "z_vorticity"};
+    for (int k = 0; k < 3; ++k) NC_TRY(ncio::read_field(path, vn[k], -1, box, vort.data() + k * fsz))
+    NC_TRY(ncio::read_field(path, "buoyancy", -1, box, buoy.data()))
+    NC_TRY(ncio::read_field(path, "humidity", -1, box, hum.data()))
+    const int rc = epic_gpu_init_from_grids(ctx, vort.data(), buoy.data(), hum.data(), zeta_flags);
+    if (rc != EPIC_OK) throw CudaError(rc, c.err);
+    API_END
 }
 
 }  // extern "C"

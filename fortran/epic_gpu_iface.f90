@@ -115,6 +115,41 @@ module epic_gpu_iface
             integer(c_int), value  :: field_id
             real(c_double)         :: out(*)
         end function
+        ! parcel and field files in the reference's netCDF layout (epic_nc.h):
+        ! write_netcdf_parcels / read_netcdf_parcels (restart) /
+        ! write_netcdf_fields / read_netcdf_fields + init_parcels_from_grids;
+        ! path is a NUL-terminated string (trim(name) // c_null_char)
+        integer(c_int) function epic_gpu_write_parcels_nc(ctx, path, t) &
+                bind(C, name="epic_gpu_write_parcels_nc")
+            import :: c_int, c_ptr, c_char, c_double
+            type(c_ptr), value            :: ctx
+            character(kind=c_char)        :: path(*)
+            real(c_double), value         :: t
+        end function
+
+        integer(c_int) function epic_gpu_read_parcels_nc(ctx, path, t) &
+                bind(C, name="epic_gpu_read_parcels_nc")
+            import :: c_int, c_ptr, c_char, c_double
+            type(c_ptr), value            :: ctx
+            character(kind=c_char)        :: path(*)
+            real(c_double)                :: t
+        end function
+
+        integer(c_int) function epic_gpu_write_fields_nc(ctx, path, t) &
+                bind(C, name="epic_gpu_write_fields_nc")
+            import :: c_int, c_ptr, c_char, c_double
+            type(c_ptr), value            :: ctx
+            character(kind=c_char)        :: path(*)
+            real(c_double), value         :: t
+        end function
+
+        integer(c_int) function epic_gpu_init_from_field_file(ctx, path, zeta_flags) &
+                bind(C, name="epic_gpu_init_from_field_file")
+            import :: c_int, c_int32_t, c_ptr, c_char
+            type(c_ptr), value            :: ctx
+            character(kind=c_char)        :: path(*)
+            integer(c_int32_t)            :: zeta_flags(2)
+        end function
     end interface
 
 end module epic_gpu_iface

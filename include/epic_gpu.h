@@ -41,6 +41,7 @@ extern "C" {
 #define EPIC_ERR_ARG          6  /* bad argument (null pointer, size) */
 #define EPIC_ERR_STATE        7  /* call out of order (e.g. step before set_parcels) */
 #define EPIC_ERR_PARCEL_COUNT 8  /* par2grid parcel count check (parcel_interpl.f90:248-250) */
+#define EPIC_ERR_IO           9  /* file missing, unreadable or of another layout (include/epic_nc.h) */
 
 /* Field identifiers for epic_gpu_get_field / epic_gpu_set_field
  * (fields.f90:21-51). */

@@ -12,15 +12,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _declared(header):
     text = open(os.path.join(ROOT, "include", header)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(epic_(?:gpu|srv)_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(epic_(?:gpu|srv|nc)_[a-z0-9_]+)\s*\(", text)))
 
 
-@pytest.mark.parametrize("header", ["epic_gpu.h", "epic_gpu_testing.h", "epic_serve.h"])
+@pytest.mark.parametrize("header", ["epic_gpu.h", "epic_gpu_testing.h", "epic_serve.h", "epic_nc.h"])
 def test_library_exports_declared_symbols(header):
     import epic_b200
     lib = ctypes.CDLL(epic_b200.LIB_PATH)
     names = _declared(header)
-    assert len(names) >= {"epic_gpu.h": 30, "epic_serve.h": 5}.get(header, 2)
+    assert len(names) >= {"epic_gpu.h": 30, "epic_serve.h": 5, "epic_nc.h": 9}.get(header, 2)
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
 
