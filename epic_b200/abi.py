@@ -73,6 +73,8 @@ class EpicCfg(C.Structure):
         ("damping_surface_vorticity", C.c_int32),
         ("damping_scalars", C.c_int32),
         ("damping_surface_scalars", C.c_int32),
+        ("labels", C.c_int32),
+        ("label_seed", C.c_int32),
     ]
 
 
@@ -136,6 +138,8 @@ _SIGNATURES = {
     "set_parcels": [_VP, C.c_int64, _D, _D, _D, _D, _D, _D],
     "get_parcels": [_VP, C.c_int64, _I64, _D, _D, _D, _D, _D, _D],
     "num_parcels": [_VP, _I64],
+    "get_labels": [_VP, C.c_int64, _I64, _I64, _D],
+    "set_labels": [_VP, C.c_int64, _I64, _D],
     "get_parcel_rk": [_VP, C.c_int64, _I64, _D, _D, _D, _D],
     "set_parcel_rk": [_VP, C.c_int64, _D, _D, _D],
     "get_field": [_VP, C.c_int, _D],
@@ -289,6 +293,19 @@ class EpicContext:
         self._call("get_parcels", C.c_int64(n), C.byref(nn), _ptr(out["pos"]), _ptr(out["vor"]),
                    _ptr(out["B"]), _ptr(out["vol"]), _ptr(out["buoy"]), _ptr(out["hum"]))
         return out
+
+    def get_labels(self):
+        """(label int64 (n,), dilution (n,)) of the parcels (cfg.labels = 1)."""
+        n = self.num_parcels()
+        lab, dil = np.empty(n, dtype=np.int64), np.empty(n)
+        nn = C.c_int64()
+        self._call("get_labels", C.c_int64(n), C.byref(nn), lab.ctypes.data_as(_I64), _ptr(dil))
+        return lab, dil
+
+    def set_labels(self, label, dilution):
+        lab = np.ascontiguousarray(label, dtype=np.int64)
+        dil = _f64(dilution, (len(lab),))
+        self._call("set_labels", C.c_int64(len(lab)), lab.ctypes.data_as(_I64), _ptr(dil))
 
     def get_parcel_rk(self) -> dict:
         n = self.num_parcels()

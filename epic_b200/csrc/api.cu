@@ -33,8 +33,24 @@ void grow_store(Ctx& c, long long need) {
         CK(cudaMemcpyAsync(reinterpret_cast<char*>(nv.base) + nv.off(k), reinterpret_cast<char*>(c.pv.base) + c.pv.off(k),
                            es * (size_t)c.n, cudaMemcpyDeviceToDevice, c.stream));
     }
+    long long* nlabel = nullptr;
+    double* ndil = nullptr;
+    if (c.label) {
+        CK(cudaMalloc(&nlabel, sizeof(long long) * (size_t)ncap));
+        CK(cudaMalloc(&ndil, sizeof(double) * (size_t)ncap));
+        CK(cudaMemsetAsync(nlabel, 0, sizeof(long long) * (size_t)ncap, c.stream));
+        CK(cudaMemsetAsync(ndil, 0, sizeof(double) * (size_t)ncap, c.stream));
+        CK(cudaMemcpyAsync(nlabel, c.label, sizeof(long long) * (size_t)c.n, cudaMemcpyDeviceToDevice, c.stream));
+        CK(cudaMemcpyAsync(ndil, c.dil, sizeof(double) * (size_t)c.n, cudaMemcpyDeviceToDevice, c.stream));
+    }
     CK(cudaStreamSynchronize(c.stream));
     CK(cudaFree(c.pv.base));
+    if (c.label) {
+        CK(cudaFree(c.label));
+        CK(cudaFree(c.dil));
+        c.label = nlabel;
+        c.dil = ndil;
+    }
     c.pv = nv;
     c.cap = ncap;
     if (c.pv_alt) {
@@ -242,7 +258,7 @@ static void free_ctx(Ctx& c) {
     c.prof.ev.clear();
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
-                    c.dvor_bar, c.box_start, c.gpack, c.binc};
+                    c.dvor_bar, c.box_start, c.gpack, c.binc, c.label, c.dil};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.scratch) cudaFree(c.scratch);
@@ -308,6 +324,12 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         c.pv.mixed = cfg->precision == EPIC_PRECISION_MIXED;
         CK(cudaMalloc(&c.pv.base, c.store_bytes()));
         CK(cudaMemsetAsync(c.pv.base, 0, c.store_bytes(), c.stream));
+        if (cfg->labels) {
+            CK(cudaMalloc(&c.label, sizeof(long long) * (size_t)c.cap));
+            CK(cudaMalloc(&c.dil, sizeof(double) * (size_t)c.cap));
+            CK(cudaMemsetAsync(c.label, 0, sizeof(long long) * (size_t)c.cap, c.stream));
+            CK(cudaMemsetAsync(c.dil, 0, sizeof(double) * (size_t)c.cap, c.stream));
+        }
         CK(cudaMalloc(&c.fields, sizeof(double) * (size_t)N_FIELDS * P.fsz));
         CK(cudaMemsetAsync(c.fields, 0, sizeof(double) * (size_t)N_FIELDS * P.fsz, c.stream));
         CK(cudaMalloc(&c.nparg, sizeof(int) * P.fsz));
@@ -377,6 +399,10 @@ int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const doub
     c.n = n;
     c.n_box = 0;
     CK(cudaMemsetAsync(c.pv.base, 0, c.store_bytes(), c.stream));
+    if (c.label) {
+        CK(cudaMemsetAsync(c.label, 0, sizeof(long long) * (size_t)c.cap, c.stream));
+        CK(cudaMemsetAsync(c.dil, 0, sizeof(double) * (size_t)c.cap, c.stream));
+    }
     upload_attr(c, pos, 3, A_X);
     upload_attr(c, vor, 3, A_VX);
     upload_attr(c, B, 5, A_B11);
@@ -427,6 +453,30 @@ int epic_gpu_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, do
     download_attr(c, vol, 1, A_VOL);
     download_attr(c, buoy, 1, A_BUOY);
     download_attr(c, hum, 1, A_HUM);
+    API_END
+}
+
+int epic_gpu_get_labels(epic_ctx* ctx, int64_t cap, int64_t* n, int64_t* label, double* dilution) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!c.label) throw CudaError(EPIC_ERR_STATE, "labels are off (cfg.labels = 0)");
+    if (!n) throw CudaError(EPIC_ERR_ARG, "get_labels: null count");
+    *n = c.n;
+    if (cap < c.n) throw CudaError(EPIC_ERR_ARG, "get_labels: capacity too small");
+    if (label) CK(cudaMemcpyAsync(label, c.label, sizeof(long long) * (size_t)c.n, cudaMemcpyDeviceToHost, c.stream));
+    if (dilution) CK(cudaMemcpyAsync(dilution, c.dil, sizeof(double) * (size_t)c.n, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    API_END
+}
+
+int epic_gpu_set_labels(epic_ctx* ctx, int64_t n, const int64_t* label, const double* dilution) {
+    API_BEGIN
+    Ctx& c = ctx->c;
+    if (!c.label) throw CudaError(EPIC_ERR_STATE, "labels are off (cfg.labels = 0)");
+    if (!label || !dilution || n != c.n) throw CudaError(EPIC_ERR_ARG, "set_labels: bad arguments");
+    CK(cudaMemcpyAsync(c.label, label, sizeof(long long) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.dil, dilution, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
     API_END
 }
 
@@ -744,8 +794,18 @@ int epic_gpu_write_parcels_nc(epic_ctx* ctx, const char* path, double t) {
     const int rc = epic_gpu_get_parcels(ctx, n, &m, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(),
                                         hum.data());
     if (rc != EPIC_OK) throw CudaError(rc, c.err);
+    std::vector<int64_t> lab;
+    std::vector<double> dil;
+    if (c.label) {
+        lab.resize(n);
+        dil.resize(n);
+        int64_t ml = 0;
+        const int rl = epic_gpu_get_labels(ctx, n, &ml, lab.data(), dil.data());
+        if (rl != EPIC_OK) throw CudaError(rl, c.err);
+    }
     NC_TRY(ncio::write_parcels(path, ctx_box(c), c.cfg.bndry_zeta_zero, t, n, pos.data(), vor.data(), B.data(),
-                               vol.data(), buoy.data(), hum.data()))
+                               vol.data(), buoy.data(), hum.data(), 0, c.label ? lab.data() : nullptr,
+                               c.label ? dil.data() : nullptr))
     API_END
 }
 
@@ -765,6 +825,15 @@ int epic_gpu_read_parcels_nc(epic_ctx* ctx, const char* path, double* t) {
     const int rc = epic_gpu_set_parcels(ctx, n, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(),
                                         hum.data());
     if (rc != EPIC_OK) throw CudaError(rc, c.err);
+    if (c.label) {
+        // read_chunk resets the labels to the file index and the dilution to 0
+        // (parcel_netcdf.f90:709-716)
+        std::vector<int64_t> lab(n);
+        for (int64_t k = 0; k < n; ++k) lab[k] = k + 1;
+        std::vector<double> dil(n, 0.0);
+        const int rl = epic_gpu_set_labels(ctx, n, lab.data(), dil.data());
+        if (rl != EPIC_OK) throw CudaError(rl, c.err);
+    }
     if (in.has_zeta)   // read_zeta_boundary_flag (parameters.f90:220-250)
         for (int b = 0; b < 2; ++b) {
             c.cfg.bndry_zeta_zero[b] = in.zeta[b];

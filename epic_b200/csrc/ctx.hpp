@@ -111,7 +111,11 @@ struct Ctx {
     bool vectors_kernel = true;   // support vectors by their own kernel before a scatter that recomputes them
     int stage_recwin = 0;         // split-form stage kernel gathers from records staged in shared memory
     bool stage_vectors = false;   // split-form stage kernel computes the next par2grid's support vectors
-    bool p2g_counted = true;      // the last par2grid scatter counted parcels per cell (nparg, nsparg)
+    bool p2g_counted = true;
+    // labels (cfg.labels): label and dilution per parcel, capacity cap
+    long long* label = nullptr;
+    double* dil = nullptr;
+    long long merge_calls = 0;    // merge calls that merged at least one parcel (key of the label draws)      // the last par2grid scatter counted parcels per cell (nparg, nsparg)
     Tables T;
     StepScalars* dsc = nullptr;     // device
     StepScalars* hsc = nullptr;     // pinned host mirror

@@ -38,6 +38,8 @@ struct InitArgs {
     int nb;
     double bub[4][4];
     double zmax;          // nextafter(upper z, lower z)
+    long long* label;     // labels (cfg.labels) or null
+    double* dil;
 };
 
 __global__ void k_init_state(InitArgs A, PView pv) {
@@ -101,6 +103,13 @@ __global__ void k_init_state(InitArgs A, PView pv) {
         pv.set(A_VOL, p, A.vol);
         pv.set(A_BUOY, p, buoy);
         pv.set(A_HUM, p, 0.0);
+        if (A.label) {
+            // parcel_init.f90:135-139
+            const long long nxp = (long long)P.nx * A.npd, nyp = (long long)P.ny * A.npd;
+            A.label[p] = 1 + ((long long)ix * A.npd + (i - 1)) +
+                         nxp * (((long long)iy * A.npd + (j - 1)) + nyp * ((long long)iz * A.npd + (k - 1)));
+            A.dil[p] = 0.0;
+        }
     }
 }
 
@@ -142,6 +151,8 @@ static void launch_init(Ctx& c, const epic_init_spec& s, int npd) {
     for (int b = 0; b < 4; ++b)
         for (int q = 0; q < 4; ++q) A.bub[b][q] = s.bubble[b][q];
     A.zmax = std::nextafter(P.upper[2], P.lower[2]);
+    A.label = c.label;
+    A.dil = c.dil;
     c.n = n;
     c.n_box = 0;
     c.n_parcel_splits = c.n_parcel_merges = c.n_big_close = 0;

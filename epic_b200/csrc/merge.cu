@@ -342,9 +342,31 @@ EPIC_DEV double pdelta(double d, double L, double Li) {
     return d - L * (double)nint_d(d * Li);
 }
 
+// The label draw of the merge (parcel_merge.f90:196, random_number): U[0, 1)
+// from a counter-based SplitMix64 keyed by (label_seed, merge call, merge
+// index m), the same in the oracle.
+EPIC_DEV unsigned long long label_mix(unsigned long long x) {
+    unsigned long long z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+EPIC_DEV double label_draw(int seed, long long call, long long m) {
+    const unsigned long long key = ((unsigned long long)(unsigned)seed * 0x9E3779B97F4A7C15ull) ^
+                                   ((((unsigned long long)call << 32) + (unsigned long long)m) * 16ull + 15ull);
+    return (double)(label_mix(label_mix(key)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+struct MergeLabels {
+    long long* label;   // null: labels off
+    double* dil;
+    int seed;
+    long long call;
+};
+
 // do_group_merge + geometric_merge for one group (parcel_merge.f90:118-361)
 __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int nm, const int* skeys,
-                              const int* svals, const int* ism, unsigned* err) {
+                              const int* svals, const int* ism, MergeLabels L, unsigned* err) {
     MLOOP(ng) {
         int s0 = gstart[i];
         int s1 = (i + 1 < ng) ? gstart[i + 1] : nm;
@@ -355,6 +377,8 @@ __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int
         double pm0 = 0.0, pm1 = 0.0, pm2 = vic * zic;
         double bm = vic * pv.get(A_BUOY, ic), hm = vic * pv.get(A_HUM, ic);
         double wm[3] = {vic * pv.get(A_VX, ic), vic * pv.get(A_VY, ic), vic * pv.get(A_VZ, ic)};
+        long long labm = L.label ? L.label[ic] : 0;
+        double dilm = L.label ? L.dil[ic] : 0.0;
         for (int q = s0; q < s1; ++q) {
             int is = ism[svals[q]];
             double p[3] = {pv.get(A_X, is), pv.get(A_Y, is), pv.get(A_Z, is)};
@@ -364,6 +388,16 @@ __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int
             pv.set(A_X, is, p[0]);
             pv.set(A_Y, is, p[1]);
             double v = pv.get(A_VOL, is);
+            if (L.label) {
+                // parcel_merge.f90:193-203, in m order within the group
+                const double rn = label_draw(L.seed, L.call, svals[q]);
+                if (rn * (vm + v) < vm) {
+                    dilm = dilm + log(vm / (vm + v));
+                } else {
+                    labm = L.label[is];
+                    dilm = L.dil[is] + log(v / (vm + v));
+                }
+            }
             vm = vm + v;
             double dx = pdelta(p[0] - x0, P.extent[0], P.extenti[0]);
             double dy = pdelta(p[1] - y0, P.extent[1], P.extenti[1]);
@@ -432,6 +466,10 @@ __global__ void k_group_merge(Params P, PView pv, const int* gstart, int ng, int
         pv.set(A_HUM, ic, hm);
         for (int k = 0; k < 3; ++k) pv.set(A_VX + k, ic, wm[k]);
         for (int k = 0; k < 5; ++k) pv.set(A_B11 + k, ic, Bm[k] * factor);
+        if (L.label) {
+            L.label[ic] = labm;
+            L.dil[ic] = dilm;
+        }
     }
 }
 
@@ -449,6 +487,14 @@ __global__ void k_move(PView pv, const int* holes, const int* srcs, int nh, int 
         int dst = holes[h];
         int src = newN + srcs[nh - 1 - h];
         pv.set(a, dst, pv.get(a, src));
+    }
+}
+
+__global__ void k_move_labels(long long* label, double* dil, const int* holes, const int* srcs, int nh, int newN) {
+    MLOOP(nh) {
+        const int dst = holes[i], src = newN + srcs[nh - 1 - i];
+        label[dst] = label[src];
+        dil[dst] = dil[src];
     }
 }
 
@@ -655,6 +701,7 @@ long long parcel_merge(Ctx& c) {
         CKL();
         return 0;
     }
+    const long long call = c.merge_calls++;
     int* ism = ar.take<int>(nm);
     int* icl = ar.take<int>(nm);
     k_pack_pairs<<<g, MB, 0, st>>>(Ls, iclo, nls, dom, dpos, ism, icl);
@@ -694,7 +741,8 @@ long long parcel_merge(Ctx& c) {
         CK(cub::DeviceSelect::Flagged(ctmp, b, gidx, head, gstart, dcount, nm, st));
     }
     const int ng = read_int(c, dcount);
-    k_group_merge<<<mgrid(ng), MB, 0, st>>>(P, c.pv, gstart, ng, nm, gk, gv, ism, err);
+    const MergeLabels ML{c.label, c.dil, c.cfg.label_seed, call};
+    k_group_merge<<<mgrid(ng), MB, 0, st>>>(P, c.pv, gstart, ng, nm, gk, gv, ism, ML, err);
     CKL();
 
     // parcel_delete
@@ -724,6 +772,10 @@ long long parcel_merge(Ctx& c) {
         CK(cub::DeviceSelect::Flagged(ctmp, b, sidx, sf, srcs, dcount + 1, N - newN, st));
         k_move<<<mgrid((long long)nh * N_ATTR), MB, 0, st>>>(c.pv, holes, srcs, nh, newN);
         CKL();
+        if (c.label) {
+            k_move_labels<<<mgrid(nh), MB, 0, st>>>(c.label, c.dil, holes, srcs, nh, newN);
+            CKL();
+        }
     }
     unsigned long long hb = 0;
     CK(cudaMemcpyAsync(&hb, bigc, sizeof(hb), cudaMemcpyDeviceToHost, st));

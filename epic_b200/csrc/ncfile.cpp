@@ -248,6 +248,8 @@ void write_file(const std::string& path, Header& h, int force_version) {
                     put_be(&be[8 * k], u, 8);
                 } else if (v.type == T_INT) {
                     put_be(&be[4 * k], (uint32_t)(int32_t)std::llround(buf[k]), 4);
+                } else if (v.type == T_INT64) {
+                    put_be(&be[8 * k], (uint64_t)(int64_t)std::llround(buf[k]), 8);
                 } else {
                     throw Error("netCDF: the writer supports int and double variables");
                 }
@@ -522,7 +524,8 @@ Info info(const std::string& path) {
 
 void write_parcels(const std::string& path, const Box& box, const int32_t zeta[2], double t, int64_t n,
                    const double* pos, const double* vor, const double* B, const double* vol,
-                   const double* buoy, const double* hum, int force_version) {
+                   const double* buoy, const double* hum, int force_version, const int64_t* label,
+                   const double* dil) {
     if (n < 0 || (n > 0 && (!pos || !vor || !B || !vol || !buoy))) throw Error("netCDF: bad parcel arrays");
     // a dimension of length 0 is the record dimension in the classic format
     if (n == 0) throw Error("netCDF: a parcel file needs at least one parcel");
@@ -560,6 +563,16 @@ void write_parcels(const std::string& path, const Box& box, const int32_t zeta[2
                                  "", "1/s", T_DOUBLE, pd, comp(vor, 3, c)));
     h.vars.push_back(dataset("buoyancy", "parcel buoyancy", "", "m/s^2", T_DOUBLE, pd, comp(buoy, 1, 0)));
     h.vars.push_back(dataset("humidity", "parcel humidity", "", "1", T_DOUBLE, pd, hum ? comp(hum, 1, 0) : zeros));
+    if (label) {
+        // parcel_netcdf.f90:971-982; 64-bit integers need CDF-5
+        h.vars.push_back(dataset("label", "parcel label", "", "1", T_INT64, pd,
+                                 [label](int64_t s, int64_t m, double* b) {
+                                     for (int64_t k = 0; k < m; ++k) b[k] = (double)label[s + k];
+                                 }));
+        h.vars.push_back(dataset("dilution", "parcel log dilution", "", "1", T_DOUBLE, pd,
+                                 dil ? comp(dil, 1, 0) : zeros));
+        force_version = 5;
+    }
     write_file(path, h, force_version);
 }
 
@@ -638,6 +651,17 @@ void write_fields(const std::string& path, const Box& box, const int32_t zeta[2]
         h.vars.push_back(dataset(fo.name, fo.long_name, "", fo.unit, fo.integer ? T_INT : T_DOUBLE, {3, 2, 1, 0}, src));
     }
     write_file(path, h, force_version);
+}
+
+int64_t read_variable(const std::string& path, const std::string& name, int64_t record, int64_t cap, double* out) {
+    Reader rd(path);
+    const Var* v = rd.var(name);
+    if (!v) throw Error("netCDF: no variable " + name + " in " + path);
+    const int64_t n = slab_elems(rd.h, *v);
+    if (!out) return n;
+    if (n > cap) throw Error("netCDF: " + name + " has more elements than the buffer holds");
+    rd.read(*v, record, 0, n, out);
+    return n;
 }
 
 bool read_field(const std::string& path, const std::string& name, int64_t step, const Box& expect, double* out) {
@@ -768,4 +792,15 @@ extern "C" int epic_nc_write_field_file(const char* path, const int32_t ncells[3
         }
         ncio::write_fields(path, make_box(ncells, origin, extent), zeta_flags, t, out);
     });
+}
+
+extern "C" int epic_nc_read_variable(const char* path, const char* name, int64_t record, int64_t cap, int64_t* n,
+                                     double* out) {
+    int64_t m = 0;
+    const int rc = nc_call([&] {
+        if (!path || !name) throw ncio::Error("netCDF: null argument");
+        m = ncio::read_variable(path, name, record, cap, out);
+    });
+    if (n) *n = m;
+    return rc;
 }

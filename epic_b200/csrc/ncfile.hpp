@@ -46,9 +46,12 @@ Info info(const std::string& path);
 void check_box(const Box& got, const Box& want, const std::string& path);
 
 // pos, vor: (3, n) interleaved per parcel; B: (5, n); vol, buoy, hum: (n).
+// label, dil (may be null): the ENABLE_LABELS attributes, written as NC_INT64
+// (which makes the file CDF-5) and NC_DOUBLE; labels below 2^53.
 void write_parcels(const std::string& path, const Box& box, const int32_t zeta[2], double t, int64_t n,
                    const double* pos, const double* vor, const double* B, const double* vol,
-                   const double* buoy, const double* hum, int force_version = 0);
+                   const double* buoy, const double* hum, int force_version = 0,
+                   const int64_t* label = nullptr, const double* dil = nullptr);
 
 // Reads the first record (the reference writes one record per parcel file,
 // read_chunk in parcel_netcdf.f90 reads record 1).  vor, buoy, hum that the
@@ -71,5 +74,10 @@ void write_fields(const std::string& path, const Box& box, const int32_t zeta[2]
 // field layout, rows 0 .. nz; other rows are left as they are.  Returns false
 // if the file has no such variable.
 bool read_field(const std::string& path, const std::string& name, int64_t step, const Box& expect, double* out);
+
+// Record `record` (ignored for a fixed-size variable) of any numeric
+// variable, converted to double, in C order; returns its element count and
+// writes it to out when it fits cap.
+int64_t read_variable(const std::string& path, const std::string& name, int64_t record, int64_t cap, double* out);
 
 }  // namespace ncio

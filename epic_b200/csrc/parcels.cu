@@ -693,7 +693,8 @@ __global__ void k_split_flag(Params P, PView pv, long long n, int* flag, unsigne
     }
 }
 
-__global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, const int* offs, unsigned* err) {
+__global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, const int* offs, long long* label,
+                              double* dil, unsigned* err) {
     const double dh = 0.5 * 0.7745966692414834;   // f12 * sqrt(3/5)
     PLOOP(n) {
         if (!flag[i]) continue;
@@ -741,6 +742,10 @@ __global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, 
         pv.set(A_VOL, i, hv);
         pv.set(A_BUOY, m, pv.get(A_BUOY, i));
         pv.set(A_HUM, m, pv.get(A_HUM, i));
+        if (label) {   // parcel_split.f90:147-150
+            label[m] = label[i];
+            dil[m] = dil[i];
+        }
     }
 }
 
@@ -766,7 +771,7 @@ long long parcel_split(Ctx& c) {
     if (ns == 0) return 0;
     // parcel_split.f90:91-94: a full container grows to grow_factor x the parcels needed
     if (n + ns > c.cap) grow_store(c, n + ns);
-    k_split_apply<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, flag, offs, &c.dsc->err);
+    k_split_apply<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, flag, offs, c.label, c.dil, &c.dsc->err);
     CKL();
     c.n = n + ns;
     c.n_parcel_splits += ns;

@@ -1256,6 +1256,18 @@ void sort_parcels(Ctx& c) {
             }
         }
     }
+    if (c.label) {
+        // labels and dilutions follow the permutation through the key arrays
+        // (free again after k_box_start; k0 and k1 hold >= 8 n bytes)
+        long long* tl = reinterpret_cast<long long*>(k0);
+        k_gather_slot<long long><<<pgrid(n), PB, 0, c.stream>>>(c.label, tl, n, i1);
+        CKL();
+        CK(cudaMemcpyAsync(c.label, tl, sizeof(long long) * n, cudaMemcpyDeviceToDevice, c.stream));
+        double* td = reinterpret_cast<double*>(k0);
+        k_gather_slot<double><<<pgrid(n), PB, 0, c.stream>>>(c.dil, td, n, i1);
+        CKL();
+        CK(cudaMemcpyAsync(c.dil, td, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.stream));
+    }
     c.n_box = n;
 }
 

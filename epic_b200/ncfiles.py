@@ -29,8 +29,9 @@ class NcFiles:
         L.epic_nc_read_field.argtypes = [C.c_char_p, C.c_char_p, C.c_int64, _I32, _D, _D, _D]
         L.epic_nc_write_field_file.argtypes = [C.c_char_p, _I32, _D, _D, _I32, C.c_double, C.c_int,
                                                C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.POINTER(_D)]
+        L.epic_nc_read_variable.argtypes = [C.c_char_p, C.c_char_p, C.c_int64, C.c_int64, _I64, _D]
         for f in (L.epic_nc_info, L.epic_nc_write_parcels, L.epic_nc_read_parcels, L.epic_nc_read_field,
-                  L.epic_nc_write_field_file):
+                  L.epic_nc_write_field_file, L.epic_nc_read_variable):
             f.restype = C.c_int
 
     def _check(self, rc, name):
@@ -88,6 +89,16 @@ class NcFiles:
         self._check(self.lib.epic_nc_write_field_file(os.fsencode(path), nc.ctypes.data_as(_I32), _ptr(og), _ptr(ex),
                                                       z.ctypes.data_as(_I32), C.c_double(t), C.c_int(len(names)),
                                                       cn, cu, cd), "epic_nc_write_field_file")
+
+    def read_variable(self, path, name, record=0) -> np.ndarray:
+        """Any numeric variable (one record) as a flat float64 array."""
+        n = C.c_int64()
+        self._check(self.lib.epic_nc_read_variable(os.fsencode(path), name.encode(), C.c_int64(record), C.c_int64(0),
+                                                   C.byref(n), None), "epic_nc_read_variable")
+        out = np.empty(n.value)
+        self._check(self.lib.epic_nc_read_variable(os.fsencode(path), name.encode(), C.c_int64(record),
+                                                   C.c_int64(n.value), C.byref(n), _ptr(out)), "epic_nc_read_variable")
+        return out
 
     def read_field(self, path, name, ncells, origin, extent, step=-1) -> np.ndarray:
         nc, og, ex = self._box(ncells, origin, extent)

@@ -31,6 +31,7 @@ module epic_gpu_iface
         real(c_double)     :: damping_vorticity_prefactor, damping_scalars_prefactor
         integer(c_int32_t) :: damping_vorticity, damping_surface_vorticity
         integer(c_int32_t) :: damping_scalars, damping_surface_scalars
+        integer(c_int32_t) :: labels, label_seed
     end type epic_cfg
 
     type, bind(C) :: epic_step_info

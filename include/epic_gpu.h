@@ -106,6 +106,11 @@ typedef struct epic_cfg {
     int32_t damping_surface_vorticity;     /* 0                              */
     int32_t damping_scalars;               /* 0                              */
     int32_t damping_surface_scalars;       /* 0                              */
+    /* labels (the reference's ENABLE_LABELS build): a 64-bit label and a
+       dilution per parcel, set at initialisation, copied by split and chosen
+       at random, weighted by volume, in merge (parcel_merge.f90:181-203) */
+    int32_t labels;                        /* 0: off                          */
+    int32_t label_seed;                    /* key of the merge's random draws */
 } epic_cfg;
 
 /* Per-step report (epic3d.f90:135-153 plus the statistics the reference
@@ -142,6 +147,12 @@ int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const doub
 int epic_gpu_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, double* vor,
                          double* B, double* vol, double* buoy, double* hum);
 int epic_gpu_num_parcels(epic_ctx* ctx, int64_t* n);
+/* Labels and dilutions of the parcels (cfg.labels = 1; EPIC_ERR_STATE
+ * otherwise), in the order of epic_gpu_get_parcels.  set_parcels zeroes them;
+ * the initial states set label = 1 + the regular-position index of
+ * init_regular_positions and dilution = 0 (parcel_init.f90:135-139). */
+int epic_gpu_get_labels(epic_ctx* ctx, int64_t cap, int64_t* n, int64_t* label, double* dilution);
+int epic_gpu_set_labels(epic_ctx* ctx, int64_t n, const int64_t* label, const double* dilution);
 
 /* Initial states generated on the device (no host arrays), the parcels of
  * init_regular_positions / parcel_default (parcel_init.f90:31-152):

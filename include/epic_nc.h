@@ -49,6 +49,11 @@ int epic_nc_read_parcels(const char* path, int64_t cap, int64_t* n, double* pos,
 int epic_nc_read_field(const char* path, const char* name, int64_t step, const int32_t ncells[3],
                        const double origin[3], const double extent[3], double* out);
 
+/* Record `record` (0-based; ignored for a fixed-size variable) of any numeric
+ * variable, converted to double in C order; *n = its element count
+ * (out NULL: the count only; EPIC_ERR_IO if it exceeds cap). */
+int epic_nc_read_variable(const char* path, const char* name, int64_t record, int64_t cap, int64_t* n,
+                          double* out);
 /* A field file of nfields FP64 fields (names[k], units[k] or NULL for "1"),
  * each in the layout of epic_gpu_set_field (rows 0 .. nz are written), e.g.
  * the vorticity, buoyancy and humidity of an initial state. */

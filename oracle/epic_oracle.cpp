@@ -47,6 +47,10 @@ struct Ctx {
     std::vector<double> pos, vor, B, vol, buoy, hum;     // (3,n) (3,n) (5,n) (n) (n) (n)
     std::vector<double> dpos, dvor, strain, dB;          // (3,n) (3,n) (8,n) (5,n)
     std::vector<double> Vetas, Vtaus;                    // (3,n) (3,n)
+    // labels (ENABLE_LABELS, parcel_container.f90:41-57): cfg.labels = 1
+    std::vector<int64_t> label;
+    std::vector<double> dil;
+    long merge_calls = 0;
     // fields (fields.f90:21-51): (nz+3) x ny x nx, z fastest, x slowest
     long nzh, fsz;
     std::vector<double> velog[3], vortg[3], vtend[3], velgradg[8];
@@ -1329,6 +1333,28 @@ void ensure_parcel_capacity(Ctx& c, long need) {
     c.vol.resize(cap); c.buoy.resize(cap); c.hum.resize(cap);
     c.dpos.resize(3 * cap); c.dvor.resize(3 * cap); c.strain.resize(8 * cap); c.dB.resize(5 * cap);
     c.Vetas.resize(3 * cap); c.Vtaus.resize(3 * cap);
+    if (c.cfg.labels) { c.label.resize(cap); c.dil.resize(cap); }
+}
+
+// The merge's label draw (parcel_merge.f90:196, random_number): U[0, 1) from
+// a counter-based SplitMix64 keyed by (label_seed, merge call, merge index m)
+// instead of the Fortran generator's stream; the same law of choice.
+static uint64_t lab_mix(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static double label_draw(int32_t seed, long call, long m) {
+    uint64_t key = ((uint64_t)(uint32_t)seed * 0x9E3779B97F4A7C15ull) ^ ((((uint64_t)call << 32) + (uint64_t)m) * 16ull + 15ull);
+    return (double)(lab_mix(lab_mix(key)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// parcel_init.f90:135-139: label of the regular position (sub-cell i, j, k
+// 1-based, cell ix, iy, iz 0-based)
+static int64_t regular_label(const Ctx& c, int npd, int ix, int iy, int iz, int i, int j, int k) {
+    const int64_t nxp = (int64_t)c.nx * npd, nyp = (int64_t)c.ny * npd;
+    return 1 + ((int64_t)ix * npd + (i - 1)) + nxp * (((int64_t)iy * npd + (j - 1)) + nyp * ((int64_t)iz * npd + (k - 1)));
 }
 
 void rk_substep(Ctx& c, double dt, int step) {
@@ -1420,6 +1446,7 @@ long parcel_split(Ctx& c) {
         c.vol[m] = c.vol[n];
         c.buoy[m] = c.buoy[n];
         c.hum[m] = c.hum[n];
+        if (c.cfg.labels) { c.label[m] = c.label[n]; c.dil[m] = c.dil[n]; }   // parcel_split.f90:147-150
         double s = dh * std::sqrt(D[0]);
         double v1[3] = {V[0] * s, V[1] * s, V[2] * s};
         for (int k = 0; k < 3; ++k) {
@@ -1691,6 +1718,9 @@ long parcel_merge(Ctx& c) {
     // do_group_merge (parcel_merge.f90:118-323), 0-based parcel indices
     std::vector<long> loca(N + 1, 0);
     std::vector<double> x0, y0, vm, posm, buoym, humm, vortm, Bm;
+    std::vector<int64_t> labelm;
+    std::vector<double> dilm;
+    const long call = c.merge_calls++;
     auto delx_p = [&](double x1, double x2) {                  // parcel_ops.f90:17-37
         double d = x1 - x2;
         return d - c.extent[0] * (double)fnint(d * c.extenti[0]);
@@ -1714,8 +1744,19 @@ long parcel_merge(Ctx& c) {
             humm.push_back(c.vol[ic] * c.hum[ic]);
             for (int k = 0; k < 3; ++k) vortm.push_back(c.vol[ic] * c.vor[3 * ic + k]);
             for (int k = 0; k < 6; ++k) Bm.push_back(0.0);
+            if (c.cfg.labels) { labelm.push_back(c.label[ic]); dilm.push_back(c.dil[ic]); }
         }
         long g = loca[ic + 1] - 1;
+        if (c.cfg.labels) {
+            // parcel_merge.f90:193-203
+            const double rn = label_draw(c.cfg.label_seed, call, m);
+            if (rn * (vm[g] + c.vol[is]) < vm[g]) {
+                dilm[g] = dilm[g] + std::log(vm[g] / (vm[g] + c.vol[is]));
+            } else {
+                labelm[g] = c.label[is];
+                dilm[g] = c.dil[is] + std::log(c.vol[is] / (vm[g] + c.vol[is]));
+            }
+        }
         vm[g] = vm[g] + c.vol[is];
         double dx_ = delx_p(P[3 * is], x0[g]);
         double dy_ = dely_p(P[3 * is + 1], y0[g]);
@@ -1764,6 +1805,7 @@ long parcel_merge(Ctx& c) {
             c.buoy[ic] = buoym[g];
             c.hum[ic] = humm[g];
             for (int k = 0; k < 3; ++k) c.vor[3 * ic + k] = vortm[3 * g + k];
+            if (c.cfg.labels) { c.label[ic] = labelm[g]; c.dil[ic] = dilm[g]; }
         }
         long g = loca[ic + 1] - 1;
         double vmerge = one / vm[g];
@@ -1817,6 +1859,7 @@ long parcel_merge(Ctx& c) {
             for (int q = 0; q < 5; ++q) { c.B[5 * d + q] = c.B[5 * s + q]; c.dB[5 * d + q] = c.dB[5 * s + q]; }
             for (int q = 0; q < 8; ++q) c.strain[8 * d + q] = c.strain[8 * s + q];
             c.vol[d] = c.vol[s]; c.buoy[d] = c.buoy[s]; c.hum[d] = c.hum[s];
+            if (c.cfg.labels) { c.label[d] = c.label[s]; c.dil[d] = c.dil[s]; }
         };
         while (mm <= k) {
             replace(pid[mm], lv);
@@ -1925,6 +1968,31 @@ int epic_oracle_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const d
     std::fill(c.dvor.begin(), c.dvor.end(), 0.0);
     std::fill(c.dB.begin(), c.dB.end(), 0.0);
     std::fill(c.strain.begin(), c.strain.end(), 0.0);
+    if (c.cfg.labels) {
+        std::fill(c.label.begin(), c.label.end(), (int64_t)0);
+        std::fill(c.dil.begin(), c.dil.end(), 0.0);
+    }
+    return EPIC_OK;
+}
+
+int epic_oracle_get_labels(epic_ctx* ctx, int64_t cap, int64_t* n, int64_t* label, double* dilution) {
+    if (!ctx || !n) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (!c.cfg.labels) { c.err = "labels are off (cfg.labels = 0)"; return EPIC_ERR_STATE; }
+    *n = c.n;
+    if (cap < c.n) { c.err = "get_labels: capacity too small"; return EPIC_ERR_ARG; }
+    if (label) std::memcpy(label, c.label.data(), sizeof(int64_t) * c.n);
+    if (dilution) std::memcpy(dilution, c.dil.data(), sizeof(double) * c.n);
+    return EPIC_OK;
+}
+
+int epic_oracle_set_labels(epic_ctx* ctx, int64_t n, const int64_t* label, const double* dilution) {
+    if (!ctx || !label || !dilution) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (!c.cfg.labels) { c.err = "labels are off (cfg.labels = 0)"; return EPIC_ERR_STATE; }
+    if (n != c.n) { c.err = "set_labels: n differs from the number of parcels"; return EPIC_ERR_ARG; }
+    std::memcpy(c.label.data(), label, sizeof(int64_t) * n);
+    std::memcpy(c.dil.data(), dilution, sizeof(double) * n);
     return EPIC_OK;
 }
 
@@ -1997,7 +2065,17 @@ int epic_oracle_init_state(epic_ctx* ctx, const epic_init_spec* s) {
         vol[p] = v;
     }
     c.n_parcel_splits = c.n_parcel_merges = c.n_big_close = 0;
-    return epic_oracle_set_parcels(ctx, n, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(), hum.data());
+    int rc = epic_oracle_set_parcels(ctx, n, pos.data(), vor.data(), B.data(), vol.data(), buoy.data(), hum.data());
+    if (rc == EPIC_OK && c.cfg.labels)
+        for (long p = 0; p < n; ++p) {
+            long q = p;
+            int sub[3];
+            for (int k = 0; k < 3; ++k) { sub[k] = (int)(q % npd) + 1; q /= npd; }
+            const int ix = (int)(q % c.nx); q /= c.nx;
+            const int iy = (int)(q % c.ny); q /= c.ny;
+            c.label[p] = regular_label(c, npd, ix, iy, (int)q, sub[0], sub[1], sub[2]);
+        }
+    return rc;
 }
 
 // The start of a run from a field file (utils.f90:223-234): parcel_default
@@ -2041,6 +2119,15 @@ int epic_oracle_init_from_grids(epic_ctx* ctx, const double* vortg, const double
     int rc = epic_oracle_set_parcels(ctx, n, pos.data(), zero3.data(), B.data(), vol.data(), zero1.data(),
                                      zero1.data());
     if (rc != EPIC_OK) return rc;
+    if (c.cfg.labels) {
+        long q = 0;
+        for (int iz = 0; iz < c.nz; ++iz)
+            for (int iy = 0; iy < c.ny; ++iy)
+                for (int ix = 0; ix < c.nx; ++ix)
+                    for (int k = 1; k <= npd; ++k)
+                        for (int j = 1; j <= npd; ++j)
+                            for (int i = 1; i <= npd; ++i) c.label[q++] = regular_label(c, npd, ix, iy, iz, i, j, k);
+    }
     // init_refine: split until parcel 1 is less elongated than lambda_max
     while (lam >= c.cfg.lambda_max) {
         parcel_split(c);
