@@ -116,6 +116,26 @@ module epic_gpu_iface
             integer(c_int), value  :: field_id
             real(c_double)         :: out(*)
         end function
+        ! labels (cfg%labels = 1): parcels%label, parcels%dilution
+        integer(c_int) function epic_gpu_get_labels(ctx, cap, n, label, dilution) &
+                bind(C, name="epic_gpu_get_labels")
+            import :: c_int, c_int64_t, c_ptr, c_double
+            type(c_ptr), value            :: ctx
+            integer(c_int64_t), value     :: cap
+            integer(c_int64_t)            :: n
+            integer(c_int64_t)            :: label(*)
+            real(c_double)                :: dilution(*)
+        end function
+
+        integer(c_int) function epic_gpu_set_labels(ctx, n, label, dilution) &
+                bind(C, name="epic_gpu_set_labels")
+            import :: c_int, c_int64_t, c_ptr, c_double
+            type(c_ptr), value            :: ctx
+            integer(c_int64_t), value     :: n
+            integer(c_int64_t), intent(in) :: label(*)
+            real(c_double), intent(in)    :: dilution(*)
+        end function
+
         ! parcel and field files in the reference's netCDF layout (epic_nc.h):
         ! write_netcdf_parcels / read_netcdf_parcels (restart) /
         ! write_netcdf_fields / read_netcdf_fields + init_parcels_from_grids;
