@@ -26,6 +26,9 @@ EPIC_DEV void cross3(const T* a, const T* b, T* c) {
     c[2] = O::sub(O::mul(a[0], b[1]), O::mul(a[1], b[0]));
 }
 
+EPIC_DEV float rsq(float v) { return rsqrtf(v); }
+EPIC_DEV double rsq(double v) { return rsqrt(v); }
+
 template <class T>
 EPIC_DEV T signum_d(T v) { return v == T(0) ? T(0) : copysign(T(1), v); }
 
@@ -66,6 +69,14 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
 #pragma unroll
         for (int it = 0; it < 3; ++it) y = y - (y * (4.0 * y * y - 3.0) - smp) * idf;
         cal = y;
+    } else if constexpr (std::is_same<O, F32Ops>::value) {
+        // the FP32 form: (3/j2)^1.5 as q sqrt(q), single-precision acos / cos
+        const float q = 3.0f / j2;
+        smp = 0.5f * j3 * (q * sqrtf(q));
+        smp = fminf(fmaxf(-1.0f, smp), 1.0f);
+        float alpha = acosf(smp) * (1.0f / 3.0f);
+        if (alpha > (float)(pi / 6.0)) alpha += (float)(2.0 * pi / 3.0);
+        cal = cosf(alpha);
     } else {
         smp = O::mul(O::mul(T(0.5), j3), pow(T(3) / j2, T(1.5)));
         smp = fmin(fmax(T(-1), smp), T(1));
@@ -79,13 +90,13 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
     r[6] = A[6];                 r[7] = A[7];                 r[8] = O::sub(A[8], eta[0]);
     int i = 0;
     T s1[3];
-    if constexpr (std::is_same<O, FastOps>::value) {
+    if constexpr (std::is_same<O, FastOps>::value || std::is_same<O, F32Ops>::value) {
         // the longest column by squared norms, normalised by a reciprocal square root
         const T q0 = dot3<O>(&r[0], &r[0]), q1 = dot3<O>(&r[3], &r[3]), q2 = dot3<O>(&r[6], &r[6]);
         T qm = q0;
         if (q1 > qm) { i = 1; qm = q1; }
         if (q2 > qm) { i = 2; qm = q2; }
-        const T ir = rsqrt(qm);
+        const T ir = rsq(qm);
 #pragma unroll
         for (int k = 0; k < 3; ++k) s1[k] = (i == 0 ? r[k] : i == 1 ? r[3 + k] : r[6 + k]) * ir;
     } else {
@@ -108,10 +119,10 @@ EPIC_DEV void sz_evaluate(T* A, T* r, T* eta, T* D) {
         r[6 + k] = O::sub(r[6 + k], O::mul(smp, r[k]));
     }
     T s2[3];
-    if constexpr (std::is_same<O, FastOps>::value) {
+    if constexpr (std::is_same<O, FastOps>::value || std::is_same<O, F32Ops>::value) {
         const T q1 = dot3<O>(&r[3], &r[3]), q2 = dot3<O>(&r[6], &r[6]);
         const int j = (q2 > q1) ? 2 : 1;
-        const T ir = rsqrt(j == 2 ? q2 : q1);
+        const T ir = rsq(j == 2 ? q2 : q1);
 #pragma unroll
         for (int k = 0; k < 3; ++k) s2[k] = (j == 2 ? r[6 + k] : r[3 + k]) * ir;
     } else {
@@ -188,17 +199,17 @@ EPIC_DEV void sz_diagonalise(T* A, T* D, T* V) {
             for (int row = 0; row < 3; ++row)
                 Ar[row + 3 * c] = O::add(O::add(O::mul(A[row], r[3 * c]), O::mul(A[row + 3], r[3 * c + 1])),
                                          O::mul(A[row + 6], r[3 * c + 2]));
-        if constexpr (std::is_same<O, FastOps>::value) {
+        if constexpr (std::is_same<O, FastOps>::value || std::is_same<O, F32Ops>::value) {
             // normalisations by reciprocal square roots
             const T q0 = dot3<O>(&Ar[0], &Ar[0]), q1 = dot3<O>(&Ar[3], &Ar[3]);
             const int i = (q1 > q0) ? 1 : 0;
-            const T il = rsqrt(i ? q1 : q0);
+            const T il = rsq(i ? q1 : q0);
 #pragma unroll
             for (int k = 0; k < 3; ++k) V[6 + k] = (i ? Ar[3 + k] : Ar[k]) * il;
             cross3<O>(&V[6], &V[0], &V[3]);
             cross3<O>(&V[0], &V[3], &V[6]);
-            const T n0 = rsqrt(dot3<O>(&V[0], &V[0])), n1 = rsqrt(dot3<O>(&V[3], &V[3]));
-            const T n2 = rsqrt(dot3<O>(&V[6], &V[6]));
+            const T n0 = rsq(dot3<O>(&V[0], &V[0])), n1 = rsq(dot3<O>(&V[3], &V[3]));
+            const T n2 = rsq(dot3<O>(&V[6], &V[6]));
 #pragma unroll
             for (int k = 0; k < 3; ++k) { V[k] *= n0; V[3 + k] *= n1; V[6 + k] *= n2; }
         } else {
