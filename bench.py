@@ -374,15 +374,53 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
+    ctx.close()
+    if mixed and rank == 0 and not args.no_error:
+        line["error"] = mixed_error(lib)
     if rank == 0:
         print(json.dumps(line))
-    ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------
+def mixed_error(lib, steps: int = 100, dt: float = 0.05) -> dict:
+    """Errors of the mixed form against the plain FP64 form from the same
+    seeded state (the rising thermal on 32^3, 262,144 parcels, merge / split /
+    corrections on): relative drift of kinetic energy and enstrophy
+    (parcel_diagnostics.f90:139-143) after `steps` steps at a fixed dt, and the
+    relative L2 and Linf errors of the gridded velocity, vorticity and
+    buoyancy (par2grid + vor2vel of the final parcels).  The step is fixed so
+    that both runs compare the same times."""
+    from epic_b200 import initial, make_context_device, abi
+    spec = initial.device_spec("thermal-32")
+    runs = {}
+    for prec in (0, 1):
+        c = make_context_device(spec, lib, precision=prec, keep_order=0, use_fixed_dt=1, fixed_dt=dt)
+        t = 0.0
+        for _ in range(steps):
+            t, info = c.step(t)
+        c.par2grid(False)
+        c.vor2vel()
+        f = {"velocity": np.stack([c.get_field(abi.VELOG[k])[:, :, 1:-1] for k in range(3)]),
+             "vorticity": np.stack([c.get_field(abi.VORTG[k])[:, :, 1:-1] for k in range(3)]),
+             "buoyancy": c.get_field(abi.TBUOYG)[:, :, 1:-1]}
+        runs[prec] = (info.parcel_stats[1], info.parcel_stats[12], f, info.n_parcels)
+        c.close()
+    ke0, en0, f0, n0 = runs[0]
+    ke1, en1, f1, n1 = runs[1]
+    out = {"workload": f"thermal 32^3, {steps} steps at fixed dt {dt}, mixed vs plain FP64 from the same seed",
+           "ke_rel_drift": abs(ke1 - ke0) / abs(ke0), "enstrophy_rel_drift": abs(en1 - en0) / abs(en0),
+           "parcels": [int(n0), int(n1)], "target": 1e-5}
+    for k in f0:
+        a, b = f1[k], f0[k]
+        out[k + "_l2_rel"] = float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+        out[k + "_linf_rel"] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    out["within_target"] = bool(out["ke_rel_drift"] < 1e-5 and out["enstrophy_rel_drift"] < 1e-5)
+    return out
+
+
 def served_requests(args, lib):
     """The served ensemble: requests with seeded Poisson arrivals, grids drawn
     uniformly from {32^3, 48^3, 64^3, 96x96x48}, a Beltrami (k, l, m in {1, 2})
@@ -463,6 +501,8 @@ def run_served(args):
                 "initial states generated on the device; results (diagnostics) read back"},
         "wall_s": wall, "span_s": span, "parcel_steps": ps,
     }
+    if rank == 0 and not args.no_error:
+        line["error"] = mixed_error(lib)
     if rank == 0:
         print(json.dumps(line))
 
@@ -557,6 +597,8 @@ def main():
                     help="generate the initial parcels on the device (always for thermal2-512x512x256)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-error", action="store_true",
+                    help="mixed and served forms: skip the error report against the plain FP64 form")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
