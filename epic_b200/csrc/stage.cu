@@ -300,6 +300,23 @@ EPIC_DEV int wrap_to(int l, int n) { return ((unsigned)l < (unsigned)n) ? l : wr
 // the corners visited once (sum_p w_p f = (sum_p w_p) f; only the rounding
 // order differs from visiting each point).
 EPIC_DEV bool same_cell(const Tri& a, const Tri& b) { return a.is == b.is && a.js == b.js && a.ks == b.ks; }
+// Whether point p lies in t's cell, and if so adds its trilinear weights to
+// t's (the arithmetic of trilinear() followed by add_weights(), without a
+// second Tri held in registers).
+EPIC_DEV bool merge_into(const Params& P, const double* p, Tri& t) {
+    const double x = (p[0] - P.lower[0]) * P.dxi[0];
+    const double y = (p[1] - P.lower[1]) * P.dxi[1];
+    const double z = (p[2] - P.lower[2]) * P.dxi[2];
+    const int is = (int)floor(x), js = (int)floor(y), ks = (int)floor(z);
+    if (is != t.is || js != t.js || ks != t.ks) return false;
+    const double px = x - (double)is, pxc = 1.0 - px;
+    const double py = y - (double)js, pyc = 1.0 - py;
+    const double pz = z - (double)ks, pzc = 1.0 - pz;
+    const double w00 = pyc * pxc, w10 = pyc * px, w01 = py * pxc, w11 = py * px;
+    t.w[0][0][0] += pzc * w00; t.w[0][0][1] += pzc * w10; t.w[0][1][0] += pzc * w01; t.w[0][1][1] += pzc * w11;
+    t.w[1][0][0] += pz * w00;  t.w[1][0][1] += pz * w10;  t.w[1][1][0] += pz * w01;  t.w[1][1][1] += pz * w11;
+    return true;
+}
 EPIC_DEV void add_weights(Tri& a, const Tri& b) {
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk)
@@ -509,12 +526,9 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         Tri cur = trilinear(P, pt);
         for (int q = 1; q < 4; ++q) {
             support_point(pos, ed, td, (s0 + q) & 3, pt);
-            const Tri tp = trilinear(P, pt);
-            if (same_cell(cur, tp)) {
-                add_weights(cur, tp);
-            } else {
+            if (!merge_into(P, pt, cur)) {
                 scatter_tri<NF, R>(P, W, acc, F, cur, vp, vs, err);
-                cur = tp;
+                cur = trilinear(P, pt);
             }
         }
         scatter_tri<NF, R>(P, W, acc, F, cur, vp, vs, err);
@@ -820,13 +834,10 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 bool ok = true;
                 for (int q = 1; q < 4; ++q) {
                     support_point(pos, ed, td, (s0 + q) & 3, pt);
-                    const Tri tp = trilinear(P, pt);
-                    if (same_cell(cur, tp)) {
-                        add_weights(cur, tp);
-                    } else {
+                    if (!merge_into(P, pt, cur)) {
                         ok = (SCATTER ? gather_tri<R>(P, pack, cur, g)
                                       : gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g)) && ok;
-                        cur = tp;
+                        cur = trilinear(P, pt);
                     }
                 }
                 ok = (SCATTER ? gather_tri<R>(P, pack, cur, g)
