@@ -810,14 +810,20 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
             for (int k = 0; k < 5; ++k) b[k] = aR<R>(pv, A_B11 + k, i);
             const double vol = a64<R>(pv, A_VOL, i);
             R vor[3] = {aR<R>(pv, A_VX, i), aR<R>(pv, A_VY, i), aR<R>(pv, A_VZ, i)};
+            // the LS-RK accumulators: the mixed form loads them before the
+            // gathers (their latency overlaps the interpolation); the FP64
+            // form after them (fewer live registers, no spills)
             double dpo[3] = {0.0, 0.0, 0.0};
             R dvo[3] = {(R)0, (R)0, (R)0}, dbo[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
-            if (S.stage > 1) {
+            auto load_accumulators = [&]() {
+                if (S.stage > 1) {
 #pragma unroll
-                for (int k = 0; k < 3; ++k) { dpo[k] = a64<R>(pv, A_DX + k, i); dvo[k] = aR<R>(pv, A_DVX + k, i); }
+                    for (int k = 0; k < 3; ++k) { dpo[k] = a64<R>(pv, A_DX + k, i); dvo[k] = aR<R>(pv, A_DVX + k, i); }
 #pragma unroll
-                for (int k = 0; k < 5; ++k) dbo[k] = aR<R>(pv, A_DB0 + k, i);
-            }
+                    for (int k = 0; k < 5; ++k) dbo[k] = aR<R>(pv, A_DB0 + k, i);
+                }
+            };
+            if constexpr (Form<R>::mixed) load_accumulators();
             R g[14];
 #pragma unroll
             for (int l = 0; l < 14; ++l) g[l] = (R)0;
@@ -844,6 +850,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                               : gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g)) && ok;
                 if (!ok) set_err(err, ERRB_ZRANGE);
             }
+            if constexpr (!Form<R>::mixed) load_accumulators();
             double dp[3];
             R dv[3];
 #pragma unroll
