@@ -350,11 +350,12 @@ EPIC_DEV int merge_start(const Params& P, const double* pos, const double* eta, 
     return 0;
 }
 
-// Scatter one support point: vp[f] = value * point weight * volume, vs[f] =
-// vp[f] in fixed-point units (plain form only).
+// Scatter one support point: vs[f] = value * point weight * volume in the
+// window's fixed-point units (a power-of-two scale, so vs[f] * inv[f] gives
+// the value back exactly for the global-atomic fallback).
 template <int NF, class R>
 EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const Fields7& F, const Tri& t,
-                          const R* vp, const double* vs, unsigned* err) {
+                          const double* vs, const double* inv, unsigned* err) {
     if (t.ks < -1 || t.ks > P.nz) { set_err(err, ERRB_ZRANGE); return; }
     int lx = wrap_to(t.is - W.gx0, P.nx), ly = wrap_to(t.js - W.gy0, P.ny), lz = t.ks - W.gz0;
     if (W.ok && lx + 1 < W.WX && ly + 1 < W.WY && lz >= 0 && lz + 1 < W.WZ) {
@@ -391,7 +392,8 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
                     const R wt = (R)t.w[kk][jj][ii];
 #pragma unroll
                     for (int f = 0; f < NF; ++f)
-                        if (field_on<NF>(F, f)) atomicAdd(&F.f[field_slot<NF>(f)][g], (double)(wt * vp[f]));
+                        if (field_on<NF>(F, f))
+                            atomicAdd(&F.f[field_slot<NF>(f)][g], (double)(wt * (R)(vs[f] * inv[f])));
                 }
     }
 }
@@ -490,9 +492,6 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
                             unsigned* acc, const Fields7& F, int* nparg, int* nsparg, bool reuse, bool store,
                             int lg, unsigned* err) {
     const Window W = ws->W;
-    double scale[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) scale[f] = ws->scale[f];
     // The lanes of a warp take groups of 2^lg consecutive parcels spaced about
     // cnt/32 * 2^lg apart (different cells of the box), so that the addresses
     // of one shared-memory atomic spread over the banks (consecutive parcels
@@ -512,11 +511,13 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         R eta[3], tau[3];
         // VEC: the support vectors may be recomputed here; else they are stored
         vectors<R>(pv, i, VEC ? reuse : true, store, eta, tau, err);
-        R vp[NF];
         double vs[NF];
-        load_values<NF, R>(P, pv, i, pos[2], vp);
+        {
+            R vp[NF];
+            load_values<NF, R>(P, pv, i, pos[2], vp);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) vs[f] = (double)vp[f] * scale[f];
+            for (int f = 0; f < NF; ++f) vs[f] = (double)vp[f] * ws->scale[f];
+        }
         if (NF != 1 && nparg) count_parcel(P, pos, a64<R>(pv, A_VOL, i), nparg, nsparg, err);
         const double ed[3] = {(double)eta[0], (double)eta[1], (double)eta[2]};
         const double td[3] = {(double)tau[0], (double)tau[1], (double)tau[2]};
@@ -527,11 +528,11 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         for (int q = 1; q < 4; ++q) {
             support_point(pos, ed, td, (s0 + q) & 3, pt);
             if (!merge_into(P, pt, cur)) {
-                scatter_tri<NF, R>(P, W, acc, F, cur, vp, vs, err);
+                scatter_tri<NF, R>(P, W, acc, F, cur, vs, ws->inv, err);
                 cur = trilinear(P, pt);
             }
         }
-        scatter_tri<NF, R>(P, W, acc, F, cur, vp, vs, err);
+        scatter_tri<NF, R>(P, W, acc, F, cur, vs, ws->inv, err);
     }
 }
 
@@ -767,9 +768,13 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
     __shared__ WinShared<7> ws;
     __shared__ double red[PB / 32][NDIAG];
     constexpr int ND = DIAG ? NDIAG : 1;
-    double dacc[ND];
+    // the diagnostic sums of this thread, in shared memory (registers are
+    // the stage kernel's limit)
+    __shared__ double dsm[ND][PB];
 #pragma unroll
-    for (int k = 0; k < ND; ++k) dacc[k] = 0.0;
+    for (int k = 0; k < ND; ++k) dsm[k][threadIdx.x] = 0.0;
+    double* dacc = &dsm[0][threadIdx.x];
+#define DACC(k) dacc[(k) * PB]
     const double dt = sc->dt;
     const Range Rg = cta_range(P, pv, B, n);
     // without the scatter pass, the dynamic shared memory holds the box's gather records
@@ -871,19 +876,19 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 sz_eigenvalues<Ops>(U, D);
                 double bu = (double)aR<R>(pv, A_BUOY, i);
                 double vx = vor[0], vy = vor[1], vz = vor[2];
-                dacc[0] += (dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]) * vol;
-                dacc[1] += (vx * vx + vy * vy + vz * vz) * vol;
+                DACC(0) += (dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]) * vol;
+                DACC(1) += (vx * vx + vy * vy + vz * vz) * vol;
                 double lam = sqrt((double)D[0] / (double)D[2]);
-                dacc[2] += lam;
-                dacc[3] += lam * lam;
-                dacc[4] += vol;
-                dacc[5] += vol * vol;
-                if (vol <= P.vmin) dacc[6] += 1.0;
-                dacc[7] += vol * (vx * vx);
-                dacc[8] += vol * (vy * vy);
-                dacc[9] += vol * (vz * vz);
-                dacc[10] = fmin(dacc[10], bu);
-                dacc[11] = fmax(dacc[11], bu);
+                DACC(2) += lam;
+                DACC(3) += lam * lam;
+                DACC(4) += vol;
+                DACC(5) += vol * vol;
+                if (vol <= P.vmin) DACC(6) += 1.0;
+                DACC(7) += vol * (vx * vx);
+                DACC(8) += vol * (vy * vy);
+                DACC(9) += vol * (vz * vz);
+                DACC(10) = fmin(DACC(10), bu);
+                DACC(11) = fmax(DACC(11), bu);
             }
             if (DIAG && S.binc) {
                 // apply_bndry_fluxes after the diagnostics, before the first
@@ -976,7 +981,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
         int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
         for (int k = 0; k < ND; ++k) {
-            double v = dacc[k];
+            double v = DACC(k);
             for (int o = 16; o > 0; o >>= 1) {
                 double u = __shfl_xor_sync(0xffffffff, v, o);
                 v = (k == 10) ? fmin(v, u) : (k == 11) ? fmax(v, u) : v + u;
@@ -992,6 +997,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
             partials[blockIdx.x * NDIAG + k] = v;
         }
     }
+#undef DACC
 }
 
 // ---------------------------------------------------------------------------
