@@ -550,7 +550,8 @@ __global__ void __launch_bounds__(PB) k_vectors(PView pv, long long n, unsigned*
 
 // par2grid scatter (NF = 7) and vol2grid (NF = 1).
 template <int NF, class R, bool VEC>
-__global__ void __launch_bounds__(PB, SB) k_scatter(Params P, PView pv, long long n, Boxes B, Fields7 F,
+// vol2grid (NF = 1) has a small window and few live values: three CTAs per SM
+__global__ void __launch_bounds__(PB, NF == 1 ? 3 : SB) k_scatter(Params P, PView pv, long long n, Boxes B, Fields7 F,
                                                     int* nparg, int* nsparg, int reuse, int store, int lg,
                                                     unsigned* err) {
     extern __shared__ __align__(16) unsigned acc[];
