@@ -934,8 +934,14 @@ EPIC_DEV void col_matvec_t(const T* __restrict__ M, int lo, int hi, const T* xs,
 // field_decompose_semi_spectral (inversion_utils.f90:370-401), optionally
 // followed by the Hou-Li filter and/or preceded by central_diffz_semi_spectral
 // (inversion_utils.f90:460-480).  mode bit 1: filter, bit 2: central diff.
+// CTAs per SM the column kernels are held to: up to 5 rows per thread (nz <
+// 160) the FP64 columns (70 KB at nz = 128) fit three times and the FP32 ones
+// four, at 80 and 64 registers; longer columns fill the shared memory alone.
 template <int R, class T>
-__global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
+constexpr int col_min_blocks() { return R > 5 ? 1 : sizeof(T) == 8 ? 3 : 4; }
+
+template <int R, class T>
+__global__ void __launch_bounds__(256, col_min_blocks<R, T>()) k_col_decompose(ColArgs A, int mode) {
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
     int nzp = A.nz + 1, nz = A.nz;
@@ -987,7 +993,7 @@ __global__ void __launch_bounds__(256) k_col_decompose(ColArgs A, int mode) {
 
 // field_combine_semi_spectral (inversion_utils.f90:421-456)
 template <int R, class T>
-__global__ void __launch_bounds__(256) k_col_combine(ColArgs A) {
+__global__ void __launch_bounds__(256, col_min_blocks<R, T>()) k_col_combine(ColArgs A) {
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
     int nzp = A.nz + 1, nz = A.nz;
