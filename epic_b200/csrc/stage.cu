@@ -540,7 +540,7 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
 // 216-260), stored for the scatter that follows: the eigen-solver and the
 // scatter run as separate kernels, each with a small instruction footprint.
 template <class R>
-__global__ void __launch_bounds__(PB) k_vectors(PView pv, long long n, unsigned* err) {
+__global__ void __launch_bounds__(PB, 4) k_vectors(PView pv, long long n, unsigned* err) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         R eta[3], tau[3];
