@@ -676,11 +676,25 @@ __global__ void k_split_flag(Params P, PView pv, long long n, int* flag, unsigne
         double b[5];
         load_B(pv, i, b);
         const double vol = pv.get(A_VOL, i);
+        const double B33 = get_B33<FastOps>(b, vol, err);
+        // No split without eigenvalues when a bound proves it: every
+        // eigenvalue is at most the Frobenius norm F of the full matrix, and
+        // det B = abc^2 (the volume constraint that defines B33), so
+        // lambda^2 = D0 / D2 = D0^2 D1 / det <= F^3 / abc^2.  The 1e-9 margin
+        // covers the rounding of F and of B33; the decision is then the same
+        // as the eigenvalue test's.
+        const double f2 = b[0] * b[0] + b[3] * b[3] + B33 * B33 + 2.0 * (b[1] * b[1] + b[2] * b[2] + b[4] * b[4]);
+        const double abc = get_abc(vol);
+        const double m = 1.0 - 1e-9;
+        if (f2 < P.amax2 * P.amax2 * m && f2 * sqrt(f2) < abc * abc * (P.lambda_max * P.lambda_max) * m) {
+            flag[i] = 0;
+            continue;
+        }
         double U[9], D[3];
         // The fast eigenvalues decide where both tests are clear of their
         // thresholds by 1e-9 (they agree with the non-contracted ones to a few
         // ulps); near a threshold the decision is the oracle's arithmetic.
-        full_matrix<FastOps>(b, get_B33<FastOps>(b, vol, err), U);
+        full_matrix<FastOps>(b, B33, U);
         sz_eigenvalues<FastOps>(U, D);
         double lam = sqrt(D[0] / D[2]);
         const bool clear = fabs(lam - P.lambda_max) > 1e-9 * P.lambda_max && fabs(D[0] - P.amax2) > 1e-9 * P.amax2;
