@@ -336,13 +336,13 @@ def run_ours(args):
     elif args.roofline_kernel == "stage":
         # DRAM bytes of one k_stage<0,0> launch (stages 2-5) from the ncu
         # captures in profiles/k_stage_thermal64.md (64^3, 2,097,152 parcels,
-        # early flow: plain 548.0 MB read + 349.2 MB written = 427.8 B per
-        # parcel; mixed 338.6 + 185.4 MB = 249.9 B), scaled by the parcels of
+        # early flow: plain 539.9 MB read + 323.1 MB written = 411.5 B per
+        # parcel; mixed 337.3 + 184.7 MB = 248.9 B), scaled by the parcels of
         # this run (the traffic grows with them), against the algorithmic
         # bytes of the same stages.  Lines still dirty in L2 when the launch
         # ends (up to its 126 MB) are not in the count, which puts the mixed
         # capture a little below its algorithmic bytes.
-        per_parcel = 249.9 if args.form == "mixed" else 427.8
+        per_parcel = 248.9 if args.form == "mixed" else 411.5
         roofline["traffic"] = per_parcel * avg_n
         roofline["traffic_source"] = (f"ncu dram__bytes_read+write of k_stage<0,0,{'float' if args.form == 'mixed' else 'double'}> "
                                       "(stages 2-5), 64^3 capture scaled by parcels")
