@@ -252,7 +252,7 @@ class EpicContext:
         rc = self.lib.fn[name](self.h, *args)
         if rc != EPIC_OK:
             msg = self.lib.fn["last_error"](self.h)
-            raise EpicError(rc, self.lib.prefix + name, msg.decode() if msg else "")
+            raise EpicError(rc, self.lib.prefix + name, msg.decode(errors="replace") if msg else "")
         return rc
 
     def close(self):

@@ -187,9 +187,15 @@ std::vector<uint8_t> serialise(const Header& h) {
 
 bool is_record(const Header& h, const Var& v) { return !v.dims.empty() && v.dims[0] == h.rec_dim; }
 
+// Elements of one record of v (of the whole variable if fixed-size); a
+// product beyond 2^56 elements (a corrupt header) is an error.
 int64_t slab_elems(const Header& h, const Var& v) {
     int64_t n = 1;
-    for (size_t k = is_record(h, v) ? 1 : 0; k < v.dims.size(); ++k) n *= h.dims[v.dims[k]].len;
+    for (size_t k = is_record(h, v) ? 1 : 0; k < v.dims.size(); ++k) {
+        const int64_t len = h.dims[v.dims[k]].len;
+        if (len < 0 || (len > 0 && n > (int64_t(1) << 56) / len)) throw Error("netCDF: variable too large");
+        n *= len;
+    }
     return n;
 }
 
@@ -299,7 +305,9 @@ struct In {
             a.name = name();
             a.type = (int32_t)u32();
             a.nelems = nonneg();
-            const int64_t bytes = a.nelems * type_size(a.type);
+            const int ts = type_size(a.type);
+            if (a.nelems < 0 || a.nelems > (int64_t)(b.size() - i) / ts) throw Error("netCDF: bad attribute length");
+            const int64_t bytes = a.nelems * ts;
             const uint8_t* p = take((size_t)round4(bytes));
             a.raw.assign(p, p + bytes);
             out.push_back(std::move(a));
@@ -338,6 +346,7 @@ struct Reader {
                 Dim d;
                 d.name = in.name();
                 d.len = in.nonneg();
+                if (d.len < 0) throw Error("netCDF: bad dimension length");
                 h.dims.push_back(d);
             }
         }
@@ -359,6 +368,8 @@ struct Reader {
                 v.type = (int32_t)in.u32();
                 v.vsize = h.version == 5 ? (int64_t)in.u64() : (int64_t)in.u32();
                 v.begin = in.offset();
+                if (v.begin < 0 || v.begin > file_size) throw Error("netCDF: bad variable offset");
+                type_size(v.type);   // an unknown type is an error here
                 h.vars.push_back(std::move(v));
             }
         }
@@ -372,6 +383,7 @@ struct Reader {
         for (const Var& v : h.vars)
             if (is_record(h, v)) {
                 h.recsize += round4(slab_elems(h, v) * type_size(v.type));
+                if (h.recsize > (int64_t(1) << 60)) throw Error("netCDF: record too large");
                 if (first_rec < 0) first_rec = v.begin;
                 ++nrec;
             }
@@ -402,6 +414,7 @@ struct Reader {
         int64_t off = v.begin + start * s;
         if (is_record(h, v)) {
             if (r < 0 || r >= h.numrecs) throw Error("netCDF: record out of range in " + v.name);
+            if (h.recsize > 0 && r > file_size / h.recsize) throw Error("netCDF: " + path + " is truncated");
             off += r * h.recsize;
         }
         if (off + count * s > file_size) throw Error("netCDF: " + path + " is truncated");

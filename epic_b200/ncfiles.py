@@ -36,7 +36,7 @@ class NcFiles:
 
     def _check(self, rc, name):
         if rc != 0:
-            raise EpicError(rc, name, self.lib.epic_nc_last_error().decode())
+            raise EpicError(rc, name, self.lib.epic_nc_last_error().decode(errors="replace"))
 
     @staticmethod
     def _box(ncells, origin, extent):
@@ -51,7 +51,7 @@ class NcFiles:
         self._check(self.lib.epic_nc_info(os.fsencode(path), ft, nc.ctypes.data_as(_I32), _ptr(og), _ptr(ex),
                                           C.byref(npar), C.byref(nst), C.byref(t), z.ctypes.data_as(_I32)),
                     "epic_nc_info")
-        return dict(file_type=ft.value.decode(), ncells=tuple(int(v) for v in nc), origin=tuple(og),
+        return dict(file_type=ft.value.decode(errors="replace"), ncells=tuple(int(v) for v in nc), origin=tuple(og),
                     extent=tuple(ex), n_parcels=npar.value, n_steps=nst.value, t=t.value,
                     zeta=(int(z[0]), int(z[1])))
 

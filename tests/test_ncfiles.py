@@ -319,3 +319,40 @@ def test_init_from_field_file_parity(olib, glib, nc, tmp_path):
     with pytest.raises(abi.EpicError) as e:   # the file's box is not the context's
         bad.init_from_field_file(f)
     assert e.value.code == 9
+
+
+def test_corrupt_files_give_errors_not_crashes(nc, tmp_path):
+    """Truncated files and random byte changes in the header or the data of
+    a valid parcel file and field file: every read returns either data or
+    EPIC_ERR_IO (a crash would end the test process).  Seeded."""
+    rng = np.random.default_rng(12)
+    good_p = str(tmp_path / "good_p.nc")
+    nc.write_parcels(good_p, t=1.0, p=_parcels(40), **BOX)
+    good_f = str(tmp_path / "good_f.nc")
+    nc.write_field_file(good_f, t=0.0, fields=_fields(), **BOX)
+    for src in (good_p, good_f):
+        raw = bytearray(open(src, "rb").read())
+        for trial in range(200):
+            b = bytearray(raw)
+            kind = trial % 4
+            if kind == 0:
+                b = b[:int(rng.integers(0, len(b)))]
+            else:
+                # header bytes (1, 2: all-ones bytes make huge counts) or anywhere (3)
+                hi = min(len(b), 600) if kind < 3 else len(b)
+                for _ in range(int(rng.integers(1, 6))):
+                    b[int(rng.integers(0, hi))] = 0xFF if kind == 2 else int(rng.integers(0, 256))
+            f = str(tmp_path / "bad.nc")
+            open(f, "wb").write(bytes(b))
+            try:
+                info = nc.info(f)
+            except abi.EpicError as e:
+                assert e.code == 9
+                continue
+            try:
+                if info["file_type"] == "parcels" and 0 <= info["n_parcels"] <= 10000:
+                    nc.read_parcels(f)
+                else:
+                    nc.read_field(f, "buoyancy", **BOX)
+            except abi.EpicError as e:
+                assert e.code in (6, 9)
