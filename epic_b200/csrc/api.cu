@@ -370,6 +370,12 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         free_ctx(c);
         delete ctx;
         return code;
+    } catch (const std::exception&) {
+        // host memory for the tables or the scratch bookkeeping: no exception
+        // leaves the C ABI
+        free_ctx(c);
+        delete ctx;
+        return EPIC_ERR_CUDA;
     }
     *out = ctx;
     return EPIC_OK;

@@ -178,13 +178,35 @@ extern "C" int epic_srv_create(int32_t max_slots, double hbm_fraction, epic_serv
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { delete s; return EPIC_ERR_CUDA; }
     s->budget = hbm_fraction * (double)free_b;
-    for (int k = 0; k < max_slots; ++k) s->workers.emplace_back(worker, s, k);
+    try {
+        for (int k = 0; k < max_slots; ++k) s->workers.emplace_back(worker, s, k);
+    } catch (const std::exception&) {
+        // a thread could not be started: stop the ones that were
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stop = true;
+            s->cv_work.notify_all();
+        }
+        for (auto& w : s->workers) w.join();
+        delete s;
+        return EPIC_ERR_CUDA;
+    }
     *out = s;
     return EPIC_OK;
 }
 
+static int submit_locked(epic_server* s, const epic_request* req, int64_t* id);
+
 extern "C" int epic_srv_submit(epic_server* s, const epic_request* req, int64_t* id) {
     if (!s || !req || !id || req->steps < 0) return EPIC_ERR_ARG;
+    try {
+        return submit_locked(s, req, id);
+    } catch (const std::exception&) {   // host memory for the queue or the results
+        return EPIC_ERR_CUDA;
+    }
+}
+
+static int submit_locked(epic_server* s, const epic_request* req, int64_t* id) {
     std::lock_guard<std::mutex> lk(s->mu);
     Job j;
     j.id = s->next_id++;
