@@ -21,7 +21,9 @@ std::atomic<long long> g_launches{0};
 
 // parcels%resize (parcel_container.f90:273-308): reallocate the store for at
 // least grow_factor x need parcels, keeping parcels [0, n); the sort buffer
-// and the per-CTA partials follow the new capacity.
+// and the per-CTA partials follow the new capacity.  The sort and merge
+// scratch are not touched here (the caller may still have live data in them):
+// grow_scratch_for_capacity sizes them once that data is read.
 void grow_store(Ctx& c, long long need) {
     long long ncap = std::max(need, (long long)std::llround(c.cfg.grow_factor * (double)need));
     ncap = (ncap + 63) & ~63LL;
@@ -61,6 +63,12 @@ void grow_store(Ctx& c, long long need) {
     CK(cudaFree(c.stage_partials));
     c.stage_partials = nullptr;
     CK(cudaMalloc(&c.stage_partials, sizeof(double) * 16 * (size_t)stage_grid_max(c.P, c.cap)));
+}
+
+// The sort and merge scratch for the current capacity, so that no step
+// allocates them mid-step.  A regrowth frees the old scratch in stream order,
+// after the kernels already queued that read it.
+void grow_scratch_for_capacity(Ctx& c) {
     if (c.box_start) c.get_scratch(sort_scratch_bytes(c.cap));
     c.get_scratch2(merge_scratch_bytes(c.cap));
 }

@@ -249,6 +249,7 @@ void allow_smem(K kernel, size_t bytes) {
 
 // api.cu
 void grow_store(Ctx& c, long long need);
+void grow_scratch_for_capacity(Ctx& c);
 void prof_begin(Ctx& c, const char* name);
 void prof_end(Ctx& c, const char* name);
 void check_device_error(Ctx& c);

@@ -784,9 +784,13 @@ long long parcel_split(Ctx& c) {
     CK(cudaStreamSynchronize(c.stream));
     if (ns == 0) return 0;
     // parcel_split.f90:91-94: a full container grows to grow_factor x the parcels needed
-    if (n + ns > c.cap) grow_store(c, n + ns);
+    const bool grow = n + ns > c.cap;
+    if (grow) grow_store(c, n + ns);
     k_split_apply<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, flag, offs, c.label, c.dil, &c.dsc->err);
     CKL();
+    // flag and offs live in the sort scratch: it is resized for the new
+    // capacity only now, behind the kernel that reads them
+    if (grow) grow_scratch_for_capacity(c);
     c.n = n + ns;
     c.n_parcel_splits += ns;
     return ns;

@@ -198,13 +198,15 @@ def test_split_bit_exact(olib, glib):
     _cmp_parcels(oc, gc)
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_split_grows_full_container(olib, glib, precision):
+@pytest.mark.parametrize("precision,keep_order", [(0, 1), (1, 1), (0, 0)])
+def test_split_grows_full_container(olib, glib, precision, keep_order):
     """A split that overflows the container grows it (parcel_split.f90:91-94,
-    grow_factor x the parcels needed) and keeps every parcel; steps go on."""
+    grow_factor x the parcels needed) and keeps every parcel; steps go on.
+    keep_order = 0: the box-sorted store, whose sort scratch (which holds the
+    split's flags) is resized for the new capacity behind the split kernel."""
     s = small_state("thermal", stretch=True)
     oc = make_context(s, olib)
-    gc = make_context(s, glib, capacity=s.n + 64, precision=precision)
+    gc = make_context(s, glib, capacity=s.n + 64, precision=precision, keep_order=keep_order)
     so, sg = oc.split(), gc.split()
     assert sg > 64
     po, pg = oc.get_parcels(), gc.get_parcels()
