@@ -12,9 +12,16 @@ namespace epic {
 
 template <class F>
 static float time_ms(Ctx& c, F&& run, int reps = 3) {
-    cudaEvent_t a, b;
-    CK(cudaEventCreate(&a));
-    CK(cudaEventCreate(&b));
+    struct Events {   // destroyed on every exit, an error in run() included
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~Events() {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } ev;
+    CK(cudaEventCreate(&ev.e[0]));
+    CK(cudaEventCreate(&ev.e[1]));
+    cudaEvent_t a = ev.e[0], b = ev.e[1];
     run();   // warm-up (module load, caches)
     float best = FLT_MAX;
     for (int r = 0; r < reps; ++r) {
@@ -26,8 +33,6 @@ static float time_ms(Ctx& c, F&& run, int reps = 3) {
         CK(cudaEventElapsedTime(&ms, a, b));
         best = std::min(best, ms);
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     return best;
 }
 
