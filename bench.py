@@ -187,6 +187,24 @@ def stage_launch_bytes(n: int, nx: int, ny: int, nz: int, form: str = "plain", l
     return (first + 4 * later) / 5.0 * n + rec * gh
 
 
+# Minimal compulsory HBM traffic of one whole step per parcel (8 parcels per
+# cell): the parcel attributes each call of the reference step must read and
+# write (288 FP64 values = 2304 B plain; 1536 B with the mixed form's FP32
+# attributes) plus the grid transforms (about 0.4 KB plain, 0.2 KB mixed per
+# parcel).
+STEP_BYTES_PER_PARCEL = {"plain": 2700.0, "mixed": 1740.0}
+
+
+def step_roofline(value: float, form: str, peak_gbs: float, peak_kind: str) -> dict:
+    """The whole step against HBM: parcel-steps/s x compulsory bytes per
+    parcel-step, as a fraction of the measured copy bandwidth."""
+    b = STEP_BYTES_PER_PARCEL[form]
+    achieved = value * b / 1e9
+    return {"bound": "hbm", "unit": "GB/s", "bytes_per_parcel_step": b, "achieved": achieved,
+            "peak": peak_gbs, "peak_source": peak_kind, "frac": achieved / peak_gbs if peak_gbs else None,
+            "meaning": "whole step: parcel-steps/s x the step's compulsory HBM bytes per parcel-step"}
+
+
 def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int, form: str = "plain") -> float:
     """Minimal compulsory DRAM bytes of one launch."""
     gh = nx * ny * (nz + 3)
@@ -414,6 +432,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"inputs larger than L2 (parcel state {store_gb:.2f} GB, fields {field_gb:.2f} GB)"},
         "roofline": roofline,
+        "step_roofline": step_roofline(value, args.form, peak, peak_kind),
         "clocks": clk,
         "e2e": e2e,
         "gpu_launches": int(l1.value - l0.value),

@@ -25,6 +25,13 @@ def test_stage_launch_bytes():
     assert bench.stage_launch_bytes(n, nx, ny, nz, "mixed") == pytest.approx((208 + 4 * 256) / 5 * n + 64 * gh)
 
 
+def test_step_roofline():
+    r = bench.step_roofline(4.0e8, "plain", 6554.2, "measured")
+    assert r["achieved"] == pytest.approx(4.0e8 * 2700 / 1e9)
+    assert r["frac"] == pytest.approx(r["achieved"] / 6554.2)
+    assert bench.step_roofline(5.0e8, "mixed", 6554.2, "measured")["bytes_per_parcel_step"] == 1740
+
+
 def test_clock_sampler_without_gpu():
     c = bench.ClockSampler(0)
     c.start()
