@@ -60,3 +60,32 @@ def test_config_struct_matches_header():
         a, b, off = map(int, subprocess.check_output([exe]).split())
     assert a == ctypes.sizeof(EpicCfg) and b == ctypes.sizeof(EpicStepInfo)
     assert off == EpicCfg.capacity.offset
+
+
+def test_every_struct_mirror_matches_c_layout():
+    """Size and every field offset of each ctypes mirror (config, step info,
+    initial-state spec, tuning, server request and result) equal the C
+    compiler's for the headers."""
+    import subprocess, tempfile
+    from epic_b200.abi import EpicCfg, EpicStepInfo, EpicInitSpec, EpicTuning
+    from epic_b200.serve import EpicRequest, EpicResult
+    mirrors = {"epic_cfg": EpicCfg, "epic_step_info": EpicStepInfo, "epic_init_spec": EpicInitSpec,
+               "epic_tuning": EpicTuning, "epic_request": EpicRequest, "epic_result": EpicResult}
+    lines = ['#include "epic_gpu.h"', '#include "epic_serve.h"', "#include <stdio.h>", "#include <stddef.h>",
+             "int main(){"]
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write("\n".join(lines))
+        exe = os.path.join(d, "t")
+        subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe])
+        out = subprocess.check_output([exe]).decode().split("\n")
+    for ln in filter(None, out):
+        cname, what, val = ln.split()
+        py = mirrors[cname]
+        got = ctypes.sizeof(py) if what == "size" else getattr(py, what).offset
+        assert got == int(val), (cname, what, got, val)
