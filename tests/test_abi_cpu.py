@@ -89,3 +89,30 @@ def test_every_struct_mirror_matches_c_layout():
         py = mirrors[cname]
         got = ctypes.sizeof(py) if what == "size" else getattr(py, what).offset
         assert got == int(val), (cname, what, got, val)
+
+
+def test_fortran_config_type_matches_mirror():
+    """The Fortran shim's bind(C) epic_cfg lists the same fields, in the same
+    order, with the same kinds and array lengths as the C struct (through its
+    ctypes mirror, checked against C above).  Textual: no Fortran compiler in
+    this image."""
+    import ctypes as C
+    from epic_b200.abi import EpicCfg
+    text = open(os.path.join(ROOT, "fortran", "epic_gpu_iface.f90")).read()
+    body = re.search(r"type, bind\(C\) :: epic_cfg\n(.*?)end type epic_cfg", text, re.S).group(1)
+    kinds = {"c_int32_t": C.c_int32, "c_int64_t": C.c_int64, "c_double": C.c_double}
+    fields = []
+    for ln in body.splitlines():
+        ln = ln.split("!")[0].strip()
+        if not ln:
+            continue
+        m = re.match(r"(?:integer|real)\((c_\w+)\)\s*::\s*(.*)", ln)
+        assert m, ln
+        for item in re.findall(r"(\w+)(?:\((\d+)\))?", m.group(2)):
+            name, dim = item
+            t = kinds[m.group(1)]
+            fields.append((name, t * int(dim) if dim else t))
+    mirror = [(n, t) for n, t in EpicCfg._fields_]
+    assert [n for n, _ in fields] == [n for n, _ in mirror]
+    for (n, t), (_, u) in zip(fields, mirror):
+        assert C.sizeof(t) == C.sizeof(u) and getattr(t, "_type_", None) == getattr(u, "_type_", None), n
