@@ -116,3 +116,23 @@ def test_fortran_config_type_matches_mirror():
     assert [n for n, _ in fields] == [n for n, _ in mirror]
     for (n, t), (_, u) in zip(fields, mirror):
         assert C.sizeof(t) == C.sizeof(u) and getattr(t, "_type_", None) == getattr(u, "_type_", None), n
+
+
+def test_fortran_interfaces_match_c_prototypes():
+    """Every bind(C) function of the Fortran shim names a declared C entry
+    point and passes as many arguments as its prototype."""
+    text = open(os.path.join(ROOT, "fortran", "epic_gpu_iface.f90")).read()
+    hdr = "".join(open(os.path.join(ROOT, "include", h)).read() for h in os.listdir(os.path.join(ROOT, "include")))
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(epic_\w+)\s*\(([^;{]*?)\)\s*;", hdr):
+        args = m.group(2).strip()
+        protos[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    found = 0
+    for m in re.finditer(r"(?:function|subroutine)\s+\w+\s*\(([^)]*)\)\s*&?\s*bind\(C,\s*name=\"(\w+)\"\)", text):
+        args, cname = m.group(1).strip(), m.group(2)
+        assert cname in protos, cname
+        n = 0 if not args else args.count(",") + 1
+        assert n == protos[cname], (cname, n, protos[cname])
+        found += 1
+    assert found == len(re.findall(r"bind\(C,\s*name=", text)) >= 17
