@@ -352,8 +352,8 @@ def run_ours(args):
     if args.traffic is not None:
         roofline["traffic"] = args.traffic
     elif args.roofline_kernel == "stage":
-        # DRAM bytes of one k_stage<0,0> launch (stages 2-5) from the ncu
-        # captures in profiles/k_stage_thermal64.md (64^3, 2,097,152 parcels,
+        # DRAM bytes of one k_stage<0,0> launch (stages 2-5) from ncu
+        # captures of the stage kernel (64^3, 2,097,152 parcels,
         # early flow: plain 539.9 MB read + 323.1 MB written = 411.5 B per
         # parcel; mixed 337.3 + 184.7 MB = 248.9 B), scaled by the parcels of
         # this run (the traffic grows with them), against the algorithmic

@@ -32,22 +32,28 @@ constexpr long long NOALLOC_CHUNK = 16384;   // parcels per block (64 per thread
 // by the final correction dvor[3].
 __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_BLOCKS * 4 + 8];
 
-// Device address of g_noalloc_scratch for each device, looked up once with
-// that device current (a host-side use of the symbol name is not a device
-// address).
+// Device address of g_noalloc_scratch for each device (a host-side use of
+// the symbol name is not a device address).  The address is looked up again,
+// with the device current, on every call whose stream is not capturing, so a
+// module that was loaded again (after cudaDeviceReset, or in a new primary
+// context) is found at its new address; a call on a capturing stream uses the
+// address found by the last call outside a capture on that device.
 constexpr int MAX_DEVICES = 64;
 double* g_scratch_addr[MAX_DEVICES] = {nullptr};
 std::mutex g_scratch_mu;
 
-int scratch_for_current_device(double** out) {
+int scratch_for_current_device(cudaStream_t st, double** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return EPIC_ERR_CUDA;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return EPIC_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return EPIC_ERR_CUDA;
         g_scratch_addr[dev] = static_cast<double*>(p);
     }
+    if (!g_scratch_addr[dev]) return EPIC_ERR_CUDA;
     *out = g_scratch_addr[dev];
     return EPIC_OK;
 }
@@ -111,10 +117,10 @@ extern "C" int epic_gpu_apply_vortcor_noalloc(int64_t n, const double* vol, doub
                                               double dvor_out[3], void* stream) {
     if (n <= 0 || !vol || !vor || !vor_bar) return EPIC_ERR_ARG;
     if (n > (int64_t)NOALLOC_MAX_BLOCKS * NOALLOC_CHUNK) return EPIC_ERR_CAPACITY;
-    double* scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
-    if (rc != EPIC_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* scratch = nullptr;
+    int rc = scratch_for_current_device(st, &scratch);
+    if (rc != EPIC_OK) return rc;
     int nb = (int)((n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK);
     k_na_partials<<<nb, NOALLOC_THREADS, 0, st>>>(n, vol, vor, scratch);
     k_na_final<<<1, 32, 0, st>>>(nb, vor_bar[0], vor_bar[1], vor_bar[2], scratch);

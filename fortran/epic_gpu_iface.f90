@@ -1,7 +1,8 @@
 ! =============================================================================
 ! ISO_C_BINDING interfaces of the B200 EPIC step (include/epic_gpu.h).
 ! Replaces, under ENABLE_B200, the calls of the run loop at
-! src/3d/epic3d.f90:137-151 (see INTEGRATION.md for the call sequence).
+! src/3d/epic3d.f90:137-151: create, set_parcels, init_correction, then one
+! epic_gpu_step per iteration of the run loop and get_parcels at output steps.
 ! =============================================================================
 module epic_gpu_iface
     use iso_c_binding
@@ -170,6 +171,20 @@ module epic_gpu_iface
             type(c_ptr), value            :: ctx
             character(kind=c_char)        :: path(*)
             integer(c_int32_t)            :: zeta_flags(2)
+        end function
+
+        ! allocation-free vorticity correction on device arrays the caller owns
+        ! (OpenACC / CUDA Fortran: pass the device addresses, e.g. from
+        ! host_data use_device); no cudaMalloc, a fixed scratch inside the
+        ! library, n <= 67108864; dvor_out may be c_null_ptr
+        integer(c_int) function epic_gpu_apply_vortcor_noalloc(n, vol, vor, vor_bar, dvor_out, stream) &
+                bind(C, name="epic_gpu_apply_vortcor_noalloc")
+            import :: c_int, c_int64_t, c_ptr, c_double
+            integer(c_int64_t), value  :: n
+            type(c_ptr), value         :: vol, vor
+            real(c_double), intent(in) :: vor_bar(3)
+            type(c_ptr), value         :: dvor_out
+            type(c_ptr), value         :: stream
         end function
     end interface
 

@@ -270,19 +270,22 @@ int epic_gpu_apply_bndry_fluxes(epic_ctx* ctx, double dt);
  * (apply_laplace, apply_gradient). */
 int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info);
 
-/* Allocation-free vorticity correction.  No counterpart in the reference
- * (it restates apply_vortcor, parcel_correction.f90:89-138, for callers that
- * cannot call cudaMalloc: codes whose device memory belongs to another
- * runtime's pool or budget, or time loops that must not take an
- * allocation's implicit synchronisation).  vol (n) and vor (3, n) are device
- * arrays owned by the caller; vor is corrected in place with
- * dvor = sum(V w) / sum(V) - vor_bar, returned in dvor_out (host, may be
- * NULL).  stream is a cudaStream_t (NULL = default stream).  The only
- * scratch is a fixed 128 KiB __device__ array in the library (kept by every
- * GPU that loads it); n above 67,108,864 returns EPIC_ERR_CAPACITY.  The
- * first call on a device looks up that array's device address, so make the
- * first call before any stream capture.  All calls share the array: calls
- * whose kernels overlap on the GPU race. */
+/* Allocation-free vorticity correction.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: codes whose device memory belongs
+ * to another runtime's pool or budget (a Fortran code keeping its parcel
+ * arrays in OpenACC or CUDA Fortran device memory), or time loops that must
+ * not take an allocation's implicit synchronisation.  vol (n) and vor (3, n)
+ * are device arrays owned by the caller; vor is corrected in place by
+ * dvor = sum(V w) / sum(V) - vor_bar (the volume-weighted mean vorticity
+ * minus its initial value), which is also returned in dvor_out (host; NULL
+ * skips the copy and the stream synchronisation).  stream is a cudaStream_t
+ * (NULL = default stream).  The only scratch is a fixed 128 KiB __device__
+ * array in the library (kept by every GPU that loads it); n above 67,108,864
+ * returns EPIC_ERR_CAPACITY.  Every call outside a stream capture looks up
+ * that array's device address on the current device; a call on a capturing
+ * stream reuses the address of the last call outside a capture, so make a
+ * first call on each device before any capture.  All calls share the array:
+ * calls whose kernels overlap on the GPU race. */
 int epic_gpu_apply_vortcor_noalloc(int64_t n, const double* vol, double* vor, const double vor_bar[3],
                                    double dvor_out[3], void* stream);
 

@@ -9,7 +9,9 @@ import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py <path of the reference source tree>")
+ref = sys.argv[1]
 d = os.path.join(ref, "unit-tests", "3d")
 B = np.loadtxt(os.path.join(d, "B.asc"), skiprows=1)
 D = np.loadtxt(os.path.join(d, "D.asc"), skiprows=1)

@@ -63,3 +63,30 @@ def test_noalloc_rejects_oversize(glib):
     vb = (C.c_double * 3)(0.0, 0.0, 0.0)
     # beyond the stated maximum of 67,108,864 parcels: refused before any launch
     assert f(67108864 + 1, d.data_ptr(), d.data_ptr(), vb, None, None) == 2   # EPIC_ERR_CAPACITY
+
+
+def test_noalloc_on_caller_stream_without_readback(glib):
+    """On a stream the caller owns and with dvor_out = NULL (no copy, no
+    synchronisation by the library), vor is still corrected: the caller
+    synchronises its own stream and compares with the regular path."""
+    import torch
+    from epic_b200 import make_context
+
+    s = small_state("thermal")
+    n = s.n
+    ctx = make_context(s, glib)
+    vbar = (s.vor * s.vol[:, None]).sum(0) / s.vol.sum()
+    vor_new = s.vor + np.random.default_rng(5).normal(0.05, 0.1, size=(n, 3))
+    ctx.set_parcels(s.pos, vor_new, s.B, s.vol, s.buoy, s.hum)
+    ctx.apply_vortcor()
+    ref = ctx.get_parcels()["vor"]
+    f = _fn(glib)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        d_vol = torch.tensor(s.vol, dtype=torch.float64, device="cuda")
+        d_vor = torch.tensor(vor_new, dtype=torch.float64, device="cuda")
+    stream.synchronize()
+    vb = (C.c_double * 3)(*vbar)
+    assert f(n, d_vol.data_ptr(), d_vor.data_ptr(), vb, None, C.c_void_p(stream.cuda_stream)) == 0
+    stream.synchronize()
+    assert rel_err(d_vor.cpu().numpy(), ref) < 1e-10
