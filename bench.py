@@ -253,12 +253,13 @@ def run_ours(args):
         # parcels generated on the device (the same state as the host generator)
         setup = initial.device_spec(args.workload)
         extra = dict(capacity=int(1.15 * setup.n)) if large else {}
-        ctx = epic_b200.make_context_device(setup, lib, keep_order=0, precision=1 if mixed else 0, **extra)
+        ctx = epic_b200.make_context_device(setup, lib, keep_order=args.keep_order, precision=1 if mixed else 0,
+                                            **extra)
         if large:
             args.no_e2e = True
     else:
         setup = initial.config(args.workload)
-        ctx = epic_b200.make_context(setup, lib, keep_order=0, precision=1 if mixed else 0)
+        ctx = epic_b200.make_context(setup, lib, keep_order=args.keep_order, precision=1 if mixed else 0)
     tuning = ctx.autotune() if not args.no_autotune else None
     import ctypes as C
     sp = C.c_void_p()
@@ -660,6 +661,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--spinup", type=int, default=0, help="untimed steps before the warm-up (developed flow)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--keep-order", type=int, default=0, choices=[0, 1],
+                    help="1: keep the reference's container order (no box sort)")
     ap.add_argument("--device-init", action="store_true",
                     help="generate the initial parcels on the device (always for thermal2-512x512x256)")
     ap.add_argument("--no-e2e", action="store_true")

@@ -45,8 +45,17 @@ void grow_store(Ctx& c, long long need) {
         CK(cudaMemcpyAsync(nlabel, c.label, sizeof(long long) * (size_t)c.n, cudaMemcpyDeviceToDevice, c.stream));
         CK(cudaMemcpyAsync(ndil, c.dil, sizeof(double) * (size_t)c.n, cudaMemcpyDeviceToDevice, c.stream));
     }
+    int* nrank = nullptr;
+    if (c.rank) {
+        CK(cudaMalloc(&nrank, sizeof(int) * (size_t)ncap));
+        CK(cudaMemcpyAsync(nrank, c.rank, sizeof(int) * (size_t)c.n, cudaMemcpyDeviceToDevice, c.stream));
+    }
     CK(cudaStreamSynchronize(c.stream));
     CK(cudaFree(c.pv.base));
+    if (c.rank) {
+        CK(cudaFree(c.rank));
+        c.rank = nrank;
+    }
     if (c.label) {
         CK(cudaFree(c.label));
         CK(cudaFree(c.dil));
@@ -172,12 +181,70 @@ __global__ void k_interleave(double* dst, int ncomp, long long n, PView pv, int 
         dst[i] = pv.get(a0 + k, p);
     }
 }
+// Container order of the box-ordered store (Ctx::rank).
+__global__ void k_rank_iota(int* rank, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        rank[i] = (int)i;
+}
+__global__ void k_rank_inverse(const int* rank, long long n, int* ord) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        ord[rank[i]] = (int)i;
+}
+// dst[r * ncomp + k] = attribute a0 + k of the parcel with container index r
+__global__ void k_interleave_ord(double* dst, int ncomp, long long n, PView pv, int a0, const int* ord) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * ncomp;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long r = i / ncomp;
+        int k = (int)(i - r * ncomp);
+        dst[i] = pv.get(a0 + k, ord[r]);
+    }
+}
+__global__ void k_deinterleave_ord(const double* src, int ncomp, long long n, PView pv, int a0, const int* ord) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * ncomp;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long r = i / ncomp;
+        int k = (int)(i - r * ncomp);
+        pv.set(a0 + k, ord[r], src[i]);
+    }
+}
+template <class T>
+__global__ void k_gather_ord(T* dst, const T* src, long long n, const int* ord) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[ord[i]];
+}
+template <class T>
+__global__ void k_scatter_ord(T* dst, const T* src, long long n, const int* ord) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[ord[i]] = src[i];
+}
 __global__ void k_int_to_double(const int* a, double* b, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (double)a[i];
 }
 
 static int cgrid(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 16)); }
+
+namespace epic {
+void reset_rank(Ctx& c) {
+    if (!c.rank || c.n == 0) return;
+    k_rank_iota<<<cgrid(c.n), 256, 0, c.stream>>>(c.rank, c.n);
+    CKL();
+}
+void container_order(Ctx& c, int* ord) {
+    if (!c.rank || c.n == 0) return;
+    k_rank_inverse<<<cgrid(c.n), 256, 0, c.stream>>>(c.rank, c.n, ord);
+    CKL();
+}
+}  // namespace epic
+
+// Container order for the ABI's parcel arrays: the slot of each container
+// index in the sort scratch, or null when slots are container indices.
+static const int* abi_order(Ctx& c) {
+    if (!c.rank || c.n == 0) return nullptr;
+    int* ord = reinterpret_cast<int*>(c.get_scratch(sizeof(int) * (size_t)c.n));
+    container_order(c, ord);
+    return ord;
+}
 
 static void upload_attr(Ctx& c, const double* h, int ncomp, int a0) {
     long long n = c.n;
@@ -188,11 +255,25 @@ static void upload_attr(Ctx& c, const double* h, int ncomp, int a0) {
     CKL();
 }
 
-static void download_attr(Ctx& c, double* h, int ncomp, int a0) {
+// An attribute of the parcels in container order into the box-ordered store.
+static void upload_attr_ord(Ctx& c, const double* h, int ncomp, int a0, const int* ord) {
+    if (!ord) return upload_attr(c, h, ncomp, a0);
+    long long n = c.n;
+    if (n == 0) return;
+    double* tmp = reinterpret_cast<double*>(c.get_scratch2(sizeof(double) * ncomp * n));
+    CK(cudaMemcpyAsync(tmp, h, sizeof(double) * ncomp * n, cudaMemcpyHostToDevice, c.stream));
+    k_deinterleave_ord<<<cgrid(n * ncomp), 256, 0, c.stream>>>(tmp, ncomp, n, c.pv, a0, ord);
+    CKL();
+}
+
+// An attribute of every parcel, in container order (ord: slot of each
+// container index, null when the slots are in container order).
+static void download_attr(Ctx& c, double* h, int ncomp, int a0, const int* ord = nullptr) {
     long long n = c.n;
     if (n == 0 || !h) return;
     double* tmp = reinterpret_cast<double*>(c.get_scratch2(sizeof(double) * ncomp * n));
-    k_interleave<<<cgrid(n * ncomp), 256, 0, c.stream>>>(tmp, ncomp, n, c.pv, a0);
+    if (ord) k_interleave_ord<<<cgrid(n * ncomp), 256, 0, c.stream>>>(tmp, ncomp, n, c.pv, a0, ord);
+    else k_interleave<<<cgrid(n * ncomp), 256, 0, c.stream>>>(tmp, ncomp, n, c.pv, a0);
     CKL();
     CK(cudaMemcpyAsync(h, tmp, sizeof(double) * ncomp * n, cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
@@ -266,7 +347,7 @@ static void free_ctx(Ctx& c) {
     c.prof.ev.clear();
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
-                    c.dvor_bar, c.box_start, c.gpack, c.binc, c.label, c.dil};
+                    c.dvor_bar, c.box_start, c.gpack, c.binc, c.label, c.dil, c.rank};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.scratch) cudaFree(c.scratch);
@@ -355,6 +436,7 @@ int epic_gpu_create(const epic_cfg* cfg, epic_ctx** out) {
         // gather records: 16 values per grid point (FP32 in the mixed form)
         CK(cudaMalloc(&c.gpack, (c.pv.mixed ? sizeof(float) : sizeof(double)) * 16 * (size_t)P.fsz));
         if (!cfg->keep_order) {
+            CK(cudaMalloc(&c.rank, sizeof(int) * (size_t)c.cap));
             c.nbox = box_count(P);
             CK(cudaMalloc(&c.box_start, sizeof(int) * ((size_t)c.nbox + 1)));
             // a second store lets the sort permute in one pass; without room
@@ -423,6 +505,7 @@ int epic_gpu_set_parcels(epic_ctx* ctx, int64_t n, const double* pos, const doub
     upload_attr(c, vol, 1, A_VOL);
     upload_attr(c, buoy, 1, A_BUOY);
     if (hum) upload_attr(c, hum, 1, A_HUM);
+    reset_rank(c);
     c.has_parcels = true;
     CK(cudaStreamSynchronize(c.stream));
     API_END
@@ -461,12 +544,13 @@ int epic_gpu_get_parcels(epic_ctx* ctx, int64_t cap, int64_t* n, double* pos, do
     if (!n) throw CudaError(EPIC_ERR_ARG, "get_parcels: null count");
     *n = c.n;
     if (cap < c.n) throw CudaError(EPIC_ERR_ARG, "get_parcels: capacity too small");
-    download_attr(c, pos, 3, A_X);
-    download_attr(c, vor, 3, A_VX);
-    download_attr(c, B, 5, A_B11);
-    download_attr(c, vol, 1, A_VOL);
-    download_attr(c, buoy, 1, A_BUOY);
-    download_attr(c, hum, 1, A_HUM);
+    const int* ord = abi_order(c);
+    download_attr(c, pos, 3, A_X, ord);
+    download_attr(c, vor, 3, A_VX, ord);
+    download_attr(c, B, 5, A_B11, ord);
+    download_attr(c, vol, 1, A_VOL, ord);
+    download_attr(c, buoy, 1, A_BUOY, ord);
+    download_attr(c, hum, 1, A_HUM, ord);
     API_END
 }
 
@@ -477,8 +561,22 @@ int epic_gpu_get_labels(epic_ctx* ctx, int64_t cap, int64_t* n, int64_t* label, 
     if (!n) throw CudaError(EPIC_ERR_ARG, "get_labels: null count");
     *n = c.n;
     if (cap < c.n) throw CudaError(EPIC_ERR_ARG, "get_labels: capacity too small");
-    if (label) CK(cudaMemcpyAsync(label, c.label, sizeof(long long) * (size_t)c.n, cudaMemcpyDeviceToHost, c.stream));
-    if (dilution) CK(cudaMemcpyAsync(dilution, c.dil, sizeof(double) * (size_t)c.n, cudaMemcpyDeviceToHost, c.stream));
+    const int* ord = abi_order(c);
+    const long long* lsrc = c.label;
+    const double* dsrc = c.dil;
+    if (ord) {
+        char* t = reinterpret_cast<char*>(c.get_scratch2(16 * (size_t)c.n + 256));
+        long long* tl = reinterpret_cast<long long*>(t);
+        double* td = reinterpret_cast<double*>(t + ((8 * (size_t)c.n + 255) & ~(size_t)255));
+        k_gather_ord<long long><<<cgrid(c.n), 256, 0, c.stream>>>(tl, c.label, c.n, ord);
+        CKL();
+        k_gather_ord<double><<<cgrid(c.n), 256, 0, c.stream>>>(td, c.dil, c.n, ord);
+        CKL();
+        lsrc = tl;
+        dsrc = td;
+    }
+    if (label) CK(cudaMemcpyAsync(label, lsrc, sizeof(long long) * (size_t)c.n, cudaMemcpyDeviceToHost, c.stream));
+    if (dilution) CK(cudaMemcpyAsync(dilution, dsrc, sizeof(double) * (size_t)c.n, cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     API_END
 }
@@ -488,8 +586,21 @@ int epic_gpu_set_labels(epic_ctx* ctx, int64_t n, const int64_t* label, const do
     Ctx& c = ctx->c;
     if (!c.label) throw CudaError(EPIC_ERR_STATE, "labels are off (cfg.labels = 0)");
     if (!label || !dilution || n != c.n) throw CudaError(EPIC_ERR_ARG, "set_labels: bad arguments");
-    CK(cudaMemcpyAsync(c.label, label, sizeof(long long) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
-    CK(cudaMemcpyAsync(c.dil, dilution, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    const int* ord = abi_order(c);
+    if (ord && n > 0) {
+        char* t = reinterpret_cast<char*>(c.get_scratch2(16 * (size_t)n + 256));
+        long long* tl = reinterpret_cast<long long*>(t);
+        double* td = reinterpret_cast<double*>(t + ((8 * (size_t)n + 255) & ~(size_t)255));
+        CK(cudaMemcpyAsync(tl, label, sizeof(long long) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+        CK(cudaMemcpyAsync(td, dilution, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+        k_scatter_ord<long long><<<cgrid(n), 256, 0, c.stream>>>(c.label, tl, n, ord);
+        CKL();
+        k_scatter_ord<double><<<cgrid(n), 256, 0, c.stream>>>(c.dil, td, n, ord);
+        CKL();
+    } else {
+        CK(cudaMemcpyAsync(c.label, label, sizeof(long long) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+        CK(cudaMemcpyAsync(c.dil, dilution, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    }
     CK(cudaStreamSynchronize(c.stream));
     API_END
 }
@@ -508,10 +619,11 @@ int epic_gpu_get_parcel_rk(epic_ctx* ctx, int64_t cap, int64_t* n, double* dpos,
     if (!n) throw CudaError(EPIC_ERR_ARG, "null");
     *n = c.n;
     if (cap < c.n) throw CudaError(EPIC_ERR_ARG, "get_parcel_rk: capacity too small");
-    download_attr(c, dpos, 3, A_DX);
-    download_attr(c, dvor, 3, A_DVX);
-    download_attr(c, strain, 8, A_S0);
-    download_attr(c, dB, 5, A_DB0);
+    const int* ord = abi_order(c);
+    download_attr(c, dpos, 3, A_DX, ord);
+    download_attr(c, dvor, 3, A_DVX, ord);
+    download_attr(c, strain, 8, A_S0, ord);
+    download_attr(c, dB, 5, A_DB0, ord);
     API_END
 }
 
@@ -519,9 +631,10 @@ int epic_gpu_set_parcel_rk(epic_ctx* ctx, int64_t n, const double* dpos, const d
     API_BEGIN
     Ctx& c = ctx->c;
     if (n != c.n) throw CudaError(EPIC_ERR_ARG, "set_parcel_rk: count mismatch");
-    if (dpos) upload_attr(c, dpos, 3, A_DX);
-    if (dvor) upload_attr(c, dvor, 3, A_DVX);
-    if (dB) upload_attr(c, dB, 5, A_DB0);
+    const int* ord = abi_order(c);
+    if (dpos) upload_attr_ord(c, dpos, 3, A_DX, ord);
+    if (dvor) upload_attr_ord(c, dvor, 3, A_DVX, ord);
+    if (dB) upload_attr_ord(c, dB, 5, A_DB0, ord);
     CK(cudaStreamSynchronize(c.stream));
     API_END
 }

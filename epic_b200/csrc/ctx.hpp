@@ -128,6 +128,13 @@ struct Ctx {
     int n_partials = 0;
     // second parcel store for the box reordering (keep_order == 0)
     double* pv_alt = nullptr;
+    // keep_order == 0: rank[i] is the index the parcel in slot i has in the
+    // reference's container (parcels%position(:, rank + 1)).  The box sort
+    // moves it with the parcel; merge (nearest-search order, merge index m,
+    // parcel_delete's hole filling) and split (child indices) follow it, so the
+    // box-ordered store takes the reference's decisions, and the ABI returns
+    // parcels in container order.  Null when keep_order == 1 (slot = index).
+    int* rank = nullptr;
     // box ranges of the sorted store: parcels [box_start[b], box_start[b + 1])
     // of [0, n_box) lie in box b at the last sort
     int* box_start = nullptr;
@@ -248,6 +255,10 @@ void allow_smem(K kernel, size_t bytes) {
 }
 
 // api.cu
+// rank[i] = i for the n parcels (a store loaded in container order)
+void reset_rank(Ctx& c);
+// ord[r] = slot of the parcel with container index r, r < n (null rank: none)
+void container_order(Ctx& c, int* ord);
 void grow_store(Ctx& c, long long need);
 void grow_scratch_for_capacity(Ctx& c);
 void prof_begin(Ctx& c, const char* name);

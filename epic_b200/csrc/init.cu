@@ -160,6 +160,7 @@ static void launch_init(Ctx& c, const epic_init_spec& s, int npd) {
     int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 16));
     k_init_state<<<grid, 256, 0, c.stream>>>(A, c.pv);
     CKL();
+    reset_rank(c);
     c.has_parcels = true;
 }
 

@@ -151,6 +151,39 @@ __global__ void k_make_copies(Params P, Box B, PView pv, const int* Ls, int nls,
 }
 
 __global__ void k_iota(int* v, long long n) { MLOOP(n) v[i] = (int)i; }
+__global__ void k_iota_from(int* v, long long n, int first) { MLOOP(n) v[i] = first + (int)i; }
+
+// Box-ordered store (Ctx::rank): per-parcel values in container order
+// (ord[r] = slot of container index r).
+__global__ void k_by_rank(const int* ord, const int* a, long long n, int* ar) { MLOOP(n) ar[i] = a[ord[i]]; }
+// the local entries of the binning sort in container order: keys cell, values slot
+__global__ void k_rank_cells(const int* ord, const int* cell0, long long n, int* cell, int* vals) {
+    MLOOP(n) {
+        const int s = ord[i];
+        cell[i] = cell0[s];
+        vals[i] = s;
+    }
+}
+__global__ void k_pairs_rank(const int* rank, const int* ism, const int* icl, int nm, int* ri, int* rc) {
+    MLOOP(nm) {
+        ri[i] = rank[ism[i]];
+        rc[i] = rank[icl[i]];
+    }
+}
+// parcel_delete in container indices (parcel_container.f90:413-458): flags of
+// the deleted indices below newN (holes) and of the kept ones from newN up
+// (sources)
+__global__ void k_del_rank_flags(const int* ord, const char* del, int N, int newN, int* hole, int* src) {
+    MLOOP(N) {
+        const int d = del[ord[i]];
+        hole[i] = (i < newN) && d;
+        src[i] = (i >= newN) && !d;
+    }
+}
+// the i-th hole (ascending) takes the kept parcel with the i-th largest index
+__global__ void k_rerank(const int* ord, const int* holes, const int* srcs, int nh, int* rank) {
+    MLOOP(nh) rank[ord[srcs[nh - 1 - i]]] = holes[i];
+}
 
 // M6: cell ranges of the sorted (cell, index) list
 __global__ void k_cell_ranges(const int* keys, long long nt, int* cstart, int* cend) {
@@ -490,6 +523,10 @@ __global__ void k_move(PView pv, const int* holes, const int* srcs, int nh, int 
     }
 }
 
+__global__ void k_move_rank(int* rank, const int* holes, const int* srcs, int nh, int newN) {
+    MLOOP(nh) rank[holes[i]] = rank[newN + srcs[nh - 1 - i]];
+}
+
 __global__ void k_move_labels(long long* label, double* dil, const int* holes, const int* srcs, int nh, int newN) {
     MLOOP(nh) {
         const int dst = holes[i], src = newN + srcs[nh - 1 - i];
@@ -533,7 +570,7 @@ static size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 size_t merge_scratch_bytes(long long n) {
     size_t cub1 = 0;
     cub::DeviceSelect::Flagged(nullptr, cub1, (int*)0, (int*)0, (int*)0, (int*)0, (int)n);
-    return al(sizeof(int) * (size_t)n) * 5 + al(cub1) + 4096;
+    return al(sizeof(int) * (size_t)n) * 7 + al(cub1) + 4096;
 }
 
 long long parcel_merge(Ctx& c) {
@@ -561,11 +598,23 @@ long long parcel_merge(Ctx& c) {
     int* idx = a1.take<int>(N);
     int* dcount = a1.take<int>(8);
     void* tmp1 = a1.take<char>(cub1);
+    // box-ordered store: the small parcels (merge index m), the cell lists and
+    // parcel_delete follow the container indices in c.rank
+    const bool ranked = c.rank != nullptr;
+    int* ord = ranked ? a1.take<int>(N) : nullptr;
+    int* smallr = ranked ? a1.take<int>(N) : nullptr;
     k_bin_locals<<<mgrid(N), MB, 0, st>>>(P, B, c.pv, N, cell0, small, bits, err);
     CKL();
-    k_iota<<<mgrid(N), MB, 0, st>>>(idx, N);
-    CKL();
-    CK(cub::DeviceSelect::Flagged(tmp1, cub1, idx, small, Ls, dcount, N, st));
+    if (ranked) {
+        container_order(c, ord);
+        k_by_rank<<<mgrid(N), MB, 0, st>>>(ord, small, N, smallr);
+        CKL();
+        CK(cub::DeviceSelect::Flagged(tmp1, cub1, ord, smallr, Ls, dcount, N, st));
+    } else {
+        k_iota<<<mgrid(N), MB, 0, st>>>(idx, N);
+        CKL();
+        CK(cub::DeviceSelect::Flagged(tmp1, cub1, idx, small, Ls, dcount, N, st));
+    }
     const int nls = read_int(c, dcount);
     if (nls == 0) {
         k_periodic_m<<<mgrid(N), MB, 0, st>>>(P, c.pv, N);
@@ -580,7 +629,9 @@ long long parcel_merge(Ctx& c) {
     cub::DeviceRadixSort::SortPairs(nullptr, c_sort, (int*)0, (int*)0, (int*)0, (int*)0, (int)NTm, 0, 32, st);
     cub::DeviceScan::ExclusiveSum(nullptr, c_scan, (int*)0, (int*)0, (int)(8LL * nls + 1), st);
     cub::DeviceSelect::Flagged(nullptr, c_sel, (int*)0, (int*)0, (int*)0, (int*)0, nls, st);
-    size_t cubb = std::max({c_sort, c_scan, c_sel});
+    size_t c_sel_n = 0;
+    if (ranked) cub::DeviceSelect::Flagged(nullptr, c_sel_n, (int*)0, (int*)0, (int*)0, (int*)0, N, st);
+    size_t cubb = std::max({c_sort, c_scan, c_sel, c_sel_n});
     size_t bytes2 = al(sizeof(int) * NTm) * 4                       // cell, vals, skeys, svals
                   + al(sizeof(int) * (8 * (size_t)nls + 1)) * 3       // F, off, copyidx
                   + al(sizeof(double) * ncp_max) * 3 + al(sizeof(int) * ncp_max) * 2   // copies
@@ -606,7 +657,12 @@ long long parcel_merge(Ctx& c) {
     int* cstart = ar.take<int>(B.hncell);
     int* cend = ar.take<int>(B.hncell);
 
-    CK(cudaMemcpyAsync(cell, cell0, sizeof(int) * (size_t)N, cudaMemcpyDeviceToDevice, st));
+    if (ranked) {
+        k_rank_cells<<<mgrid(N), MB, 0, st>>>(ord, cell0, N, cell, vals);
+        CKL();
+    } else {
+        CK(cudaMemcpyAsync(cell, cell0, sizeof(int) * (size_t)N, cudaMemcpyDeviceToDevice, st));
+    }
     k_copy_flags<<<mgrid(8LL * nls), MB, 0, st>>>(Ls, nls, bits, F);
     CKL();
     CK(cudaMemsetAsync(F + 8LL * nls, 0, sizeof(int), st));
@@ -619,7 +675,9 @@ long long parcel_merge(Ctx& c) {
     CK(cudaMemsetAsync(copyidx, 0xff, sizeof(int) * 8 * (size_t)nls, st));
     k_make_copies<<<mgrid(8LL * nls), MB, 0, st>>>(P, B, c.pv, Ls, nls, F, off, C, cell + N, copyidx, err);
     CKL();
-    k_iota<<<mgrid(NT), MB, 0, st>>>(vals, NT);
+    // locals in container order (their slots), then the copies N + q
+    if (ranked) k_iota_from<<<mgrid(ncp), MB, 0, st>>>(vals + N, ncp, N);
+    else k_iota<<<mgrid(NT), MB, 0, st>>>(vals, NT);
     CKL();
     int endbit = 1;
     while ((1LL << endbit) < B.hncell) ++endbit;
@@ -708,8 +766,21 @@ long long parcel_merge(Ctx& c) {
     CKL();
     c.last_isma.resize(nm);
     c.last_iclo.resize(nm);
-    CK(cudaMemcpyAsync(c.last_isma.data(), ism, sizeof(int) * nm, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(c.last_iclo.data(), icl, sizeof(int) * nm, cudaMemcpyDeviceToHost, st));
+    {
+        // the pairs as container indices
+        const int* pi = ism;
+        const int* pc = icl;
+        if (ranked) {
+            int* ri = ar.take<int>(nm);
+            int* rc = ar.take<int>(nm);
+            k_pairs_rank<<<mgrid(nm), MB, 0, st>>>(c.rank, ism, icl, nm, ri, rc);
+            CKL();
+            pi = ri;
+            pc = rc;
+        }
+        CK(cudaMemcpyAsync(c.last_isma.data(), pi, sizeof(int) * nm, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(c.last_iclo.data(), pc, sizeof(int) * nm, cudaMemcpyDeviceToHost, st));
+    }
 
     // collect_merge_stats (parcel_merge.f90:365-394)
     unsigned long long* bigc = ar.take<unsigned long long>(1);
@@ -751,6 +822,28 @@ long long parcel_merge(Ctx& c) {
     CK(cudaMemsetAsync(del, 0, N, st));
     k_mark_deleted<<<mgrid(nm), MB, 0, st>>>(ism, nm, del);
     CKL();
+    if (ranked) {
+        // the container indices after parcel_delete; the binning arrays are
+        // free now (the group merge reads gk, gv and ism)
+        int* hole_f = cell;
+        int* src_f = vals;
+        int* iota = skeys;
+        int* holes_r = svals;
+        int* srcs_r = svals + N;
+        k_del_rank_flags<<<mgrid(N), MB, 0, st>>>(ord, del, N, newN, hole_f, src_f);
+        CKL();
+        k_iota<<<mgrid(N), MB, 0, st>>>(iota, N);
+        CKL();
+        size_t b = cubb;
+        CK(cub::DeviceSelect::Flagged(ctmp, b, iota, hole_f, holes_r, dcount, N, st));
+        b = cubb;
+        CK(cub::DeviceSelect::Flagged(ctmp, b, iota, src_f, srcs_r, dcount + 1, N, st));
+        const int nhr = read_int(c, dcount);
+        if (nhr > 0) {
+            k_rerank<<<mgrid(nhr), MB, 0, st>>>(ord, holes_r, srcs_r, nhr, c.rank);
+            CKL();
+        }
+    }
     int* hf = head;      // reuse nm-sized arrays
     int* holes = gidx;
     k_hole_flags<<<mgrid(nm), MB, 0, st>>>(ism, nm, newN, hf);
@@ -772,6 +865,10 @@ long long parcel_merge(Ctx& c) {
         CK(cub::DeviceSelect::Flagged(ctmp, b, sidx, sf, srcs, dcount + 1, N - newN, st));
         k_move<<<mgrid((long long)nh * N_ATTR), MB, 0, st>>>(c.pv, holes, srcs, nh, newN);
         CKL();
+        if (ranked) {
+            k_move_rank<<<mgrid(nh), MB, 0, st>>>(c.rank, holes, srcs, nh, newN);
+            CKL();
+        }
         if (c.label) {
             k_move_labels<<<mgrid(nh), MB, 0, st>>>(c.label, c.dil, holes, srcs, nh, newN);
             CKL();

@@ -763,6 +763,18 @@ __global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, 
     }
 }
 
+// Container indices of the children (box-ordered store): the reference
+// appends them in ascending parent index (parcel_split.f90:132-137 with one
+// thread), so child of parent i gets n + (splitting parents before rank[i]).
+__global__ void k_flags_by_rank(const int* flag, const int* ord, long long n, int* flagr) {
+    PLOOP(n) flagr[i] = flag[ord[i]];
+}
+__global__ void k_split_rank(const int* flag, const int* offs, const int* offr, long long n, int* rank) {
+    PLOOP(n) {
+        if (flag[i]) rank[n + offs[i]] = (int)(n + offr[rank[i]]);
+    }
+}
+
 long long parcel_split(Ctx& c) {
     long long n = c.n;
     if (n == 0) return 0;
@@ -788,6 +800,21 @@ long long parcel_split(Ctx& c) {
     if (grow) grow_store(c, n + ns);
     k_split_apply<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, flag, offs, c.label, c.dil, &c.dsc->err);
     CKL();
+    if (c.rank) {
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        char* b2 = reinterpret_cast<char*>(c.get_scratch2(al(sizeof(int) * n) + 2 * al(sizeof(int) * (n + 1)) + al(need_cub)));
+        int* ord = reinterpret_cast<int*>(b2);
+        int* flagr = reinterpret_cast<int*>(b2 + al(sizeof(int) * n));
+        int* offr = reinterpret_cast<int*>(b2 + al(sizeof(int) * n) + al(sizeof(int) * (n + 1)));
+        void* tmp2 = b2 + al(sizeof(int) * n) + 2 * al(sizeof(int) * (n + 1));
+        container_order(c, ord);
+        k_flags_by_rank<<<pgrid(n), PB, 0, c.stream>>>(flag, ord, n, flagr);
+        CKL();
+        CK(cudaMemsetAsync(flagr + n, 0, sizeof(int), c.stream));
+        CK(cub::DeviceScan::ExclusiveSum(tmp2, need_cub, flagr, offr, (int)n + 1, c.stream));
+        k_split_rank<<<pgrid(n), PB, 0, c.stream>>>(flag, offs, offr, n, c.rank);
+        CKL();
+    }
     // flag and offs live in the sort scratch: it is resized for the new
     // capacity only now, behind the kernel that reads them
     if (grow) grow_scratch_for_capacity(c);

@@ -1281,6 +1281,13 @@ void sort_parcels(Ctx& c) {
             }
         }
     }
+    if (c.rank) {
+        // container indices follow the permutation through the key arrays
+        int* tr = reinterpret_cast<int*>(k0);
+        k_gather_slot<int><<<pgrid(n), PB, 0, c.stream>>>(c.rank, tr, n, i1);
+        CKL();
+        CK(cudaMemcpyAsync(c.rank, tr, sizeof(int) * n, cudaMemcpyDeviceToDevice, c.stream));
+    }
     if (c.label) {
         // labels and dilutions follow the permutation through the key arrays
         // (free again after k_box_start; k0 and k1 hold >= 8 n bytes)

@@ -62,3 +62,21 @@ def pair(setup, olib, glib, init=True, **overrides):
     oc = make_context(setup, olib, **overrides)
     gc = make_context(setup, glib, **overrides)
     return oc, gc
+
+
+def parcel_errors(a, b, extent):
+    """Relative errors (to the largest |value| of b) of every parcel attribute
+    of a against b, parcel by parcel in container order.  Horizontal position
+    differences are taken modulo the period: a parcel within rounding of a
+    periodic edge may be stored on either side of it (apply_periodic_bc,
+    parcel_bc.f90:17-40, truncates (x - centre) * 2 / L, so one ulp decides)."""
+    out = {}
+    for k in a:
+        x = np.asarray(a[k], dtype=np.float64)
+        y = np.asarray(b[k], dtype=np.float64)
+        d = x - y
+        if k == "pos":
+            for c in (0, 1):
+                d[:, c] -= extent[c] * np.round(d[:, c] / extent[c])
+        out[k] = float(np.abs(d).max() / max(np.abs(y).max(), 1e-300)) if len(y) else 0.0
+    return out
