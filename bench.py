@@ -230,10 +230,112 @@ def algorithmic_bytes(kernel: str, n: int, nx: int, ny: int, nz: int, form: str 
     raise KeyError(kernel)
 
 
+class Timer:
+    """The library's own CUDA-event timers around a window of steps: the
+    window on the context's stream, one named kernel (every launch of it),
+    the launch count and the SM clocks sampled meanwhile."""
+
+    def __init__(self, lib, ctx, stream, dev):
+        import ctypes as C
+        self.C, self.lib, self.ctx, self.stream, self.dev = C, lib, ctx, stream, dev
+        L = lib.lib
+        L.epic_gpu_profile_kernel.argtypes = [C.c_void_p, C.c_char_p]
+        L.epic_gpu_kernel_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.epic_gpu_launch_count.argtypes = [C.POINTER(C.c_int64)]
+
+    def window(self, t, steps, kernel="stage", barrier=lambda: None):
+        import torch
+        C, L, ctx = self.C, self.lib.lib, self.ctx
+        L.epic_gpu_profile_kernel(ctx.h, kernel.encode())
+        clocks = ClockSampler(self.dev)
+        barrier()
+        torch.cuda.synchronize()
+        ctx.sync()
+        clocks.start()
+        l0 = C.c_int64()
+        L.epic_gpu_launch_count(C.byref(l0))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        psteps, infos = 0, []
+        nmin = nmax = ctx.num_parcels()
+        for _ in range(steps):
+            psteps += ctx.num_parcels()
+            t, info = ctx.step(t)
+            infos.append(info)
+            nmin, nmax = min(nmin, info.n_parcels), max(nmax, info.n_parcels)
+        e1.record(self.stream)
+        ctx.sync()
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop()
+        l1 = C.c_int64()
+        L.epic_gpu_launch_count(C.byref(l1))
+        kms, kl = C.c_double(), C.c_int64()
+        L.epic_gpu_kernel_time(ctx.h, C.byref(kms), C.byref(kl))
+        L.epic_gpu_profile_kernel(ctx.h, b"")
+        return t, {"ms": e0.elapsed_time(e1), "psteps": psteps, "nmin": int(nmin), "nmax": int(nmax),
+                   "kernel_ms": kms.value, "kernel_launches": kl.value, "clocks": clk,
+                   "launches": int(l1.value - l0.value), "infos": infos}
+
+
+def stage_roofline(w: dict, steps: int, setup, form: str) -> dict:
+    """The dominant kernel against HBM: one k_stage launch (grid2par + LS-RK
+    update of every parcel), its algorithmic bytes over its average
+    CUDA-event duration in the timed window."""
+    peak, peak_kind = peaks()
+    avg_n = w["psteps"] / steps
+    unit_ms = w["kernel_ms"] / max(w["kernel_launches"], 1)
+    alg = stage_launch_bytes(int(avg_n), setup.nx, setup.ny, setup.nz, form)
+    achieved = alg / (unit_ms * 1e-3) / 1e9 if w["kernel_launches"] else None
+    r = {"bound": "hbm", "kernel": "stage",
+         "unit_of_work": "one k_stage launch (grid2par + LS-RK update of every parcel), averaged over the 5 stages",
+         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak if achieved else None),
+         "traffic": None, "peak_source": peak_kind, "ms_per_unit": unit_ms, "launches": w["kernel_launches"],
+         "share_of_step_time": w["kernel_ms"] / w["ms"] if w["ms"] else None, "algorithmic_bytes_per_unit": alg}
+    # DRAM bytes of one k_stage<0,0> launch (stages 2-5) from ncu captures of
+    # the stage kernel (64^3, 2,097,152 parcels, early flow: plain 539.9 MB
+    # read + 323.1 MB written = 411.5 B per parcel; mixed 337.3 + 184.7 MB =
+    # 248.9 B), scaled by the parcels of this run (the traffic grows with
+    # them), against the algorithmic bytes of the same stages.  Lines still
+    # dirty in L2 when the launch ends (up to its 126 MB) are not counted,
+    # which puts the mixed capture a little below its algorithmic bytes.
+    per_parcel = 248.9 if form == "mixed" else 411.5
+    r["traffic"] = per_parcel * avg_n
+    r["traffic_source"] = (f"ncu dram__bytes_read+write of k_stage<0,0,{'float' if form == 'mixed' else 'double'}> "
+                           "(stages 2-5), 64^3 capture scaled by parcels")
+    r["traffic_over_algorithmic"] = r["traffic"] / stage_launch_bytes(int(avg_n), setup.nx, setup.ny, setup.nz, form,
+                                                                      later_only=True)
+    return r
+
+
+def form_line(w: dict, steps: int, setup, form: str, extra: dict | None = None) -> dict:
+    """The summary of one timed window of a form (parcel-steps/s on the
+    device, with its roofline, clocks and launches)."""
+    value = w["psteps"] / (w["ms"] * 1e-3)
+    peak, peak_kind = peaks()
+    out = {"value": value, "unit": UNIT, "ms_per_step": w["ms"] / steps, "steps": steps,
+           "parcels_range_timed": [w["nmin"], w["nmax"]], "grid": [setup.nx, setup.ny, setup.nz],
+           "roofline": stage_roofline(w, steps, setup, form), "step_roofline": step_roofline(value, form, peak, peak_kind),
+           "clocks": w["clocks"], "gpu_launches": w["launches"]}
+    if extra:
+        out.update(extra)
+    return out
+
+
+def context_stream(lib, ctx, dev):
+    import ctypes as C
+    import torch
+    sp = C.c_void_p()
+    lib.lib.epic_gpu_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.lib.epic_gpu_get_stream(ctx.h, C.byref(sp))
+    return torch.cuda.ExternalStream(sp.value, device=dev)
+
+
 def run_ours(args):
     import torch
     import epic_b200
-    from epic_b200 import initial, abi
+    from epic_b200 import initial
 
     world, rank, local = dist_setup()
     if world > 1:
@@ -245,8 +347,9 @@ def run_ours(args):
     dev = torch.cuda.current_device()
 
     lib = epic_b200.load()
-    # the device keeps parcels ordered by boxes of cells (keep_order=0); the
-    # parcel set is the reference's, its storage order is not
+    # keep_order = 0: the device keeps the parcels ordered by boxes of cells
+    # and carries each one's index in the reference's container, so merges and
+    # splits take the reference's decisions
     mixed = args.form == "mixed"
     large = args.workload == "thermal2-512x512x256"
     if args.device_init or large:
@@ -261,14 +364,8 @@ def run_ours(args):
         setup = initial.config(args.workload)
         ctx = epic_b200.make_context(setup, lib, keep_order=args.keep_order, precision=1 if mixed else 0)
     tuning = ctx.autotune() if not args.no_autotune else None
-    import ctypes as C
-    sp = C.c_void_p()
-    lib.lib.epic_gpu_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
-    lib.lib.epic_gpu_get_stream(ctx.h, C.byref(sp))
-    stream = torch.cuda.ExternalStream(sp.value, device=dev)
-    lib.lib.epic_gpu_profile_kernel.argtypes = [C.c_void_p, C.c_char_p]
-    lib.lib.epic_gpu_kernel_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
-    lib.lib.epic_gpu_launch_count.argtypes = [C.POINTER(C.c_int64)]
+    stream = context_stream(lib, ctx, dev)
+    timer = Timer(lib, ctx, stream, dev if world == 1 else local)
 
     def barrier():
         if world > 1:
@@ -276,51 +373,23 @@ def run_ours(args):
             dist.barrier()
 
     t = 0.0
+    done = 0
     # optional untimed spin-up to a developed flow (deformed parcels, splits)
-    for _ in range(args.spinup):
+    for _ in range(args.spinup + args.warmup):
         t, _info = ctx.step(t)
-    for _ in range(args.warmup):
-        t, _info = ctx.step(t)
-    # ---- device-resident timed region
-    lib.lib.epic_gpu_profile_kernel(ctx.h, args.roofline_kernel.encode())
-    clocks = ClockSampler(dev if world == 1 else local)
-    barrier()
-    torch.cuda.synchronize()
-    ctx.sync()
-    clocks.start()
-    l0 = C.c_int64()
-    lib.lib.epic_gpu_launch_count(C.byref(l0))
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    psteps = 0
-    nmin = nmax = ctx.num_parcels()
-    infos = []
-    for _ in range(args.steps):
-        n_start = ctx.num_parcels()
-        psteps += n_start
-        t, info = ctx.step(t)
-        infos.append(info)
-        nmin = min(nmin, info.n_parcels)
-        nmax = max(nmax, info.n_parcels)
-    e1.record(stream)
-    ctx.sync()
-    torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    l1 = C.c_int64()
-    lib.lib.epic_gpu_launch_count(C.byref(l1))
-    kms = C.c_double()
-    kl = C.c_int64()
-    lib.lib.epic_gpu_kernel_time(ctx.h, C.byref(kms), C.byref(kl))
-    lib.lib.epic_gpu_profile_kernel(ctx.h, b"")
+        done += 1
+    t, w = timer.window(t, args.steps, args.roofline_kernel, barrier)
+    done += args.steps
+    ms, psteps = w["ms"], w["psteps"]
+    infos = w["infos"]
 
     # per-kernel CUDA-event times over one extra (untimed) step each
     kernel_times = {}
+    import ctypes as C
     for kname in [k for k in args.profile_kernels.split(",") if k]:
         lib.lib.epic_gpu_profile_kernel(ctx.h, kname.encode())
         t, _ = ctx.step(t)
+        done += 1
         km, kn = C.c_double(), C.c_int64()
         lib.lib.epic_gpu_kernel_time(ctx.h, C.byref(km), C.byref(kn))
         kernel_times[kname] = {"ms_per_step": km.value, "launches_per_step": kn.value}
@@ -331,42 +400,18 @@ def run_ours(args):
     # max over ranks, sum of work
     ms_max, ps_total = reduce_timing(ms, float(psteps))
     value = ps_total / (ms_max * 1e-3)
-
-    # roofline of the dominant kernel: one launch of the stage kernel (grid2par +
-    # LS-RK update, 5 per step), or of the kernel named
     peak, peak_kind = peaks()
-    avg_n = psteps / args.steps
     if args.roofline_kernel == "stage":
-        unit_ms = kms.value / max(kl.value, 1)
-        alg = stage_launch_bytes(int(avg_n), setup.nx, setup.ny, setup.nz, args.form)
-        what = "one k_stage launch (grid2par + LS-RK update of every parcel), averaged over the 5 stages"
+        roofline = stage_roofline(w, args.steps, setup, args.form)
     else:
-        unit_ms = kms.value / max(kl.value, 1)
+        avg_n = psteps / args.steps
+        unit_ms = w["kernel_ms"] / max(w["kernel_launches"], 1)
         alg = algorithmic_bytes(args.roofline_kernel, int(avg_n), setup.nx, setup.ny, setup.nz, args.form)
-        what = f"one {args.roofline_kernel} launch"
-    achieved = alg / (unit_ms * 1e-3) / 1e9 if kl.value else None
-    roofline = {"bound": "hbm", "kernel": args.roofline_kernel, "unit_of_work": what, "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": (achieved / peak if achieved else None), "traffic": None,
-                "peak_source": peak_kind, "ms_per_unit": unit_ms, "launches": kl.value,
-                "share_of_step_time": kms.value / ms if ms else None,
-                "algorithmic_bytes_per_unit": alg}
-    if args.traffic is not None:
-        roofline["traffic"] = args.traffic
-    elif args.roofline_kernel == "stage":
-        # DRAM bytes of one k_stage<0,0> launch (stages 2-5) from ncu
-        # captures of the stage kernel (64^3, 2,097,152 parcels,
-        # early flow: plain 539.9 MB read + 323.1 MB written = 411.5 B per
-        # parcel; mixed 337.3 + 184.7 MB = 248.9 B), scaled by the parcels of
-        # this run (the traffic grows with them), against the algorithmic
-        # bytes of the same stages.  Lines still dirty in L2 when the launch
-        # ends (up to its 126 MB) are not in the count, which puts the mixed
-        # capture a little below its algorithmic bytes.
-        per_parcel = 248.9 if args.form == "mixed" else 411.5
-        roofline["traffic"] = per_parcel * avg_n
-        roofline["traffic_source"] = (f"ncu dram__bytes_read+write of k_stage<0,0,{'float' if args.form == 'mixed' else 'double'}> "
-                                      "(stages 2-5), 64^3 capture scaled by parcels")
-        roofline["traffic_over_algorithmic"] = roofline["traffic"] / stage_launch_bytes(
-            int(avg_n), setup.nx, setup.ny, setup.nz, args.form, later_only=True)
+        achieved = alg / (unit_ms * 1e-3) / 1e9 if w["kernel_launches"] else None
+        roofline = {"bound": "hbm", "kernel": args.roofline_kernel, "unit_of_work": f"one {args.roofline_kernel} launch",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak if achieved else None),
+                    "traffic": args.traffic, "peak_source": peak_kind, "ms_per_unit": unit_ms,
+                    "launches": w["kernel_launches"], "algorithmic_bytes_per_unit": alg}
 
     # ---- end-to-end through the C ABI with host buffers (drop-in serial step:
     # the host container owns the parcels; every step copies them in, steps,
@@ -383,6 +428,20 @@ def run_ours(args):
         P = C.POINTER(C.c_double)
         fn_set = lib.fn["set_parcels"]
         fn_get = lib.fn["get_parcels"]
+        names = ("pos", "vor", "B", "vol", "buoy", "hum")
+
+        def e2e_step(t, n_now):
+            rc = fn_set(ctx.h, C.c_int64(n_now), *(host[k].ctypes.data_as(P) for k in names))
+            assert rc == 0, ctx.lib.fn["last_error"](ctx.h)
+            t, info = ctx.step(t)
+            nn = C.c_int64()
+            rc = fn_get(ctx.h, C.c_int64(cap), C.byref(nn), *(host[k].ctypes.data_as(P) for k in names))
+            assert rc == 0
+            return t, nn.value
+
+        # one untimed step warms the pinned copies and the reloaded store
+        t, n_now = e2e_step(t, n_now)
+        done += 1
         barrier()
         torch.cuda.synchronize()
         h2d = d2h = 0
@@ -392,16 +451,11 @@ def run_ours(args):
         f1 = torch.cuda.Event(enable_timing=True)
         f0.record(stream)
         for _ in range(args.e2e_steps):
-            rc = fn_set(ctx.h, C.c_int64(n_now), *(host[k].ctypes.data_as(P) for k in ("pos", "vor", "B", "vol", "buoy", "hum")))
-            assert rc == 0, ctx.lib.fn["last_error"](ctx.h)
             h2d += n_now * 14 * 8
             eps += n_now
-            t, info = ctx.step(t)
-            nn = C.c_int64()
-            rc = fn_get(ctx.h, C.c_int64(cap), C.byref(nn), *(host[k].ctypes.data_as(P) for k in ("pos", "vor", "B", "vol", "buoy", "hum")))
-            assert rc == 0
-            n_now = nn.value
+            t, n_now = e2e_step(t, n_now)
             d2h += n_now * 14 * 8
+            done += 1
         f1.record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
@@ -409,7 +463,7 @@ def run_ours(args):
         ems_max, eps_total = reduce_timing(ems, float(eps))
         e2e = {"value": eps_total / (ems_max * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.e2e_steps, "d2h_bytes_per_step": d2h // args.e2e_steps,
-               "steps": args.e2e_steps, "wall_s": wall,
+               "steps": args.e2e_steps, "warmup_steps": 1, "wall_s": wall,
                "mode": "host-owned parcel container: set_parcels (pinned H2D) + step + get_parcels (D2H) every step"}
 
     store_gb = int(setup.n) * (184 if mixed else 312) / 1e9
@@ -427,22 +481,42 @@ def run_ours(args):
                                "merge/split/corrections on",
                    "form": args.form,
                    "grid": [setup.nx, setup.ny, setup.nz], "parcels_at_start": int(setup.n),
-                   "parcels_range_timed": [int(nmin), int(nmax)], "precision": precision,
+                   "parcels_range_timed": [w["nmin"], w["nmax"]], "precision": precision,
+                   "timed_steps": f"steps {args.spinup + args.warmup + 1}-{args.spinup + args.warmup + args.steps} from t = 0",
+                   "store_order": ("box-ordered store with container indices (keep_order 0)" if args.keep_order == 0
+                                   else "reference container order (keep_order 1)"),
                    "spinup_steps": args.spinup, "autotune": tuning,
                    "device_memory_used_gb": round(used_gb, 2), "device_memory_total_gb": round(total_b / 1e9, 2),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"inputs larger than L2 (parcel state {store_gb:.2f} GB, fields {field_gb:.2f} GB)"},
         "roofline": roofline,
         "step_roofline": step_roofline(value, args.form, peak, peak_kind),
-        "clocks": clk,
+        "clocks": w["clocks"],
         "e2e": e2e,
-        "gpu_launches": int(l1.value - l0.value),
+        "gpu_launches": w["launches"],
         "kernel_times": kernel_times,
         "dt_last": infos[-1].dt if infos else None,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
-    ctx.close()
+    all_forms = (world == 1 and not args.no_forms and args.form == "plain" and args.workload == "thermal-128"
+                 and args.spinup == 0)
+    if all_forms:
+        # the same run later in its life: deformed parcels, splits and merges
+        forms = {}
+        while done < args.developed_at:
+            t, _ = ctx.step(t)
+            done += 1
+        t, wd = timer.window(t, args.steps, "stage")
+        forms["plain_developed"] = form_line(wd, args.steps, setup, "plain", {
+            "workload": f"the same thermal-128 run, steps {done + 1}-{done + args.steps}",
+            "timed_steps": [done + 1, done + args.steps]})
+        ctx.close()
+        forms["mixed"] = mixed_form(args, lib, dev)
+        forms["served"] = served_form(args, lib, dev)
+        line["forms"] = forms
+    else:
+        ctx.close()
     if mixed and rank == 0 and not args.no_error:
         line["error"] = mixed_error(lib)
     if rank == 0:
@@ -450,6 +524,98 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def mixed_form(args, lib, dev) -> dict:
+    """The mixed-precision form on its own workload: the thermal on
+    256x256x128 (67,108,864 parcels, 6.28 x 6.28 x 3.14), parcels generated on
+    the device, warm-up then the timed window; with its errors against FP64."""
+    import epic_b200
+    from epic_b200 import initial
+    spec = initial.device_spec("thermal-256x256x128")
+    ctx = epic_b200.make_context_device(spec, lib, keep_order=0, precision=1)
+    tuning = ctx.autotune() if not args.no_autotune else None
+    timer = Timer(lib, ctx, context_stream(lib, ctx, dev), dev)
+    t = 0.0
+    for _ in range(args.warmup):
+        t, _ = ctx.step(t)
+    t, w = timer.window(t, args.steps, "stage")
+    ctx.close()
+    out = form_line(w, args.steps, spec, "mixed", {
+        "workload": f"thermal-256x256x128: rising thermal, 256x256x128 grid, {spec.n:,} parcels at t=0, "
+                    f"mixed form, steps {args.warmup + 1}-{args.warmup + args.steps}",
+        "precision": "FP32 vorticity, B, buoyancy, humidity, delta_vor, delta_b, support vectors, par2grid sums "
+                     "and grid2par interpolation, FFTs and z transforms; FP64 positions, volume, delta_pos, "
+                     "B33, tridiagonal solve and fields",
+        "autotune": tuning})
+    if not args.no_error:
+        out["error"] = mixed_error_at_size(lib, args)
+    return out
+
+
+def run_pair(lib, spec, steps, *overrides, fields=True):
+    """Runs from the same device-generated state, one after the other:
+    kinetic energy, enstrophy, parcel counts and (optionally) the gridded
+    velocity, vorticity and buoyancy after `steps` steps."""
+    from epic_b200 import make_context_device, abi
+    out = []
+    for ov in overrides:
+        c = make_context_device(spec, lib, **ov)
+        t = 0.0
+        for _ in range(steps):
+            t, info = c.step(t)
+        f = None
+        if fields:
+            c.par2grid(False)
+            c.vor2vel()
+            f = {"velocity": np.stack([c.get_field(abi.VELOG[k])[:, :, 1:-1] for k in range(3)]),
+                 "vorticity": np.stack([c.get_field(abi.VORTG[k])[:, :, 1:-1] for k in range(3)]),
+                 "buoyancy": c.get_field(abi.TBUOYG)[:, :, 1:-1]}
+        out.append((info.parcel_stats[1], info.parcel_stats[12], f, int(info.n_parcels), t))
+        c.close()
+    return out
+
+
+def pair_errors(a, b) -> dict:
+    ke1, en1, f1, n1, t1 = a
+    ke0, en0, f0, n0, t0 = b
+    out = {"ke_rel_drift": abs(ke1 - ke0) / abs(ke0), "enstrophy_rel_drift": abs(en1 - en0) / abs(en0),
+           "parcels": [n0, n1], "t": [t0, t1]}
+    if f0 is not None:
+        for k in f0:
+            x, y = f1[k], f0[k]
+            out[k + "_l2_rel"] = float(np.sqrt(((x - y) ** 2).sum() / max((y ** 2).sum(), 1e-300)))
+            out[k + "_linf_rel"] = float(np.abs(x - y).max() / max(np.abs(y).max(), 1e-300))
+    return out
+
+
+def mixed_error_at_size(lib, args) -> dict:
+    """Errors of the mixed form against the plain FP64 form from the same
+    seed.  On its own workload (256x256x128): 100 steps at the fixed dt 0.05
+    (both runs at the same times; merge, split and corrections on).  With the
+    adaptive dt (thermal 64^3, 100 steps): mixed against plain, and, as the
+    flow's own sensitivity, plain against plain in the reference's container
+    order (the same FP64 arithmetic with other summation orders)."""
+    from epic_b200 import initial
+    steps = args.error_steps
+    spec = initial.device_spec("thermal-256x256x128")
+    fixed = dict(use_fixed_dt=1, fixed_dt=0.05, keep_order=0)
+    m, p = run_pair(lib, spec, steps, dict(fixed, precision=1), dict(fixed, precision=0))
+    out = {"fixed_dt": dict(pair_errors(m, p), workload=f"thermal-256x256x128, {steps} steps at fixed dt 0.05, "
+                                                          "mixed vs plain FP64 from the same seed"),
+           "target": 1e-5}
+    spec64 = initial.device_spec("thermal-64")
+    m, p, q = run_pair(lib, spec64, steps, dict(precision=1, keep_order=0), dict(precision=0, keep_order=0),
+                       dict(precision=0, keep_order=1), fields=False)
+    out["adaptive_dt"] = {"workload": f"thermal-64, {steps} steps, adaptive dt",
+                          "mixed_vs_plain": pair_errors(m, p), "plain_vs_plain_other_order": pair_errors(q, p)}
+    out["within_target"] = bool(out["fixed_dt"]["ke_rel_drift"] < 1e-5 and out["fixed_dt"]["enstrophy_rel_drift"] < 1e-5)
+    return out
+
+
+def served_form(args, lib, dev) -> dict:
+    """The served ensemble as a form of the default run (see run_served)."""
+    return run_served(args, lib=lib, dev=dev, emit=False)
 
 
 # ---------------------------------------------------------------------------
@@ -461,30 +627,13 @@ def mixed_error(lib, steps: int = 100, dt: float = 0.05) -> dict:
     relative L2 and Linf errors of the gridded velocity, vorticity and
     buoyancy (par2grid + vor2vel of the final parcels).  The step is fixed so
     that both runs compare the same times."""
-    from epic_b200 import initial, make_context_device, abi
+    from epic_b200 import initial
     spec = initial.device_spec("thermal-32")
-    runs = {}
-    for prec in (0, 1):
-        c = make_context_device(spec, lib, precision=prec, keep_order=0, use_fixed_dt=1, fixed_dt=dt)
-        t = 0.0
-        for _ in range(steps):
-            t, info = c.step(t)
-        c.par2grid(False)
-        c.vor2vel()
-        f = {"velocity": np.stack([c.get_field(abi.VELOG[k])[:, :, 1:-1] for k in range(3)]),
-             "vorticity": np.stack([c.get_field(abi.VORTG[k])[:, :, 1:-1] for k in range(3)]),
-             "buoyancy": c.get_field(abi.TBUOYG)[:, :, 1:-1]}
-        runs[prec] = (info.parcel_stats[1], info.parcel_stats[12], f, info.n_parcels)
-        c.close()
-    ke0, en0, f0, n0 = runs[0]
-    ke1, en1, f1, n1 = runs[1]
-    out = {"workload": f"thermal 32^3, {steps} steps at fixed dt {dt}, mixed vs plain FP64 from the same seed",
-           "ke_rel_drift": abs(ke1 - ke0) / abs(ke0), "enstrophy_rel_drift": abs(en1 - en0) / abs(en0),
-           "parcels": [int(n0), int(n1)], "target": 1e-5}
-    for k in f0:
-        a, b = f1[k], f0[k]
-        out[k + "_l2_rel"] = float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
-        out[k + "_linf_rel"] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    fixed = dict(use_fixed_dt=1, fixed_dt=dt, keep_order=0)
+    m, p = run_pair(lib, spec, steps, dict(fixed, precision=1), dict(fixed, precision=0))
+    out = pair_errors(m, p)
+    out.update({"workload": f"thermal 32^3, {steps} steps at fixed dt {dt}, mixed vs plain FP64 from the same seed",
+                "target": 1e-5})
     out["within_target"] = bool(out["ke_rel_drift"] < 1e-5 and out["enstrophy_rel_drift"] < 1e-5)
     return out
 
@@ -510,15 +659,16 @@ def served_requests(args, lib):
     return reqs, arrivals, meta
 
 
-def run_served(args):
+def run_served(args, lib=None, dev=None, emit=True):
     import torch
     import epic_b200
     from epic_b200 import serve
 
     world, rank, local = dist_setup()
-    torch.cuda.set_device(local if world > 1 else 0)
-    dev = torch.cuda.current_device()
-    lib = epic_b200.load()
+    if dev is None:
+        torch.cuda.set_device(local if world > 1 else 0)
+        dev = torch.cuda.current_device()
+    lib = lib or epic_b200.load()
     reqs, arrivals, meta = served_requests(args, lib)
     clocks = ClockSampler(dev)
     srv = serve.Server(slots=args.served_slots, hbm_fraction=0.8, lib=lib)
@@ -540,27 +690,34 @@ def run_served(args):
     span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
     value = ps / span
     ps_total = value
-    if world > 1:
+    if world > 1 and emit:
         # replicas: every rank serves its own copy of the ensemble
         _, ps_total = reduce_timing(span * 1e3, float(ps))
         ps_total = ps_total / span
     req_bytes = C_sizeof_request()
+    workload = (f"served ensemble: {len(reqs)} requests, Poisson arrivals {args.served_rate}/s "
+                f"(seed {args.served_seed}), grids 32^3/48^3/64^3/96x96x48, Beltrami (k,l,m in 1..2) "
+                f"or thermal, {args.served_steps} mixed-precision steps each, "
+                f"{args.served_slots} slots, admission by free HBM")
+    latency = {"p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+               "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+               "mean_s": float(lat.mean()) if len(lat) else None,
+               "max_s": float(lat.max()) if len(lat) else None}
+    timing = ("host steady clock of the server: submit to completion per request; "
+              "aggregate = parcel-steps / (last completion - first submission)")
+    if not emit:
+        return {"value": value, "unit": UNIT, "workload": workload, "latency": latency, "failed": len(failed),
+                "clocks": clk, "wall_s": wall, "span_s": span, "parcel_steps": ps, "timing": timing,
+                "arrival_span_s": arrivals[-1] if arrivals else 0.0}
     line = {
         "metric": METRIC, "value": ps_total, "unit": UNIT, "n_gpus": world, "steps": args.served_steps,
         "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32/f64", "data": "synthetic",
-        "config": {"workload": f"served ensemble: {len(reqs)} requests, Poisson arrivals {args.served_rate}/s "
-                               f"(seed {args.served_seed}), grids 32^3/48^3/64^3/96x96x48, Beltrami (k,l,m in 1..2) "
-                               f"or thermal, {args.served_steps} mixed-precision steps each, "
-                               f"{args.served_slots} slots, admission by free HBM",
+        "config": {"workload": workload,
                    "form": "served", "requests": len(reqs), "slots": args.served_slots,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "timing": "host steady clock of the server: submit to completion per request; "
-                             "aggregate = parcel-steps / (last completion - first submission)"},
-        "latency": {"p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
-                    "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
-                    "mean_s": float(lat.mean()) if len(lat) else None,
-                    "max_s": float(lat.max()) if len(lat) else None},
+                   "timing": timing},
+        "latency": latency,
         "failed": len(failed),
         "failures": [dict(meta[k], message=r["message"]) for k, r in enumerate(res) if r["status"] != 0][:8],
         "clocks": clk,
@@ -613,7 +770,7 @@ def run_reference(args):
     import oracle
     lib = oracle.load(threads=True)
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    from epic_b200 import make_context
+    from epic_b200 import initial, make_context
     s = oracle_sample_workload()
     ctx = make_context(s, lib)
     t = 0.0
@@ -625,13 +782,30 @@ def run_reference(args):
         ps += ctx.num_parcels()
         t, _ = ctx.step(t)
     el = time.perf_counter() - t0
+    ctx.close()
     v = ps / el
+    # the per-parcel-step rate of the sample against the full workload: one
+    # step of the 128^3 thermal itself (16,777,216 parcels)
+    full = None
+    if not args.no_full_check:
+        sf = initial.config("thermal-128")
+        cf = make_context(sf, lib)
+        n0 = cf.num_parcels()
+        t1 = time.perf_counter()
+        cf.step(0.0)
+        ef = time.perf_counter() - t1
+        cf.close()
+        full = {"workload": "thermal-128 (the GPU arm's workload), first step", "parcels": n0, "seconds": ef,
+                "value": n0 / ef, "unit": UNIT, "ratio_to_sample": (n0 / ef) / v}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": args.workload, "sample": "each step is one step of the rising thermal on a "
-                       "64^3 grid (2,097,152 parcels, 8/cell, same physics) as a bounded sample of the workload"},
+                       "64^3 grid (2,097,152 parcels, 8/cell, same physics) as a bounded sample of the workload; "
+                       "parcel-steps/s per parcel-step is size-independent (full_size_check: one step of the "
+                       "128^3 workload itself)",
+                       "full_size_check": full},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": "64^3 rising thermal, one step per timed step"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -658,7 +832,14 @@ def main():
     ap.add_argument("--roofline-kernel", default="stage", choices=["stage", "p2g", "g2p", "fft"])
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of that kernel")
     ap.add_argument("--profile-kernels", default="", help="comma list of kernels to time over one extra step each")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="default plain run: skip the developed-flow window and the mixed and served forms")
+    ap.add_argument("--developed-at", type=int, default=100,
+                    help="the developed-flow window of the default run starts after this many steps")
+    ap.add_argument("--error-steps", type=int, default=100)
+    ap.add_argument("--no-full-check", action="store_true",
+                    help="reference arm: skip the one step of the full 128^3 workload")
     ap.add_argument("--spinup", type=int, default=0, help="untimed steps before the warm-up (developed flow)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--keep-order", type=int, default=0, choices=[0, 1],

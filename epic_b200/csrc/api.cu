@@ -157,6 +157,7 @@ void check_device_error(Ctx& c) {
     if (e & ERRB_CELL) throw CudaError(EPIC_ERR_NUMERICAL, "in nearest_parcel_to_local_cell_index: Parcel not in local domain.");
     if (e & ERRB_DT) throw CudaError(EPIC_ERR_NUMERICAL, "Time step <= 0!");
     if (e & ERRB_ZRANGE) throw CudaError(EPIC_ERR_NUMERICAL, "interpolation point outside the vertical halo");
+    if (e & ERRB_NONFINITE) throw CudaError(EPIC_ERR_NUMERICAL, "par2grid: non-finite parcel attribute");
     if (e & (1u << 30)) throw CudaError(EPIC_ERR_PARCEL_COUNT, "par2grid: Wrong total number of parcels!");
     throw CudaError(EPIC_ERR_NUMERICAL, "device error word " + std::to_string(e));
 }

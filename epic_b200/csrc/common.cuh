@@ -127,6 +127,7 @@ enum ErrBits {
     ERRB_CELL = 1u << 3,          // nearest: parcel not in local domain
     ERRB_TREE = 1u << 4,          // resolve_tree first stage error
     ERRB_DT = 1u << 5,            // time step <= 0
+    ERRB_NONFINITE = 1u << 6,     // par2grid: a non-finite parcel value
 };
 
 EPIC_DEV void set_err(unsigned* err, unsigned bit) { atomicOr(err, bit); }

@@ -70,6 +70,10 @@ struct StepScalars {
     long long n;                    // parcel count
     long long count;                // scratch counter
     double vsum, vor[3];            // vorticity correction sums
+    // largest |value| of each par2grid field over the parcels (ordered bits
+    // of non-negative doubles): vortg x, y, z, dbuoyg, humg, tbuoyg, volg;
+    // the fixed-point scales of a scatter and of its tail
+    unsigned long long pbound[8];
 };
 
 // CUDA-event timing of every launch of one named kernel on the context stream.
@@ -107,7 +111,6 @@ struct Ctx {
     // log2 of the consecutive parcels a lane group scatters (vol2grid,
     // par2grid, fused stage)
     int scatter_lg[3] = {1, 1, 0};
-    bool fused_scatter = false;   // stage kernel runs the next par2grid itself (else a separate scatter kernel)
     bool vectors_kernel = true;   // support vectors by their own kernel before a scatter that recomputes them
     int stage_recwin = 0;         // split-form stage kernel gathers from records staged in shared memory
     bool stage_vectors = false;   // split-form stage kernel computes the next par2grid's support vectors
@@ -214,6 +217,8 @@ void sort_parcels(Ctx& c);
 int box_count(const Params& P);
 long long stage_grid_max(const Params& P, long long cap);
 void p2g_tail(Ctx& c);
+// fixed-point bits of the par2grid sums (the scale of the tail's conversion)
+int p2g_fx_bits(const Ctx& c);
 
 // init.cu
 void init_state(Ctx& c, const epic_init_spec& s);

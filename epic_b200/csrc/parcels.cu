@@ -21,7 +21,19 @@ namespace epic {
 // ---------------------------------------------------------------------------
 // par2grid scatter (parcel_interpl.f90:160-233)
 
-// z folds (parcel_interpl.f90:237-243, 256-275), per (x, y) column
+// The scatter leaves 64-bit integer grid sums in the field arrays (q / s_f,
+// s_f = 2^(b - e_f) from the field's bound in pbound, stage.cu); the tail
+// folds them in integers and converts them to FP64.
+EPIC_DEV double fx_inv(const unsigned long long* pbound, int k, int bits) {
+    const double m = __longlong_as_double((long long)pbound[k]);
+    if (!(m > 0.0 && m <= 1.0e300)) return 0.0;   // no contribution (or a non-finite one, reported by the scatter)
+    int e = 0;
+    frexp(m, &e);
+    return ldexp(1.0, e - bits);
+}
+
+// z folds (parcel_interpl.f90:237-243, 256-275), per (x, y) column, on the
+// integer sums (exact)
 __global__ void k_p2g_fold(Params P, ScatterFields F, int nf, int* nparg, int* nsparg, long long* count) {
     long long ncol = (long long)P.nx * P.ny;
     long long local = 0;
@@ -30,9 +42,9 @@ __global__ void k_p2g_fold(Params P, ScatterFields F, int nf, int* nparg, int* n
         long long t = c * P.nzh + 1;
         int nz = P.nz;
         for (int f = 0; f < nf; ++f) {
-            double* p = F.f[f] + t;
-            p[0] = 2.0 * p[0];
-            p[nz] = 2.0 * p[nz];
+            long long* p = reinterpret_cast<long long*>(F.f[f]) + t;
+            p[0] = 2 * p[0];
+            p[nz] = 2 * p[nz];
             p[1] = p[1] + p[-1];
             p[nz - 1] = p[nz - 1] + p[nz + 1];
         }
@@ -52,18 +64,32 @@ __global__ void k_p2g_fold(Params P, ScatterFields F, int nf, int* nparg, int* n
     }
 }
 
-// divide by the gridded volume, zeta boundary zeroing (parcel_interpl.f90:278-313)
-__global__ void k_p2g_divide(Params P, ScatterFields F) {
-    long long nel = (long long)P.nx * P.ny * (P.nz + 1);
-    int nzp = P.nz + 1;
+// The integer sums to FP64 on every row; rows 0 .. nz divided by the gridded
+// volume, with the zeta boundary zeroing (parcel_interpl.f90:278-313).
+__global__ void k_p2g_divide(Params P, ScatterFields F, const unsigned long long* pbound, int bits) {
+    double inv[7];
+#pragma unroll
+    for (int l = 0; l < 7; ++l) inv[l] = fx_inv(pbound, l, bits);
+    const long long nel = (long long)P.nx * P.ny * P.nzh;
     PLOOP(nel) {
-        long long c = i / nzp;
-        int iz = (int)(i - c * nzp);
-        long long a = c * P.nzh + 1 + iz;
-        double v = F.f[6][a];
-        for (int l = 0; l < 6; ++l) F.f[l][a] = F.f[l][a] / v;
-        if ((iz == 0 && P.zeta_zero[0]) || (iz == P.nz && P.zeta_zero[1])) F.f[2][a] = 0.0;
+        const int iz = (int)(i % P.nzh) - 1;
+        double v[7];
+#pragma unroll
+        for (int l = 0; l < 7; ++l) v[l] = (double)reinterpret_cast<const long long*>(F.f[l])[i] * inv[l];
+        if (iz >= 0 && iz <= P.nz) {
+#pragma unroll
+            for (int l = 0; l < 6; ++l) v[l] = v[l] / v[6];
+            if ((iz == 0 && P.zeta_zero[0]) || (iz == P.nz && P.zeta_zero[1])) v[2] = 0.0;
+        }
+#pragma unroll
+        for (int l = 0; l < 7; ++l) F.f[l][i] = v[l];
     }
+}
+
+// vol2grid's integer sums to FP64
+__global__ void k_v2g_convert(long long fsz, double* volg, const unsigned long long* pbound, int bits) {
+    const double inv = fx_inv(pbound, 6, bits);
+    PLOOP(fsz) volg[i] = (double)reinterpret_cast<const long long*>(volg)[i] * inv;
 }
 
 __global__ void k_p2g_halo(Params P, ScatterFields F) {
@@ -102,7 +128,7 @@ void p2g_tail(Ctx& c) {
         k_count_check<<<1, 1, 0, c.stream>>>(c.dsc, c.n);
         CKL();
     }
-    k_p2g_divide<<<pgrid((long long)P.nx * P.ny * (P.nz + 1)), PB, 0, c.stream>>>(P, F);
+    k_p2g_divide<<<pgrid((long long)P.nx * P.ny * P.nzh), PB, 0, c.stream>>>(P, F, c.dsc->pbound, p2g_fx_bits(c));
     CKL();
     k_p2g_halo<<<(int)((ncol + 255) / 256), 256, 0, c.stream>>>(P, F);
     CKL();
@@ -122,6 +148,8 @@ void vol2grid(Ctx& c, bool reuse) {
     F.f[0] = c.volg();
     long long ncol = (long long)P.nx * P.ny;
     k_p2g_fold<<<(int)((ncol + 255) / 256), 256, 0, c.stream>>>(P, F, 1, nullptr, nullptr, nullptr);
+    CKL();
+    k_v2g_convert<<<pgrid(P.fsz), PB, 0, c.stream>>>(P.fsz, c.volg(), c.dsc->pbound, p2g_fx_bits(c));
     CKL();
 }
 

@@ -1,36 +1,29 @@
-// Box-decomposed scatter (par2grid, vol2grid), the fused LS-RK stage kernel,
-// and the box ordering of the parcel store.
+// Box-decomposed scatter (par2grid, vol2grid), the LS-RK stage kernel, and
+// the box ordering of the parcel store.
 //
 // Ordering: at the start of a step the parcel store is sorted by box of
 // BOXX x BOXY x BOXZ cells (cells z fastest inside a box), and the first
 // parcel of every box is recorded.  One CTA takes one box; parcels appended
-// later (split children) are handled in tail chunks of SCHUNK parcels, and
-// parcels moved into merge holes as strays.
+// later (split children) are handled in tail chunks of SCHUNK parcels.
 //
-// Scatter (parcel_interpl.f90:160-233): a CTA first finds the bounding box of
-// the cells of its parcels (ignoring parcels more than STRAY cells outside
-// its box) and the largest contribution of each field, then accumulates the
-// 4 support points x 8 corners of every parcel into a shared-memory window
-// covering that box plus the support-point reach, and adds the window to the
-// global fields once.  Window sums are fixed point: each contribution is
-// scaled by a power of two so that its magnitude is at most 2^(b+2)
-// (b <= 48; the +2 covers the merged weights of up to 4 support points),
-// rounded to an integer, and added as three 32-bit limbs (two unsigned
-// 18-bit limbs and a signed top limb) with integer shared-memory atomics,
-// which run at several times the rate of FP64 shared atomics, do not
-// serialise on equal addresses, and make the window sums independent of the
-// order of the adds.  A round holds at most ROUND parcels (at most 4 ROUND
-// contributions per grid point), which keeps every limb sum inside 32 bits
-// and the total inside 62.  Points outside the window go straight to the
-// global fields (FP64 atomics).
+// Scatter (parcel_interpl.f90:160-233): every contribution w * v of a support
+// point (trilinear weight w of a corner, value v = attribute x point weight
+// 1/4 x volume) is a fixed-point integer q = round(w v s_f) at one scale
+// s_f = 2^(b - e_f) per field and launch, 2^e_f above the largest |v| of the
+// field over all parcels (a bound computed before the scatter).  Grid sums
+// are integer sums, exact and therefore independent of the order of the adds:
+// par2grid is bitwise reproducible run to run and for any launch shape.  A box
+// CTA adds its parcels' contributions into a shared-memory window (the box's
+// grid points and WM more on every side) as three 32-bit limbs with integer
+// shared atomics, then adds the window to the 64-bit integer grid sums held in
+// the field arrays; points outside the window, and tail chunks whose parcels
+// do not fit a window, add to the grid sums directly.  The tail kernels
+// (parcels.cu) fold the z halos in integers and convert to FP64.
 //
-// Fused stage (ls_rk.f90:142-217 + parcel_interpl.f90:405-470 + the next
-// stage's par2grid): pass A gathers the 14 interpolated quantities at the
-// support points (support vectors stored by the preceding scatter, computed
-// from the same B, parcel_ellipsoid.f90:216-247), computes dB/dt, advances
-// x, w, B and scales the accumulators; pass B (same parcels, hot in L1/L2)
-// computes the support vectors of the advanced shape, stores them, and
-// scatters into the next stage's fields.
+// Stage (ls_rk.f90:142-217 + parcel_interpl.f90:405-470): grid2par at the
+// support points (support vectors stored by the preceding scatter, from the
+// same B, parcel_ellipsoid.f90:216-247), dB/dt, the update of x, w, B and the
+// scaling of the accumulators; it also bounds the next par2grid's values.
 #include "parcel_ops.cuh"
 
 #include <cub/cub.cuh>
@@ -43,8 +36,12 @@ constexpr int BOXX = 8, BOXY = 4, BOXZ = 4;   // cells per box
 constexpr int BOXC = BOXX * BOXY * BOXZ;
 constexpr int SCHUNK = 2048;    // parcels per tail chunk
 constexpr int ROUND = 4096;     // parcels per fixed-point round
-constexpr int WCAP = 1024;      // grid points per shared-memory window
-constexpr int STRAY = 2;        // cells outside its box a parcel may be and still shape the window
+// Window of a box CTA: the box's grid points and WM more on every side
+// (parcels that moved up to a cell out of the box since the sort, plus half
+// a cell of support-point reach), 13 x 9 x 9 grid points.
+constexpr int WM = 2;
+constexpr int WCAP = (BOXX + 1 + 2 * WM) * (BOXY + 1 + 2 * WM) * (BOXZ + 1 + 2 * WM);
+constexpr int WSTRIDE = (WCAP + 3) & ~3;   // words per limb plane
 constexpr int NLIMB = 3;
 constexpr int SB = 2;           // CTAs per SM the scatter kernels are sized for
 
@@ -65,7 +62,8 @@ struct Window {
 // Parcel range and reference cell of this CTA.
 struct Range {
     long long r0, r1;
-    int ref[3], ext[3], margin;
+    int ref[3];
+    bool box;            // a box of the sorted store (else a tail chunk)
 };
 
 // Cell of a position (get_index, fields.f90:165-172).
@@ -84,8 +82,7 @@ EPIC_DEV Range cta_range(const Params& P, const PView& pv, const Boxes& B, long 
         int bz = b % B.nbz, r = b / B.nbz;
         int by = r % B.nby, bx = r / B.nby;
         R.ref[0] = bx * BOXX; R.ref[1] = by * BOXY; R.ref[2] = bz * BOXZ;
-        R.ext[0] = BOXX; R.ext[1] = BOXY; R.ext[2] = BOXZ;
-        R.margin = STRAY;
+        R.box = true;
     } else {
         long long t = b - B.nbox;
         R.r0 = B.n_box + t * SCHUNK;
@@ -97,8 +94,7 @@ EPIC_DEV Range cta_range(const Params& P, const PView& pv, const Boxes& B, long 
             R.ref[0] = wrapi(R.ref[0], P.nx);
             R.ref[1] = wrapi(R.ref[1], P.ny);
         }
-        R.ext[0] = R.ext[1] = R.ext[2] = 1;
-        R.margin = 1 << 20;
+        R.box = false;
     }
     return R;
 }
@@ -109,109 +105,68 @@ EPIC_DEV int rel_periodic(int c, int r, int n) {
     return d >= n - n / 2 ? d - n : d;
 }
 
-// Per-thread partial of the window pass.
-template <int NF>
-struct WinPart {
-    int mn[3], mx[3];
-    double vmax[NF];
-    EPIC_DEV void init() {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { mn[k] = INT_MAX; mx[k] = INT_MIN; }
-#pragma unroll
-        for (int f = 0; f < NF; ++f) vmax[f] = 0.0;
-    }
-    // a parcel at position p with contributions vp[f]
-    EPIC_DEV void add(const Params& P, const Range& R, const double* p, const double* vp) {
-        int c[3];
-        cell_of(P, p, c[0], c[1], c[2]);
-        int d[3] = {rel_periodic(c[0], R.ref[0], P.nx), rel_periodic(c[1], R.ref[1], P.ny), c[2] - R.ref[2]};
-        bool in = true;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) in = in && d[k] >= -R.margin && d[k] < R.ext[k] + R.margin;
-        if (in) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) { mn[k] = min(mn[k], d[k]); mx[k] = max(mx[k], d[k]); }
-        }
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            double a = fabs(vp[f]);
-            vmax[f] = (a > vmax[f] || a != a) ? a : vmax[f];   // keeps a NaN once seen
-        }
-    }
-};
-
+// Shared state of a scatter CTA: the cell bounds of a tail chunk (relative
+// to its first parcel), the window and the fixed-point scales.
 template <int NF>
 struct WinShared {
     int mn[3], mx[3];
-    unsigned long long vbits[NF];
     Window W;
-    double scale[NF], inv[NF];
+    double scale[NF];
 };
 
-template <int NF>
-EPIC_DEV void win_begin(WinShared<NF>* ws) {
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < 3; ++k) { ws->mn[k] = INT_MAX; ws->mx[k] = INT_MIN; }
-        for (int f = 0; f < NF; ++f) ws->vbits[f] = 0ull;
-    }
+// Window of a box CTA: fixed, the box's grid points +- WM (z clipped to the
+// halo rows -1 .. nz + 1).
+EPIC_DEV Window box_window(const Params& P, const Range& R) {
+    Window W;
+    W.gx0 = R.ref[0] - WM;
+    W.gy0 = R.ref[1] - WM;
+    W.gz0 = max(R.ref[2] - WM, -1);
+    W.WX = BOXX + 1 + 2 * WM;
+    W.WY = BOXY + 1 + 2 * WM;
+    W.WZ = min(R.ref[2] + BOXZ + WM, P.nz + 1) - W.gz0 + 1;
+    W.ok = W.WX <= P.nx && W.WY <= P.ny;   // no grid point twice in one window
+    return W;
 }
 
-// Block reduction of the partials (after win_begin and a barrier).
+// Cell bounds of a tail chunk (one thread per parcel, then a block reduction
+// into ws->mn / mx, which thread 0 cleared); the window covers the chunk's
+// cells with one cell below and two above (support points and corners).
 template <int NF>
-EPIC_DEV void win_reduce(WinShared<NF>* ws, WinPart<NF>& wp) {
+EPIC_DEV void tail_bounds(const Params& P, const Range& R, const PView& pv, WinShared<NF>* ws) {
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (long long i = R.r0 + threadIdx.x; i < R.r1; i += blockDim.x) {
+        const double p[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
+        int c[3];
+        cell_of(P, p, c[0], c[1], c[2]);
+        const int d[3] = {rel_periodic(c[0], R.ref[0], P.nx), rel_periodic(c[1], R.ref[1], P.ny), c[2] - R.ref[2]};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { mn[k] = min(mn[k], d[k]); mx[k] = max(mx[k], d[k]); }
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        int a = wp.mn[k], b = wp.mx[k];
         for (int o = 16; o > 0; o >>= 1) {
-            a = min(a, __shfl_xor_sync(0xffffffff, a, o));
-            b = max(b, __shfl_xor_sync(0xffffffff, b, o));
+            mn[k] = min(mn[k], __shfl_xor_sync(0xffffffff, mn[k], o));
+            mx[k] = max(mx[k], __shfl_xor_sync(0xffffffff, mx[k], o));
         }
-        wp.mn[k] = a; wp.mx[k] = b;
     }
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        // fmax drops NaN: carry it as +inf so that the round falls back to FP64
-        double v = isnan(wp.vmax[f]) ? INFINITY : wp.vmax[f];
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffff, v, o));
-        wp.vmax[f] = v;
-    }
-    if ((threadIdx.x & 31) == 0) {
-        for (int k = 0; k < 3; ++k) { atomicMin(&ws->mn[k], wp.mn[k]); atomicMax(&ws->mx[k], wp.mx[k]); }
-        // non-negative doubles order like their bit patterns
-        for (int f = 0; f < NF; ++f) atomicMax(&ws->vbits[f], (unsigned long long)__double_as_longlong(wp.vmax[f]));
-    }
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < 3; ++k) { atomicMin(&ws->mn[k], mn[k]); atomicMax(&ws->mx[k], mx[k]); }
 }
 
-// Window and fixed-point scales of a round of `count` parcels (one thread).
-template <int NF>
-EPIC_DEV void win_make(const Params& P, const Range& R, WinShared<NF>* ws, long long count, int max_bits = 50) {
-    Window& W = ws->W;
-    W.gx0 = R.ref[0] + ws->mn[0] - 1;
-    W.gy0 = R.ref[1] + ws->mn[1] - 1;
-    W.gz0 = max(R.ref[2] + ws->mn[2] - 1, -1);
-    W.WX = ws->mx[0] - ws->mn[0] + 4;
-    W.WY = ws->mx[1] - ws->mn[1] + 4;
-    int gz1 = min(R.ref[2] + ws->mx[2] + 2, P.nz + 1);
-    W.WZ = gz1 - W.gz0 + 1;
-    bool ok = ws->mn[0] <= ws->mx[0] && W.WX <= P.nx && W.WY <= P.ny && W.WZ > 0 &&
-              (long long)W.WX * W.WY * W.WZ <= WCAP;
-    // contributions per grid point <= 4 count <= 2^lg; |window sum| <= 2^(bits + lg) <= 2^62;
-    // one contribution (merged weights of up to 4 points, <= 4) <= 2^(bits + 2)
-    int lg = 32 - __clz((unsigned)(4 * count - 1));
-    int bits = min(max_bits, 62 - lg);
-    for (int f = 0; f < NF; ++f) {
-        double m = __longlong_as_double((long long)ws->vbits[f]);
-        if (!(m <= 1.0e300)) ok = false;
-        int e = 0;
-        if (m > 0.0) frexp(m, &e);          // m < 2^e
-        ws->scale[f] = ldexp(1.0, bits - e);
-        ws->inv[f] = ldexp(1.0, e - bits);
-    }
-    W.ok = ok;
+EPIC_DEV Window tail_window(const Params& P, const Range& R, const int* mn, const int* mx) {
+    Window W;
+    W.gx0 = R.ref[0] + mn[0] - 1;
+    W.gy0 = R.ref[1] + mn[1] - 1;
+    W.gz0 = max(R.ref[2] + mn[2] - 1, -1);
+    W.WX = mx[0] - mn[0] + 4;
+    W.WY = mx[1] - mn[1] + 4;
+    W.WZ = min(R.ref[2] + mx[2] + 2, P.nz + 1) - W.gz0 + 1;
+    W.ok = mn[0] <= mx[0] && W.WX <= P.nx && W.WY <= P.ny && W.WZ > 0 && (long long)W.WX * W.WY * W.WZ <= WCAP;
+    return W;
 }
 
 struct Fields7 {
-    double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg
+    double* f[7];   // vortg x,y,z, dbuoyg, humg, tbuoyg, volg (64-bit integer sums during the scatter)
     int mask;       // bit f set: field f is accumulated (NF = 7)
 };
 constexpr int ALL_FIELDS = 0x7f;
@@ -222,6 +177,12 @@ constexpr int DRY_FIELDS = 0x67;   // without dbuoyg (3) and humg (4)
 template <int NF>
 EPIC_HD constexpr int field_slot(int f) {
     return NF == 5 ? (f < 3 ? f : f + 2) : f;
+}
+// Slot of field f's bound in StepScalars::pbound (the 7 par2grid fields;
+// vol2grid's volume shares the par2grid volume's slot).
+template <int NF>
+EPIC_HD constexpr int bound_slot(int f) {
+    return NF == 1 ? 6 : field_slot<NF>(f);
 }
 template <int NF>
 EPIC_DEV bool field_on(const Fields7& F, int f) {
@@ -251,46 +212,66 @@ EPIC_DEV R& aR(const PView& pv, int k, long long i) {
                                 (Form<R>::mixed ? mixed_slot_off(k) : 8LL * k) * pv.cap)[i];
 }
 
-// Window accumulator words per field: three fixed-point limbs (plain, 2^-50
-// resolution) or two (mixed, 2^-36, far below FP32 rounding).
+// Fixed-point bits: |w v s_f| <= 2^(b + 2) (merged weights of up to 4 support
+// points).  Plain: b = 46, three window limbs (18 + 18 bits unsigned and a
+// signed top), 4 x ROUND contributions per grid point per round within 32
+// bits each, 2^15 contributions per grid point within the 64-bit grid sums;
+// rounding 2^-47 of the field's largest value.  Mixed: b = 34, two limbs
+// (19 bits unsigned and a signed top) for 4 x 2048 contributions per round,
+// far below FP32 rounding.
+template <class R> constexpr int fx_bits() { return Form<R>::mixed ? 34 : 46; }
 template <class R> constexpr int win_words() { return Form<R>::mixed ? 2 : NLIMB; }
-template <class R, int NF> constexpr size_t win_bytes() { return sizeof(unsigned) * NF * win_words<R>() * WCAP; }
-// Parcels per round: at most 4 rounds contributions per grid point, 2^14
-// (plain) or 2^13 (mixed: keeps the 19-bit limb sums inside 32 bits).
+template <class R, int NF> constexpr size_t win_bytes() { return sizeof(unsigned) * NF * win_words<R>() * WSTRIDE; }
 template <class R> constexpr int round_max() { return Form<R>::mixed ? 2048 : ROUND; }
 
-// Fixed-point accumulation.  r = wt * vs + 1.5 * 2^52 rounds wt * vs
-// (|wt * vs| <= 2^50) to the integer q once; the low 52 bits of r hold
-// m = 2^51 + q, split as q = ((m >> 36) - 2^15) * 2^36
-// + ((m >> 18) & 0x3ffff) * 2^18 + (m & 0x3ffff).
-constexpr double FX_MAGIC = 6755399441055744.0;   // 1.5 * 2^52
+// Scale of field slot k from its bound (largest |value| as ordered bits).
+EPIC_DEV double fx_scale(const unsigned long long* pbound, int k, int bits, unsigned* err) {
+    const double m = __longlong_as_double((long long)pbound[k]);
+    if (!(m <= 1.0e300)) {   // a non-finite parcel value
+        set_err(err, ERRB_NONFINITE);
+        return 0.0;
+    }
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);   // m < 2^e
+    return ldexp(1.0, bits - e);
+}
 
+// Rounding of w * vs (|w vs| <= 2^50) to an integer: r = w vs + 1.5 * 2^52
+// rounds once; the low 52 bits of r hold 2^51 + q.
+constexpr double FX_MAGIC = 6755399441055744.0;   // 1.5 * 2^52
+EPIC_DEV long long fx_round(double wt, double vs) {
+    const double r = fma(wt, vs, FX_MAGIC);
+    return (__double_as_longlong(r) & 0xfffffffffffffll) - (1ll << 51);
+}
+
+// q = ((m >> 36) - 2^15) * 2^36 + ((m >> 18) & 0x3ffff) * 2^18 + (m & 0x3ffff), m = 2^51 + q
 EPIC_DEV void fx_add(unsigned* acc, int w, double wt, double vs) {
     double r = fma(wt, vs, FX_MAGIC);
     unsigned lo = (unsigned)__double2loint(r), hi = (unsigned)__double2hiint(r);
     atomicAdd(&acc[w], lo & 0x3ffffu);
-    atomicAdd(&acc[WCAP + w], (lo >> 18) | ((hi & 0xfu) << 14));
-    atomicAdd(&acc[2 * WCAP + w], ((hi & 0xfffffu) >> 4) - 32768u);
+    atomicAdd(&acc[WSTRIDE + w], (lo >> 18) | ((hi & 0xfu) << 14));
+    atomicAdd(&acc[2 * WSTRIDE + w], ((hi & 0xfffffu) >> 4) - 32768u);
+}
+EPIC_DEV long long fx_sum(const unsigned* acc, int w) {
+    return (long long)(int)acc[2 * WSTRIDE + w] * (1ll << 36) + (long long)acc[WSTRIDE + w] * (1ll << 18) +
+           (long long)acc[w];
 }
 
-EPIC_DEV double fx_value(const unsigned* acc, int w, double inv) {
-    long long q = (long long)(int)acc[2 * WCAP + w] * (1ll << 36) + (long long)acc[WCAP + w] * (1ll << 18) +
-                  (long long)acc[w];
-    return (double)q * inv;
-}
-
-// Two-limb variant (mixed form, |wt * vs| <= 2^36): q = h * 2^19 + l with
-// l = q mod 2^19 and h = floor(q / 2^19), |h| <= 2^17.
+// Two-limb variant: q = h * 2^19 + l, l = q mod 2^19, h = floor(q / 2^19).
 EPIC_DEV void fx2_add(unsigned* acc, int w, double wt, double vs) {
     double r = fma(wt, vs, FX_MAGIC);
     long long m = __double_as_longlong(r) & 0xfffffffffffffll;   // 2^51 + q
     atomicAdd(&acc[w], (unsigned)(m & 0x7ffff));
-    atomicAdd(&acc[WCAP + w], (unsigned)((m >> 19) - (1ll << 32)));
+    atomicAdd(&acc[WSTRIDE + w], (unsigned)((m >> 19) - (1ll << 32)));
+}
+EPIC_DEV long long fx2_sum(const unsigned* acc, int w) {
+    return (long long)(int)acc[WSTRIDE + w] * (1ll << 19) + (long long)acc[w];
 }
 
-EPIC_DEV double fx2_value(const unsigned* acc, int w, double inv) {
-    long long q = (long long)(int)acc[WCAP + w] * (1ll << 19) + (long long)acc[w];
-    return (double)q * inv;
+// A contribution straight into the 64-bit grid sum of field f at point g.
+EPIC_DEV void fx_global(double* f, long long g, double wt, double vs) {
+    const long long q = fx_round(wt, vs);
+    if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(f) + g, (unsigned long long)q);
 }
 
 EPIC_DEV int wrap_to(int l, int n) { return ((unsigned)l < (unsigned)n) ? l : wrapi(l, n); }
@@ -350,12 +331,11 @@ EPIC_DEV int merge_start(const Params& P, const double* pos, const double* eta, 
     return 0;
 }
 
-// Scatter one support point: vs[f] = value * point weight * volume in the
-// window's fixed-point units (a power-of-two scale, so vs[f] * inv[f] gives
-// the value back exactly for the global-atomic fallback).
+// Scatter one support point (or the merged points of one parcel in one cell):
+// vs[f] = value x volume x point weight x s_f.
 template <int NF, class R>
 EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const Fields7& F, const Tri& t,
-                          const double* vs, const double* inv, unsigned* err) {
+                          const double* vs, unsigned* err) {
     if (t.ks < -1 || t.ks > P.nz) { set_err(err, ERRB_ZRANGE); return; }
     int lx = wrap_to(t.is - W.gx0, P.nx), ly = wrap_to(t.js - W.gy0, P.ny), lz = t.ks - W.gz0;
     if (W.ok && lx + 1 < W.WX && ly + 1 < W.WY && lz >= 0 && lz + 1 < W.WZ) {
@@ -371,12 +351,12 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
                         const double wt = (double)(float)t.w[kk][jj][ii];
 #pragma unroll
                         for (int f = 0; f < NF; ++f)
-                            if (field_on<NF>(F, f)) fx2_add(acc + f * 2 * WCAP, w, wt, vs[f]);
+                            if (field_on<NF>(F, f)) fx2_add(acc + f * 2 * WSTRIDE, w, wt, vs[f]);
                     } else {
                         const double wt = t.w[kk][jj][ii];
 #pragma unroll
                         for (int f = 0; f < NF; ++f)
-                            if (field_on<NF>(F, f)) fx_add(acc + f * NLIMB * WCAP, w, wt, vs[f]);
+                            if (field_on<NF>(F, f)) fx_add(acc + f * NLIMB * WSTRIDE, w, wt, vs[f]);
                     }
                 }
     } else {
@@ -389,11 +369,10 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     long long g = a[jj][ii] + kk;
-                    const R wt = (R)t.w[kk][jj][ii];
+                    const double wt = Form<R>::mixed ? (double)(float)t.w[kk][jj][ii] : t.w[kk][jj][ii];
 #pragma unroll
                     for (int f = 0; f < NF; ++f)
-                        if (field_on<NF>(F, f))
-                            atomicAdd(&F.f[field_slot<NF>(f)][g], (double)(wt * (R)(vs[f] * inv[f])));
+                        if (field_on<NF>(F, f)) fx_global(F.f[field_slot<NF>(f)], g, wt, vs[f]);
                 }
     }
 }
@@ -403,12 +382,12 @@ EPIC_DEV void win_zero(unsigned* acc, const Window& W) {
     if (!W.ok) return;
     int n = W.WX * W.WY * W.WZ;
     for (int f = 0; f < NF * win_words<R>(); ++f)
-        for (int w = threadIdx.x; w < n; w += blockDim.x) acc[f * WCAP + w] = 0u;
+        for (int w = threadIdx.x; w < n; w += blockDim.x) acc[f * WSTRIDE + w] = 0u;
 }
 
+// The window's integer sums into the 64-bit grid sums.
 template <int NF, class R>
-EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF>* ws, const Fields7& F) {
-    const Window W = ws->W;
+EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const Window& W, const Fields7& F) {
     if (!W.ok) return;
     int n = W.WX * W.WY * W.WZ;
     for (int w = threadIdx.x; w < n; w += blockDim.x) {
@@ -420,10 +399,11 @@ EPIC_DEV void win_flush(const Params& P, const unsigned* acc, const WinShared<NF
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
             if (!field_on<NF>(F, f)) continue;
-            double v;
-            if constexpr (Form<R>::mixed) v = fx2_value(acc + f * 2 * WCAP, w, ws->inv[f]);
-            else v = fx_value(acc + f * NLIMB * WCAP, w, ws->inv[f]);
-            if (v != 0.0) atomicAdd(&F.f[field_slot<NF>(f)][g], v);
+            long long q;
+            if constexpr (Form<R>::mixed) q = fx2_sum(acc + f * 2 * WSTRIDE, w);
+            else q = fx_sum(acc + f * NLIMB * WSTRIDE, w);
+            if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(F.f[field_slot<NF>(f)]) + g,
+                                  (unsigned long long)q);
         }
     }
 }
@@ -457,6 +437,32 @@ EPIC_DEV void load_values(const Params& P, const PView& pv, long long i, double 
     }
 }
 
+// Largest |value| of each scattered field over all parcels (as ordered bits of
+// a non-negative double; a NaN counts as +inf), into pbound, which the caller
+// cleared: the fixed-point scales of the scatter that follows.
+EPIC_DEV unsigned long long max_bits(double a) { return (unsigned long long)__double_as_longlong(a); }
+template <int NF, class R>
+__global__ void __launch_bounds__(PB) k_p2g_bounds(Params P, PView pv, long long n, unsigned long long* pbound) {
+    double mx[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) mx[f] = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        R vp[NF];
+        load_values<NF, R>(P, pv, i, a64<R>(pv, A_Z, i), vp);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            const double a = fabs((double)vp[f]);
+            mx[f] = (a > mx[f] || a != a) ? a : mx[f];
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        double v = isnan(mx[f]) ? INFINITY : mx[f];
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffff, v, o));
+        if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(&pbound[bound_slot<NF>(f)], max_bits(v));
+    }
+}
+
 EPIC_DEV void count_parcel(const Params& P, const double* pos, double vol, int* nparg, int* nsparg, unsigned* err) {
     int ci, cj, ck;
     cell_of(P, pos, ci, cj, ck);
@@ -485,8 +491,7 @@ EPIC_DEV void vectors(const PView& pv, long long i, bool reuse, bool store, R* e
     }
 }
 
-// Pass B of a scatter round: support points of parcels [q0, q1) into the
-// window (or the global fields).
+// The support points of parcels [q0, q1) into the window (or the grid sums).
 template <int NF, class R, bool VEC = true>
 EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long long q1, const WinShared<NF>* ws,
                             unsigned* acc, const Fields7& F, int* nparg, int* nsparg, bool reuse, bool store,
@@ -528,11 +533,11 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         for (int q = 1; q < 4; ++q) {
             support_point(pos, ed, td, (s0 + q) & 3, pt);
             if (!merge_into(P, pt, cur)) {
-                scatter_tri<NF, R>(P, W, acc, F, cur, vs, ws->inv, err);
+                scatter_tri<NF, R>(P, W, acc, F, cur, vs, err);
                 cur = trilinear(P, pt);
             }
         }
-        scatter_tri<NF, R>(P, W, acc, F, cur, vs, ws->inv, err);
+        scatter_tri<NF, R>(P, W, acc, F, cur, vs, err);
     }
 }
 
@@ -548,39 +553,34 @@ __global__ void __launch_bounds__(PB, 4) k_vectors(PView pv, long long n, unsign
     }
 }
 
-// par2grid scatter (NF = 7) and vol2grid (NF = 1).
+// par2grid scatter (NF = 7 or 5) and vol2grid (NF = 1).
 template <int NF, class R, bool VEC>
 // vol2grid (NF = 1) has a small window and few live values: three CTAs per SM
 __global__ void __launch_bounds__(PB, NF == 1 ? 3 : SB) k_scatter(Params P, PView pv, long long n, Boxes B, Fields7 F,
-                                                    int* nparg, int* nsparg, int reuse, int store, int lg,
-                                                    unsigned* err) {
+                                                    const unsigned long long* pbound, int* nparg, int* nsparg,
+                                                    int reuse, int store, int lg, unsigned* err) {
     extern __shared__ __align__(16) unsigned acc[];
     __shared__ WinShared<NF> ws;
     const Range Rg = cta_range(P, pv, B, n);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 3; ++k) { ws.mn[k] = INT_MAX; ws.mx[k] = INT_MIN; }
+        for (int f = 0; f < NF; ++f) ws.scale[f] = fx_scale(pbound, bound_slot<NF>(f), fx_bits<R>(), err);
+        if (Rg.box) ws.W = box_window(P, Rg);
+    }
+    __syncthreads();
+    if (!Rg.box) {
+        tail_bounds<NF>(P, Rg, pv, &ws);
+        __syncthreads();
+        if (threadIdx.x == 0) ws.W = tail_window(P, Rg, ws.mn, ws.mx);
+        __syncthreads();
+    }
     for (long long q0 = Rg.r0; q0 < Rg.r1; q0 += round_max<R>()) {
-        long long q1 = min(q0 + round_max<R>(), Rg.r1);
-        win_begin(&ws);
-        __syncthreads();
-        WinPart<NF> wp;
-        wp.init();
-        for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
-            double p[3] = {a64<R>(pv, A_X, i), a64<R>(pv, A_Y, i), a64<R>(pv, A_Z, i)};
-            R vpr[NF];
-            load_values<NF, R>(P, pv, i, p[2], vpr);
-            double vp[NF];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) vp[f] = (double)vpr[f];
-            wp.add(P, Rg, p, vp);
-        }
-        win_reduce(&ws, wp);
-        __syncthreads();
-        if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 34 : 48);
-        __syncthreads();
+        const long long q1 = min(q0 + round_max<R>(), Rg.r1);
         win_zero<NF, R>(acc, ws.W);
         __syncthreads();
         scatter_round<NF, R, VEC>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, reuse != 0, store != 0, lg, err);
         __syncthreads();
-        win_flush<NF, R>(P, acc, &ws, F);
+        win_flush<NF, R>(P, acc, ws.W, F);
         __syncthreads();
     }
 }
@@ -760,13 +760,12 @@ EPIC_DEV void dBdt_r(const R* s, const R* b, R B33, R* o) {
     o[4] = s[I_DWDX] * b[1] + s[I_DVDX] * b[2] + s[I_DWDY] * b[3] - s[I_DUDX] * b[4] + s[I_DVDZ] * B33;
 }
 
-template <bool DIAG, bool SCATTER, class R, bool VOUT = false>
+template <bool DIAG, class R, bool VOUT = false>
 __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long n, Boxes B, const R* pack,
-                                                  Fields7 F, int* nparg, int* nsparg, FusedArgs S,
-                                                  const StepScalars* sc, double* partials, unsigned* err) {
+                                                  FusedArgs S, const StepScalars* sc, double* partials,
+                                                  unsigned* err) {
     using Ops = typename Form<R>::Ops;
     extern __shared__ __align__(16) unsigned acc[];
-    __shared__ WinShared<7> ws;
     __shared__ double red[PB / 32][NDIAG];
     constexpr int ND = DIAG ? NDIAG : 1;
     // the diagnostic sums of this thread, in shared memory (registers are
@@ -781,22 +780,16 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
     // without the scatter pass, the dynamic shared memory holds the box's gather records
     RecWin RW;
     RW.ok = 0;
-    if (!SCATTER && S.recwin) {
+    if (S.recwin) {
         RW = recwin_load<R>(P, Rg, blockIdx.x < B.nbox, pack, reinterpret_cast<R*>(acc));
         __syncthreads();
     }
-    for (long long q0 = Rg.r0; q0 < Rg.r1; q0 += round_max<R>()) {
-        long long q1 = min(q0 + round_max<R>(), Rg.r1);
-        if (SCATTER) {
-            win_begin(&ws);
-            __syncthreads();
-        }
-        WinPart<7> wp;
-        wp.init();
-        // pass A: grid2par + dB/dt + LS-RK update
+    {
+        const long long q0 = Rg.r0, q1 = Rg.r1;
+        // grid2par + dB/dt + LS-RK update
         for (long long i = q0 + threadIdx.x; i < q1; i += blockDim.x) {
             // bring the next parcel's attribute lines into L2 (one lane per 128-byte line)
-            if (!SCATTER && (threadIdx.x & 15) == 0 && i + blockDim.x < q1) {
+            if ((threadIdx.x & 15) == 0 && i + blockDim.x < q1) {
                 const long long j = i + blockDim.x;
 #pragma unroll
                 for (int k = 0; k < 29; ++k) {
@@ -847,13 +840,11 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 for (int q = 1; q < 4; ++q) {
                     support_point(pos, ed, td, (s0 + q) & 3, pt);
                     if (!merge_into(P, pt, cur)) {
-                        ok = (SCATTER ? gather_tri<R>(P, pack, cur, g)
-                                      : gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g)) && ok;
+                        ok = gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g) && ok;
                         cur = trilinear(P, pt);
                     }
                 }
-                ok = (SCATTER ? gather_tri<R>(P, pack, cur, g)
-                              : gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g)) && ok;
+                ok = gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g) && ok;
                 if (!ok) set_err(err, ERRB_ZRANGE);
             }
             if constexpr (!Form<R>::mixed) load_accumulators();
@@ -955,27 +946,6 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
 #pragma unroll
                 for (int k = 0; k < 3; ++k) { aR<R>(pv, A_ETA0 + k, i) = eta[k]; aR<R>(pv, A_TAU0 + k, i) = tau[k]; }
             }
-            if (SCATTER) {
-                R vpr[7];
-                p2g_values<R>(P, vor, pos[2], vol, aR<R>(pv, A_BUOY, i), aR<R>(pv, A_HUM, i), vpr);
-                double vp[7];
-#pragma unroll
-                for (int f = 0; f < 7; ++f) vp[f] = (double)vpr[f];
-                wp.add(P, Rg, pos, vp);
-            }
-        }
-        if (SCATTER) {
-            win_reduce(&ws, wp);
-            __syncthreads();
-            if (threadIdx.x == 0) win_make(P, Rg, &ws, q1 - q0, Form<R>::mixed ? 34 : 48);
-            __syncthreads();
-            win_zero<7, R>(acc, ws.W);
-            __syncthreads();
-            // pass B: support vectors of the advanced shape + next par2grid
-            scatter_round<7, R>(P, pv, q0, q1, &ws, acc, F, nparg, nsparg, false, true, S.lg, err);
-            __syncthreads();
-            win_flush<7, R>(P, acc, &ws, F);
-            __syncthreads();
         }
     }
     if (DIAG) {
@@ -1052,6 +1022,10 @@ static void set_smem(K kernel, size_t bytes) {
 // count: par2grid's parcel counts nparg / nsparg (NF = 7 or 5)
 template <int NF, class R>
 static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int lg, bool count) {
+    // the fixed-point scales: the largest value of every scattered field
+    CK(cudaMemsetAsync(c.dsc->pbound, 0, sizeof(c.dsc->pbound), c.stream));
+    k_p2g_bounds<NF, R><<<pgrid(c.n), PB, 0, c.stream>>>(c.P, c.pv, c.n, c.dsc->pbound);
+    CKL();
     if (!reuse && store && c.vectors_kernel) {
         k_vectors<R><<<pgrid(c.n), PB, 0, c.stream>>>(c.pv, c.n, &c.dsc->err);
         CKL();
@@ -1063,7 +1037,8 @@ static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int
     int* nsp = count ? c.nsparg : nullptr;
     auto run = [&](auto kernel) {
         set_smem(kernel, sm);
-        kernel<<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, np, nsp, reuse, store, lg, &c.dsc->err);
+        kernel<<<sgrid(c, B), PB, sm, c.stream>>>(c.P, c.pv, c.n, B, F, c.dsc->pbound, np, nsp, reuse, store, lg,
+                                                   &c.dsc->err);
         CKL();
     };
     if (reuse) run(k_scatter<NF, R, false>);
@@ -1099,6 +1074,8 @@ void scatter_v2g(Ctx& c, bool reuse) {
     prof_end(c, "v2g");
 }
 
+int p2g_fx_bits(const Ctx& c) { return c.pv.mixed ? fx_bits<float>() : fx_bits<double>(); }
+
 template <class R>
 static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatter) {
     GatherFields G;
@@ -1117,30 +1094,23 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
         c.n_partials = g;
         c.diag_buf = c.stage_partials;
     }
-    // split form: the stage kernel without its scatter pass, then the scatter
-    // kernel (its own register budget; one more read of the parcels)
-    const bool split = scatter && !c.fused_scatter;
     const bool moist = S.stage + 1 == c.n_stages;
-    if (split) scatter = false;
-    size_t sm = scatter ? win_bytes<R, 7>() : S.recwin ? recwin_bytes<R>() : 0;
+    size_t sm = S.recwin ? recwin_bytes<R>() : 0;
     auto launch = [&](auto kernel) {
         if (sm) set_smem(kernel, sm);
         prof_begin(c, "stage");
-        // this scatter is the par2grid of stage + 1: dbuoyg and humg only for the last stage
-        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, pack, fields7(c, moist), c.nparg,
-                                        c.nsparg, S, c.dsc, c.stage_partials, &c.dsc->err);
+        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, pack, S, c.dsc, c.stage_partials, &c.dsc->err);
         CKL();
         prof_end(c, "stage");
     };
-    // in the split form the stage kernel may also compute the support vectors
-    // of the advanced shapes, which the scatter then reads
-    const bool vout = split && c.stage_vectors;
-    if (with_diag && scatter) launch(k_stage<true, true, R>);
-    else if (with_diag) vout ? launch(k_stage<true, false, R, true>) : launch(k_stage<true, false, R>);
-    else if (scatter) launch(k_stage<false, true, R>);
-    else vout ? launch(k_stage<false, false, R, true>) : launch(k_stage<false, false, R>);
-    if (split) {
+    // the stage kernel may also compute the support vectors of the advanced
+    // shapes, which the scatter then reads
+    const bool vout = scatter && c.stage_vectors;
+    if (with_diag) vout ? launch(k_stage<true, R, true>) : launch(k_stage<true, R>);
+    else vout ? launch(k_stage<false, R, true>) : launch(k_stage<false, R>);
+    if (scatter) {
         prof_begin(c, "stage_p2g");
+        // the par2grid of stage + 1: dbuoyg and humg only for the last stage;
         // the parcel counts of the intermediate stages are not read (field
         // diagnostics use the step's first par2grid); the last one keeps them
         launch_p2g<R>(c, moist, vout, true, moist);
@@ -1148,7 +1118,7 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
     }
 }
 
-// One LS-RK stage (grid2par + update) fused with the next stage's par2grid
+// One LS-RK stage (grid2par + update), then the next stage's par2grid
 // scatter (not after the last stage).
 void fused_stage(Ctx& c, int stage, bool with_diag) {
     FusedArgs S;

@@ -79,12 +79,6 @@ extern "C" int epic_gpu_test_set_scatter_groups(epic_ctx* ctx, int lg_vol2grid, 
     return EPIC_OK;
 }
 
-extern "C" int epic_gpu_test_set_stage_form(epic_ctx* ctx, int fused) {
-    if (!ctx) return EPIC_ERR_ARG;
-    ctx->c.fused_scatter = fused != 0;
-    return EPIC_OK;
-}
-
 extern "C" int epic_gpu_test_set_vectors_kernel(epic_ctx* ctx, int on) {
     if (!ctx) return EPIC_ERR_ARG;
     ctx->c.vectors_kernel = on != 0;

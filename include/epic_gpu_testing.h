@@ -39,10 +39,6 @@ int epic_gpu_test_set_fft_path(struct epic_ctx* ctx, int path);
  * setting computes the same sums; it only changes the memory access order. */
 int epic_gpu_test_set_scatter_groups(struct epic_ctx* ctx, int lg_vol2grid, int lg_par2grid, int lg_stage);
 
-/* fused != 0: each LS-RK stage kernel also scatters the next stage's
- * par2grid; 0: a separate scatter kernel does (same sums). */
-int epic_gpu_test_set_stage_form(struct epic_ctx* ctx, int fused);
-
 /* Free the second parcel store, as when the device had no room for it: the
  * box sort then permutes slot by slot through scratch memory. */
 /* Support vectors by a kernel of their own before a scatter that recomputes

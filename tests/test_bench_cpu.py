@@ -42,7 +42,7 @@ def test_clock_sampler_without_gpu():
 
 def test_reference_arm_line():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "3"], capture_output=True, text=True, cwd=ROOT, timeout=600)
+                        "--warmup", "3", "--no-full-check"], capture_output=True, text=True, cwd=ROOT, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True

@@ -389,3 +389,31 @@ def test_stage_variants_agree(glib):
         assert n == out[0][1] and rel_err(t, out[0][0]) < 1e-12
         for k in p:
             assert rel_err(p[k], out[0][2][k]) < 1e-11, k
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_par2grid_bitwise_reproducible(glib, precision):
+    """par2grid and vol2grid sum exact integers at one fixed-point scale per
+    field, so the gridded fields do not depend on the order of the adds: two
+    calls on the same store, and calls with other lane mappings of the
+    scatter, give bitwise the same fields.  The store is box ordered with
+    split children in a tail (one step of a stretched state), so box windows,
+    tail chunks and direct adds all take part."""
+    import ctypes as C
+    s = small_state("thermal", n=32, small_frac=0.02, seed=3, stretch=True)
+    gc = make_context(s, glib, keep_order=0, precision=precision)
+    _, info = gc.step(0.0)
+    assert info.n_splits > 0
+    ids = list(abi.VORTG) + [abi.TBUOYG, abi.DBUOYG, abi.HUMG, abi.VOLG, abi.NPARG, abi.NSPARG]
+    f = glib.lib.epic_gpu_test_set_scatter_groups
+    f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    runs = []
+    for lg in (1, 1, 0, 3):
+        assert f(gc.h, lg, lg, lg) == 0
+        gc.par2grid(False)
+        p2g = [gc.get_field(i).copy() for i in ids]
+        gc.vol2grid(False)
+        runs.append(p2g + [gc.get_field(abi.VOLG).copy()])
+    for r in runs[1:]:
+        for a, b in zip(r, runs[0]):
+            assert np.array_equal(a.view(np.int64), b.view(np.int64))
