@@ -236,6 +236,8 @@ void apply_bndry_fluxes(Ctx& c);
 void autotune(Ctx& c, epic_tuning* out);
 // spectral.cu: a forward horizontal FFT of one field into work arrays (timing probe)
 void fft_forward_probe(Ctx& c);
+// fftxyp2s, lapinv1, fftxys2p of a device field into out (test hook)
+void lapinv_probe(Ctx& c, const double* in, double* out);
 
 // merge.cu
 long long parcel_merge(Ctx& c);

@@ -695,6 +695,27 @@ void periodic_all(Ctx& c) {
     CKL();
 }
 
+__global__ void k_reflective(Params P, PView pv, long long n) {
+    PLOOP(n) {
+        double p[3] = {pv.get(A_X, i), pv.get(A_Y, i), pv.get(A_Z, i)};
+        double b[5];
+        load_B(pv, i, b);
+        const double z0 = p[2];
+        reflective_bc(P, p, b);
+        if (p[2] != z0) {
+            pv.set(A_Z, i, p[2]);
+            pv.set(A_B13, i, b[2]);
+            pv.set(A_B23, i, b[4]);
+        }
+    }
+}
+
+void reflective_all(Ctx& c) {
+    if (c.n == 0) return;
+    k_reflective<<<pgrid(c.n), PB, 0, c.stream>>>(c.P, c.pv, c.n);
+    CKL();
+}
+
 // ---------------------------------------------------------------------------
 // Split (parcel_split.f90:37-198).  The test uses non-contracted arithmetic
 // so the decision rounds like the oracle; children are appended in

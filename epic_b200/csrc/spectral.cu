@@ -1712,6 +1712,29 @@ static void diverge_laplace_t(Ctx& c, double* phi, double* grad[3]) {
     halo(c, {{grad[0], 0}, {grad[1], 0}, {grad[2], 0}});
 }
 
+// fftxyp2s, lapinv1, fftxys2p of a device field (rows 0 .. nz) into out:
+// the transforms and the tridiagonal solve of diverge (test hook).
+template <class T>
+static void lapinv_probe_t(Ctx& c, const double* in, double* out) {
+    const Params& P = c.P;
+    T* ds = wk<T>(c, 0);
+    const double* fin[1] = {in};
+    T* fs[1] = {ds};
+    fft_xy(c, fin, fs, 1, true);
+    int ncol = P.nx * P.ny;
+    size_t lsm = col_smem<double>(c, 3);
+    allow_smem(k_lapinv<T>, lsm);
+    k_lapinv<T><<<(ncol + CT - 1) / CT, 256, lsm, c.stream>>>(ds, c.T.etdv, c.T.htdv, P.ap, ncol, P.nz, P.nzh);
+    CKL();
+    const T* gin[1] = {ds};
+    double* gout[1] = {out};
+    fft_xy(c, gin, gout, 1, false);
+}
+void lapinv_probe(Ctx& c, const double* in, double* out) {
+    if (c.pv.mixed) lapinv_probe_t<float>(c, in, out);
+    else lapinv_probe_t<double>(c, in, out);
+}
+
 void fft_forward_probe(Ctx& c) {
     const double* in[3] = {c.tbuoyg(), c.velog(0), c.velog(1)};
     if (c.pv.mixed) {

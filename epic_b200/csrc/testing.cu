@@ -63,6 +63,38 @@ extern "C" int epic_gpu_test_diverge(epic_ctx* ctx, const double* phi, double* g
     return EPIC_OK;
 }
 
+extern "C" int epic_gpu_test_spectral(epic_ctx* ctx, int op, const double* f, double* out) {
+    if (!ctx || !f || !out) return EPIC_ERR_ARG;
+    if (op != 0) return EPIC_ERR_ARG;   // the step's vertical differences live inside fused column kernels
+    Ctx& c = ctx->c;
+    try {
+        double* din = c.w(7);
+        double* dout = c.w(8);
+        CK(cudaMemcpyAsync(din, f, sizeof(double) * c.P.fsz, cudaMemcpyHostToDevice, c.stream));
+        CK(cudaMemsetAsync(dout, 0, sizeof(double) * c.P.fsz, c.stream));
+        lapinv_probe(c, din, dout);
+        CK(cudaMemcpyAsync(out, dout, sizeof(double) * c.P.fsz, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+    } catch (const CudaError& e) {
+        c.err = e.what();
+        return e.code;
+    }
+    return EPIC_OK;
+}
+
+extern "C" int epic_gpu_test_reflective_bc(epic_ctx* ctx) {
+    if (!ctx) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    try {
+        reflective_all(c);
+        CK(cudaStreamSynchronize(c.stream));
+    } catch (const CudaError& e) {
+        c.err = e.what();
+        return e.code;
+    }
+    return EPIC_OK;
+}
+
 extern "C" int epic_gpu_test_set_fft_path(epic_ctx* ctx, int path) {
     if (!ctx) return EPIC_ERR_ARG;
     if (path < 0 || path > 3) return EPIC_ERR_ARG;

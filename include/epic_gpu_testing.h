@@ -25,6 +25,16 @@ struct epic_ctx;
  * with the halo rows extrapolated like apply_laplace. */
 int epic_gpu_test_diverge(struct epic_ctx* ctx, const double* phi, double* grad);
 
+/* fftxyp2s, lapinv1 and fftxys2p (sta3dfft.f90:134-257,
+ * inversion_utils.f90:567-589) of a physical field f ((nz+3) x ny x nx, z
+ * fastest, rows 0 .. nz) into out (op 0; test_lapinv1.f90).  Other ops are
+ * the oracle's (epic_oracle_test_spectral): the device has no standalone
+ * vertical differences, they are fused into the inversion's column kernels. */
+int epic_gpu_test_spectral(struct epic_ctx* ctx, int op, const double* f, double* out);
+
+/* apply_reflective_bc (parcel_bc.f90:45-57) on every parcel. */
+int epic_gpu_test_reflective_bc(struct epic_ctx* ctx);
+
 /* Selects the horizontal FFT implementation of the context: 0 (default) the
  * 2-D plane kernel for square grids of 16, 32, 64 or 128 points, else the
  * tiled line kernel; 1 the tiled line kernel (power-of-two axes 16 .. 256);

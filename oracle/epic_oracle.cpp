@@ -417,6 +417,27 @@ void central_diffz(Ctx& c, const Arr& f, Arr& df) {
         }
 }
 
+// diffz (inversion_utils.f90:523-559): d/dz of a field in the decomposed
+// semi-spectral form (linear part through dphim / dphip, the sine series
+// through rkz and a cosine transform), returned decomposed.  Not called by
+// the step; its unit tests (test_mpi_diffz0..5) pin the decomposition.
+void diffz(Ctx& c, const Arr& fs, Arr& ds) {
+    int nx = c.nx, ny = c.ny, nz = c.nz;
+    ds.assign(fs.size(), 0.0);
+    std::vector<double> as(nz + 1);
+    for (int kx = 0; kx < nx; ++kx)
+        for (int ky = 0; ky < ny; ++ky) {
+            long t = c.si(0, ky, kx);
+            for (int iz = 0; iz <= nz; ++iz) ds[t + iz] = fs[t] * c.dphim[t + iz] + fs[t + nz] * c.dphip[t + iz];
+            as[0] = zero;
+            for (int kz = 1; kz <= nz - 1; ++kz) as[kz] = c.rkz[kz] * fs[t + kz];
+            as[nz] = zero;
+            c.tz.dct(as.data());
+            for (int iz = 0; iz <= nz; ++iz) ds[t + iz] = ds[t + iz] + as[iz];
+        }
+    field_decompose_semi_spectral(c, ds);
+}
+
 // lapinv1 (inversion_utils.f90:567-589)
 void lapinv1(Ctx& c, Arr& fs) {
     int nx = c.nx, ny = c.ny, nz = c.nz;
@@ -2350,5 +2371,40 @@ extern "C" int epic_oracle_test_diverge(epic_ctx* ctx, const double* phi, double
         extrap_halo(c, g[k]);
         std::memcpy(grad + (size_t)k * c.fsz, g[k].data(), sizeof(double) * c.fsz);
     }
+    return EPIC_OK;
+}
+
+// Known-answer hooks of the vertical operators, on a physical field f
+// ((nz+3) x ny x nx, z fastest; rows 0 .. nz used and written):
+//   op 0: fftxyp2s, lapinv1, fftxys2p              (test_lapinv1.f90)
+//   op 1: fftxyp2s, central_diffz_semi_spectral, fftxys2p
+//   op 2: field_decompose_physical, diffz, field_combine_physical
+//                                                  (test_mpi_diffz0..5.f90)
+extern "C" int epic_oracle_test_spectral(epic_ctx* ctx, int op, const double* f, double* out) {
+    if (!ctx || !f || !out || op < 0 || op > 2) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    Arr fp(f, f + c.fsz), fs, ds, dp(c.fsz, 0.0);
+    if (op == 0) {
+        fftxyp2s(c, fp, fs);
+        lapinv1(c, fs);
+        fftxys2p(c, fs, dp);
+    } else if (op == 1) {
+        fftxyp2s(c, fp, fs);
+        central_diffz_semi_spectral(c, fs, ds);
+        fftxys2p(c, ds, dp);
+    } else {
+        field_decompose_physical(c, fp, fs);
+        diffz(c, fs, ds);
+        field_combine_physical(c, ds, dp);
+    }
+    std::memcpy(out, dp.data(), sizeof(double) * c.fsz);
+    return EPIC_OK;
+}
+
+// apply_reflective_bc (parcel_bc.f90:45-57) on every parcel.
+extern "C" int epic_oracle_test_reflective_bc(epic_ctx* ctx) {
+    if (!ctx) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    for (long n = 0; n < c.n; ++n) apply_reflective_bc(c, &c.pos[3 * n], &c.B[5 * n]);
     return EPIC_OK;
 }

@@ -136,3 +136,15 @@ def test_fortran_interfaces_match_c_prototypes():
         assert n == protos[cname], (cname, n, protos[cname])
         found += 1
     assert found == len(re.findall(r"bind\(C,\s*name=", text)) >= 17
+
+
+def test_library_has_no_undefined_own_symbols():
+    """Every function of the library's own namespace is defined: a shared
+    library links with undefined symbols and would only fail when loaded."""
+    import subprocess
+    lib = os.path.join(ROOT, "epic_b200", "libepic_b200.so")
+    if not os.path.exists(lib):
+        pytest.skip("library not built")
+    out = subprocess.check_output(["nm", "-D", "--undefined-only", lib]).decode()
+    own = [ln for ln in out.splitlines() if "epic" in ln.lower()]
+    assert not own, own

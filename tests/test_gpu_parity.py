@@ -311,6 +311,24 @@ def test_nearest_constellations_gpu(olib, glib, case):
     _cmp_parcels(oc, gc)
 
 
+def _kat_params():
+    from tests import test_oracle_cpu as T
+    return T.NEAREST_KATS
+
+
+@pytest.mark.parametrize("name,setup,expected,cell", _kat_params(),
+                         ids=[f"{n[9:]}-{s}" for n, s, _, _ in _kat_params()])
+def test_nearest_reference_kats_gpu(olib, glib, name, setup, expected, cell):
+    """test_mpi_nearest_5.f90 .. _20.f90 on the device: the stated merge
+    counts, and the oracle's pairs and merged parcels."""
+    from tests import test_oracle_cpu as T
+    oc, _ = T._nearest_case(olib, T.kat_placement(cell))
+    gc, _ = T._nearest_case(glib, T.kat_placement(cell))
+    assert gc.merge() == expected == oc.merge()
+    assert all(np.array_equal(a, b) for a, b in zip(gc.merge_pairs(), oc.merge_pairs()))
+    _cmp_parcels(oc, gc)
+
+
 @pytest.mark.parametrize("kind", ["thermal", "beltrami"])
 def test_par2grid_box_windows(olib, glib, kind):
     """par2grid and vol2grid through the box-ordered store (shared-memory

@@ -160,6 +160,46 @@ def _p4(i, j, dx):   # test_mpi_nearest_4.f90:95-135 ((2) a - B)
     return [(x, y + 0.1 * dx, 1.1), (x, y + dx * 0.35, 0.9), (x, y - 0.42 * dx, 1.1)]
 
 
+def _load_kats():
+    import json
+    with open(os.path.join(os.path.dirname(__file__), "golden", "nearest_kats.json")) as f:
+        return json.load(f)
+
+
+NEAREST_KATS = [(name, c["setup"], c["expected"], c["cell"]) for name, t in sorted(_load_kats().items())
+                for c in t["cases"]]
+
+
+def kat_placement(cell):
+    """The constellation of one cell of a test_mpi_nearest_5.._20 case: each
+    parcel at the cell centre (x, y) moved by sign x (cell width x factor)
+    along x and y, in the reference's evaluation order x + dx(k) * c."""
+    def place(i, j, dx):
+        x, y = (0.5 + i) * dx, (0.5 + j) * dx
+        out = []
+        for p in cell:
+            q = []
+            for base, (sgn, _axis, fac) in zip((x, y), p["off"]):
+                q.append(base + dx * fac if sgn > 0 else base - dx * fac if sgn < 0 else base)
+            out.append((q[0], q[1], p["vol"]))
+        return out
+    return place
+
+
+@pytest.mark.parametrize("name,setup,expected,cell", NEAREST_KATS,
+                         ids=[f"{n[9:]}-{s}" for n, s, _, _ in NEAREST_KATS])
+def test_nearest_reference_kats(olib, name, setup, expected, cell):
+    """unit-tests/3d/test_mpi_nearest_5.f90 .. _20.f90 (fixture made from
+    them by tests/golden/make_nearest_kats.py): chains of small and big
+    parcels across the periodic edges (a = b - c, a - b - C, a - B - c,
+    a - b = c - d, a - b - c = d, ...); the number of merges equals the count
+    each test states, and no parcel is lost."""
+    ctx, n0 = _nearest_case(olib, kat_placement(cell))
+    nm = ctx.merge()
+    assert nm == expected
+    assert ctx.num_parcels() == n0 - nm
+
+
 @pytest.mark.parametrize("placement,expected", [(_p1, 200), (_p2, 200), (_p3, 100), (_p4, 100)])
 def test_nearest_constellations(olib, placement, expected):
     ctx, n0 = _nearest_case(olib, placement)
