@@ -382,7 +382,10 @@ class EpicContext:
 
     def merge_pairs(self):
         """(isma, iclo) of the last merge, 1-based, in merge order."""
-        cap = max(self.num_parcels(), 1)
+        n = C.c_int64()
+        # the count first (a zero capacity only reports it)
+        self.lib.fn["get_merge_pairs"](self.h, C.c_int64(0), C.byref(n), None, None)
+        cap = max(n.value, 1)
         isma = np.empty(cap, dtype=np.int32)
         iclo = np.empty(cap, dtype=np.int32)
         n = C.c_int64()

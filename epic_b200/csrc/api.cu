@@ -697,7 +697,14 @@ static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
     // with the following par2grid (stage.cu)
     double tt = t;
     CK(cudaMemcpyAsync(&c.dsc->t, &tt, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    // the first par2grid's scales and the step bounds of the later scatters
+    // (surface fluxes change buoyancy and humidity in stage 1: then every
+    // scatter bounds its own values)
+    p2g_step_bounds(c);
+    c.p2g_bound_ready = true;
     par2grid(c, t > c.cfg.t_initial, true, c.n_stages == 1);
+    c.p2g_bound_ready = false;
+    c.pstep_valid = !c.flux_on;
     prof_begin(c, "vor2vel");
     vor2vel(c);
     prof_end(c, "vor2vel");
@@ -729,6 +736,7 @@ static double rk_step(Ctx& c, double& t, double* pstats, double* fstats) {
         parcel_damp(c);
         prof_end(c, "damping");
     }
+    c.pstep_valid = false;
     if (pstats) finish_parcel_diag(c, pstats);
     double dt = 0.0;
     CK(cudaMemcpyAsync(&dt, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -839,6 +847,9 @@ int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info) {
     prof_begin(c, "split");
     parcel_split(c);
     prof_end(c, "split");
+    // the split test bounded the volumes (children halve theirs): the
+    // corrections' vol2grid scales
+    c.v2g_bound_ready = c.n > 0;
     for (int it = 1; it <= c.cfg.correction_iters; ++it) {
         prof_begin(c, "laplace");
         apply_laplace(c, it > 1);
@@ -847,6 +858,7 @@ int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info) {
         apply_gradient(c, true);
         prof_end(c, "gradient");
     }
+    c.v2g_bound_ready = false;
     check_device_error(c);
     info->t = *t;
     info->n_parcels = c.n;

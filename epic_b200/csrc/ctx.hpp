@@ -74,6 +74,12 @@ struct StepScalars {
     // of non-negative doubles): vortg x, y, z, dbuoyg, humg, tbuoyg, volg;
     // the fixed-point scales of a scatter and of its tail
     unsigned long long pbound[8];
+    // bounds that hold for a whole RK step (volume, buoyancy and humidity do
+    // not change between its stages): 0.25 V |b|, 0.25 V |h|,
+    // 0.25 V (|b| + glat max(h, 0)) (above |tbuoyg|'s values), 0.25 V
+    unsigned long long pstep[4];
+    // 0.25 V over the parcels after the split test (vol2grid of the corrections)
+    unsigned long long vbound;
 };
 
 // CUDA-event timing of every launch of one named kernel on the context stream.
@@ -115,6 +121,17 @@ struct Ctx {
     int stage_recwin = 0;         // split-form stage kernel gathers from records staged in shared memory
     bool stage_vectors = false;   // split-form stage kernel computes the next par2grid's support vectors
     bool p2g_counted = true;
+    // mixed form with FP64 spectral work (an accuracy experiment; test toggle)
+    bool spectral_fp64 = false;
+    // the next scatter's bounds are already in pbound (computed by the
+    // kernel that produced its values); else a bound pass runs first
+    bool p2g_bound_ready = false;
+    // vol2grid may take its volume bound from vbound (set by the step between
+    // its split and its corrections)
+    bool v2g_bound_ready = false;
+    // StepScalars::pstep holds this step's bounds (set by rk_step's first
+    // par2grid when the stages change no volume, buoyancy or humidity)
+    bool pstep_valid = false;
     // labels (cfg.labels): label and dilution per parcel, capacity cap
     long long* label = nullptr;
     double* dil = nullptr;
@@ -219,6 +236,8 @@ long long stage_grid_max(const Params& P, long long cap);
 void p2g_tail(Ctx& c);
 // fixed-point bits of the par2grid sums (the scale of the tail's conversion)
 int p2g_fx_bits(const Ctx& c);
+// bounds of the step's first par2grid and of the step (StepScalars::pstep)
+void p2g_step_bounds(Ctx& c);
 
 // init.cu
 void init_state(Ctx& c, const epic_init_spec& s);

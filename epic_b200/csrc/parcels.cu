@@ -720,11 +720,15 @@ void reflective_all(Ctx& c) {
 // Split (parcel_split.f90:37-198).  The test uses non-contracted arithmetic
 // so the decision rounds like the oracle; children are appended in
 // ascending parent order (the reference's single-thread order).
-__global__ void k_split_flag(Params P, PView pv, long long n, int* flag, unsigned* err) {
+// Also bounds 0.25 V over the parcels (vbound, cleared by the host), which
+// covers the children's volumes: the scale of the corrections' vol2grid.
+__global__ void k_split_flag(Params P, PView pv, long long n, int* flag, unsigned long long* vbound, unsigned* err) {
+    double vmax = 0.0;
     PLOOP(n) {
         double b[5];
         load_B(pv, i, b);
         const double vol = pv.get(A_VOL, i);
+        vmax = (0.25 * vol > vmax || vol != vol) ? 0.25 * vol : vmax;
         const double B33 = get_B33<FastOps>(b, vol, err);
         // No split without eigenvalues when a bound proves it: every
         // eigenvalue is at most the Frobenius norm F of the full matrix, and
@@ -754,6 +758,9 @@ __global__ void k_split_flag(Params P, PView pv, long long n, int* flag, unsigne
         }
         flag[i] = (lam < P.lambda_max && D[0] < P.amax2) ? 0 : 1;
     }
+    vmax = isnan(vmax) ? INFINITY : vmax;
+    for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffff, vmax, o));
+    if ((threadIdx.x & 31) == 0 && vmax > 0.0) atomicMax(vbound, (unsigned long long)__double_as_longlong(vmax));
 }
 
 __global__ void k_split_apply(Params P, PView pv, long long n, const int* flag, const int* offs, long long* label,
@@ -837,7 +844,8 @@ long long parcel_split(Ctx& c) {
     int* offs = flag + (n + 1);
     void* tmp = reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(offs + (n + 1)) + 255) & ~(uintptr_t)255);
     CK(cudaMemsetAsync(flag + n, 0, sizeof(int), c.stream));
-    k_split_flag<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, flag, &c.dsc->err);
+    CK(cudaMemsetAsync(&c.dsc->vbound, 0, sizeof(unsigned long long), c.stream));
+    k_split_flag<<<pgrid(n), PB, 0, c.stream>>>(c.P, c.pv, n, flag, &c.dsc->vbound, &c.dsc->err);
     CKL();
     CK(cub::DeviceScan::ExclusiveSum(tmp, need_cub, flag, offs, (int)n + 1, c.stream));
     int ns = 0;

@@ -1,6 +1,7 @@
 // Served ensembles (include/epic_serve.h): a pool of worker threads, one per
 // slot, each running one simulation at a time on its own context and CUDA
-// stream; first-come-first-served admission by slot and by free HBM; idle
+// stream; admission of the first queued request (in arrival order) that fits
+// the free slots and the HBM budget; idle
 // contexts kept per configuration and reused, so that a steady stream of
 // requests allocates (and frees, which synchronises the whole device) no
 // device memory.
@@ -13,6 +14,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <set>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -54,12 +56,13 @@ struct epic_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Job> queue;
-    std::map<int64_t, epic_result> results;
+    std::map<int64_t, epic_result> results;   // finished, not yet waited for
+    std::set<int64_t> pending;                 // submitted, not yet finished
     std::vector<PooledCtx> idle;
     std::vector<std::thread> workers;
     int device = 0;
     double budget = 0.0, in_use = 0.0;   // bytes: running requests + idle contexts
-    int64_t next_id = 1, running = 0;
+    int64_t next_id = 1, running = 0, n_collected = 0;
     bool stop = false;
     std::chrono::steady_clock::time_point t0;
 
@@ -68,7 +71,26 @@ struct epic_server {
     }
 };
 
-static bool same_cfg(const epic_cfg& a, const epic_cfg& b) { return std::memcmp(&a, &b, sizeof(epic_cfg)) == 0; }
+// Field by field (the struct has padding, which callers need not clear).
+static bool same_cfg(const epic_cfg& a, const epic_cfg& b) {
+    auto eq3 = [](const double* x, const double* y) { return x[0] == y[0] && x[1] == y[1] && x[2] == y[2]; };
+    return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && eq3(a.lower, b.lower) && eq3(a.extent, b.extent) &&
+           a.size_factor == b.size_factor && a.grow_factor == b.grow_factor && a.shrink_factor == b.shrink_factor &&
+           a.n_per_cell == b.n_per_cell && a.lambda_max == b.lambda_max && a.min_vratio == b.min_vratio &&
+           a.correction_iters == b.correction_iters && a.gradient_pref == b.gradient_pref &&
+           a.max_compression == b.max_compression && a.t_initial == b.t_initial && a.t_limit == b.t_limit &&
+           a.alpha == b.alpha && a.precise_stop == b.precise_stop && a.use_fixed_dt == b.use_fixed_dt &&
+           a.fixed_dt == b.fixed_dt && a.rk_order == b.rk_order && a.gravity == b.gravity && a.L_v == b.L_v &&
+           a.c_p == b.c_p && a.theta_0 == b.theta_0 && a.q_0 == b.q_0 && a.height_c == b.height_c &&
+           a.ang_vel == b.ang_vel && a.lat_degrees == b.lat_degrees &&
+           a.l_planetary_vorticity == b.l_planetary_vorticity && a.bndry_zeta_zero[0] == b.bndry_zeta_zero[0] &&
+           a.bndry_zeta_zero[1] == b.bndry_zeta_zero[1] && a.capacity == b.capacity && a.precision == b.precision &&
+           a.keep_order == b.keep_order && a.damping_vorticity_prefactor == b.damping_vorticity_prefactor &&
+           a.damping_scalars_prefactor == b.damping_scalars_prefactor && a.damping_vorticity == b.damping_vorticity &&
+           a.damping_surface_vorticity == b.damping_surface_vorticity && a.damping_scalars == b.damping_scalars &&
+           a.damping_surface_scalars == b.damping_surface_scalars && a.labels == b.labels &&
+           a.label_seed == b.label_seed;
+}
 
 // Take an idle context of this configuration out of the pool (nullptr if none).
 static epic_ctx* pool_take(epic_server* s, const epic_cfg& cfg, double* bytes) {
@@ -120,6 +142,7 @@ static void run_job(epic_server* s, const Job& job, int slot, epic_ctx* ctx, epi
     }
     --s->running;
     s->results[job.id] = r;
+    s->pending.erase(job.id);
     s->cv_done.notify_all();
     s->cv_work.notify_all();
 }
@@ -138,21 +161,44 @@ static void worker(epic_server* s, int slot) {
                     s->cv_work.wait(lk);
                     continue;
                 }
-                Job& head = s->queue.front();
-                ctx = pool_take(s, head.req.cfg, &pooled_bytes);
-                if (ctx) break;                                   // its memory is already counted
-                // make room by freeing idle contexts of other configurations
-                while (s->in_use + head.bytes > s->budget && !s->idle.empty()) {
-                    PooledCtx p = s->idle.back();
-                    s->idle.pop_back();
-                    s->in_use -= p.bytes;
-                    epic_gpu_destroy(p.ctx);
+                // the first queued request (in arrival order) that can start now:
+                // a pooled context of its configuration, or room in the budget
+                // (after freeing idle contexts of other configurations)
+                size_t pick = s->queue.size();
+                for (size_t q = 0; q < s->queue.size() && pick == s->queue.size(); ++q) {
+                    Job& cand = s->queue[q];
+                    ctx = pool_take(s, cand.req.cfg, &pooled_bytes);
+                    if (ctx) { pick = q; break; }                    // its memory is already counted
+                    double idle_bytes = 0.0;
+                    for (auto& p : s->idle) idle_bytes += p.bytes;
+                    if (s->in_use - idle_bytes + cand.bytes <= s->budget) {
+                        while (s->in_use + cand.bytes > s->budget && !s->idle.empty()) {
+                            PooledCtx p = s->idle.back();
+                            s->idle.pop_back();
+                            s->in_use -= p.bytes;
+                            epic_gpu_destroy(p.ctx);
+                        }
+                        pick = q;
+                    }
                 }
-                if (s->in_use + head.bytes <= s->budget || s->running == 0) break;
-                s->cv_work.wait(lk);                              // wait for a running job to finish
+                // nothing fits while nothing runs: the head starts anyway (it
+                // passed the budget check at submission)
+                if (pick == s->queue.size() && s->running == 0) {
+                    while (!s->idle.empty()) {
+                        PooledCtx p = s->idle.back();
+                        s->idle.pop_back();
+                        s->in_use -= p.bytes;
+                        epic_gpu_destroy(p.ctx);
+                    }
+                    pick = 0;
+                }
+                if (pick < s->queue.size()) {
+                    job = s->queue[pick];
+                    s->queue.erase(s->queue.begin() + (long)pick);
+                    break;
+                }
+                s->cv_work.wait(lk);                                  // wait for a running job to finish
             }
-            job = s->queue.front();
-            s->queue.pop_front();
             if (ctx) job.bytes = pooled_bytes;
             else s->in_use += job.bytes;
             ++s->running;
@@ -227,6 +273,7 @@ static int submit_locked(epic_server* s, const epic_request* req, int64_t* id) {
         return EPIC_OK;
     }
     s->queue.push_back(j);
+    s->pending.insert(j.id);
     s->cv_work.notify_all();
     return EPIC_OK;
 }
@@ -234,9 +281,11 @@ static int submit_locked(epic_server* s, const epic_request* req, int64_t* id) {
 extern "C" int epic_srv_wait(epic_server* s, int64_t id, epic_result* out) {
     if (!s || !out || id < 1) return EPIC_ERR_ARG;
     std::unique_lock<std::mutex> lk(s->mu);
-    if (id >= s->next_id) return EPIC_ERR_ARG;
+    if (id >= s->next_id || (!s->results.count(id) && !s->pending.count(id))) return EPIC_ERR_ARG;   // unknown or collected
     s->cv_done.wait(lk, [&] { return s->results.count(id) != 0; });
     *out = s->results[id];
+    s->results.erase(id);   // handed over: the server keeps no finished results
+    ++s->n_collected;
     return EPIC_OK;
 }
 
@@ -245,7 +294,7 @@ extern "C" int epic_srv_counts(epic_server* s, int64_t* queued, int64_t* running
     std::lock_guard<std::mutex> lk(s->mu);
     if (queued) *queued = (int64_t)s->queue.size();
     if (running) *running = s->running;
-    if (done) *done = (int64_t)s->results.size();
+    if (done) *done = (int64_t)s->results.size() + s->n_collected;
     return EPIC_OK;
 }
 

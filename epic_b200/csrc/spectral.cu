@@ -1749,15 +1749,15 @@ void fft_forward_probe(Ctx& c) {
 // Dispatch by form: the mixed form's spectral temporaries and arithmetic are
 // FP32 (the physical fields stay FP64; lapinv solves in FP64).
 void vor2vel(Ctx& c) {
-    if (c.pv.mixed) vor2vel_t<float>(c);
+    if (c.pv.mixed && !c.spectral_fp64) vor2vel_t<float>(c);
     else vor2vel_t<double>(c);
 }
 void vorticity_tendency(Ctx& c) {
-    if (c.pv.mixed) vorticity_tendency_t<float>(c);
+    if (c.pv.mixed && !c.spectral_fp64) vorticity_tendency_t<float>(c);
     else vorticity_tendency_t<double>(c);
 }
 void diverge_laplace(Ctx& c, double* phi, double* grad[3]) {
-    if (c.pv.mixed) diverge_laplace_t<float>(c, phi, grad);
+    if (c.pv.mixed && !c.spectral_fp64) diverge_laplace_t<float>(c, phi, grad);
     else diverge_laplace_t<double>(c, phi, grad);
 }
 

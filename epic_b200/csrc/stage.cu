@@ -41,7 +41,10 @@ constexpr int ROUND = 4096;     // parcels per fixed-point round
 // a cell of support-point reach), 13 x 9 x 9 grid points.
 constexpr int WM = 2;
 constexpr int WCAP = (BOXX + 1 + 2 * WM) * (BOXY + 1 + 2 * WM) * (BOXZ + 1 + 2 * WM);
-constexpr int WSTRIDE = (WCAP + 3) & ~3;   // words per limb plane
+// Words per limb plane: at least WCAP, and 11 banks apart (WSTRIDE = 11 mod
+// 32), so that two lanes adding different limbs of the same grid point hit
+// different banks (see LimbOrder).
+constexpr int WSTRIDE = ((WCAP + 31 - 11) / 32) * 32 + 11;
 constexpr int NLIMB = 3;
 constexpr int SB = 2;           // CTAs per SM the scatter kernels are sized for
 
@@ -244,13 +247,39 @@ EPIC_DEV long long fx_round(double wt, double vs) {
     return (__double_as_longlong(r) & 0xfffffffffffffll) - (1ll << 51);
 }
 
+// The order in which a lane adds the limbs of a contribution.  The two lanes
+// of a lane pair take consecutive parcels, usually of one cell, so at every
+// corner they add to the same grid point: the odd lane adds its limbs in
+// rotated order, and with the limb planes 11 banks apart the pair's atomics
+// of one instruction hit different banks instead of the same word.  The
+// sums do not depend on the order.
+struct LimbOrder {
+    int p0, p1, p2;   // plane offsets (words) of the 1st, 2nd and 3rd add
+    bool rot;
+    EPIC_DEV explicit LimbOrder(int nlimb) {
+        rot = (threadIdx.x & 1) != 0;
+        if (nlimb == 3) {
+            p0 = rot ? WSTRIDE : 0;
+            p1 = rot ? 2 * WSTRIDE : WSTRIDE;
+            p2 = rot ? 0 : 2 * WSTRIDE;
+        } else {
+            p0 = rot ? WSTRIDE : 0;
+            p1 = rot ? 0 : WSTRIDE;
+            p2 = 0;
+        }
+    }
+};
+
 // q = ((m >> 36) - 2^15) * 2^36 + ((m >> 18) & 0x3ffff) * 2^18 + (m & 0x3ffff), m = 2^51 + q
-EPIC_DEV void fx_add(unsigned* acc, int w, double wt, double vs) {
+EPIC_DEV void fx_add(unsigned* acc, int w, double wt, double vs, const LimbOrder& o) {
     double r = fma(wt, vs, FX_MAGIC);
     unsigned lo = (unsigned)__double2loint(r), hi = (unsigned)__double2hiint(r);
-    atomicAdd(&acc[w], lo & 0x3ffffu);
-    atomicAdd(&acc[WSTRIDE + w], (lo >> 18) | ((hi & 0xfu) << 14));
-    atomicAdd(&acc[2 * WSTRIDE + w], ((hi & 0xfffffu) >> 4) - 32768u);
+    const unsigned l0 = lo & 0x3ffffu;
+    const unsigned l1 = (lo >> 18) | ((hi & 0xfu) << 14);
+    const unsigned l2 = ((hi & 0xfffffu) >> 4) - 32768u;
+    atomicAdd(&acc[o.p0 + w], o.rot ? l1 : l0);
+    atomicAdd(&acc[o.p1 + w], o.rot ? l2 : l1);
+    atomicAdd(&acc[o.p2 + w], o.rot ? l0 : l2);
 }
 EPIC_DEV long long fx_sum(const unsigned* acc, int w) {
     return (long long)(int)acc[2 * WSTRIDE + w] * (1ll << 36) + (long long)acc[WSTRIDE + w] * (1ll << 18) +
@@ -258,11 +287,13 @@ EPIC_DEV long long fx_sum(const unsigned* acc, int w) {
 }
 
 // Two-limb variant: q = h * 2^19 + l, l = q mod 2^19, h = floor(q / 2^19).
-EPIC_DEV void fx2_add(unsigned* acc, int w, double wt, double vs) {
+EPIC_DEV void fx2_add(unsigned* acc, int w, double wt, double vs, const LimbOrder& o) {
     double r = fma(wt, vs, FX_MAGIC);
     long long m = __double_as_longlong(r) & 0xfffffffffffffll;   // 2^51 + q
-    atomicAdd(&acc[w], (unsigned)(m & 0x7ffff));
-    atomicAdd(&acc[WSTRIDE + w], (unsigned)((m >> 19) - (1ll << 32)));
+    const unsigned l0 = (unsigned)(m & 0x7ffff);
+    const unsigned l1 = (unsigned)((m >> 19) - (1ll << 32));
+    atomicAdd(&acc[o.p0 + w], o.rot ? l1 : l0);
+    atomicAdd(&acc[o.p1 + w], o.rot ? l0 : l1);
 }
 EPIC_DEV long long fx2_sum(const unsigned* acc, int w) {
     return (long long)(int)acc[WSTRIDE + w] * (1ll << 19) + (long long)acc[w];
@@ -335,7 +366,7 @@ EPIC_DEV int merge_start(const Params& P, const double* pos, const double* eta, 
 // vs[f] = value x volume x point weight x s_f.
 template <int NF, class R>
 EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const Fields7& F, const Tri& t,
-                          const double* vs, unsigned* err) {
+                          const double* vs, const LimbOrder& lo, unsigned* err) {
     if (t.ks < -1 || t.ks > P.nz) { set_err(err, ERRB_ZRANGE); return; }
     int lx = wrap_to(t.is - W.gx0, P.nx), ly = wrap_to(t.js - W.gy0, P.ny), lz = t.ks - W.gz0;
     if (W.ok && lx + 1 < W.WX && ly + 1 < W.WY && lz >= 0 && lz + 1 < W.WZ) {
@@ -351,12 +382,12 @@ EPIC_DEV void scatter_tri(const Params& P, const Window& W, unsigned* acc, const
                         const double wt = (double)(float)t.w[kk][jj][ii];
 #pragma unroll
                         for (int f = 0; f < NF; ++f)
-                            if (field_on<NF>(F, f)) fx2_add(acc + f * 2 * WSTRIDE, w, wt, vs[f]);
+                            if (field_on<NF>(F, f)) fx2_add(acc + f * 2 * WSTRIDE, w, wt, vs[f], lo);
                     } else {
                         const double wt = t.w[kk][jj][ii];
 #pragma unroll
                         for (int f = 0; f < NF; ++f)
-                            if (field_on<NF>(F, f)) fx_add(acc + f * NLIMB * WSTRIDE, w, wt, vs[f]);
+                            if (field_on<NF>(F, f)) fx_add(acc + f * NLIMB * WSTRIDE, w, wt, vs[f], lo);
                     }
                 }
     } else {
@@ -439,27 +470,44 @@ EPIC_DEV void load_values(const Params& P, const PView& pv, long long i, double 
 
 // Largest |value| of each scattered field over all parcels (as ordered bits of
 // a non-negative double; a NaN counts as +inf), into pbound, which the caller
-// cleared: the fixed-point scales of the scatter that follows.
+// cleared: the fixed-point scales of the scatter that follows.  STEP also
+// records the step bounds (StepScalars::pstep) for the later stages' scatters.
 EPIC_DEV unsigned long long max_bits(double a) { return (unsigned long long)__double_as_longlong(a); }
-template <int NF, class R>
-__global__ void __launch_bounds__(PB) k_p2g_bounds(Params P, PView pv, long long n, unsigned long long* pbound) {
-    double mx[NF];
+EPIC_DEV double nan_inf(double a) { return isnan(a) ? INFINITY : a; }
+EPIC_DEV double keep_max(double m, double a) { return (a > m || a != a) ? a : m; }
+// warp maximum, then one atomic per warp
+EPIC_DEV void warp_max_to(unsigned long long* dst, double v) {
+    v = nan_inf(v);
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffff, v, o));
+    if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(dst, max_bits(v));
+}
+template <int NF, class R, bool STEP>
+__global__ void __launch_bounds__(PB) k_p2g_bounds(Params P, PView pv, long long n, unsigned long long* pbound,
+                                                   unsigned long long* pstep) {
+    double mx[NF], ms[4];
 #pragma unroll
     for (int f = 0; f < NF; ++f) mx[f] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ms[k] = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         R vp[NF];
         load_values<NF, R>(P, pv, i, a64<R>(pv, A_Z, i), vp);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const double a = fabs((double)vp[f]);
-            mx[f] = (a > mx[f] || a != a) ? a : mx[f];
+        for (int f = 0; f < NF; ++f) mx[f] = keep_max(mx[f], fabs((double)vp[f]));
+        if (STEP) {
+            const double pw = 0.25 * a64<R>(pv, A_VOL, i);
+            const double b = fabs((double)aR<R>(pv, A_BUOY, i)), h = (double)aR<R>(pv, A_HUM, i);
+            ms[0] = keep_max(ms[0], pw * b);
+            ms[1] = keep_max(ms[1], pw * fabs(h));
+            ms[2] = keep_max(ms[2], pw * (b + P.glat * fmax(h, 0.0)));
+            ms[3] = keep_max(ms[3], pw);
         }
     }
 #pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        double v = isnan(mx[f]) ? INFINITY : mx[f];
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffff, v, o));
-        if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(&pbound[bound_slot<NF>(f)], max_bits(v));
+    for (int f = 0; f < NF; ++f) warp_max_to(&pbound[bound_slot<NF>(f)], mx[f]);
+    if (STEP) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) warp_max_to(&pstep[k], ms[k]);
     }
 }
 
@@ -507,6 +555,7 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
     const int cols = 32 >> lg;                          // groups side by side in a warp
     const int S = (U + cols - 1) / cols;                // groups per column
     const int lane = threadIdx.x & 31, gi = lane >> lg, m = lane & ((1 << lg) - 1);
+    const LimbOrder lo(win_words<R>());
     for (int r = threadIdx.x >> 5; r < S; r += blockDim.x >> 5) {
         const int u = gi * S + r;
         const int slot = (u << lg) + m;
@@ -533,11 +582,11 @@ EPIC_DEV void scatter_round(const Params& P, const PView& pv, long long q0, long
         for (int q = 1; q < 4; ++q) {
             support_point(pos, ed, td, (s0 + q) & 3, pt);
             if (!merge_into(P, pt, cur)) {
-                scatter_tri<NF, R>(P, W, acc, F, cur, vs, err);
+                scatter_tri<NF, R>(P, W, acc, F, cur, vs, lo, err);
                 cur = trilinear(P, pt);
             }
         }
-        scatter_tri<NF, R>(P, W, acc, F, cur, vs, err);
+        scatter_tri<NF, R>(P, W, acc, F, cur, vs, lo, err);
     }
 }
 
@@ -595,6 +644,9 @@ struct FusedArgs {
     const double* binc;
     const double* hinc;
     double zdepth;
+    // the next par2grid's vorticity bounds (StepScalars::pbound[0..2], cleared
+    // by the host), or null
+    unsigned long long* vbound;
 };
 
 // The 14 gathered fields (velog 3, velgradg 8, vtend 3) of a grid point as
@@ -771,6 +823,11 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
     // the diagnostic sums of this thread, in shared memory (registers are
     // the stage kernel's limit)
     __shared__ double dsm[ND][PB];
+    // largest |0.25 V w_k| of this thread's advanced parcels (the next
+    // par2grid's vorticity bounds)
+    __shared__ double vmx[3][PB];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) vmx[k][threadIdx.x] = 0.0;
 #pragma unroll
     for (int k = 0; k < ND; ++k) dsm[k][threadIdx.x] = 0.0;
     double* dacc = &dsm[0][threadIdx.x];
@@ -929,6 +986,12 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 a64<R>(pv, A_DX + k, i) = dp[k];
                 aR<R>(pv, A_DVX + k, i) = dv[k];
             }
+            if (S.vbound) {
+                // the values p2g_values will scatter, in the same arithmetic
+                const R pw = (R)(0.25 * vol);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) vmx[k][threadIdx.x] = keep_max(vmx[k][threadIdx.x], fabs((double)(pw * vor[k])));
+            }
 #pragma unroll
             for (int k = 0; k < 5; ++k) {
                 aR<R>(pv, A_B11 + k, i) = b[k];
@@ -947,6 +1010,10 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 for (int k = 0; k < 3; ++k) { aR<R>(pv, A_ETA0 + k, i) = eta[k]; aR<R>(pv, A_TAU0 + k, i) = tau[k]; }
             }
         }
+    }
+    if (S.vbound) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) warp_max_to(&S.vbound[k], vmx[k][threadIdx.x]);
     }
     if (DIAG) {
         int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -1022,10 +1089,16 @@ static void set_smem(K kernel, size_t bytes) {
 // count: par2grid's parcel counts nparg / nsparg (NF = 7 or 5)
 template <int NF, class R>
 static void launch_scatter(Ctx& c, const Fields7& F, bool reuse, bool store, int lg, bool count) {
-    // the fixed-point scales: the largest value of every scattered field
-    CK(cudaMemsetAsync(c.dsc->pbound, 0, sizeof(c.dsc->pbound), c.stream));
-    k_p2g_bounds<NF, R><<<pgrid(c.n), PB, 0, c.stream>>>(c.P, c.pv, c.n, c.dsc->pbound);
-    CKL();
+    // the fixed-point scales: the largest value of every scattered field,
+    // from the kernels that produced the values or from a pass of their own
+    if (NF == 1 && c.v2g_bound_ready) {
+        CK(cudaMemcpyAsync(&c.dsc->pbound[6], &c.dsc->vbound, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                           c.stream));
+    } else if (NF == 1 || !c.p2g_bound_ready) {
+        CK(cudaMemsetAsync(c.dsc->pbound, 0, sizeof(c.dsc->pbound), c.stream));
+        k_p2g_bounds<NF, R, false><<<pgrid(c.n), PB, 0, c.stream>>>(c.P, c.pv, c.n, c.dsc->pbound, nullptr);
+        CKL();
+    }
     if (!reuse && store && c.vectors_kernel) {
         k_vectors<R><<<pgrid(c.n), PB, 0, c.stream>>>(c.pv, c.n, &c.dsc->err);
         CKL();
@@ -1074,6 +1147,16 @@ void scatter_v2g(Ctx& c, bool reuse) {
     prof_end(c, "v2g");
 }
 
+// The scales of the step's first par2grid and the step bounds (pstep) that
+// the later stages' scatters take with their vorticity bounds.
+void p2g_step_bounds(Ctx& c) {
+    CK(cudaMemsetAsync(c.dsc->pbound, 0, sizeof(c.dsc->pbound) + sizeof(c.dsc->pstep), c.stream));
+    if (c.n == 0) return;
+    if (c.pv.mixed) k_p2g_bounds<7, float, true><<<pgrid(c.n), PB, 0, c.stream>>>(c.P, c.pv, c.n, c.dsc->pbound, c.dsc->pstep);
+    else k_p2g_bounds<7, double, true><<<pgrid(c.n), PB, 0, c.stream>>>(c.P, c.pv, c.n, c.dsc->pbound, c.dsc->pstep);
+    CKL();
+}
+
 int p2g_fx_bits(const Ctx& c) { return c.pv.mixed ? fx_bits<float>() : fx_bits<double>(); }
 
 template <class R>
@@ -1096,10 +1179,21 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
     }
     const bool moist = S.stage + 1 == c.n_stages;
     size_t sm = S.recwin ? recwin_bytes<R>() : 0;
+    // the next scatter's scales: vorticity bounds from this kernel, the rest
+    // from the step bounds (volume, buoyancy and humidity are those of the
+    // step's first par2grid)
+    FusedArgs Sk = S;
+    Sk.vbound = nullptr;
+    const bool fuse_bounds = scatter && c.pstep_valid;
+    if (fuse_bounds) {
+        CK(cudaMemsetAsync(c.dsc->pbound, 0, 3 * sizeof(unsigned long long), c.stream));
+        CK(cudaMemcpyAsync(&c.dsc->pbound[3], c.dsc->pstep, sizeof(c.dsc->pstep), cudaMemcpyDeviceToDevice, c.stream));
+        Sk.vbound = c.dsc->pbound;
+    }
     auto launch = [&](auto kernel) {
         if (sm) set_smem(kernel, sm);
         prof_begin(c, "stage");
-        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, pack, S, c.dsc, c.stage_partials, &c.dsc->err);
+        kernel<<<g, PB, sm, c.stream>>>(c.P, c.pv, c.n, B, pack, Sk, c.dsc, c.stage_partials, &c.dsc->err);
         CKL();
         prof_end(c, "stage");
     };
@@ -1113,7 +1207,9 @@ static void launch_stage(Ctx& c, const FusedArgs& S, bool with_diag, bool scatte
         // the par2grid of stage + 1: dbuoyg and humg only for the last stage;
         // the parcel counts of the intermediate stages are not read (field
         // diagnostics use the step's first par2grid); the last one keeps them
+        c.p2g_bound_ready = fuse_bounds;
         launch_p2g<R>(c, moist, vout, true, moist);
+        c.p2g_bound_ready = false;
         prof_end(c, "stage_p2g");
     }
 }
@@ -1135,6 +1231,7 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     S.binc = flux && with_diag ? c.binc : nullptr;
     S.hinc = flux && with_diag ? c.hinc : nullptr;
     S.zdepth = c.zdepth;
+    S.vbound = nullptr;
     bool scatter = !S.last;
     if (c.pv.mixed) launch_stage<float>(c, S, with_diag, scatter);
     else launch_stage<double>(c, S, with_diag, scatter);

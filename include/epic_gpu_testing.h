@@ -54,6 +54,10 @@ int epic_gpu_test_set_scatter_groups(struct epic_ctx* ctx, int lg_vol2grid, int 
 /* Support vectors by a kernel of their own before a scatter that recomputes
  * them (1, default) or inside the scatter kernel (0); same results. */
 int epic_gpu_test_set_vectors_kernel(struct epic_ctx* ctx, int on);
+/* Mixed form only: the spectral work (FFTs, column transforms, spectral
+ * algebra) in FP64 instead of FP32, to measure that part's share of the
+ * form's error against FP64. */
+int epic_gpu_test_set_spectral_fp64(struct epic_ctx* ctx, int on);
 /* Stage kernel (split form) gathers from the box's records staged in shared
  * memory (1) or from global memory (0, default); same results. */
 int epic_gpu_test_set_stage_window(struct epic_ctx* ctx, int on);

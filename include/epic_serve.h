@@ -4,10 +4,11 @@
  * No counterpart in the reference (it runs one simulation per MPI job).  A
  * server keeps up to max_slots simulations on the device at once, each with
  * its own context and CUDA stream, so their kernels overlap on the GPU.
- * Requests are admitted first come, first served, as soon as a slot is free
- * and the request's device memory fits in the server's share of the free
- * HBM; a request that arrives while others run starts without waiting for
- * them (continuous admission).  Contexts of finished requests are kept and
+ * A slot that frees up takes the first queued request (in arrival order)
+ * whose device memory fits in the server's share of the free HBM, so a large
+ * request at the head does not hold back smaller ones behind it; a request
+ * that arrives while others run starts without waiting for them (continuous
+ * admission).  Contexts of finished requests are kept and
  * reused by later requests with the same configuration, so steady-state
  * serving allocates no device memory.  Initial states are generated on the
  * device (epic_gpu_init_state).
@@ -55,7 +56,8 @@ int epic_srv_create(int32_t max_slots, double hbm_fraction, epic_server** out);
 /* Queue a request; *id identifies it.  A request larger than the server's
  * whole budget completes at once with status EPIC_ERR_CAPACITY. */
 int epic_srv_submit(epic_server* srv, const epic_request* req, int64_t* id);
-/* Block until request id has finished; fills *out (status included). */
+/* Block until request id has finished; fills *out (status included).  The
+ * result is handed over: a second wait on the same id returns EPIC_ERR_ARG. */
 int epic_srv_wait(epic_server* srv, int64_t id, epic_result* out);
 int epic_srv_counts(epic_server* srv, int64_t* queued, int64_t* running, int64_t* done);
 /* Finish all queued work, then free every context. */

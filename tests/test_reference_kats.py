@@ -277,7 +277,7 @@ def _reflection_parcels():
 def _reflection_error(lib):
     import ctypes as C
     pos, B, vol, dx = _reflection_parcels()
-    ctx = _context(lib, (4, 4, 2), (0.0, 0.0, 0.0), (2.0, 2.0, 1.0))
+    ctx = _context(lib, (4, 4, 2), (0.0, 0.0, 0.0), (2.0, 2.0, 1.0), capacity=len(vol))
     ctx.set_parcels(pos, np.zeros_like(pos), B, vol, np.zeros(len(vol)))
     assert _hook(lib, "test_reflective_bc", C.c_void_p)(ctx.h) == 0
     p = ctx.get_parcels()

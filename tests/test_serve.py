@@ -66,3 +66,15 @@ def test_serve_reuses_idle_contexts(glib):
     assert res[0]["n_parcels"] == res[2]["n_parcels"]
     a = _alone(glib, reqs[1])
     assert res[1]["ke"] == pytest.approx(a["ke"], rel=1e-10)
+
+
+@pytest.mark.gpu
+def test_serve_results_are_handed_over(glib):
+    """A result is handed over by its wait: a second wait on the same id is an
+    error instead of blocking."""
+    from epic_b200 import abi
+    with serve.Server(slots=2, hbm_fraction=0.5, lib=glib) as srv:
+        rid = srv.submit(serve.request("thermal", (16, 16, 16), seed=3, steps=2, precision=0, lib=glib))
+        assert srv.wait(rid)["status"] == 0
+        with pytest.raises(abi.EpicError):
+            srv.wait(rid)
