@@ -265,7 +265,12 @@ template <int N, bool FWD, class T>
 EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
     constexpr int N1 = Radix<N>::N1, N2 = Radix<N>::N2, KPT = N1 / N2, H = N / 2;
     auto EL = [&](int c) { return g.a0 + (c & g.msk) * g.es + (c >> g.sh) * g.es2; };
+    // Scratch slot of complex element k, XOR-swizzled within blocks of 8: the
+    // transposed reads (k = t * N1 + ...) of the lanes of a quarter warp then
+    // fall into 8 different 16-byte bank groups instead of one.
+    constexpr int LG1 = N1 >= 32 ? 5 : N1 >= 16 ? 4 : N1 >= 8 ? 3 : N1 >= 4 ? 2 : 1;
     auto SC = [&](int k) -> CX<T>& {
+        k ^= (k >> LG1) & 7;
         return *reinterpret_cast<CX<T>*>(P + g.s0 + (k & g.msk) * g.cs + (k >> g.sh) * g.es2);
     };
     CX<T> v[N1];
