@@ -293,16 +293,16 @@ def stage_roofline(w: dict, steps: int, setup, form: str) -> dict:
          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak if achieved else None),
          "traffic": None, "peak_source": peak_kind, "ms_per_unit": unit_ms, "launches": w["kernel_launches"],
          "share_of_step_time": w["kernel_ms"] / w["ms"] if w["ms"] else None, "algorithmic_bytes_per_unit": alg}
-    # DRAM bytes of one k_stage<0,0> launch (stages 2-5) from ncu captures of
-    # the stage kernel (64^3, 2,097,152 parcels, early flow: plain 539.9 MB
-    # read + 323.1 MB written = 411.5 B per parcel; mixed 337.3 + 184.7 MB =
+    # DRAM bytes of one k_stage launch of stages 2-5 from ncu captures of
+    # the stage kernel (64^3, 2,097,152 parcels, early flow: plain 536.6 MB
+    # read + 319.2 MB written = 408.1 B per parcel; mixed 337.3 + 184.7 MB =
     # 248.9 B), scaled by the parcels of this run (the traffic grows with
     # them), against the algorithmic bytes of the same stages.  Lines still
     # dirty in L2 when the launch ends (up to its 126 MB) are not counted,
-    # which puts the mixed capture a little below its algorithmic bytes.
-    per_parcel = 248.9 if form == "mixed" else 411.5
+    # which puts the captures a little below their algorithmic bytes.
+    per_parcel = 248.9 if form == "mixed" else 408.1
     r["traffic"] = per_parcel * avg_n
-    r["traffic_source"] = (f"ncu dram__bytes_read+write of k_stage<0,0,{'float' if form == 'mixed' else 'double'}> "
+    r["traffic_source"] = (f"ncu dram__bytes_read+write of k_stage<0,{'float' if form == 'mixed' else 'double'},0> "
                            "(stages 2-5), 64^3 capture scaled by parcels")
     r["traffic_over_algorithmic"] = r["traffic"] / stage_launch_bytes(int(avg_n), setup.nx, setup.ny, setup.nz, form,
                                                                       later_only=True)
@@ -364,6 +364,13 @@ def run_ours(args):
         setup = initial.config(args.workload)
         ctx = epic_b200.make_context(setup, lib, keep_order=args.keep_order, precision=1 if mixed else 0)
     tuning = ctx.autotune() if not args.no_autotune else None
+    if args.scatter_groups is not None:
+        # lanes per group of consecutive parcels in the scatters, 2^lg
+        import ctypes as C
+        f = lib.lib.epic_gpu_test_set_scatter_groups
+        f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        lg = args.scatter_groups
+        assert f(ctx.h, lg, lg, lg) == 0
     stream = context_stream(lib, ctx, dev)
     timer = Timer(lib, ctx, stream, dev if world == 1 else local)
 
@@ -842,6 +849,8 @@ def main():
                     help="reference arm: skip the one step of the full 128^3 workload")
     ap.add_argument("--spinup", type=int, default=0, help="untimed steps before the warm-up (developed flow)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--scatter-groups", type=int, default=None, choices=range(6),
+                    help="log2 of the consecutive parcels a lane group of the scatters takes (overrides the tuner)")
     ap.add_argument("--keep-order", type=int, default=0, choices=[0, 1],
                     help="1: keep the reference's container order (no box sort)")
     ap.add_argument("--device-init", action="store_true",

@@ -260,6 +260,8 @@ void lapinv_probe(Ctx& c, const double* in, double* out);
 
 // merge.cu
 long long parcel_merge(Ctx& c);
+// parcel_delete of nm distinct container indices (host array; test hook)
+void test_delete(Ctx& c, const int* idx, int nm);
 size_t merge_scratch_bytes(long long n);
 // stage.cu
 size_t sort_scratch_bytes(long long n);

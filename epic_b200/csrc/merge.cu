@@ -543,6 +543,78 @@ __global__ void k_periodic_m(Params P, PView pv, long long n) {
     }
 }
 
+// Buffers of parcel_delete for N parcels of which nm go: del (N bytes);
+// hf, holes, sf, sidx, srcs (nm ints each); with container indices (ord:
+// slot of each container index) also hole_f, src_f, iota, holes_r, srcs_r (N
+// ints each); CUB temporary storage for a selection over N items; 2 counters.
+struct DeleteBufs {
+    char* del;
+    int *hf, *holes, *sf, *sidx, *srcs;
+    int *hole_f, *src_f, *iota, *holes_r, *srcs_r;
+    const int* ord;
+    void* ctmp;
+    size_t cubb;
+    int* dcount;
+};
+
+static int read_int(Ctx& c, const int* d);
+
+// parcel_delete (parcel_container.f90:413-458) of the nm parcels in slots
+// ism: the i-th hole (ascending, below the new count) receives the i-th
+// surviving parcel from the top; with container indices the same rule runs
+// on the indices (the slots are compacted the same way, and each parcel keeps
+// the index the reference's container gives it).  Leaves c.n to the caller.
+static void delete_slots(Ctx& c, int N, const int* ism, int nm, const DeleteBufs& b) {
+    cudaStream_t st = c.stream;
+    const int newN = N - nm;
+    const int* ord = b.ord;
+    const bool ranked = c.rank != nullptr;
+    char* del = b.del;
+    CK(cudaMemsetAsync(del, 0, N, st));
+    k_mark_deleted<<<mgrid(nm), MB, 0, st>>>(ism, nm, del);
+    CKL();
+    if (ranked) {
+        k_del_rank_flags<<<mgrid(N), MB, 0, st>>>(ord, del, N, newN, b.hole_f, b.src_f);
+        CKL();
+        k_iota<<<mgrid(N), MB, 0, st>>>(b.iota, N);
+        CKL();
+        size_t bb = b.cubb;
+        CK(cub::DeviceSelect::Flagged(b.ctmp, bb, b.iota, b.hole_f, b.holes_r, b.dcount, N, st));
+        bb = b.cubb;
+        CK(cub::DeviceSelect::Flagged(b.ctmp, bb, b.iota, b.src_f, b.srcs_r, b.dcount + 1, N, st));
+        const int nhr = read_int(c, b.dcount);
+        if (nhr > 0) {
+            k_rerank<<<mgrid(nhr), MB, 0, st>>>(ord, b.holes_r, b.srcs_r, nhr, c.rank);
+            CKL();
+        }
+    }
+    k_hole_flags<<<mgrid(nm), MB, 0, st>>>(ism, nm, newN, b.hf);
+    CKL();
+    {
+        size_t bb = b.cubb;
+        CK(cub::DeviceSelect::Flagged(b.ctmp, bb, ism, b.hf, b.holes, b.dcount, nm, st));
+    }
+    const int nh = read_int(c, b.dcount);
+    if (nh > 0) {
+        k_src_flags<<<mgrid(nm), MB, 0, st>>>(del, newN, N, b.sf);
+        CKL();
+        k_iota<<<mgrid(nm), MB, 0, st>>>(b.sidx, nm);
+        CKL();
+        size_t bb = b.cubb;
+        CK(cub::DeviceSelect::Flagged(b.ctmp, bb, b.sidx, b.sf, b.srcs, b.dcount + 1, N - newN, st));
+        k_move<<<mgrid((long long)nh * N_ATTR), MB, 0, st>>>(c.pv, b.holes, b.srcs, nh, newN);
+        CKL();
+        if (ranked) {
+            k_move_rank<<<mgrid(nh), MB, 0, st>>>(c.rank, b.holes, b.srcs, nh, newN);
+            CKL();
+        }
+        if (c.label) {
+            k_move_labels<<<mgrid(nh), MB, 0, st>>>(c.label, c.dil, b.holes, b.srcs, nh, newN);
+            CKL();
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 struct Arena {
     char* base;
@@ -818,61 +890,15 @@ long long parcel_merge(Ctx& c) {
 
     // parcel_delete
     const int newN = N - nm;
-    char* del = merged;
-    CK(cudaMemsetAsync(del, 0, N, st));
-    k_mark_deleted<<<mgrid(nm), MB, 0, st>>>(ism, nm, del);
-    CKL();
-    if (ranked) {
-        // the container indices after parcel_delete; the binning arrays are
-        // free now (the group merge reads gk, gv and ism)
-        int* hole_f = cell;
-        int* src_f = vals;
-        int* iota = skeys;
-        int* holes_r = svals;
-        int* srcs_r = svals + N;
-        k_del_rank_flags<<<mgrid(N), MB, 0, st>>>(ord, del, N, newN, hole_f, src_f);
-        CKL();
-        k_iota<<<mgrid(N), MB, 0, st>>>(iota, N);
-        CKL();
-        size_t b = cubb;
-        CK(cub::DeviceSelect::Flagged(ctmp, b, iota, hole_f, holes_r, dcount, N, st));
-        b = cubb;
-        CK(cub::DeviceSelect::Flagged(ctmp, b, iota, src_f, srcs_r, dcount + 1, N, st));
-        const int nhr = read_int(c, dcount);
-        if (nhr > 0) {
-            k_rerank<<<mgrid(nhr), MB, 0, st>>>(ord, holes_r, srcs_r, nhr, c.rank);
-            CKL();
-        }
-    }
-    int* hf = head;      // reuse nm-sized arrays
-    int* holes = gidx;
-    k_hole_flags<<<mgrid(nm), MB, 0, st>>>(ism, nm, newN, hf);
-    CKL();
     {
-        size_t b = cubb;
-        CK(cub::DeviceSelect::Flagged(ctmp, b, ism, hf, holes, dcount, nm, st));
-    }
-    const int nh = read_int(c, dcount);
-    if (nh > 0) {
-        int* sf = mvals;
-        int* sidx = gk;
-        int* srcs = gv;
-        k_src_flags<<<mgrid(nm), MB, 0, st>>>(del, newN, N, sf);
-        CKL();
-        k_iota<<<mgrid(nm), MB, 0, st>>>(sidx, nm);
-        CKL();
-        size_t b = cubb;
-        CK(cub::DeviceSelect::Flagged(ctmp, b, sidx, sf, srcs, dcount + 1, N - newN, st));
-        k_move<<<mgrid((long long)nh * N_ATTR), MB, 0, st>>>(c.pv, holes, srcs, nh, newN);
-        CKL();
-        if (ranked) {
-            k_move_rank<<<mgrid(nh), MB, 0, st>>>(c.rank, holes, srcs, nh, newN);
-            CKL();
-        }
-        if (c.label) {
-            k_move_labels<<<mgrid(nh), MB, 0, st>>>(c.label, c.dil, holes, srcs, nh, newN);
-            CKL();
-        }
+        DeleteBufs db;
+        db.del = merged;
+        db.hf = head; db.holes = gidx; db.sf = mvals; db.sidx = gk; db.srcs = gv;
+        // with container indices: the binning arrays are free now (the group
+        // merge reads gk, gv and ism)
+        db.hole_f = cell; db.src_f = vals; db.iota = skeys; db.holes_r = svals; db.srcs_r = svals + N;
+        db.ord = ord; db.ctmp = ctmp; db.cubb = cubb; db.dcount = dcount;
+        delete_slots(c, N, ism, nm, db);
     }
     unsigned long long hb = 0;
     CK(cudaMemcpyAsync(&hb, bigc, sizeof(hb), cudaMemcpyDeviceToHost, st));
@@ -884,6 +910,65 @@ long long parcel_merge(Ctx& c) {
     k_periodic_m<<<mgrid(newN), MB, 0, st>>>(P, c.pv, newN);
     CKL();
     return nm;
+}
+
+__global__ void k_slots_of(const int* ord, const int* idx, int n, int* ism) {
+    MLOOP(n) ism[i] = ord ? ord[idx[i]] : idx[i];
+}
+
+// parcel_delete alone (test hook): idx holds nm distinct container indices
+// (0-based), host memory.
+void test_delete(Ctx& c, const int* idx, int nm) {
+    const int N = (int)c.n;
+    if (nm <= 0) return;
+    if (nm > N) throw CudaError(EPIC_ERR_ARG, "delete: more parcels than there are");
+    size_t cubb = 0;
+    cub::DeviceSelect::Flagged(nullptr, cubb, (int*)0, (int*)0, (int*)0, (int*)0, N, c.stream);
+    std::vector<void*> mem;
+    auto grab = [&](size_t bytes) {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+        mem.push_back(p);
+        return p;
+    };
+    try {
+        DeleteBufs b;
+        int* didx = static_cast<int*>(grab(sizeof(int) * nm));
+        int* ism = static_cast<int*>(grab(sizeof(int) * nm));
+        b.del = static_cast<char*>(grab(N));
+        b.hf = static_cast<int*>(grab(sizeof(int) * nm));
+        b.holes = static_cast<int*>(grab(sizeof(int) * nm));
+        b.sf = static_cast<int*>(grab(sizeof(int) * nm));
+        b.sidx = static_cast<int*>(grab(sizeof(int) * nm));
+        b.srcs = static_cast<int*>(grab(sizeof(int) * nm));
+        int* ord = nullptr;
+        b.hole_f = b.src_f = b.iota = b.holes_r = b.srcs_r = nullptr;
+        if (c.rank) {
+            ord = static_cast<int*>(grab(sizeof(int) * N));
+            b.hole_f = static_cast<int*>(grab(sizeof(int) * N));
+            b.src_f = static_cast<int*>(grab(sizeof(int) * N));
+            b.iota = static_cast<int*>(grab(sizeof(int) * N));
+            b.holes_r = static_cast<int*>(grab(sizeof(int) * N));
+            b.srcs_r = static_cast<int*>(grab(sizeof(int) * N));
+            container_order(c, ord);
+        }
+        b.ord = ord;
+        b.ctmp = grab(cubb);
+        b.cubb = cubb;
+        b.dcount = static_cast<int*>(grab(sizeof(int) * 2));
+        CK(cudaMemcpyAsync(didx, idx, sizeof(int) * nm, cudaMemcpyHostToDevice, c.stream));
+        k_slots_of<<<mgrid(nm), MB, 0, c.stream>>>(ord, didx, nm, ism);
+        CKL();
+        delete_slots(c, N, ism, nm, b);
+        CK(cudaStreamSynchronize(c.stream));
+        c.n = N - nm;
+        c.n_box = std::min<long long>(c.n_box, c.n);
+    } catch (...) {
+        cudaStreamSynchronize(c.stream);
+        for (void* p : mem) cudaFree(p);
+        throw;
+    }
+    for (void* p : mem) cudaFree(p);
 }
 
 }  // namespace epic

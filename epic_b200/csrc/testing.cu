@@ -82,6 +82,18 @@ extern "C" int epic_gpu_test_spectral(epic_ctx* ctx, int op, const double* f, do
     return EPIC_OK;
 }
 
+extern "C" int epic_gpu_test_delete(epic_ctx* ctx, int64_t n, const int32_t* idx) {
+    if (!ctx || n < 0 || (n > 0 && !idx)) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    try {
+        test_delete(c, idx, (int)n);
+    } catch (const CudaError& e) {
+        c.err = e.what();
+        return e.code;
+    }
+    return EPIC_OK;
+}
+
 extern "C" int epic_gpu_test_reflective_bc(epic_ctx* ctx) {
     if (!ctx) return EPIC_ERR_ARG;
     Ctx& c = ctx->c;

@@ -32,6 +32,10 @@ int epic_gpu_test_diverge(struct epic_ctx* ctx, const double* phi, double* grad)
  * vertical differences, they are fused into the inversion's column kernels. */
 int epic_gpu_test_spectral(struct epic_ctx* ctx, int op, const double* f, double* out);
 
+/* parcel_delete (parcel_container.f90:413-458) of n distinct parcels given
+ * by their 0-based container indices (test_mpi_parcel_delete.f90). */
+int epic_gpu_test_delete(struct epic_ctx* ctx, int64_t n, const int32_t* idx);
+
 /* apply_reflective_bc (parcel_bc.f90:45-57) on every parcel. */
 int epic_gpu_test_reflective_bc(struct epic_ctx* ctx);
 

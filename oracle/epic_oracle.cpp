@@ -1514,6 +1514,40 @@ void bin_parcel(Ctx& c, Near& nr, std::vector<double>& P, long n) {
 }
 
 // Directions (mpi_tags.f90:3-11): 1 N, 2 S, 3 W, 4 E, 5 NW, 6 NE, 7 SW, 8 SE.
+// parcel_delete (parcel_container.f90:413-458): pid holds the 1-based indices
+// of the parcels to delete, ascending; the holes below the new count are
+// filled with the last valid parcels, from the top.
+void parcel_delete(Ctx& c, const std::vector<long>& pids) {
+    const long n_merge = (long)pids.size();
+    std::vector<long> pid(n_merge + 1);
+    for (long m = 0; m < n_merge; ++m) pid[m + 1] = pids[m];
+    long lv = c.n, k = n_merge;
+    while (k > 0 && lv == pid[k]) { lv -= 1; k -= 1; }
+    long mm = 1;
+    auto replace = [&](long dst1, long src1) {
+        long d = dst1 - 1, s = src1 - 1;
+        for (int q = 0; q < 3; ++q) {
+            c.pos[3 * d + q] = c.pos[3 * s + q];
+            c.vor[3 * d + q] = c.vor[3 * s + q];
+            c.dpos[3 * d + q] = c.dpos[3 * s + q];
+            c.dvor[3 * d + q] = c.dvor[3 * s + q];
+            c.Vetas[3 * d + q] = c.Vetas[3 * s + q];
+            c.Vtaus[3 * d + q] = c.Vtaus[3 * s + q];
+        }
+        for (int q = 0; q < 5; ++q) { c.B[5 * d + q] = c.B[5 * s + q]; c.dB[5 * d + q] = c.dB[5 * s + q]; }
+        for (int q = 0; q < 8; ++q) c.strain[8 * d + q] = c.strain[8 * s + q];
+        c.vol[d] = c.vol[s]; c.buoy[d] = c.buoy[s]; c.hum[d] = c.hum[s];
+        if (c.cfg.labels) { c.label[d] = c.label[s]; c.dil[d] = c.dil[s]; }
+    };
+    while (mm <= k) {
+        replace(pid[mm], lv);
+        lv -= 1;
+        while (k > 0 && lv == pid[k]) { lv -= 1; k -= 1; }
+        mm += 1;
+    }
+    c.n = c.n - n_merge;
+}
+
 long parcel_merge(Ctx& c) {
     const long N = c.n;
     Near nr;
@@ -1862,33 +1896,8 @@ long parcel_merge(Ctx& c) {
     }
     // parcel_delete (parcel_container.f90:413-458) with pid = isma (ascending)
     {
-        std::vector<long> pid(n_merge + 1);
-        for (long m = 0; m < n_merge; ++m) pid[m + 1] = ism[m];
-        long lv = c.n, k = n_merge;
-        while (k > 0 && lv == pid[k]) { lv -= 1; k -= 1; }
-        long mm = 1;
-        auto replace = [&](long dst1, long src1) {
-            long d = dst1 - 1, s = src1 - 1;
-            for (int q = 0; q < 3; ++q) {
-                c.pos[3 * d + q] = c.pos[3 * s + q];
-                c.vor[3 * d + q] = c.vor[3 * s + q];
-                c.dpos[3 * d + q] = c.dpos[3 * s + q];
-                c.dvor[3 * d + q] = c.dvor[3 * s + q];
-                c.Vetas[3 * d + q] = c.Vetas[3 * s + q];
-                c.Vtaus[3 * d + q] = c.Vtaus[3 * s + q];
-            }
-            for (int q = 0; q < 5; ++q) { c.B[5 * d + q] = c.B[5 * s + q]; c.dB[5 * d + q] = c.dB[5 * s + q]; }
-            for (int q = 0; q < 8; ++q) c.strain[8 * d + q] = c.strain[8 * s + q];
-            c.vol[d] = c.vol[s]; c.buoy[d] = c.buoy[s]; c.hum[d] = c.hum[s];
-            if (c.cfg.labels) { c.label[d] = c.label[s]; c.dil[d] = c.dil[s]; }
-        };
-        while (mm <= k) {
-            replace(pid[mm], lv);
-            lv -= 1;
-            while (k > 0 && lv == pid[k]) { lv -= 1; k -= 1; }
-            mm += 1;
-        }
-        c.n = c.n - n_merge;
+        std::vector<long> pid(ism.begin(), ism.begin() + n_merge);
+        parcel_delete(c, pid);
     }
     parcel_communicate(c);
     return n_merge;
@@ -2406,5 +2415,17 @@ extern "C" int epic_oracle_test_reflective_bc(epic_ctx* ctx) {
     if (!ctx) return EPIC_ERR_ARG;
     Ctx& c = ctx->c;
     for (long n = 0; n < c.n; ++n) apply_reflective_bc(c, &c.pos[3 * n], &c.B[5 * n]);
+    return EPIC_OK;
+}
+
+// parcel_delete (test_mpi_parcel_delete.f90) of n distinct 0-based indices.
+extern "C" int epic_oracle_test_delete(epic_ctx* ctx, int64_t n, const int32_t* idx) {
+    if (!ctx || n < 0 || (n > 0 && !idx)) return EPIC_ERR_ARG;
+    Ctx& c = ctx->c;
+    if (n > c.n) return EPIC_ERR_ARG;
+    std::vector<long> pid(idx, idx + n);
+    std::sort(pid.begin(), pid.end());
+    for (auto& p : pid) p += 1;
+    parcel_delete(c, pid);
     return EPIC_OK;
 }

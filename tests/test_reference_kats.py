@@ -22,6 +22,9 @@ numbers.
   mean gridded-volume error of a randomly displaced regular lattice.
 * test_mpi_vtend.f90: the vorticity tendency of Beltrami-like fields on
   128^3 is within 1.2 of the analytic one (second-order z differences).
+* test_mpi_parcel_delete.f90: 100 deletions of 222 random parcels out of
+  1000 keep exactly the others, every attribute intact; on the device in the
+  oracle's container order, with both store orders.
 """
 import math
 
@@ -431,3 +434,58 @@ def test_vtend_gpu(olib, glib):
     a, b = _vtend(g, vel, vor), _vtend(o, vel, vor)
     for q in range(3):
         assert np.abs(a[q] - b[q]).max() <= 1e-10 * np.abs(b[q]).max()
+
+
+# ---- parcel delete -----------------------------------------------------------
+def _delete_parcels():
+    n = 1000
+    a = np.arange(n) * 100.0
+    pos = np.stack([1.0 + a, 2.0 + a, 3.0 + a], 1)
+    vor = np.stack([4.0 + a, 5.0 + a, 6.0 + a], 1)
+    B = np.stack([7.0 + a, 8.0 + a, 9.0 + a, 10.0 + a, 11.0 + a], 1)
+    return pos, vor, B, 12.0 + a, 13.0 + a, 14.0 + a
+
+
+def _delete_runs(lib, **kw):
+    """test_mpi_parcel_delete.f90: 100 times, 222 of 1000 parcels (distinct,
+    random) are deleted; returns the parcels left, in container order."""
+    import ctypes as C
+    f = _hook(lib, "test_delete", C.c_void_p, C.c_int64, C.POINTER(C.c_int32))
+    rng = np.random.default_rng(222)
+    out = []
+    for _ in range(100):
+        ctx = _context(lib, (16, 16, 16), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), **kw)
+        ctx.set_parcels(*_delete_parcels())
+        inv = rng.choice(1000, size=222, replace=False).astype(np.int32)
+        assert f(ctx.h, len(inv), inv.ctypes.data_as(C.POINTER(C.c_int32))) == 0
+        out.append((inv, ctx.get_parcels()))
+        ctx.close()
+    return out
+
+
+def _check_delete(inv, p):
+    keep = np.setdiff1d(np.arange(1000), inv)
+    assert len(p["vol"]) == len(keep)
+    order = np.argsort(p["pos"][:, 0])
+    a = keep * 100.0
+    assert np.array_equal(p["pos"][order], np.stack([1.0 + a, 2.0 + a, 3.0 + a], 1))
+    assert np.array_equal(p["vor"][order], np.stack([4.0 + a, 5.0 + a, 6.0 + a], 1))
+    assert np.array_equal(p["B"][order], np.stack([7.0 + a, 8.0 + a, 9.0 + a, 10.0 + a, 11.0 + a], 1))
+    assert np.array_equal(p["vol"][order], 12.0 + a)
+    assert np.array_equal(p["buoy"][order], 13.0 + a) and np.array_equal(p["hum"][order], 14.0 + a)
+
+
+def test_parcel_delete_oracle(olib):
+    for inv, p in _delete_runs(olib):
+        _check_delete(inv, p)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("keep_order", [1, 0])
+def test_parcel_delete_gpu(olib, glib, keep_order):
+    """The survivors of every deletion, and their container order, equal
+    the oracle's (the reference's hole filling from the top)."""
+    for (inv, p), (_, q) in zip(_delete_runs(glib, keep_order=keep_order), _delete_runs(olib)):
+        _check_delete(inv, p)
+        for k in p:
+            assert np.array_equal(p[k], q[k]), k
