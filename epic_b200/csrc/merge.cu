@@ -560,8 +560,9 @@ struct DeleteBufs {
 static int read_int(Ctx& c, const int* d);
 
 // parcel_delete (parcel_container.f90:413-458) of the nm parcels in slots
-// ism: the i-th hole (ascending, below the new count) receives the i-th
-// surviving parcel from the top; with container indices the same rule runs
+// ism (ascending where the slots are the container indices, keep_order = 1:
+// the holes are filled in that order): the i-th hole (below the new count)
+// receives the i-th surviving parcel from the top; with container indices the same rule runs
 // on the indices (the slots are compacted the same way, and each parcel keeps
 // the index the reference's container gives it).  Leaves c.n to the caller.
 static void delete_slots(Ctx& c, int N, const int* ism, int nm, const DeleteBufs& b) {
@@ -956,11 +957,14 @@ void test_delete(Ctx& c, const int* idx, int nm) {
         b.ctmp = grab(cubb);
         b.cubb = cubb;
         b.dcount = static_cast<int*>(grab(sizeof(int) * 2));
-        CK(cudaMemcpyAsync(didx, idx, sizeof(int) * nm, cudaMemcpyHostToDevice, c.stream));
+        // ascending, as parcel_delete takes them
+        std::vector<int> sorted(idx, idx + nm);
+        std::sort(sorted.begin(), sorted.end());
+        CK(cudaMemcpyAsync(didx, sorted.data(), sizeof(int) * nm, cudaMemcpyHostToDevice, c.stream));
         k_slots_of<<<mgrid(nm), MB, 0, c.stream>>>(ord, didx, nm, ism);
         CKL();
         delete_slots(c, N, ism, nm, b);
-        CK(cudaStreamSynchronize(c.stream));
+        CK(cudaStreamSynchronize(c.stream));   // before the host copy of the indices goes
         c.n = N - nm;
         c.n_box = std::min<long long>(c.n_box, c.n);
     } catch (...) {
