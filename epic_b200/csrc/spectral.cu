@@ -14,6 +14,7 @@
 #include "ctx.hpp"
 #include "eigen.cuh"
 
+#include <climits>
 #include <cmath>
 #include <vector>
 #include <algorithm>
@@ -373,9 +374,23 @@ __global__ void __launch_bounds__((N / 2) * Radix<N>::N2) k_fft_plane(PlaneBatch
     const TI* in = static_cast<const TI*>(B.in[blockIdx.y]);
     TO* out = static_cast<TO*>(B.out[blockIdx.y]);
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = cx<TC>((TC)B.tw[i].x, (TC)B.tw[i].y);
-    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-        const int ix = idx / N, iy = idx - ix * N;
-        P[ix * S + iy] = (TC)in[((long long)ix * B.ny + iy) * B.nzh + 1 + z];
+    // With z fastest in memory every element of the plane is a separate
+    // sector: each thread issues U independent loads before it stores any of
+    // them, so that a CTA keeps NT * U loads in flight.
+    constexpr int NT = (N / 2) * N2, IT = N * N / NT, U = IT < 16 ? IT : 16;
+    static_assert(IT * NT == N * N && IT % U == 0, "plane load batches");
+    for (int b = 0; b < IT; b += U) {
+        TI r[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = threadIdx.x + (b + u) * NT, ix = idx / N, iy = idx - ix * N;
+            r[u] = in[((long long)ix * B.ny + iy) * B.nzh + 1 + z];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = threadIdx.x + (b + u) * NT, ix = idx / N, iy = idx - ix * N;
+            P[ix * S + iy] = (TC)r[u];
+        }
     }
     __syncthreads();
     const int line = threadIdx.x / N2, t = threadIdx.x - line * N2;
@@ -393,8 +408,9 @@ __global__ void __launch_bounds__((N / 2) * Radix<N>::N2) k_fft_plane(PlaneBatch
         line_fft<N, false, TC>(P, gy, t, tw, scale);
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-        const int ix = idx / N, iy = idx - ix * N;
+#pragma unroll 8
+    for (int k = 0; k < IT; ++k) {
+        const int idx = threadIdx.x + k * NT, ix = idx / N, iy = idx - ix * N;
         out[((long long)ix * B.ny + iy) * B.nzh + 1 + z] = (TO)P[ix * S + iy];
     }
 }
@@ -430,37 +446,80 @@ static void launch_plane(Ctx& c, const TI* const* in, TO* const* out, int nf, bo
 }
 
 // Tiled line FFT along x (axis 0) or y (axis 1) for power-of-two lengths
-// n = 16 .. 512: a CTA loads TL = 32 consecutive z-lines (coalesced 256-byte
-// rows) of one (y or x) index into shared memory as rows of n + 2, and
-// transforms them as TL/2 complex line pairs with line_fft.
-constexpr int TL = 32;
+// n = 16 .. 512.  A CTA holds TL consecutive z-lines (TL a multiple of 16,
+// chosen per grid by tile_lines_for) of one y (or x) index in shared memory
+// as P[l * S + e], S = n + 1, and transforms them as TL/2 complex line pairs
+// (lines 2p, 2p+1) with line_fft.
+//  * Loads and stores: a warp takes 16 consecutive lines x 2 elements, so a
+//    global access covers two 128-byte runs of z and, with S odd, the 16
+//    lines of a half-warp fall into 16 different 8-byte bank pairs.
+//  * Line pairs: the L = n2 lanes of a pair read L consecutive elements of
+//    its lines; the pairs of one half-warp are chosen Q apart (Q = 4 for
+//    L = 8, Q = 2 for L = 4) so that, with S odd, their elements lie 16 (8)
+//    banks apart and the half-warp touches every bank once.
+//  * Each thread issues its 2 n1 loads in batches before storing any of them.
+constexpr int TLMAX = 64;
+
+template <int L>
+EPIC_DEV int tile_pair(int w, int g) {
+    if (L >= 16) return w * (32 / L) + g;
+    if (L == 8) return 8 * (w >> 1) + 2 * (w & 1) + 4 * (g & 1) + (g >> 1);
+    return 8 * w + 2 * (g & 3) + (g >> 2);   // L == 4
+}
 
 template <int N, bool FWD, class TI, class TO, class TC>
-__global__ void __launch_bounds__((TL / 2) * Radix<N>::N2) k_fft_tile(FFTBatch B) {
-    constexpr int S = N + 2, N2 = Radix<N>::N2;
+__global__ void __launch_bounds__((TLMAX / 2) * Radix<N>::N2) k_fft_tile(FFTBatch B) {
+    constexpr int S = N + 1, L = Radix<N>::N2, IT = 2 * Radix<N>::N1, U = IT < 8 ? IT : 8;
+    static_assert(L == 4 || L == 8 || L == 16, "lanes per line pair");
     extern __shared__ __align__(16) unsigned char smraw[];
     TC* P = reinterpret_cast<TC*>(smraw);
     __shared__ CX<TC> tw[N];
     const TI* in = static_cast<const TI*>(B.in[blockIdx.z]);
     TO* out = static_cast<TO*>(B.out[blockIdx.z]);
-    const int l0 = blockIdx.x * TL;
+    const int TL = B.T, l0 = blockIdx.x * TL, lb = TL >> 4;
     const long long rowbase = (long long)blockIdx.y * B.row_stride + 1;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int li = lane & 15, ei = lane >> 4;
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = cx<TC>((TC)B.tw[i].x, (TC)B.tw[i].y);
-    for (int idx = threadIdx.x; idx < TL * N; idx += blockDim.x) {
-        const int l = idx % TL, e = idx / TL;
-        const int line = l0 + l;
-        P[l * S + e] = (line < B.nl) ? (TC)in[rowbase + line + (long long)e * B.es] : TC(0);
+    // Blocks b = w + k nw of 16 lines x 2 elements: lines 16 (b mod lb) + li,
+    // elements 2 (b / lb) + ei.  nw is a multiple of lb (nw / lb = L / 4), so
+    // a thread keeps its line l and steps its element by L / 2.
+    const int l = 16 * (w % lb) + li, e0 = 2 * (w / lb) + ei;
+    constexpr int DE = L / 2;
+    const bool live = l0 + l < B.nl;
+    const TI* src = in + rowbase + l0 + l + (long long)e0 * B.es;
+    const long long step = (long long)DE * B.es;
+    TC* dst = P + l * S + e0;
+    for (int k0 = 0; k0 < IT; k0 += U) {
+        TI r[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) r[u] = live ? src[(k0 + u) * step] : TI(0);
+#pragma unroll
+        for (int u = 0; u < U; ++u) dst[(k0 + u) * DE] = (TC)r[u];
     }
     __syncthreads();
-    const int pair = threadIdx.x / N2, t = threadIdx.x - pair * N2;
+    const int pair = tile_pair<L>(w, lane / L), t = lane & (L - 1);
     const LineGeo g = {2 * pair * S, 1, S, 2 * pair * S, 2};
     line_fft<N, FWD, TC>(P, g, t, tw, (TC)B.scale);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < TL * N; idx += blockDim.x) {
-        const int l = idx % TL, e = idx / TL;
-        const int line = l0 + l;
-        if (line < B.nl) out[rowbase + line + (long long)e * B.es] = (TO)P[l * S + e];
+    if (live) {
+        TO* o = out + rowbase + l0 + l + (long long)e0 * B.es;
+#pragma unroll 8
+        for (int k = 0; k < IT; ++k) o[k * step] = (TO)dst[k * DE];
     }
+}
+
+// z-lines per tile: the multiple of 16 (up to 64) that pads nl least, the
+// larger on a tie, with the tile under 100 KB of shared memory.
+static int tile_lines_for(int nl, int n, size_t elem) {
+    int best = 16;
+    long long best_pad = LLONG_MAX;
+    for (int tl = 16; tl <= TLMAX; tl += 16) {
+        if (tl > 16 && elem * (size_t)tl * (n + 1) > 100 * 1024) break;
+        const long long pad = (long long)((nl + tl - 1) / tl) * tl;
+        if (pad <= best_pad) { best_pad = pad; best = tl; }
+    }
+    return best;
 }
 
 template <int N, class TI, class TO>
@@ -473,13 +532,14 @@ static void launch_tile_axis(Ctx& c, const FFTPlan& pl, int axis, const TI* cons
     B.n = N;
     B.tw = pl.tw;
     B.nl = P.nz + 1;
+    B.T = tile_lines_for(B.nl, N, sizeof(TC));
     B.scale = 1.0 / std::sqrt((double)N);
     int nrows;
     if (axis == 0) { B.es = (long long)P.ny * P.nzh; B.row_stride = P.nzh; nrows = P.ny; }
     else { B.es = P.nzh; B.row_stride = (long long)P.ny * P.nzh; nrows = P.nx; }
-    size_t sm = sizeof(TC) * (size_t)TL * (N + 2);
-    dim3 grid((B.nl + TL - 1) / TL, nrows, nf);
-    int threads = (TL / 2) * Radix<N>::N2;
+    size_t sm = sizeof(TC) * (size_t)B.T * (N + 1);
+    dim3 grid((B.nl + B.T - 1) / B.T, nrows, nf);
+    int threads = (B.T / 2) * Radix<N>::N2;
     prof_begin(c, "fft");
     if (forward) {
         allow_smem(k_fft_tile<N, true, TI, TO, TC>, sm);

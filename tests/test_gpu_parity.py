@@ -81,7 +81,9 @@ def test_eigen_exact_matches_oracle_bitwise(glib, olib):
                                          ((64, 64, 64), 3), ((128, 128, 32), 3),
                                          ((16, 16, 16), 0), ((32, 32, 24), 0), ((128, 128, 32), 0),
                                          ((48, 32, 16), 0), ((256, 256, 16), 0), ((64, 256, 16), 0),
-                                         ((512, 512, 8), 0)])
+                                         ((512, 512, 8), 0), ((128, 128, 128), 1), ((128, 128, 32), 1),
+                                         ((32, 32, 24), 1), ((16, 16, 16), 1), ((256, 256, 16), 1),
+                                         ((512, 512, 8), 1)])
 def test_vor2vel_taylor_green_kat(glib, shape, plane):
     """test_mpi_vor2vel.f90: Taylor-Green vorticity on 64^3, max err < 1e-14; the
     same flow on other grids through the horizontal FFT paths (2-D plane

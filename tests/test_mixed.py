@@ -96,3 +96,28 @@ def test_mixed_par2grid_box_windows(olib, glib):
     gc.par2grid(False)
     for fid in list(abi.VORTG) + [abi.TBUOYG, abi.VOLG]:
         assert _rel(gc.get_field(fid), oc.get_field(fid)) < 1e-5, fid
+
+
+@pytest.mark.parametrize("shape,path", [((128, 128, 32), 0), ((128, 128, 32), 1), ((128, 128, 32), 2),
+                                        ((64, 64, 64), 1), ((128, 128, 128), 1), ((16, 16, 16), 1)])
+def test_mixed_vor2vel_fft_paths(glib, shape, path):
+    """Taylor-Green vorticity (test_mpi_vor2vel.f90) through each horizontal
+    FFT path in the mixed form, whose spectral work is FP32: velocity within
+    FIELD_TOL of the exact solution's scale."""
+    import math
+    nx, ny, nz = shape
+    lower = (-math.pi, -math.pi, -0.5 * math.pi)
+    extent = (2 * math.pi, 2 * math.pi, 2 * math.pi)
+    ctx = abi.EpicContext(glib, glib.default_config(nx, ny, nz, lower, extent, precision=MIXED))
+    glib.lib.epic_gpu_test_set_fft_path(ctx.h, path)
+    dx = np.array(extent) / np.array([nx, ny, nz])
+    X, Y, Z = np.meshgrid(lower[0] + np.arange(nx) * dx[0], lower[1] + np.arange(ny) * dx[1],
+                          lower[2] + np.arange(-1, nz + 2) * dx[2], indexing="ij")
+    ctx.set_field(abi.VORTG[0], -3.0 * np.sin(X) * np.cos(Y) * np.cos(Z))
+    ctx.set_field(abi.VORTG[1], 3.0 * np.cos(X) * np.sin(Y) * np.cos(Z))
+    ctx.set_field(abi.VORTG[2], 0.0 * X)
+    ctx.vor2vel()
+    ref = [np.cos(X) * np.sin(Y) * np.sin(Z), np.sin(X) * np.cos(Y) * np.sin(Z), -2.0 * np.sin(X) * np.sin(Y) * np.cos(Z)]
+    for i in range(3):
+        assert np.abs(ctx.get_field(abi.VELOG[i])[:, :, 1:-1] - ref[i][:, :, 1:-1]).max() < FIELD_TOL * 2.0, i
+    ctx.close()
