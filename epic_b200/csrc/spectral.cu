@@ -446,45 +446,60 @@ static void launch_plane(Ctx& c, const TI* const* in, TO* const* out, int nf, bo
 }
 
 // Tiled line FFT along x (axis 0) or y (axis 1) for power-of-two lengths
-// n = 16 .. 512.  A CTA holds TL consecutive z-lines (TL a multiple of 16,
-// chosen per grid by tile_lines_for) of one y (or x) index in shared memory
-// as P[l * S + e], S = n + 1, and transforms them as TL/2 complex line pairs
-// (lines 2p, 2p+1) with line_fft.
-//  * Loads and stores: a warp takes 16 consecutive lines x 2 elements, so a
-//    global access covers two 128-byte runs of z and, with S odd, the 16
-//    lines of a half-warp fall into 16 different 8-byte bank pairs.
+// n = 16 .. 512.  A CTA holds TL consecutive z-lines (TL a multiple of 16 for
+// FP64, of 32 for FP32, chosen per grid by tile_lines_for) of one y (or x)
+// index in shared memory as P[l * S + e], S = n + 1, and transforms them as
+// TL/2 complex line pairs (lines 2p, 2p+1) with line_fft.  The mappings keep
+// every shared access of a warp at its minimum number of wavefronts:
+//  * Loads and stores: a warp takes LB consecutive lines x 32/LB elements
+//    (LB = 16 for 8-byte words, 32 for 4-byte words), so a global access
+//    covers 128-byte runs of z, and with S odd the LB lines fall into LB
+//    different banks (bank pairs).
 //  * Line pairs: the L = n2 lanes of a pair read L consecutive elements of
-//    its lines; the pairs of one half-warp are chosen Q apart (Q = 4 for
-//    L = 8, Q = 2 for L = 4) so that, with S odd, their elements lie 16 (8)
-//    banks apart and the half-warp touches every bank once.
+//    its lines, so the pairs that share a wavefront are placed at element
+//    offsets 2 p S that differ by 32 / (pairs per wavefront) banks
+//    (tile_pair); S = n + 1 with n >= 16 a power of two satisfies
+//    S = 1 (mod 8), which those offsets need.
 //  * Each thread issues its 2 n1 loads in batches before storing any of them.
 constexpr int TLMAX = 64;
 
-template <int L>
+// Line pair of lane group g (lanes g L .. g L + L - 1) of warp w.
+template <int L, int WB>
 EPIC_DEV int tile_pair(int w, int g) {
-    if (L >= 16) return w * (32 / L) + g;
-    if (L == 8) return 8 * (w >> 1) + 2 * (w & 1) + 4 * (g & 1) + (g >> 1);
-    return 8 * w + 2 * (g & 3) + (g >> 2);   // L == 4
+    if (WB == 8) {
+        // a wavefront serves a half-warp: its pairs 16 (L = 8) or 8 (L = 4) banks apart
+        if (L >= 16) return w * (32 / L) + g;
+        if (L == 8) return 8 * (w >> 1) + 2 * (w & 1) + 4 * (g & 1) + (g >> 1);
+        return 8 * w + 2 * (g & 3) + (g >> 2);
+    }
+    // 4-byte words: the pairs of a warp 32 / (32 / L) banks apart for the
+    // element reads, and those of each half-warp 16 banks apart for the
+    // 8-byte complex scratch
+    if (L >= 16) return 16 * (w >> 3) + (w & 7) + 8 * g;
+    if (L == 8) return 16 * (w >> 2) + (w & 3) + 4 * (((g & 1) << 1) | (g >> 1));
+    return 16 * (w >> 1) + (w & 1) + 2 * (2 * (g & 3) + (g >> 2));
 }
 
 template <int N, bool FWD, class TI, class TO, class TC>
 __global__ void __launch_bounds__((TLMAX / 2) * Radix<N>::N2) k_fft_tile(FFTBatch B) {
     constexpr int S = N + 1, L = Radix<N>::N2, IT = 2 * Radix<N>::N1, U = IT < 8 ? IT : 8;
+    constexpr int WB = sizeof(TC), LB = WB == 8 ? 16 : 32, EB = 32 / LB;
     static_assert(L == 4 || L == 8 || L == 16, "lanes per line pair");
+    static_assert(S % 8 == 1, "row stride");
     extern __shared__ __align__(16) unsigned char smraw[];
     TC* P = reinterpret_cast<TC*>(smraw);
     __shared__ CX<TC> tw[N];
     const TI* in = static_cast<const TI*>(B.in[blockIdx.z]);
     TO* out = static_cast<TO*>(B.out[blockIdx.z]);
-    const int TL = B.T, l0 = blockIdx.x * TL, lb = TL >> 4;
+    const int TL = B.T, l0 = blockIdx.x * TL, lb = TL / LB;
     const long long rowbase = (long long)blockIdx.y * B.row_stride + 1;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int li = lane & 15, ei = lane >> 4;
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = cx<TC>((TC)B.tw[i].x, (TC)B.tw[i].y);
-    // Blocks b = w + k nw of 16 lines x 2 elements: lines 16 (b mod lb) + li,
-    // elements 2 (b / lb) + ei.  nw is a multiple of lb (nw / lb = L / 4), so
-    // a thread keeps its line l and steps its element by L / 2.
-    const int l = 16 * (w % lb) + li, e0 = 2 * (w / lb) + ei;
+    // Blocks b = w + k nw of LB lines x EB elements: lines LB (b mod lb) +
+    // lane mod LB, elements EB (b / lb) + lane / LB.  nw is a multiple of lb
+    // (nw / lb = L LB / 64), so a thread keeps its line and steps its element
+    // by DE = EB L LB / 64 = L / 2.
+    const int l = LB * (w % lb) + lane % LB, e0 = EB * (w / lb) + lane / LB;
     constexpr int DE = L / 2;
     const bool live = l0 + l < B.nl;
     const TI* src = in + rowbase + l0 + l + (long long)e0 * B.es;
@@ -498,7 +513,7 @@ __global__ void __launch_bounds__((TLMAX / 2) * Radix<N>::N2) k_fft_tile(FFTBatc
         for (int u = 0; u < U; ++u) dst[(k0 + u) * DE] = (TC)r[u];
     }
     __syncthreads();
-    const int pair = tile_pair<L>(w, lane / L), t = lane & (L - 1);
+    const int pair = tile_pair<L, WB>(w, lane / L), t = lane & (L - 1);
     const LineGeo g = {2 * pair * S, 1, S, 2 * pair * S, 2};
     line_fft<N, FWD, TC>(P, g, t, tw, (TC)B.scale);
     __syncthreads();
@@ -509,13 +524,15 @@ __global__ void __launch_bounds__((TLMAX / 2) * Radix<N>::N2) k_fft_tile(FFTBatc
     }
 }
 
-// z-lines per tile: the multiple of 16 (up to 64) that pads nl least, the
-// larger on a tie, with the tile under 100 KB of shared memory.
+// z-lines per tile: the multiple of 16 (FP64) or 32 (FP32), up to 64, that
+// pads nl least, the larger on a tie, with the tile under 100 KB of shared
+// memory.
 static int tile_lines_for(int nl, int n, size_t elem) {
-    int best = 16;
+    const int m = elem == 8 ? 16 : 32;
+    int best = m;
     long long best_pad = LLONG_MAX;
-    for (int tl = 16; tl <= TLMAX; tl += 16) {
-        if (tl > 16 && elem * (size_t)tl * (n + 1) > 100 * 1024) break;
+    for (int tl = m; tl <= TLMAX; tl += m) {
+        if (tl > m && elem * (size_t)tl * (n + 1) > 100 * 1024) break;
         const long long pad = (long long)((nl + tl - 1) / tl) * tl;
         if (pad <= best_pad) { best_pad = pad; best = tl; }
     }
