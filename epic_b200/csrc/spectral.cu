@@ -950,23 +950,29 @@ EPIC_DEV void col_ztransform(const T* __restrict__ Q, int qld, T* xs, T* ys, int
     }
 }
 
+// Element-wise work over the CTA's columns (256 threads): 8 threads per
+// column on consecutive z, so that global accesses run along z and the 16
+// lanes of a half-warp (2 columns x 8 rows, row stride CP = 34) hit 16
+// different bank pairs; no index division.
+static_assert(CT * 8 == 256, "column kernels run 256 threads");
+template <class F>
+EPIC_DEV void col_each(int nzp, F&& f) {
+    const int col = threadIdx.x >> 3;
+    for (int j = threadIdx.x & 7; j < nzp; j += 8) f(col, j);
+}
 template <class T>
 EPIC_DEV void col_load(const T* f, T* xs, int c0, const ColArgs& A) {
-    int nzp = A.nz + 1;
-    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx / nzp, j = idx - col * nzp;
-        int c = c0 + col;
-        xs[j * CP + col] = (c < A.ncol) ? f[(long long)c * A.nzh + 1 + j] : T(0);
-    }
+    const int c = c0 + (threadIdx.x >> 3);
+    const bool ok = c < A.ncol;
+    const T* src = f + (long long)c * A.nzh + 1;
+    col_each(A.nz + 1, [&](int col, int j) { xs[j * CP + col] = ok ? src[j] : T(0); });
 }
 template <class T>
 EPIC_DEV void col_store(T* f, const T* xs, int c0, const ColArgs& A) {
-    int nzp = A.nz + 1;
-    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx / nzp, j = idx - col * nzp;
-        int c = c0 + col;
-        if (c < A.ncol) f[(long long)c * A.nzh + 1 + j] = xs[j * CP + col];
-    }
+    const int c = c0 + (threadIdx.x >> 3);
+    if (c >= A.ncol) return;
+    T* dst = f + (long long)c * A.nzh + 1;
+    col_each(A.nz + 1, [&](int col, int j) { dst[j] = xs[j * CP + col]; });
 }
 // table value for (column c, z = j)
 EPIC_DEV double tabv(const double* t, int c, int j, const ColArgs& A) {
@@ -1049,11 +1055,11 @@ __global__ void __launch_bounds__(256, col_min_blocks<R, T>()) k_col_decompose(C
         __syncthreads();
     }
     // subtract harmonic part (lanes along z: the per-column tables are read coalesced)
-    for (int idx = threadIdx.x; idx < CT * (nz - 1); idx += blockDim.x) {
-        int col = idx / (nz - 1), j = 1 + idx - col * (nz - 1);
-        int c = min(c0 + col, A.ncol - 1);
+    col_each(nzp, [&](int col, int j) {
+        if (j < 1 || j > nz - 1) return;
+        const int c = min(c0 + col, A.ncol - 1);
         xs[j * CP + col] = xs[j * CP + col] - (xs[col] * (T)tabv(phim, c, j, A) + xs[nz * CP + col] * (T)tabv(phip, c, j, A));
-    }
+    });
     __syncthreads();
     if (A.qdst) col_ztransform<0, false, T>(static_cast<const T*>(A.qdst), A.qld_dst, xs, ys, nz, (T)A.sn);
     else col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
@@ -1063,11 +1069,10 @@ __global__ void __launch_bounds__(256, col_min_blocks<R, T>()) k_col_decompose(C
     }
     __syncthreads();
     if (mode & 1) {
-        for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-            int col = idx / nzp, j = idx - col * nzp;
-            int c = min(c0 + col, A.ncol - 1);
+        col_each(nzp, [&](int col, int j) {
+            const int c = min(c0 + col, A.ncol - 1);
             ys[j * CP + col] = (T)tabv(filt, c, j, A) * ys[j * CP + col];
-        }
+        });
         __syncthreads();
     }
     col_store(static_cast<T*>(A.out[blockIdx.y]), ys, c0, A);
@@ -1089,15 +1094,14 @@ __global__ void __launch_bounds__(256, col_min_blocks<R, T>()) k_col_combine(Col
     if (A.qdst) col_ztransform<0, false, T>(static_cast<const T*>(A.qdst), A.qld_dst, xs, ys, nz, (T)A.sn);
     else col_matvec_t<R, false, T>(static_cast<const T*>(A.mdst), 1, nz - 1, xs, ys, nz);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx / nzp, j = idx - col * nzp;
-        int c = min(c0 + col, A.ncol - 1);
+    col_each(nzp, [&](int col, int j) {
+        const int c = min(c0 + col, A.ncol - 1);
         T v;
         if (j == 0) v = xs[col];
         else if (j == nz) v = xs[nz * CP + col];
         else v = ys[j * CP + col] + xs[col] * (T)tabv(phim, c, j, A) + xs[nz * CP + col] * (T)tabv(phip, c, j, A);
         xs[j * CP + col] = v;
-    }
+    });
     __syncthreads();
     col_store(static_cast<T*>(A.out[blockIdx.y]), xs, c0, A);
 }
@@ -1122,25 +1126,23 @@ __global__ void __launch_bounds__(256) k_col_wsolve(ColArgs A) {
     const double* rkz = A.tab[5];
     col_load(static_cast<const T*>(A.in[0]), ds, c0, A);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx / nzp, j = idx - col * nzp;
-        int c = min(c0 + col, A.ncol - 1);
-        T d0 = ds[col], dn = ds[nz * CP + col];
+    col_each(nzp, [&](int col, int j) {
+        const int c = min(c0 + col, A.ncol - 1);
+        const T d0 = ds[col], dn = ds[nz * CP + col];
         if (j >= 1 && j <= nz - 1) bs[j * CP + col] = d0 * (T)tabv(thetam, c, j, A) + dn * (T)tabv(thetap, c, j, A);
         es[j * CP + col] = d0 * (T)tabv(dthetam, c, j, A) + dn * (T)tabv(dthetap, c, j, A);
-    }
+    });
     __syncthreads();
-    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx / nzp, j = idx - col * nzp;
-        int c = min(c0 + col, A.ncol - 1);
+    col_each(nzp, [&](int col, int j) {
+        const int c = min(c0 + col, A.ncol - 1);
         if (j >= 1 && j <= nz - 1) {
-            T g = (T)tabv(green, c, j, A) * ds[j * CP + col];
+            const T g = (T)tabv(green, c, j, A) * ds[j * CP + col];
             ds[j * CP + col] = g;
             as[j * CP + col] = (T)rkz[j] * g;
         } else {
             as[j * CP + col] = T(0);
         }
-    }
+    });
     __syncthreads();
     // es += DCT(as); then as(1:nz-1) = DST(ds(1:nz-1))
     if (A.qdct) col_ztransform<1, true, T>(static_cast<const T*>(A.qdct), A.qld_dct, as, es, nz, (T)A.sn);
@@ -1414,11 +1416,10 @@ __global__ void k_vtend_rows(FluxArgs A, Ptr8 divxy, MPtr8 vt, double dzi, doubl
 // coalesced loads; one warp then solves its 32 columns, one lane each.
 template <class T>
 EPIC_DEV void cols_load(const T* f, double* xs, int c0, int ncol, int nzp, int nzh) {
-    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx / nzp, j = idx - col * nzp;
-        int c = c0 + col;
-        xs[j * CP + col] = (c < ncol) ? f[(long long)c * nzh + 1 + j] : 0.0;
-    }
+    const int c = c0 + (threadIdx.x >> 3);
+    const bool ok = c < ncol;
+    const T* src = f + (long long)c * nzh + 1;
+    col_each(nzp, [&](int col, int j) { xs[j * CP + col] = ok ? (double)src[j] : 0.0; });
 }
 
 template <class T>
@@ -1450,11 +1451,10 @@ __global__ void __launch_bounds__(256) k_lapinv(T* fs, const double* etdv, const
         }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < CT * nzp; idx += blockDim.x) {
-        int col = idx / nzp, j = idx - col * nzp;
-        int c = c0 + col;
-        if (c < ncol) fs[(long long)c * nzh + 1 + j] = (T)f[j * CP + col];
-    }
+    const int c = c0 + (threadIdx.x >> 3);
+    if (c >= ncol) return;
+    T* dst = fs + (long long)c * nzh + 1;
+    col_each(nzp, [&](int col, int j) { dst[j] = (T)f[j * CP + col]; });
 }
 
 // phi = volg * vcelli - 1 (parcel_correction.f90:158)
