@@ -552,12 +552,17 @@ __global__ void __launch_bounds__(PB) k_vortsum(PView pv, long long n, double* p
     }
 }
 
-// one warp: fixed-order sum of the partials -> dvor (or vor_bar)
+// one warp: fixed-order sum of the partials -> dvor (or vor_bar).  Lane l
+// sums blocks l, l + 32, ... in order, then a fixed butterfly adds the lanes,
+// so the result does not depend on timing.
 __global__ void k_vortsum_final(const double* partials, int nb, const double* vor_bar, double* out, int mode) {
-    if (threadIdx.x != 0) return;
     double s[4] = {0, 0, 0, 0};
-    for (int b = 0; b < nb; ++b)
+    for (int b = threadIdx.x; b < nb; b += 32)
         for (int k = 0; k < 4; ++k) s[k] += partials[b * 4 + k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        for (int k = 0; k < 4; ++k) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
+    if (threadIdx.x != 0) return;
     for (int k = 0; k < 3; ++k) out[k] = mode == 0 ? s[1 + k] / s[0] : s[1 + k] / s[0] - vor_bar[k];
 }
 
