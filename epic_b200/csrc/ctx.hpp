@@ -120,7 +120,6 @@ struct Ctx {
     bool vectors_kernel = true;   // support vectors by their own kernel before a scatter that recomputes them
     int stage_recwin = 0;         // split-form stage kernel gathers from records staged in shared memory
     bool stage_vectors = false;   // split-form stage kernel computes the next par2grid's support vectors
-    int stage_async_acc = 0;      // stage kernel copies the LS-RK accumulators asynchronously into shared memory
     bool p2g_counted = true;
     // mixed form with FP64 spectral work (an accuracy experiment; test toggle)
     bool spectral_fp64 = false;

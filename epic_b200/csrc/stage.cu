@@ -647,9 +647,6 @@ struct FusedArgs {
     // the next par2grid's vorticity bounds (StepScalars::pbound[0..2], cleared
     // by the host), or null
     unsigned long long* vbound;
-    // LS-RK accumulators copied asynchronously (cp.async) into shared memory
-    // before the gathers and read after them
-    int async_acc;
 };
 
 // The 14 gathered fields (velog 3, velgradg 8, vtend 3) of a grid point as
@@ -815,16 +812,6 @@ EPIC_DEV void dBdt_r(const R* s, const R* b, R B33, R* o) {
     o[4] = s[I_DWDX] * b[1] + s[I_DVDX] * b[2] + s[I_DWDY] * b[3] - s[I_DUDX] * b[4] + s[I_DVDZ] * B33;
 }
 
-// Asynchronous global -> shared copies (cp.async, 4 or 8 bytes): the copy
-// runs while the thread goes on; cp_wait() makes this thread's copies
-// visible to it.
-EPIC_DEV void cp_async(void* smem, const void* gmem, int bytes) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-EPIC_DEV void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-EPIC_DEV void cp_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <bool DIAG, class R, bool VOUT = false>
 __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long n, Boxes B, const R* pack,
@@ -842,9 +829,6 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
     __shared__ double vmx[3][PB];
 #pragma unroll
     for (int k = 0; k < 3; ++k) vmx[k][threadIdx.x] = 0.0;
-    // this thread's LS-RK accumulators in flight (S.async_acc; stages 2-5,
-    // never the diagnostic stage 1)
-    __shared__ double accs[DIAG ? 1 : 11][PB];
 #pragma unroll
     for (int k = 0; k < ND; ++k) dsm[k][threadIdx.x] = 0.0;
     double* dacc = &dsm[0][threadIdx.x];
@@ -890,36 +874,13 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
             R dvo[3] = {(R)0, (R)0, (R)0}, dbo[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
             auto load_accumulators = [&]() {
                 if (S.stage > 1) {
-                    if constexpr (!DIAG) if (S.async_acc) {
-                        cp_wait();
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            dpo[k] = accs[DIAG ? 0 : k][threadIdx.x];
-                            dvo[k] = *reinterpret_cast<const R*>(&accs[DIAG ? 0 : 3 + k][threadIdx.x]);
-                        }
-#pragma unroll
-                        for (int k = 0; k < 5; ++k) dbo[k] = *reinterpret_cast<const R*>(&accs[DIAG ? 0 : 6 + k][threadIdx.x]);
-                        return;
-                    }
 #pragma unroll
                     for (int k = 0; k < 3; ++k) { dpo[k] = a64<R>(pv, A_DX + k, i); dvo[k] = aR<R>(pv, A_DVX + k, i); }
 #pragma unroll
                     for (int k = 0; k < 5; ++k) dbo[k] = aR<R>(pv, A_DB0 + k, i);
                 }
             };
-            if (!DIAG && S.stage > 1 && S.async_acc) {
-                // the accumulators fly while the gathers run
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    cp_async(&accs[DIAG ? 0 : k][threadIdx.x], &a64<R>(pv, A_DX + k, i), 8);
-                    cp_async(&accs[DIAG ? 0 : 3 + k][threadIdx.x], &aR<R>(pv, A_DVX + k, i), (int)sizeof(R));
-                }
-#pragma unroll
-                for (int k = 0; k < 5; ++k) cp_async(&accs[DIAG ? 0 : 6 + k][threadIdx.x], &aR<R>(pv, A_DB0 + k, i), (int)sizeof(R));
-                cp_commit();
-            } else if constexpr (Form<R>::mixed) {
-                load_accumulators();
-            }
+            if constexpr (Form<R>::mixed) load_accumulators();
             R g[14];
 #pragma unroll
             for (int l = 0; l < 14; ++l) g[l] = (R)0;
@@ -944,7 +905,7 @@ __global__ void __launch_bounds__(PB, SB) k_stage(Params P, PView pv, long long 
                 ok = gather_tri_win<R>(P, pack, reinterpret_cast<const R*>(acc), RW, cur, g) && ok;
                 if (!ok) set_err(err, ERRB_ZRANGE);
             }
-            if (!Form<R>::mixed || S.async_acc) load_accumulators();
+            if constexpr (!Form<R>::mixed) load_accumulators();
             double dp[3];
             R dv[3];
 #pragma unroll
@@ -1264,7 +1225,6 @@ void fused_stage(Ctx& c, int stage, bool with_diag) {
     S.cb = c.cb[stage - 1];
     S.lg = c.scatter_lg[2];
     S.recwin = c.stage_recwin;
-    S.async_acc = c.stage_async_acc;
     // surface fluxes: inside the stage-1 kernel after its diagnostics, or
     // (no diagnostics) by their own kernel before it
     const bool flux = stage == 1 && c.flux_on;

@@ -135,12 +135,6 @@ extern "C" int epic_gpu_test_set_spectral_fp64(epic_ctx* ctx, int on) {
     return EPIC_OK;
 }
 
-extern "C" int epic_gpu_test_set_stage_async(epic_ctx* ctx, int on) {
-    if (!ctx) return EPIC_ERR_ARG;
-    ctx->c.stage_async_acc = on != 0;
-    return EPIC_OK;
-}
-
 extern "C" int epic_gpu_test_set_stage_window(epic_ctx* ctx, int on) {
     if (!ctx) return EPIC_ERR_ARG;
     ctx->c.stage_recwin = on != 0;

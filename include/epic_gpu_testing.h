@@ -62,9 +62,6 @@ int epic_gpu_test_set_vectors_kernel(struct epic_ctx* ctx, int on);
  * algebra) in FP64 instead of FP32, to measure that part's share of the
  * form's error against FP64. */
 int epic_gpu_test_set_spectral_fp64(struct epic_ctx* ctx, int on);
-/* Stage kernel copies the LS-RK accumulators of stages 2-5 asynchronously
- * (cp.async) into shared memory before its gathers and reads them after. */
-int epic_gpu_test_set_stage_async(struct epic_ctx* ctx, int on);
 /* Stage kernel (split form) gathers from the box's records staged in shared
  * memory (1) or from global memory (0, default); same results. */
 int epic_gpu_test_set_stage_window(struct epic_ctx* ctx, int on);

@@ -437,25 +437,3 @@ def test_par2grid_bitwise_reproducible(glib, precision):
     for r in runs[1:]:
         for a, b in zip(r, runs[0]):
             assert np.array_equal(a.view(np.int64), b.view(np.int64))
-
-
-@pytest.mark.parametrize("precision", [0, 1])
-def test_stage_async_accumulators_agree(glib, precision):
-    """The stage kernel's asynchronous copies of the LS-RK accumulators give
-    bitwise the same steps as its plain loads."""
-    import ctypes as C
-    s = small_state("thermal", small_frac=0.02, seed=8)
-    L = glib.lib
-    L.epic_gpu_test_set_stage_async.argtypes = [C.c_void_p, C.c_int]
-    out = []
-    for flag in (0, 1):
-        ctx = make_context(s, glib, keep_order=0, precision=precision)
-        L.epic_gpu_test_set_stage_async(ctx.h, flag)
-        t = 0.0
-        for _ in range(3):
-            t, info = ctx.step(t)
-        out.append((t, info.n_parcels, ctx.get_parcels()))
-        ctx.close()
-    assert out[0][:2] == out[1][:2]
-    for k in out[0][2]:
-        assert np.array_equal(out[0][2][k], out[1][2][k]), k
