@@ -352,9 +352,12 @@ def run_ours(args):
     # splits take the reference's decisions
     mixed = args.form == "mixed"
     large = args.workload == "thermal2-512x512x256"
-    if args.device_init or large:
+    if args.device_init or large or args.parcels_per_cell:
         # parcels generated on the device (the same state as the host generator)
         setup = initial.device_spec(args.workload)
+        if args.parcels_per_cell:
+            # the grid's kernels at full size on a smaller device footprint
+            setup.n_per_cell = args.parcels_per_cell
         extra = dict(capacity=int(1.15 * setup.n)) if large else {}
         ctx = epic_b200.make_context_device(setup, lib, keep_order=args.keep_order, precision=1 if mixed else 0,
                                             **extra)
@@ -371,6 +374,12 @@ def run_ours(args):
         f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         lg = args.scatter_groups
         assert f(ctx.h, lg, lg, lg) == 0
+    if args.fft_path is not None:
+        # horizontal FFT implementation (overrides the tuner)
+        import ctypes as C
+        f = lib.lib.epic_gpu_test_set_fft_path
+        f.argtypes = [C.c_void_p, C.c_int]
+        assert f(ctx.h, args.fft_path) == 0
     stream = context_stream(lib, ctx, dev)
     timer = Timer(lib, ctx, stream, dev if world == 1 else local)
 
@@ -493,6 +502,7 @@ def run_ours(args):
                    "store_order": ("box-ordered store with container indices (keep_order 0)" if args.keep_order == 0
                                    else "reference container order (keep_order 1)"),
                    "spinup_steps": args.spinup, "autotune": tuning,
+                   "fft_path_override": args.fft_path,
                    "device_memory_used_gb": round(used_gb, 2), "device_memory_total_gb": round(total_b / 1e9, 2),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"inputs larger than L2 (parcel state {store_gb:.2f} GB, fields {field_gb:.2f} GB)"},
@@ -851,6 +861,12 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--scatter-groups", type=int, default=None, choices=range(6),
                     help="log2 of the consecutive parcels a lane group of the scatters takes (overrides the tuner)")
+    ap.add_argument("--fft-path", type=int, default=None, choices=range(4),
+                    help="horizontal FFT: 0 plane, 1 tiled lines, 2 Stockham lines, 3 half-plane clusters "
+                         "(overrides the tuner)")
+    ap.add_argument("--parcels-per-cell", type=int, default=0,
+                    help="device-generated initial state with this many parcels per cell (profiling the grid "
+                         "kernels on a small device footprint); 0: the workload's 8")
     ap.add_argument("--keep-order", type=int, default=0, choices=[0, 1],
                     help="1: keep the reference's container order (no box sort)")
     ap.add_argument("--device-init", action="store_true",
