@@ -688,7 +688,7 @@ def run_served(args, lib=None, dev=None, emit=True):
     lib = lib or epic_b200.load()
     reqs, arrivals, meta = served_requests(args, lib)
     clocks = ClockSampler(dev)
-    srv = serve.Server(slots=args.served_slots, hbm_fraction=0.8, lib=lib)
+    srv = serve.Server(slots=args.served_slots, hbm_fraction=0.8, lib=lib, policy=args.served_policy)
     ids = []
     clocks.start()
     w0 = time.perf_counter()
@@ -715,7 +715,7 @@ def run_served(args, lib=None, dev=None, emit=True):
     workload = (f"served ensemble: {len(reqs)} requests, Poisson arrivals {args.served_rate}/s "
                 f"(seed {args.served_seed}), grids 32^3/48^3/64^3/96x96x48, Beltrami (k,l,m in 1..2) "
                 f"or thermal, {args.served_steps} mixed-precision steps each, "
-                f"{args.served_slots} slots, admission by free HBM")
+                f"{args.served_slots} slots, admission by free HBM, {args.served_policy} order")
     latency = {"p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
                "mean_s": float(lat.mean()) if len(lat) else None,
@@ -846,6 +846,8 @@ def main():
     ap.add_argument("--served-steps", type=int, default=100)
     ap.add_argument("--served-slots", type=int, default=8)
     ap.add_argument("--served-seed", type=int, default=2024)
+    ap.add_argument("--served-policy", default="arrival", choices=["arrival", "shortest-first"],
+                    help="admission order of the server's queue")
     ap.add_argument("--roofline-kernel", default="stage", choices=["stage", "p2g", "g2p", "fft"])
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of that kernel")
     ap.add_argument("--profile-kernels", default="", help="comma list of kernels to time over one extra step each")

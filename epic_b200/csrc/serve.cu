@@ -1,13 +1,14 @@
 // Served ensembles (include/epic_serve.h): a pool of worker threads, one per
 // slot, each running one simulation at a time on its own context and CUDA
-// stream; admission of the first queued request (in arrival order) that fits
-// the free slots and the HBM budget; idle
+// stream; admission of the first queued request (in arrival order, or the
+// smallest estimated work first) that fits the free slots and the HBM budget; idle
 // contexts kept per configuration and reused, so that a steady stream of
 // requests allocates (and frees, which synchronises the whole device) no
 // device memory.
 #include "ctx.hpp"
 #include "../../include/epic_serve.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <condition_variable>
@@ -40,6 +41,7 @@ struct Job {
     epic_request req;
     double t_submit;
     double bytes;
+    double work;   // estimated parcel-steps: cells x parcels per cell x steps
 };
 
 struct PooledCtx {
@@ -63,6 +65,7 @@ struct epic_server {
     int device = 0;
     double budget = 0.0, in_use = 0.0;   // bytes: running requests + idle contexts
     int64_t next_id = 1, running = 0, n_collected = 0;
+    int policy = EPIC_SRV_ARRIVAL;
     bool stop = false;
     std::chrono::steady_clock::time_point t0;
 
@@ -165,7 +168,13 @@ static void worker(epic_server* s, int slot) {
                 // a pooled context of its configuration, or room in the budget
                 // (after freeing idle contexts of other configurations)
                 size_t pick = s->queue.size();
-                for (size_t q = 0; q < s->queue.size() && pick == s->queue.size(); ++q) {
+                std::vector<size_t> order(s->queue.size());
+                for (size_t q = 0; q < order.size(); ++q) order[q] = q;
+                if (s->policy == EPIC_SRV_SHORTEST_FIRST)
+                    std::stable_sort(order.begin(), order.end(),
+                                     [&](size_t a, size_t b) { return s->queue[a].work < s->queue[b].work; });
+                for (size_t oq = 0; oq < order.size() && pick == s->queue.size(); ++oq) {
+                    const size_t q = order[oq];
                     Job& cand = s->queue[q];
                     ctx = pool_take(s, cand.req.cfg, &pooled_bytes);
                     if (ctx) { pick = q; break; }                    // its memory is already counted
@@ -259,6 +268,8 @@ static int submit_locked(epic_server* s, const epic_request* req, int64_t* id) {
     j.req = *req;
     j.t_submit = s->now();
     j.bytes = estimate_bytes(req->cfg);
+    j.work = (double)req->cfg.nx * req->cfg.ny * req->cfg.nz * std::max(1, (int)req->init.n_per_cell) *
+             (double)req->steps;
     *id = j.id;
     if (j.bytes > s->budget) {
         epic_result r{};
@@ -295,6 +306,13 @@ extern "C" int epic_srv_counts(epic_server* s, int64_t* queued, int64_t* running
     if (queued) *queued = (int64_t)s->queue.size();
     if (running) *running = s->running;
     if (done) *done = (int64_t)s->results.size() + s->n_collected;
+    return EPIC_OK;
+}
+
+extern "C" int epic_srv_set_policy(epic_server* s, int32_t policy) {
+    if (!s || (policy != EPIC_SRV_ARRIVAL && policy != EPIC_SRV_SHORTEST_FIRST)) return EPIC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->policy = policy;
     return EPIC_OK;
 }
 

@@ -40,9 +40,10 @@ def _bind(lib):
     L.epic_srv_submit.argtypes = [C.c_void_p, C.POINTER(EpicRequest), C.POINTER(C.c_int64)]
     L.epic_srv_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(EpicResult)]
     L.epic_srv_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.epic_srv_set_policy.argtypes = [C.c_void_p, C.c_int32]
     L.epic_srv_destroy.argtypes = [C.c_void_p]
     L.epic_srv_destroy.restype = None
-    for f in (L.epic_srv_create, L.epic_srv_submit, L.epic_srv_wait, L.epic_srv_counts):
+    for f in (L.epic_srv_create, L.epic_srv_submit, L.epic_srv_wait, L.epic_srv_counts, L.epic_srv_set_policy):
         f.restype = C.c_int
     return L
 
@@ -89,10 +90,18 @@ def beltrami_zeta_flags(n, klm):
     return initial.zeta_boundary_flags(zg)
 
 
-class Server:
-    """epic_server: submit(request) -> id; wait(id) -> result dict."""
+ARRIVAL = 0          # EPIC_SRV_ARRIVAL
+SHORTEST_FIRST = 1   # EPIC_SRV_SHORTEST_FIRST
+POLICIES = {"arrival": ARRIVAL, "shortest-first": SHORTEST_FIRST}
 
-    def __init__(self, slots: int = 4, hbm_fraction: float = 0.8, lib=None):
+
+class Server:
+    """epic_server: submit(request) -> id; wait(id) -> result dict.  policy:
+    admission order, "arrival" or "shortest-first" (smallest estimated work,
+    cells x parcels per cell x steps, first)."""
+
+    def __init__(self, slots: int = 4, hbm_fraction: float = 0.8, lib=None, policy: str = "arrival"):
+        code = POLICIES[policy]
         self.lib = lib or load()
         self.L = _bind(self.lib)
         h = C.c_void_p()
@@ -100,6 +109,10 @@ class Server:
         if rc != 0:
             raise abi.EpicError(rc, "epic_srv_create", "server creation failed")
         self.h = h
+        rc = self.L.epic_srv_set_policy(self.h, code)
+        if rc != 0:
+            self.close()
+            raise abi.EpicError(rc, "epic_srv_set_policy", policy)
 
     def submit(self, req: EpicRequest) -> int:
         i = C.c_int64()

@@ -60,6 +60,17 @@ int epic_srv_submit(epic_server* srv, const epic_request* req, int64_t* id);
  * result is handed over: a second wait on the same id returns EPIC_ERR_ARG. */
 int epic_srv_wait(epic_server* srv, int64_t id, epic_result* out);
 int epic_srv_counts(epic_server* srv, int64_t* queued, int64_t* running, int64_t* done);
+
+/* Admission order: the order in which a slot that frees up looks through the
+ * queued requests for one that fits.  EPIC_SRV_ARRIVAL (the default) takes
+ * them in arrival order; EPIC_SRV_SHORTEST_FIRST takes the smallest
+ * estimated work first (cells x parcels per cell x steps, ties in arrival
+ * order), which lowers the median time to completion when the offered load
+ * exceeds the device, at the cost of the largest requests' wait.  Applies
+ * to every later admission. */
+#define EPIC_SRV_ARRIVAL 0
+#define EPIC_SRV_SHORTEST_FIRST 1
+int epic_srv_set_policy(epic_server* srv, int32_t policy);
 /* Finish all queued work, then free every context. */
 void epic_srv_destroy(epic_server* srv);
 

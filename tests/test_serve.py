@@ -78,3 +78,30 @@ def test_serve_results_are_handed_over(glib):
         assert srv.wait(rid)["status"] == 0
         with pytest.raises(abi.EpicError):
             srv.wait(rid)
+
+
+@pytest.mark.parametrize("policy", ["shortest-first", "arrival"])
+def test_serve_admission_policy(glib, policy):
+    """With one slot busy, the two queued requests start in the policy's
+    order: the smaller estimated work first under "shortest-first", arrival
+    order otherwise; the result is the same as the request run alone."""
+    first = serve.request("thermal", (16, 16, 16), seed=1, steps=20, lib=glib, **FIXED)
+    big = serve.request("thermal", (32, 32, 16), seed=2, steps=4, lib=glib, **FIXED)
+    small = serve.request("thermal", (16, 16, 16), seed=3, steps=2, lib=glib, **FIXED)
+    with serve.Server(slots=1, lib=glib, policy=policy) as srv:
+        ids = [srv.submit(r) for r in (first, big, small)]
+        rf, rb, rs = [srv.wait(i) for i in ids]
+    for r in (rf, rb, rs):
+        assert r["status"] == 0, r["message"]
+    if policy == "shortest-first":
+        assert rs["t_start"] < rb["t_start"]
+    else:
+        assert rb["t_start"] < rs["t_start"]
+    a = _alone(glib, small)
+    assert rs["n_parcels"] == a["n_parcels"]
+    assert abs(rs["ke"] - a["ke"]) <= 1e-10 * abs(a["ke"])
+
+
+def test_serve_rejects_unknown_policy(glib):
+    with pytest.raises(KeyError):
+        serve.Server(slots=1, lib=glib, policy="random")
