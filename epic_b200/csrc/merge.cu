@@ -199,10 +199,25 @@ EPIC_DEV void entry_pos(const PView& pv, const CopyArgs& C, int N, int j, double
     else { x = C.cx[j - N]; y = C.cy[j - N]; z = C.cz[j - N]; }
 }
 
+// Positions of the sorted entries in cell order, with the entry index as the
+// bit pattern of w: the search then streams through a cell's candidates
+// (one 32-byte record each) instead of gathering an index and three
+// attributes per candidate from the parcel store.
+__global__ void k_sorted_pos(PView pv, CopyArgs C, int N, const int* sorted_idx, long long nt, double4* sp) {
+    MLOOP(nt) {
+        const int j = sorted_idx[i];
+        double x, y, z;
+        entry_pos(pv, C, N, j, x, y, z);
+        sp[i] = make_double4(x, y, z, __longlong_as_double((long long)j));
+    }
+}
+
 // M8: find_closest_parcel_locally (parcel_nearest.f90:675-747) for every small
-// entry m (locals 0..nls-1, then copies).
+// entry m (locals 0..nls-1, then copies).  sp: the sorted entries' positions
+// (k_sorted_pos), or null to read them through sorted_idx.
 __global__ void k_search(Params P, Box B, PView pv, CopyArgs C, int N, const int* Ls, int nls, int ncp,
-                         const int* sorted_idx, const int* cstart, const int* cend, int* iclo, double* dclo) {
+                         const int* sorted_idx, const double4* sp, const int* cstart, const int* cend, int* iclo,
+                         double* dclo) {
     MLOOP((long long)nls + ncp) {
         int is = i < nls ? Ls[i] : N + (int)(i - nls);
         double xs, ys, zs;
@@ -220,10 +235,17 @@ __global__ void k_search(Params P, Box B, PView pv, CopyArgs C, int N, const int
                     long long ijk = (long long)ix + (long long)B.hs1 * iy + (long long)B.hs1 * B.hs2 * iz;
                     int k1 = cstart[ijk], k2 = cend[ijk];
                     for (int k = k1; k < k2; ++k) {
-                        int nn = sorted_idx[k];
-                        if (nn == is) continue;
+                        int nn;
                         double xn, yn, zn;
-                        entry_pos(pv, C, N, nn, xn, yn, zn);
+                        if (sp) {
+                            const double4 e = sp[k];
+                            nn = (int)__double_as_longlong(e.w);
+                            xn = e.x; yn = e.y; zn = e.z;
+                        } else {
+                            nn = sorted_idx[k];
+                            if (nn != is) entry_pos(pv, C, N, nn, xn, yn, zn);
+                        }
+                        if (nn == is) continue;
                         double delz = ExactOps::sub(zn, zs);
                         if (ExactOps::mul(delz, delz) < dsqmin) {
                             double delx = ExactOps::sub(xn, xs);
@@ -660,6 +682,7 @@ long long parcel_merge(Ctx& c) {
     unsigned* err = &c.dsc->err;
 
     // ---- phase 1: binning and the local small list (parcel_nearest.f90:416-431)
+    prof_begin(c, "merge_bin");
     size_t cub1 = 0;
     cub::DeviceSelect::Flagged(nullptr, cub1, (int*)0, (int*)0, (int*)0, (int*)0, N, st);
     size_t bytes1 = merge_scratch_bytes(N);
@@ -689,6 +712,7 @@ long long parcel_merge(Ctx& c) {
         CK(cub::DeviceSelect::Flagged(tmp1, cub1, idx, small, Ls, dcount, N, st));
     }
     const int nls = read_int(c, dcount);
+    prof_end(c, "merge_bin");
     if (nls == 0) {
         k_periodic_m<<<mgrid(N), MB, 0, st>>>(P, c.pv, N);
         CKL();
@@ -730,6 +754,7 @@ long long parcel_merge(Ctx& c) {
     int* cstart = ar.take<int>(B.hncell);
     int* cend = ar.take<int>(B.hncell);
 
+    prof_begin(c, "merge_cells");
     if (ranked) {
         k_rank_cells<<<mgrid(N), MB, 0, st>>>(ord, cell0, N, cell, vals);
         CKL();
@@ -762,15 +787,26 @@ long long parcel_merge(Ctx& c) {
     CK(cudaMemsetAsync(cend, 0, sizeof(int) * B.hncell, st));
     k_cell_ranges<<<mgrid(NT), MB, 0, st>>>(skeys, NT, cstart, cend);
     CKL();
+    prof_end(c, "merge_cells");
+    prof_begin(c, "merge_search");
 
     int* iclo = ar.take<int>((size_t)nls + ncp);
     double* dclo = ar.take<double>((size_t)nls + ncp);
-    k_search<<<mgrid((long long)nls + ncp), MB, 0, st>>>(P, B, c.pv, C, N, Ls, nls, ncp, svals, cstart, cend,
+    // the second parcel store (free between the step's sorts) holds the
+    // sorted entries' positions when there is one
+    double4* sp = nullptr;
+    if (c.pv_alt && (size_t)NT * sizeof(double4) <= c.store_bytes()) {
+        sp = reinterpret_cast<double4*>(c.pv_alt);
+        k_sorted_pos<<<mgrid(NT), MB, 0, st>>>(c.pv, C, N, svals, NT, sp);
+        CKL();
+    }
+    k_search<<<mgrid((long long)nls + ncp), MB, 0, st>>>(P, B, c.pv, C, N, Ls, nls, ncp, svals, sp, cstart, cend,
                                                          iclo, dclo);
     CKL();
     k_globally<<<mgrid(nls), MB, 0, st>>>(nls, copyidx, iclo, dclo, err);
     CKL();
     check_device_error(c);
+    prof_end(c, "merge_search");
 
     // resolve_tree
     char* merged = ar.take<char>(N);
@@ -781,6 +817,7 @@ long long parcel_merge(Ctx& c) {
     CK(cudaMemsetAsync(avail, 0, N, st));
     const int g = mgrid(nls);
     for (int it = 0;; ++it) {
+        prof_begin(c, "merge_tree1");
         CK(cudaMemsetAsync(dcount, 0, sizeof(int), st));
         k_tree_a<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail);
         CKL();
@@ -790,7 +827,9 @@ long long parcel_merge(Ctx& c) {
         CKL();
         k_tree_d<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail, dcount);
         CKL();
-        if (!read_int(c, dcount)) break;
+        const int more = read_int(c, dcount);
+        prof_end(c, "merge_tree1");
+        if (!more) break;
         if (it > 1000000) throw CudaError(EPIC_ERR_TIMEOUT, "resolve_tree: stage 1 did not terminate");
     }
     char* dom = ar.take<char>(nls);
@@ -804,10 +843,13 @@ long long parcel_merge(Ctx& c) {
     k_tree_f_init<<<g, MB, 0, st>>>(Ls, iclo, nls, merged, leaf, avail, dom, status, err);
     CKL();
     for (int it = 0;; ++it) {
+        prof_begin(c, "merge_tree2");
         CK(cudaMemsetAsync(dcount, 0, sizeof(int), st));
         k_tree_f_round<<<g, MB, 0, st>>>(iclo, nls, minv, avail, status, dcount);
         CKL();
-        if (!read_int(c, dcount)) break;
+        const int more = read_int(c, dcount);
+        prof_end(c, "merge_tree2");
+        if (!more) break;
         if (it > 1000000) throw CudaError(EPIC_ERR_TIMEOUT, "resolve_tree: stage 2 did not terminate");
     }
     k_tree_f_apply<<<g, MB, 0, st>>>(Ls, nls, status, avail, dom);
@@ -817,6 +859,7 @@ long long parcel_merge(Ctx& c) {
     check_device_error(c);
 
     // merging pairs in m order
+    prof_begin(c, "merge_group");
     int* domi = ar.take<int>((size_t)nls + 1);
     int* dpos = ar.take<int>((size_t)nls + 1);
     k_char_to_int<<<g, MB, 0, st>>>(dom, domi, nls);
@@ -828,6 +871,7 @@ long long parcel_merge(Ctx& c) {
     }
     const int nm = read_int(c, dpos + nls);
     if (nm == 0) {
+        prof_end(c, "merge_group");
         k_periodic_m<<<mgrid(N), MB, 0, st>>>(P, c.pv, N);
         CKL();
         return 0;
@@ -889,7 +933,9 @@ long long parcel_merge(Ctx& c) {
     k_group_merge<<<mgrid(ng), MB, 0, st>>>(P, c.pv, gstart, ng, nm, gk, gv, ism, ML, err);
     CKL();
 
+    prof_end(c, "merge_group");
     // parcel_delete
+    prof_begin(c, "merge_delete");
     const int newN = N - nm;
     {
         DeleteBufs db;
@@ -910,6 +956,7 @@ long long parcel_merge(Ctx& c) {
     c.n_parcel_merges += nm;
     k_periodic_m<<<mgrid(newN), MB, 0, st>>>(P, c.pv, newN);
     CKL();
+    prof_end(c, "merge_delete");
     return nm;
 }
 
