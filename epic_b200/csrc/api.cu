@@ -348,7 +348,7 @@ static void free_ctx(Ctx& c) {
     c.prof.ev.clear();
     spectral_free(c);
     void* ptrs[] = {c.pv.base, c.pv_alt, c.fields, c.nparg, c.nsparg, c.work, c.dsc, c.partials, c.stage_partials,
-                    c.dvor_bar, c.box_start, c.gpack, c.binc, c.label, c.dil, c.rank};
+                    c.dvor_bar, c.box_start, c.gpack, c.binc, c.label, c.dil, c.rank, c.pairs_dev};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.scratch) cudaFree(c.scratch);
@@ -793,11 +793,16 @@ int epic_gpu_get_merge_pairs(epic_ctx* ctx, int64_t cap, int64_t* n, int32_t* is
     API_BEGIN
     Ctx& c = ctx->c;
     if (!n) throw CudaError(EPIC_ERR_ARG, "null");
-    *n = (int64_t)c.last_isma.size();
+    *n = (int64_t)c.n_pairs;
     if (cap < *n) throw CudaError(EPIC_ERR_ARG, "get_merge_pairs: capacity too small");
-    for (size_t m = 0; m < c.last_isma.size(); ++m) {
-        if (isma) isma[m] = c.last_isma[m] + 1;
-        if (iclo) iclo[m] = c.last_iclo[m] + 1;
+    if (c.n_pairs > 0) {
+        std::vector<int> h(2 * (size_t)c.n_pairs);
+        CK(cudaMemcpyAsync(h.data(), c.pairs_dev, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        for (long long m = 0; m < c.n_pairs; ++m) {
+            if (isma) isma[m] = h[m] + 1;
+            if (iclo) iclo[m] = h[c.n_pairs + m] + 1;
+        }
     }
     API_END
 }
@@ -842,7 +847,7 @@ int epic_gpu_step(epic_ctx* ctx, double* t, epic_step_info* info) {
     apply_vortcor(c);
     info->dt = rk_step(c, *t, info->parcel_stats, info->field_stats);
     prof_begin(c, "merge");
-    parcel_merge(c);
+    parcel_merge(c, true);
     prof_end(c, "merge");
     prof_begin(c, "split");
     parcel_split(c);

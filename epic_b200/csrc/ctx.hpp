@@ -165,7 +165,10 @@ struct Ctx {
     size_t scratch_bytes = 0;
     void* scratch2 = nullptr;
     size_t scratch2_bytes = 0;
-    std::vector<int> last_isma, last_iclo;
+    // pairs of the last merge (isma then iclo, container indices, m order),
+    // kept on the device and copied when the ABI asks for them
+    int* pairs_dev = nullptr;
+    long long pairs_cap = 0, n_pairs = 0;
     long long n_parcel_splits = 0, n_parcel_merges = 0, n_big_close = 0;
     bool has_parcels = false;
     // surface fluxes (bndry_fluxes.f90:25-36): binc, hinc are (ny, nx), y
@@ -259,7 +262,9 @@ void fft_forward_probe(Ctx& c);
 void lapinv_probe(Ctx& c, const double* in, double* out);
 
 // merge.cu
-long long parcel_merge(Ctx& c);
+// in_step: inside epic_gpu_step, where only the state attributes (and labels,
+// container indices) are live at the merge, so parcel_delete moves those
+long long parcel_merge(Ctx& c, bool in_step = false);
 // parcel_delete of nm distinct container indices (host array; test hook)
 void test_delete(Ctx& c, const int* idx, int nm);
 size_t merge_scratch_bytes(long long n);

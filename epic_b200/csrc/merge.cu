@@ -535,8 +535,9 @@ __global__ void k_src_flags(const char* del, int newN, int N, int* f) {
     MLOOP(N - newN) f[i] = del[newN + i] ? 0 : 1;
 }
 __global__ void k_hole_flags(const int* ism, int nm, int newN, int* f) { MLOOP(nm) f[i] = ism[i] < newN; }
-__global__ void k_move(PView pv, const int* holes, const int* srcs, int nh, int newN) {
-    MLOOP((long long)nh * N_ATTR) {
+// the first nattr attributes of the nh sources into the holes
+__global__ void k_move(PView pv, const int* holes, const int* srcs, int nh, int newN, int nattr) {
+    MLOOP((long long)nh * nattr) {
         int h = (int)(i % nh);
         int a = (int)(i / nh);
         int dst = holes[h];
@@ -583,11 +584,13 @@ static int read_int(Ctx& c, const int* d);
 
 // parcel_delete (parcel_container.f90:413-458) of the nm parcels in slots
 // ism (ascending where the slots are the container indices, keep_order = 1:
-// the holes are filled in that order): the i-th hole (below the new count)
+// the holes are filled in that order; state_only: the attributes a parcel
+// carries between steps, the rest being dead inside a step's merge): the
+// i-th hole (below the new count)
 // receives the i-th surviving parcel from the top; with container indices the same rule runs
 // on the indices (the slots are compacted the same way, and each parcel keeps
 // the index the reference's container gives it).  Leaves c.n to the caller.
-static void delete_slots(Ctx& c, int N, const int* ism, int nm, const DeleteBufs& b) {
+static void delete_slots(Ctx& c, int N, const int* ism, int nm, const DeleteBufs& b, bool state_only) {
     cudaStream_t st = c.stream;
     const int newN = N - nm;
     const int* ord = b.ord;
@@ -625,7 +628,8 @@ static void delete_slots(Ctx& c, int N, const int* ism, int nm, const DeleteBufs
         CKL();
         size_t bb = b.cubb;
         CK(cub::DeviceSelect::Flagged(b.ctmp, bb, b.sidx, b.sf, b.srcs, b.dcount + 1, N - newN, st));
-        k_move<<<mgrid((long long)nh * N_ATTR), MB, 0, st>>>(c.pv, b.holes, b.srcs, nh, newN);
+        const int nattr = state_only ? N_STATE : N_ATTR;
+        k_move<<<mgrid((long long)nh * nattr), MB, 0, st>>>(c.pv, b.holes, b.srcs, nh, newN, nattr);
         CKL();
         if (ranked) {
             k_move_rank<<<mgrid(nh), MB, 0, st>>>(c.rank, b.holes, b.srcs, nh, newN);
@@ -668,11 +672,10 @@ size_t merge_scratch_bytes(long long n) {
     return al(sizeof(int) * (size_t)n) * 7 + al(cub1) + 4096;
 }
 
-long long parcel_merge(Ctx& c) {
+long long parcel_merge(Ctx& c, bool in_step) {
     const Params& P = c.P;
     const int N = (int)c.n;
-    c.last_isma.clear();
-    c.last_iclo.clear();
+    c.n_pairs = 0;
     if (N == 0) return 0;
     Box B;
     B.hs1 = P.nx + 3;
@@ -881,8 +884,6 @@ long long parcel_merge(Ctx& c) {
     int* icl = ar.take<int>(nm);
     k_pack_pairs<<<g, MB, 0, st>>>(Ls, iclo, nls, dom, dpos, ism, icl);
     CKL();
-    c.last_isma.resize(nm);
-    c.last_iclo.resize(nm);
     {
         // the pairs as container indices
         const int* pi = ism;
@@ -895,8 +896,17 @@ long long parcel_merge(Ctx& c) {
             pi = ri;
             pc = rc;
         }
-        CK(cudaMemcpyAsync(c.last_isma.data(), pi, sizeof(int) * nm, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(c.last_iclo.data(), pc, sizeof(int) * nm, cudaMemcpyDeviceToHost, st));
+        if (2LL * nm > c.pairs_cap) {
+            if (c.pairs_dev) CK(cudaFreeAsync(c.pairs_dev, st));
+            c.pairs_dev = nullptr;
+            c.pairs_cap = 0;
+            const long long cap = 3LL * nm + 1024;
+            CK(cudaMallocAsync(&c.pairs_dev, sizeof(int) * (size_t)cap, st));
+            c.pairs_cap = cap;
+        }
+        CK(cudaMemcpyAsync(c.pairs_dev, pi, sizeof(int) * nm, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(c.pairs_dev + nm, pc, sizeof(int) * nm, cudaMemcpyDeviceToDevice, st));
+        c.n_pairs = nm;
     }
 
     // collect_merge_stats (parcel_merge.f90:365-394)
@@ -945,7 +955,7 @@ long long parcel_merge(Ctx& c) {
         // merge reads gk, gv and ism)
         db.hole_f = cell; db.src_f = vals; db.iota = skeys; db.holes_r = svals; db.srcs_r = svals + N;
         db.ord = ord; db.ctmp = ctmp; db.cubb = cubb; db.dcount = dcount;
-        delete_slots(c, N, ism, nm, db);
+        delete_slots(c, N, ism, nm, db, in_step);
     }
     unsigned long long hb = 0;
     CK(cudaMemcpyAsync(&hb, bigc, sizeof(hb), cudaMemcpyDeviceToHost, st));
@@ -1010,7 +1020,7 @@ void test_delete(Ctx& c, const int* idx, int nm) {
         CK(cudaMemcpyAsync(didx, sorted.data(), sizeof(int) * nm, cudaMemcpyHostToDevice, c.stream));
         k_slots_of<<<mgrid(nm), MB, 0, c.stream>>>(ord, didx, nm, ism);
         CKL();
-        delete_slots(c, N, ism, nm, b);
+        delete_slots(c, N, ism, nm, b, false);
         CK(cudaStreamSynchronize(c.stream));   // before the host copy of the indices goes
         c.n = N - nm;
         c.n_box = std::min<long long>(c.n_box, c.n);
