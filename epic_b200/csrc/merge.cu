@@ -212,13 +212,28 @@ __global__ void k_sorted_pos(PView pv, CopyArgs C, int N, const int* sorted_idx,
     }
 }
 
+// Cells of the small entries (locals m < nls, then the copies), for the
+// search order.
+__global__ void k_small_keys(const int* Ls, int nls, int ncp, const int* cell0, const int* cell_copies, int* keys,
+                             int* vals) {
+    MLOOP((long long)nls + ncp) {
+        keys[i] = i < nls ? cell0[Ls[i]] : cell_copies[i - nls];
+        vals[i] = (int)i;
+    }
+}
+
 // M8: find_closest_parcel_locally (parcel_nearest.f90:675-747) for every small
 // entry m (locals 0..nls-1, then copies).  sp: the sorted entries' positions
-// (k_sorted_pos), or null to read them through sorted_idx.
+// (k_sorted_pos), or null to read them through sorted_idx.  order: the small
+// entries by cell, so that the lanes of a warp search neighbouring cells (the
+// same candidates, similar trip counts), or null; each entry's result does
+// not depend on the order.
 __global__ void k_search(Params P, Box B, PView pv, CopyArgs C, int N, const int* Ls, int nls, int ncp,
-                         const int* sorted_idx, const double4* sp, const int* cstart, const int* cend, int* iclo,
-                         double* dclo) {
-    MLOOP((long long)nls + ncp) {
+                         const int* sorted_idx, const double4* sp, const int* order, const int* cstart,
+                         const int* cend, int* iclo, double* dclo) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nls + ncp;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long i = order ? order[t] : t;
         int is = i < nls ? Ls[i] : N + (int)(i - nls);
         double xs, ys, zs;
         entry_pos(pv, C, N, is, xs, ys, zs);
@@ -737,6 +752,7 @@ long long parcel_merge(Ctx& c, bool in_step) {
                   + al(sizeof(double) * ncp_max) * 3 + al(sizeof(int) * ncp_max) * 2   // copies
                   + al(sizeof(int) * B.hncell) * 2                    // cell ranges
                   + al(sizeof(int) * (size_t)nls) * 14 + al(sizeof(double) * (size_t)nls)
+                  + al(sizeof(int) * ((size_t)nls + ncp_max)) * 4       // search order
                   + al((size_t)N) * 3 + al(sizeof(int) * (size_t)N)    // tree flags, minv
                   + al(cubb) + 64 * 256;
     Arena ar{reinterpret_cast<char*>(c.get_scratch(bytes2)), 0, bytes2};
@@ -803,8 +819,20 @@ long long parcel_merge(Ctx& c, bool in_step) {
         k_sorted_pos<<<mgrid(NT), MB, 0, st>>>(c.pv, C, N, svals, NT, sp);
         CKL();
     }
-    k_search<<<mgrid((long long)nls + ncp), MB, 0, st>>>(P, B, c.pv, C, N, Ls, nls, ncp, svals, sp, cstart, cend,
-                                                         iclo, dclo);
+    // the small entries in cell order
+    const int nse = nls + ncp;
+    int* okeys = ar.take<int>(nse);
+    int* ovals = ar.take<int>(nse);
+    int* skeys2 = ar.take<int>(nse);
+    int* order = ar.take<int>(nse);
+    k_small_keys<<<mgrid(nse), MB, 0, st>>>(Ls, nls, ncp, cell0, cell + N, okeys, ovals);
+    CKL();
+    {
+        size_t b = cubb;
+        CK(cub::DeviceRadixSort::SortPairs(ctmp, b, okeys, skeys2, ovals, order, nse, 0, endbit, st));
+    }
+    k_search<<<mgrid((long long)nse), MB, 0, st>>>(P, B, c.pv, C, N, Ls, nls, ncp, svals, sp, order, cstart,
+                                                   cend, iclo, dclo);
     CKL();
     k_globally<<<mgrid(nls), MB, 0, st>>>(nls, copyidx, iclo, dclo, err);
     CKL();
