@@ -245,7 +245,62 @@ EPIC_DEV void fft_reg(CX<T> (&v)[N]) {
     }
 }
 
+// a * exp(-2 pi i j / 24), j mod 24 (multiples of 15 degrees), quarter turns exact
+constexpr double C15 = 0.96592582628906831, S15 = 0.25881904510252074, C30 = 0.86602540378443865;
+EPIC_DEV double w24c(int j) {
+    const double c[24] = {1.0, C15, C30, K4, 0.5, S15, 0.0, -S15, -0.5, -K4, -C30, -C15,
+                          -1.0, -C15, -C30, -K4, -0.5, -S15, 0.0, S15, 0.5, K4, C30, C15};
+    return c[j % 24];
+}
+template <class T>
+EPIC_DEV CX<T> rot24(CX<T> a, int j) {
+    j %= 24;
+    if (j == 0) return a;
+    if (j == 6) return cx<T>(a.y, -a.x);
+    if (j == 12) return cx<T>(-a.x, -a.y);
+    if (j == 18) return cx<T>(-a.y, a.x);
+    return cmulw(a, cx<T>((T)w24c(j), (T)-w24c((j + 18) % 24)));
+}
+
+// Forward DFT of N = 3 M values in registers (M = 4 or 8, natural order in
+// and out): DFTs of the three decimated subsequences v[3 q + r], twiddles
+// exp(-2 pi i r k / N), and radix-3 butterflies.
+template <int N, class T>
+EPIC_DEV void fft_reg3(CX<T> (&v)[N]) {
+    constexpr int M = N / 3;
+    static_assert(M * 3 == N && 24 % N == 0, "N = 12 or 24");
+    CX<T> u[3][M];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < M; ++q) u[r][q] = v[3 * q + r];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) fft_reg<M>(u[r]);
+#pragma unroll
+    for (int r = 1; r < 3; ++r)
+#pragma unroll
+        for (int k = 1; k < M; ++k) u[r][k] = rot24(u[r][k], (24 / N) * r * k);
+    const T h = (T)C30;   // sqrt(3) / 2
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        const CX<T> a = u[0][k], s = u[1][k] + u[2][k], d = u[1][k] - u[2][k];
+        const CX<T> m = cx<T>(a.x - T(0.5) * s.x, a.y - T(0.5) * s.y);
+        const CX<T> rr = cx<T>(h * d.x, h * d.y);
+        v[k] = a + s;
+        v[k + M] = cx<T>(m.x + rr.y, m.y - rr.x);       // m - i rr
+        v[k + 2 * M] = cx<T>(m.x - rr.y, m.y + rr.x);   // m + i rr
+    }
+}
+
+template <int N, class T>
+EPIC_DEV void fft_any(CX<T> (&v)[N]) {
+    if constexpr ((N & (N - 1)) == 0) fft_reg<N>(v);
+    else fft_reg3<N>(v);
+}
+
 template <int N> struct Radix;
+template <> struct Radix<48> { static constexpr int N1 = 12, N2 = 4; };
+template <> struct Radix<96> { static constexpr int N1 = 24, N2 = 4; };
 template <> struct Radix<16> { static constexpr int N1 = 4, N2 = 4; };
 template <> struct Radix<32> { static constexpr int N1 = 8, N2 = 4; };
 template <> struct Radix<64> { static constexpr int N1 = 8, N2 = 8; };
@@ -296,7 +351,7 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
             v[m] = cx<T>(ra - ib, -(ia + rb));
         }
     }
-    fft_reg<N1>(v);
+    fft_any<N1>(v);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmulw(v[k1], tw[t * k1]);
     __syncwarp();
@@ -309,7 +364,7 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
 #pragma unroll
         for (int t2 = 0; t2 < N2; ++t2) y[e][t2] = SC((t * KPT + e) * N2 + t2);
 #pragma unroll
-    for (int e = 0; e < KPT; ++e) fft_reg<N2>(y[e]);
+    for (int e = 0; e < KPT; ++e) fft_any<N2>(y[e]);
     __syncwarp();
     if (FWD) {
         // natural order into the scratch, then split into the two real lines
@@ -325,7 +380,7 @@ EPIC_DEV void line_fft(T* P, const LineGeo g, int t, const CX<T>* tw, T scale) {
             const int k = t + N2 * j;
             if (k <= H) {
                 zk[j] = SC(k);
-                zn[j] = SC((N - k) & (N - 1));
+                zn[j] = SC(k == 0 ? 0 : N - k);
             }
         }
         __syncwarp();
@@ -574,6 +629,8 @@ static bool tile_axis(Ctx& c, const FFTPlan& pl, int axis, const TI* const* in, 
                       bool forward) {
     switch (pl.n) {
         case 16: launch_tile_axis<16>(c, pl, axis, in, out, nf, forward); return true;
+        case 48: launch_tile_axis<48>(c, pl, axis, in, out, nf, forward); return true;
+        case 96: launch_tile_axis<96>(c, pl, axis, in, out, nf, forward); return true;
         case 32: launch_tile_axis<32>(c, pl, axis, in, out, nf, forward); return true;
         case 64: launch_tile_axis<64>(c, pl, axis, in, out, nf, forward); return true;
         case 128: launch_tile_axis<128>(c, pl, axis, in, out, nf, forward); return true;

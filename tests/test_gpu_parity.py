@@ -83,12 +83,14 @@ def test_eigen_exact_matches_oracle_bitwise(glib, olib):
                                          ((48, 32, 16), 0), ((256, 256, 16), 0), ((64, 256, 16), 0),
                                          ((512, 512, 8), 0), ((128, 128, 128), 1), ((128, 128, 32), 1),
                                          ((32, 32, 24), 1), ((16, 16, 16), 1), ((256, 256, 16), 1),
-                                         ((512, 512, 8), 1)])
+                                         ((512, 512, 8), 1), ((48, 48, 48), 1), ((96, 96, 48), 1),
+                                         ((96, 48, 16), 0), ((48, 48, 48), 0)])
 def test_vor2vel_taylor_green_kat(glib, shape, plane):
     """test_mpi_vor2vel.f90: Taylor-Green vorticity on 64^3, max err < 1e-14; the
     same flow on other grids through the horizontal FFT paths (2-D plane
     kernel for square 16..128 grids, tiled register FFT for power-of-two axes
-    up to 256, Stockham lines otherwise, half-plane cluster kernel for square
+    up to 512 and for 48 and 96 (radix 3 x 4 and 3 x 8 in registers), Stockham
+    lines otherwise, half-plane cluster kernel for square
     64 and 128)."""
     nx, ny, nz = shape
     lower = (-math.pi, -math.pi, -0.5 * math.pi)

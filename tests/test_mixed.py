@@ -99,7 +99,8 @@ def test_mixed_par2grid_box_windows(olib, glib):
 
 
 @pytest.mark.parametrize("shape,path", [((128, 128, 32), 0), ((128, 128, 32), 1), ((128, 128, 32), 2),
-                                        ((64, 64, 64), 1), ((128, 128, 128), 1), ((16, 16, 16), 1)])
+                                        ((64, 64, 64), 1), ((128, 128, 128), 1), ((16, 16, 16), 1),
+                                        ((48, 48, 48), 1), ((96, 96, 48), 1), ((96, 96, 48), 2)])
 def test_mixed_vor2vel_fft_paths(glib, shape, path):
     """Taylor-Green vorticity (test_mpi_vor2vel.f90) through each horizontal
     FFT path in the mixed form, whose spectral work is FP32: velocity within
