@@ -115,8 +115,9 @@ struct Ctx {
     int fft_path = 0;
     double* gpack = nullptr;     // gathered fields, 16 doubles per grid point
     // log2 of the consecutive parcels a lane group scatters (vol2grid,
-    // par2grid, fused stage)
-    int scatter_lg[3] = {1, 1, 0};
+    // par2grid, fused stage); the defaults are the tuner's choice on the
+    // 128^3 thermal and the 64^3 Beltrami flow (the sums do not depend on it)
+    int scatter_lg[3] = {3, 1, 0};
     bool vectors_kernel = true;   // support vectors by their own kernel before a scatter that recomputes them
     int stage_recwin = 0;         // split-form stage kernel gathers from records staged in shared memory
     bool stage_vectors = false;   // split-form stage kernel computes the next par2grid's support vectors
