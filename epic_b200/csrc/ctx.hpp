@@ -121,7 +121,7 @@ struct Ctx {
     bool vectors_kernel = true;   // support vectors by their own kernel before a scatter that recomputes them
     int stage_recwin = 0;         // split-form stage kernel gathers from records staged in shared memory
     bool stage_vectors = false;   // split-form stage kernel computes the next par2grid's support vectors
-    bool p2g_counted = true;
+    bool p2g_counted = true;      // the last par2grid scatter counted parcels per cell (nparg, nsparg)
     // mixed form with FP64 spectral work (an accuracy experiment; test toggle)
     bool spectral_fp64 = false;
     // the next scatter's bounds are already in pbound (computed by the
@@ -136,7 +136,7 @@ struct Ctx {
     // labels (cfg.labels): label and dilution per parcel, capacity cap
     long long* label = nullptr;
     double* dil = nullptr;
-    long long merge_calls = 0;    // merge calls that merged at least one parcel (key of the label draws)      // the last par2grid scatter counted parcels per cell (nparg, nsparg)
+    long long merge_calls = 0;    // merge calls that merged at least one parcel (key of the label draws)
     Tables T;
     StepScalars* dsc = nullptr;     // device
     StepScalars* hsc = nullptr;     // pinned host mirror
