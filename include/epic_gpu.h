@@ -234,7 +234,9 @@ int epic_gpu_rk_step(epic_ctx* ctx, double* t, double* dt);
 /* parcel_merge (parcel_merge.f90:47-108) incl. find_nearest/resolve_tree
  * (parcel_nearest.f90:375-1377) with single-rank semantics; n_merge out. */
 int epic_gpu_merge(epic_ctx* ctx, int64_t* n_merge);
-/* The merge pairs of the last epic_gpu_merge (isma, iclo; 1-based, m order). */
+/* The merge pairs of the last merge, by epic_gpu_merge or inside epic_gpu_step
+ * (isma, iclo; 1-based container indices, m order).  They stay on the device
+ * until this call copies them (it synchronises the context's stream). */
 int epic_gpu_get_merge_pairs(epic_ctx* ctx, int64_t cap, int64_t* n, int32_t* isma,
                              int32_t* iclo);
 /* parcel_split (parcel_split.f90:37-198); n_split out. */
